@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark: assembly + dense solve of the 72k-DoF penny crack on one B200.
+
+Workload (the configuration the headline metric is quoted on): unit-disk
+crack in z = 0, 4000 quadratic 6-node triangles (concentric rings, seeded
+in-plane jitter <= 5 % of the ring spacing), N = 18 x 4000 = 72000 DoF,
+G = 1, nu = 0.35, collocation offset 0.125, no fixed tip DoF, uniform
+internal pressure 1 (sigma_zz = 1).  Synthetic seeded mesh (the reference has
+no mesher).  One step = assemble the FP64 collocation matrix in HBM
+(41.5 GB) + LU factorisation + solve to a relative residual <= 1e-10.
+
+  --mode mixed (default): FP32 copy of the matrix factored with TF32
+        tensor-core trailing updates, FP64 iterative refinement;
+  --mode fp64: the plain FP64 GPU path (in-place FP64 LU).
+The other mode is timed once after the timed loop for the speed-up and the
+opening error between the two (rel err target <= 1e-8).
+
+Multi-GPU: the path has no exchange step; --gpus N runs N independent
+replicas (one process per GPU, weak scaling); value = seconds per
+assembly+solve, max over ranks.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+G, NU, BETA = 1.0, 0.35, 0.125
+S_ZZ = np.array([0.0, 0.0, 1.0, 0.0, 0.0, 0.0])
+METRIC = 'assembly+solve s at 72k DOF, mixed/learned vs plain FP64 GPU, rel err <=1e-8'
+UNIT = 's'
+
+
+def peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get('hbm_gbs', 6650.0), 'measured'
+    return 6650.0, 'fallback'
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device, self.samples, self.proc = device, [], None
+
+    def __enter__(self):
+        q = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+             'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+             'clocks_event_reasons.sw_power_cap')
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.device), f'--query-gpu={q}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(',')])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        sm = [float(s[0]) for s in self.samples if s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower() == 'active'})
+        load = [x for x in sm if x > 0.5 * max(sm)] if sm else []
+        return {'sm_mhz': statistics.median(load) if load else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(self.samples)}
+
+
+def workload(n_el, seed=2026):
+    from hfpx3d_b200 import meshgen
+    return meshgen.penny(n_el, seed=seed)
+
+
+# ---------------------------------------------------------------- engine arm
+def run_engine(args, rank, world, local_rank):
+    import torch
+    from hfpx3d_b200 import build, engine
+    if rank == 0:
+        build.build()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.set_device(local_rank)
+    ctx = engine.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f'cuda:{local_rank}')
+    nods, conn = workload(args.n_el)
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, S_ZZ)
+    d_rhs = torch.empty(n, dtype=torch.float64, device=f'cuda:{local_rank}')
+    d_x = torch.empty_like(d_rhs)
+    d_rhs.copy_(torch.from_numpy(rhs))
+    A = engine.assemble(ctx, dm, dof, n, G, NU)
+    mode = engine.HFPX_LU_MIXED if args.mode == 'mixed' else engine.HFPX_LU_FP64
+    other = engine.HFPX_LU_FP64 if mode == engine.HFPX_LU_MIXED else engine.HFPX_LU_MIXED
+    info = engine.SolveInfo()
+    L = engine.lib()
+
+    def step(m, ev=None):
+        if ev:
+            ev[0].record(stream)
+        engine.assemble_into(ctx, dm, dof, n, G, NU, A)
+        if ev:
+            ev[1].record(stream)
+        info_ = ctypes.c_int64()
+        ctx.check(L.hfpx_lu_factor(ctx.h, A.h, m, ctypes.byref(info_)))
+        if ev:
+            ev[2].record(stream)
+        d_x.copy_(d_rhs)
+        torch.cuda.synchronize()
+        ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), 1, n, args.tol, 50,
+                                         ctypes.byref(info)))
+        if ev:
+            ev[3].record(stream)
+
+    for _ in range(args.warmup):
+        step(mode)
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    launches0 = L.hfpx_ctx_launch_count(ctx.h)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for k in range(args.steps):
+            step(mode, evs[k])
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = L.hfpx_ctx_launch_count(ctx.h) - launches0
+    total_ms = start.elapsed_time(end)
+    t_asm = [e[0].elapsed_time(e[1]) for e in evs]
+    t_fac = [e[1].elapsed_time(e[2]) for e in evs]
+    t_sol = [e[2].elapsed_time(e[3]) for e in evs]
+    ms = total_ms / args.steps
+    x_main = d_x.cpu().numpy()
+    res_main, iters_main = info.residual, info.iterations
+    if world > 1:
+        t = torch.tensor([ms], device=f'cuda:{local_rank}')
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # the other precision, once, for the speed-up and the opening error
+    other_s, rel_err = None, None
+    if args.compare and rank == 0:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        step(other, ev)
+        torch.cuda.synchronize()
+        other_s = ev[0].elapsed_time(ev[3]) / 1e3
+        x_other = d_x.cpu().numpy()
+        x64 = x_other if other == engine.HFPX_LU_FP64 else x_main
+        xm = x_main if other == engine.HFPX_LU_FP64 else x_other
+        opening = lambda x: x[2::3]   # global z components of the nodal DD (tip free: 18 per element)
+        rel_err = float(np.abs(opening(xm) - opening(x64)).max() / np.abs(opening(x64)).max())
+
+    # end to end through the C-ABI with host buffers (pinned)
+    e2e = None
+    if rank == 0 and args.e2e_steps > 0:
+        e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A)
+
+    if rank != 0:
+        return None
+    hbm, peak_src = peaks()
+    asm_ms = statistics.mean(t_asm)
+    bytes_asm = float(n) * n * 8
+    line = {
+        'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64+tf32' if mode == engine.HFPX_LU_MIXED else 'f64',
+        'data': 'synthetic (seeded 4000-triangle penny mesh, pressure 1)',
+        'config': {'workload': f'penny crack {args.n_el} el, N={n} DoF, assembly + LU + solve to rel residual '
+                               f'{args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'mode': args.mode,
+                   'parallelism': f'replicas x{world}',
+                   'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
+        'phases_ms': {'assembly': asm_ms, 'factor': statistics.mean(t_fac), 'solve': statistics.mean(t_sol)},
+        'refinement': {'iterations': iters_main, 'residual': res_main},
+        'assemblies_per_s': 1e3 / asm_ms,
+        'solves_per_s': 1e3 / ms,
+        'roofline': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
+                     'achieved': bytes_asm / (asm_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
+                     'frac': bytes_asm / (asm_ms / 1e3) / 1e9 / hbm, 'traffic': None,
+                     'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm},
+        'gpu_launches': int(launches),
+        'clocks': clk.summary(),
+        'e2e': e2e,
+    }
+    if other_s is not None:
+        line['other_mode_s'] = other_s
+        line['speedup_vs_plain_fp64'] = (other_s / (ms / 1e3)) if mode == engine.HFPX_LU_MIXED else None
+        line['opening_rel_err_mixed_vs_fp64'] = rel_err
+    if args.cpu_baseline:
+        line['cpu_baseline'] = cpu_baseline(args)
+    return line
+
+
+def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
+    """hfpx_mesh_create -> hfpx_assemble_into -> hfpx_rhs_sinf -> hfpx_lu_factor ->
+    hfpx_lu_solve from pinned host buffers, the solution read back each step
+    (the device matrix storage of the main loop is reused)."""
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a.reshape(-1, order='F'))).pin_memory()
+        return t, t.numpy()
+    tn, hn = pinned(nods)
+    tc, hc = pinned(conn)
+    td, hd = pinned(dof)
+    tr, hr = pinned(np.zeros(n))
+    s = np.ascontiguousarray(S_ZZ)
+    times = []
+    for k in range(args.e2e_warmup + args.e2e_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        mh = ctypes.c_void_p()
+        ctx.check(L.hfpx_mesh_create(ctx.h, engine._dp(hn), nods.shape[0], nods.shape[1], engine._lp(hc),
+                                     conn.shape[0], conn.shape[1], BETA, ctypes.byref(mh)))
+        ctx.check(L.hfpx_assemble_into(ctx.h, mh, engine._lp(hd), n, G, NU, 0, 0, A.h))
+        hr[:] = 0.0
+        ctx.check(L.hfpx_rhs_sinf(ctx.h, mh, engine._lp(hd), n, engine._dp(s), 1, engine._dp(hr), n))
+        info_ = ctypes.c_int64()
+        ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
+        si = engine.SolveInfo()
+        ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        L.hfpx_mesh_destroy(mh)
+        if k >= args.e2e_warmup:
+            times.append(e0.elapsed_time(e1))
+    h2d = hn.nbytes + hc.nbytes + 2 * hd.nbytes + hr.nbytes + s.nbytes  # dof_h goes up twice
+    return {'value': statistics.mean(times) / 1e3, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
+            'd2h_bytes_per_step': int(hr.nbytes), 'steps': len(times)}
+
+
+# ------------------------------------------------------------- CPU reference
+def ref_sample(n_el_sample, threads):
+    """The reference's own assembly (make_3dbem_matrix_s, OpenMP build) and
+    LAPACK dgesv on a smaller penny of the same family; returns
+    (t_assembly, t_solve, n_dof_sample, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, 'tests'))
+    import oracle_lib
+    from hfpx3d_b200 import meshgen
+    os.environ.setdefault('OMP_NUM_THREADS', str(threads))
+    nods, conn = meshgen.penny(n_el_sample, seed=7)
+    nods, conn = np.asfortranarray(nods), np.asfortranarray(conn, dtype=np.int64)
+    ne = conn.shape[1]
+    omp = os.path.join(ROOT, 'oracle', '_ref', 'libhfpx_ref_omp.so')
+    n = 18 * ne
+    A = np.zeros((n, n), order='F')
+    if os.path.exists(omp):
+        lib = oracle_lib._bind(omp, oracle_lib._REF_SIG)
+        dof = np.zeros((ne, 18), dtype=np.int64, order='F')
+        nd = ctypes.c_int64()
+        t0 = time.perf_counter()
+        lib.ref_assemble(oracle_lib.dp(nods), nods.shape[0], nods.shape[1], oracle_lib.lp(conn), conn.shape[0], ne,
+                         G, NU, BETA, 0, 0, 0, oracle_lib.dp(A), oracle_lib.lp(dof), ctypes.byref(nd))
+        t_asm = time.perf_counter() - t0
+        kind = 'reference'
+    else:
+        o = oracle_lib.Oracle()
+        dof, n = o.dof_handle(nods, conn, 0)
+        t0 = time.perf_counter()
+        A = o.assemble(nods, conn, dof, n)
+        t_asm = time.perf_counter() - t0
+        kind = 'port'
+    b = np.ones(n)
+    t0 = time.perf_counter()
+    np.linalg.solve(A, b)
+    t_sol = time.perf_counter() - t0
+    return t_asm, t_sol, n, kind
+
+
+def cpu_baseline(args):
+    threads = len(os.sched_getaffinity(0))
+    t_asm, t_sol, n_s, kind = ref_sample(args.cpu_sample_el, threads)
+    N = 18 * args.n_el
+    scale_asm = (args.n_el / args.cpu_sample_el) ** 2   # pair evaluations
+    scale_lu = (N / n_s) ** 3                              # 2/3 n^3
+    v = t_asm * scale_asm + t_sol * scale_lu
+    return {'value': v, 'unit': UNIT, 'cores': threads, 'kind': kind,
+            'sample': (f'reference assembly (OpenMP, {threads} threads) + LAPACK dgesv on a '
+                       f'{args.cpu_sample_el}-element penny ({n_s} DoF): {t_asm:.2f} s + {t_sol:.2f} s, '
+                       f'extrapolated to {args.n_el} elements by pair count (x{scale_asm:.1f}) and n^3 '
+                       f'(x{scale_lu:.0f})'),
+            'assembly_s': t_asm * scale_asm, 'solve_s': t_sol * scale_lu}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    threads = len(os.sched_getaffinity(0))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        t_asm, t_sol, n_s, kind = ref_sample(args.cpu_sample_el, threads)
+        N = 18 * args.n_el
+        v = t_asm * (args.n_el / args.cpu_sample_el) ** 2 + t_sol * (N / n_s) ** 3
+        if k >= args.warmup:
+            vals.append(v)
+    v = statistics.mean(vals)
+    sample = (f'reference assembly (OpenMP) + LAPACK dgesv on a {args.cpu_sample_el}-element penny per step, '
+              f'extrapolated to {args.n_el} elements (pair count, n^3)')
+    return {'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': v * 1e3, 'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f64', 'data': 'synthetic (seeded penny meshes)', 'impl': 'reference',
+            'config': {'workload': f'penny crack {args.n_el} el, N={18 * args.n_el} DoF, assembly + LU solve',
+                       'n_el': args.n_el},
+            'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': threads, 'kind': kind, 'sample': sample},
+            'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
+    ap.add_argument('--mode', default='mixed', choices=['mixed', 'fp64'])
+    ap.add_argument('--n-el', type=int, default=4000)
+    ap.add_argument('--tol', type=float, default=1e-10)
+    ap.add_argument('--no-compare', dest='compare', action='store_false')
+    ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--cpu-sample-el', type=int, default=600)
+    ap.add_argument('--e2e-steps', type=int, default=2)
+    ap.add_argument('--e2e-warmup', type=int, default=1)
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        line = run_reference(args, rank)
+        if line:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
+    if rank != 0 or world > 1:
+        args.cpu_baseline = args.cpu_baseline and rank == 0 and world == 1
+    line = run_engine(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,635 @@
+// Assembly, right-hand side, volume-control border and stress kernels.
+//
+// Matrix fill (make_3dbem_matrix_s, system_assembly.cpp:30-219): grid
+// (tiles of 128 target collocation points) x (source elements).  Each CTA
+// stages its source element's record in shared memory with one bulk (TMA)
+// copy, each thread evaluates one (collocation point, source element) pair --
+// a 3 x 18 block of final matrix entries (global traction at the point due to
+// global DD at the element's 6 nodes) -- and the CTA writes its 18 columns x
+// 384 rows as contiguous column segments (column-major matrix, each source
+// element owns 18 full columns).  No atomics: every entry has one writer.
+//
+// In-plane pairs (|h| < 2.221e-16, every pair of a planar crack) run the
+// closed-form path in assemble_kernel<false>; the rare off-plane pairs are
+// skipped there and evaluated by assemble_kernel<true> (quadrature moments),
+// which exits at once when the first pass found none.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cmath>
+#include "hfpx_device.cuh"
+#include "engine_internal.h"
+
+namespace hfpx {
+
+__constant__ GL12 c_gl;
+static bool g_gl_ready = false;
+
+static void gl_host_init(cudaStream_t s) {
+  if (g_gl_ready) return;
+  GL12 g;
+  const int n = 12;
+  for (int i = 0; i < n; ++i) {
+    double x = std::cos(kPi * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = x;
+      for (int k = 2; k <= n; ++k) {
+        double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (x * p1 - p0) / (x * x - 1.0);
+      double dx = p1 / dp;
+      x -= dx;
+      if (std::fabs(dx) < 1e-16) break;
+    }
+    g.x[i] = x;
+    g.w[i] = 2.0 / ((1.0 - x * x) * dp * dp);
+  }
+  cudaMemcpyToSymbolAsync(c_gl, &g, sizeof(g), 0, cudaMemcpyHostToDevice, s);
+  g_gl_ready = true;
+}
+
+// ------------------------------------------------------------- bulk copy
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Stage `bytes` (multiple of 16, both addresses 16-byte aligned) from global
+// to shared memory with one bulk copy completed on an mbarrier.  The wait is
+// bounded; on timeout a status bit is set and false returned.
+__device__ bool stage_bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                           int* status) {
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+  }
+  auto wait = [&](int limit) {
+    uint32_t done = 0;
+    for (int it = 0; it < limit && !done; ++it) {
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(smem_u32(bar))
+          : "memory");
+    }
+    return done != 0;
+  };
+  // every thread agrees on the outcome before anyone leaves
+  if (__syncthreads_and(wait(1 << 22))) return true;
+  if (threadIdx.x == 0 && status) atomicOr(status, 1);
+  wait(1 << 22);  // give a late copy the chance to land before the CTA exits
+  return false;
+}
+
+// --------------------------------------------------------- geometry (rn)
+// Geometry that decides branches (h of a point, collocation points) uses
+// round-to-nearest products and sums in the reference's order, so that the
+// in-plane test |h| < h_tol sees the same value as the CPU.
+__device__ __forceinline__ double dot3_rn(const double* r, const double* b) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(r[0], b[0]), __dmul_rn(r[1], b[1])), __dmul_rn(r[2], b[2]));
+}
+
+__device__ __forceinline__ void point_hz(const ElemRec& E, const double* pt, double& h, cplx& z) {
+  double b[3];
+  for (int k = 0; k < 3; ++k) b[k] = __dsub_rn(pt[k], E.v0[k]);
+  z = mk(dot3_rn(E.r, b), dot3_rn(E.r + 3, b));
+  h = -dot3_rn(E.r + 6, b);
+}
+
+__device__ __forceinline__ double norm3_rn(const double* a) {
+  return __dsqrt_rn(dot3_rn(a, a));
+}
+
+// element_utilities.cpp:62-238, 364-395: frame, tau, shape functions, CPs.
+__global__ void element_precompute_kernel(const double* __restrict__ nods, int64_t ld_nods,
+                                          const int64_t* __restrict__ conn, int64_t ld_conn,
+                                          int64_t n_el, double beta, ElemRec* __restrict__ out) {
+  const int64_t el = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (el >= n_el) return;
+  double v[3][3];
+  for (int j = 0; j < 3; ++j) {
+    const int64_t n = conn[j + ld_conn * el];
+    for (int k = 0; k < 3; ++k) v[j][k] = nods[k + ld_nods * n];
+  }
+  ElemRec E;
+  double a1[3], a2[3], e1[3], a3[3], e3[3], a4[3];
+  for (int k = 0; k < 3; ++k) { a1[k] = __dsub_rn(v[1][k], v[0][k]); a2[k] = __dsub_rn(v[2][k], v[0][k]); }
+  const double n1 = norm3_rn(a1);
+  for (int k = 0; k < 3; ++k) e1[k] = __ddiv_rn(a1[k], n1);
+  a3[0] = __dsub_rn(__dmul_rn(e1[1], a2[2]), __dmul_rn(e1[2], a2[1]));
+  a3[1] = __dsub_rn(__dmul_rn(e1[2], a2[0]), __dmul_rn(e1[0], a2[2]));
+  a3[2] = __dsub_rn(__dmul_rn(e1[0], a2[1]), __dmul_rn(e1[1], a2[0]));
+  const double n3 = norm3_rn(a3);
+  for (int k = 0; k < 3; ++k) e3[k] = __ddiv_rn(a3[k], n3);
+  a4[0] = __dsub_rn(__dmul_rn(e3[1], e1[2]), __dmul_rn(e3[2], e1[1]));
+  a4[1] = __dsub_rn(__dmul_rn(e3[2], e1[0]), __dmul_rn(e3[0], e1[2]));
+  a4[2] = __dsub_rn(__dmul_rn(e3[0], e1[1]), __dmul_rn(e3[1], e1[0]));
+  const double n4 = norm3_rn(a4);
+  for (int k = 0; k < 3; ++k) {
+    E.v0[k] = v[0][k];
+    E.r[k] = e1[k];
+    E.r[3 + k] = __ddiv_rn(a4[k], n4);
+    E.r[6 + k] = e3[k];
+    E.nrm[k] = -e3[k];
+  }
+  cplx tau[3];
+  for (int j = 0; j < 3; ++j) {
+    double b[3];
+    for (int k = 0; k < 3; ++k) b[k] = __dsub_rn(v[j][k], v[0][k]);
+    tau[j] = mk(dot3_rn(E.r, b), dot3_rn(E.r + 3, b));
+    E.tau[2 * j] = tau[j].re;
+    E.tau[2 * j + 1] = tau[j].im;
+  }
+  // quadratic Lagrange shape functions in monomials [1, t, tc, t^2, tc^2, t tc]
+  const cplx det = tau[1] * conj(tau[2]) - tau[2] * conj(tau[1]);
+  const double dn = det.re * det.re + det.im * det.im;
+  const cplx idet = mk(det.re / dn, -det.im / dn);
+  cplx L[3][3];
+  L[1][0] = mk(0.0); L[1][1] = conj(tau[2]) * idet; L[1][2] = -(tau[2] * idet);
+  L[2][0] = mk(0.0); L[2][1] = -(conj(tau[1]) * idet); L[2][2] = tau[1] * idet;
+  for (int i = 0; i < 3; ++i) L[0][i] = -(L[1][i] + L[2][i]);
+  L[0][0] = L[0][0] + mk(1.0);
+  cplx sf[6][6];
+  for (int a = 0; a < 6; ++a)
+    for (int j = 0; j < 6; ++j) sf[a][j] = mk(0.0);
+  auto prod = [](cplx* P, const cplx* A, const cplx* B, double s) {
+    P[0] += s * (A[0] * B[0]);
+    P[1] += s * (A[0] * B[1] + A[1] * B[0]);
+    P[2] += s * (A[0] * B[2] + A[2] * B[0]);
+    P[3] += s * (A[1] * B[1]);
+    P[4] += s * (A[2] * B[2]);
+    P[5] += s * (A[1] * B[2] + A[2] * B[1]);
+  };
+  for (int vx = 0; vx < 3; ++vx) {
+    prod(sf[vx], L[vx], L[vx], 2.0);
+    for (int i = 0; i < 3; ++i) sf[vx][i] -= L[vx][i];
+    prod(sf[3 + vx], L[(vx + 1) % 3], L[(vx + 2) % 3], 4.0);
+  }
+  for (int a = 0; a < 6; ++a)
+    for (int j = 0; j < 6; ++j) {
+      E.sfm[2 * (6 * a + j)] = sf[a][j].re;
+      E.sfm[2 * (6 * a + j) + 1] = sf[a][j].im;
+    }
+  // collocation points, reference order of operations (element_utilities.cpp:364-395)
+  double c[3];
+  for (int k = 0; k < 3; ++k)
+    c[k] = __dadd_rn(__dadd_rn(__ddiv_rn(v[0][k], 3.0), __ddiv_rn(v[1][k], 3.0)), __ddiv_rn(v[2][k], 3.0));
+  const double omb = 1.0 - beta;
+  for (int vx = 0; vx < 3; ++vx) {
+    const int m = (vx + 1) % 3, l = (m + 1) % 3;
+    for (int k = 0; k < 3; ++k) {
+      E.cp[3 * vx + k] = __dadd_rn(__dmul_rn(omb, v[vx][k]), __dmul_rn(beta, c[k]));
+      E.cp[3 * (vx + 3) + k] =
+          __dadd_rn(__dmul_rn(__dmul_rn(0.5, omb), __dadd_rn(v[m][k], v[l][k])), __dmul_rn(beta, c[k]));
+    }
+  }
+  E.area = 0.5 * norm3_rn(a3) * n1;
+  E.pad[0] = E.pad[1] = 0.0;
+  out[el] = E;
+}
+
+// -------------------------------------------------------------- pair math
+// Local 6x(3 per node) stress of the in-plane closed form, contracted per node.
+struct InPlaneBlock {
+  cplx Ps[6], Qs[6];  // shifted moments: shift(z) applied on the monomial side
+};
+
+__device__ __forceinline__ void inplane_moments(const ElemRec& S, cplx z, cplx* P, cplx* Q) {
+  EdgeSet E;
+  edge_setup(S.tau, z, E);
+  for (int j = 0; j < 6; ++j) { P[j] = mk(0.0); Q[j] = mk(0.0); }
+  for (int m = 0; m < 3; ++m)
+    if (E.use[m]) lim_moments_diff(E.chi[0][m], E.chi[1][m], E.d[m], P, Q);
+}
+
+// sink(a, S[6][3]) receives the local stress columns of node a.
+template <class F>
+__device__ __forceinline__ void inplane_nodes(const ElemRec& S, cplx z, const cplx* P,
+                                              const cplx* Q, double nu, double scale, F&& sink) {
+  const cplx zc = conj(z), z2 = z * z, zc2 = zc * zc, zz = z * zc;
+  const double ca = -0.5 * (1.0 + 2.0 * nu), cb = -1.5 * (1.0 - 2.0 * nu);
+  const double cp_ = 0.25 * (2.0 - nu), cq = 0.75 * nu;
+  for (int a = 0; a < 6; ++a) {
+    const cplx* sr = reinterpret_cast<const cplx*>(S.sfm) + 6 * a;
+    cplx sz[6];
+    sz[0] = sr[0] + sr[1] * z + sr[2] * zc + sr[3] * z2 + sr[4] * zc2 + sr[5] * zz;
+    sz[1] = sr[1] + 2.0 * (sr[3] * z) + sr[5] * zc;
+    sz[2] = sr[2] + 2.0 * (sr[4] * zc) + sr[5] * z;
+    sz[3] = sr[3];
+    sz[4] = sr[4];
+    sz[5] = sr[5];
+    cplx p = mk(0.0), q = mk(0.0);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) { p += sz[j] * P[j]; q += sz[j] * Q[j]; }
+    const cplx s0 = ca * p, s1 = cb * q, s3 = -p;
+    const cplx t0 = -(cp_ * p + cq * q);
+    const cplx t1 = -mul_i(cp_ * p - cq * q);
+    double Sx[6][3];
+    Sx[0][2] = scale * (s0.re + s1.re);
+    Sx[1][2] = scale * (s0.re - s1.re);
+    Sx[2][2] = scale * s3.re;
+    Sx[3][2] = scale * s1.im;
+    Sx[4][2] = 0.0;
+    Sx[5][2] = 0.0;
+    Sx[0][0] = Sx[1][0] = Sx[2][0] = Sx[3][0] = 0.0;
+    Sx[4][0] = scale * 2.0 * t0.re;
+    Sx[5][0] = scale * 2.0 * t0.im;
+    Sx[0][1] = Sx[1][1] = Sx[2][1] = Sx[3][1] = 0.0;
+    Sx[4][1] = scale * 2.0 * t1.re;
+    Sx[5][1] = scale * 2.0 * t1.im;
+    sink(a, Sx);
+  }
+}
+
+// Off-plane monomial tensor (6x4x3) from the quadrature moments.
+__device__ __noinline__ void offplane_smon(const ElemRec& S, cplx z, double h, double nu,
+                                           cplx* smon) {
+  EdgeSet E;
+  edge_setup(S.tau, z, E);
+  // Points below the element's span integrate the regular parts F_p and add
+  // the h-singular lower-limit parts in closed form (exact vertex cancellation
+  // around the contour); points higher up integrate I_p directly.
+  const bool upper = fabs(h) < 0.05 * E.span;
+  cplx W[HFPX_N_MOMENTS];
+  for (int m = 0; m < HFPX_N_MOMENTS; ++m) W[m] = mk(0.0);
+  int vcount[3] = {0, 0, 0};
+  double angle = 0.0;
+  for (int m = 0; m < 3; ++m)
+    if (E.use[m]) {
+      gen_moments_edge(E.chi[0][m], E.chi[1][m], E.d[m], h, upper, c_gl, W);
+      vcount[(m + 1) % 3] += 1;
+      vcount[m] -= 1;
+      angle += E.chi[1][m] - E.chi[0][m];
+    }
+  for (int i = 0; i < 72; ++i) smon[i] = mk(0.0);
+  double hq[5] = {1.0, h, h * h, h * h * h, h * h * h * h};
+  for (int t = 0; t < HFPX_N_TERMS; ++t) {
+    const hfpx_term_t tm = hfpx_terms[t];
+    const cplx coef = mk(tm.cr0 + nu * tm.cr1, tm.ci0 + nu * tm.ci1);
+    smon[tm.jck] -= (hq[tm.q] * coef) * W[tm.moment];
+  }
+  if (upper) {
+    const double ah = fabs(h), lg = log(ah), sg = h > 0 ? 1.0 : -1.0;
+    for (int t = 0; t < HFPX_N_LOWER; ++t) {
+      const hfpx_lower_t lw = hfpx_lower[t];
+      cplx A = mk(0.0);
+      if (lw.sigma == 0) {
+        A = mk(angle);
+      } else {
+        for (int v = 0; v < 3; ++v)
+          if (vcount[v]) {
+            double sn, cs;
+            sincos(lw.sigma * E.phi[v], &sn, &cs);
+            // e^{i s phi} / (i s) = (sin - i cos) / s
+            A += (vcount[v] / (double)lw.sigma) * mk(sn, -cs);
+          }
+      }
+      const double f = (lw.esg ? sg : 1.0) * (lw.ea == 1 ? ah : (lw.ea == -1 ? 1.0 / ah : 1.0)) *
+                       (lw.elog ? lg : 1.0);
+      const cplx coef = mk(lw.cr0 + nu * lw.cr1, lw.ci0 + nu * lw.ci1);
+      smon[lw.jck] -= (f * coef) * A;
+    }
+  }
+}
+
+// Traction block rows for node a: 3x3 (traction comp, DD comp) in global
+// coordinates, from local stress columns Sx (system_assembly.cpp:138-185).
+__device__ __forceinline__ void traction_3x3(const double* r, const double* nl, const double Sx[6][3],
+                                             int is_dd_local, double B[3][3]) {
+  double tl[3][3], tg[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    tl[0][k] = nl[0] * Sx[0][k] + nl[1] * Sx[3][k] + nl[2] * Sx[4][k];
+    tl[1][k] = nl[1] * Sx[1][k] + nl[0] * Sx[3][k] + nl[2] * Sx[5][k];
+    tl[2][k] = nl[2] * Sx[2][k] + nl[0] * Sx[4][k] + nl[1] * Sx[5][k];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) tg[a][k] = r[a] * tl[0][k] + r[3 + a] * tl[1][k] + r[6 + a] * tl[2][k];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      B[a][j] = is_dd_local ? tg[a][j] : tg[a][0] * r[j] + tg[a][1] * r[3 + j] + tg[a][2] * r[6 + j];
+}
+
+// ------------------------------------------------------------ assembly
+constexpr int kTile = 128;
+constexpr int kStageRows = 3 * kTile;
+
+struct AsmSmem {
+  ElemRec src;
+  uint64_t bar;
+  int32_t cols[18];
+  int32_t rows[kStageRows];
+  double stage[18][kStageRows];
+};
+
+template <bool GENERAL>
+__global__ void __launch_bounds__(kTile) assemble_kernel(const ElemRec* __restrict__ elems,
+                                                         int64_t n_el,
+                                                         const int32_t* __restrict__ dof,
+                                                         double G, double nu, int is_dd_local,
+                                                         double* __restrict__ A, int64_t ld,
+                                                         int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
+  if (GENERAL && status[1] == 0) return;  // first pass met no off-plane pair
+  const int64_t s = blockIdx.y;
+  const int tid = threadIdx.x;
+  if (!stage_bulk(&sm.src, elems + s, sizeof(ElemRec), &sm.bar, status)) return;
+  if (tid < 18) sm.cols[tid] = dof[s + n_el * tid];
+  const int64_t g = (int64_t)blockIdx.x * kTile + tid;
+  const bool valid = g < 6 * n_el;
+  const int64_t t = valid ? g / 6 : 0;
+  const int nt = (int)(g - 6 * t);
+  double pt[3] = {0.0, 0.0, 0.0}, nrm[3] = {0.0, 0.0, 0.0};
+  if (valid) {
+    const ElemRec* T = elems + t;
+    for (int k = 0; k < 3; ++k) { pt[k] = T->cp[3 * nt + k]; nrm[k] = T->nrm[k]; }
+  }
+  const ElemRec& S = sm.src;
+  double h;
+  cplx z;
+  point_hz(S, pt, h, z);
+  const bool inplane = fabs(h) < kHTol;
+  const double scale = -G / (4.0 * kPi * (1.0 - nu));
+  double nl[3];
+  for (int i = 0; i < 3; ++i) nl[i] = S.r[3 * i] * nrm[0] + S.r[3 * i + 1] * nrm[1] + S.r[3 * i + 2] * nrm[2];
+
+  if (!GENERAL) {
+    const bool mine = valid && inplane;
+    for (int k = 0; k < 3; ++k)
+      sm.rows[3 * tid + k] = mine ? dof[t + n_el * (3 * nt + k)] : -1;
+    const unsigned off = __ballot_sync(0xffffffffu, valid && !inplane);
+    if (off && (tid & 31) == 0) atomicAdd(status + 1, __popc(off));
+    if (mine) {
+      cplx P[6], Q[6];
+      inplane_moments(S, z, P, Q);
+      inplane_nodes(S, z, P, Q, nu, scale, [&](int a, const double Sx[6][3]) {
+        double B[3][3];
+        traction_3x3(S.r, nl, Sx, is_dd_local, B);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) sm.stage[3 * a + j][3 * tid + i] = B[i][j];
+      });
+    }
+    __syncthreads();
+    // coalesced column-segment stores: 18 columns x 384 rows
+    for (int c = 0; c < 18; ++c) {
+      const int32_t col = sm.cols[c];
+      if (col < 0) continue;
+      double* colp = A + (int64_t)col * ld;
+      for (int r = tid; r < kStageRows; r += kTile) {
+        const int32_t row = sm.rows[r];
+        if (row >= 0) colp[row] = sm.stage[c][r];
+      }
+    }
+  } else {
+    __syncthreads();
+    if (!(valid && !inplane)) return;
+    cplx smon[72];
+    offplane_smon(S, z, h, nu, smon);
+    int32_t rows[3];
+    for (int k = 0; k < 3; ++k) rows[k] = dof[t + n_el * (3 * nt + k)];
+    contract_nodes(S.sfm, z, smon, scale, [&](int a, const double Sx[6][3]) {
+      double B[3][3];
+      traction_3x3(S.r, nl, Sx, is_dd_local, B);
+      for (int j = 0; j < 3; ++j) {
+        const int32_t col = sm.cols[3 * a + j];
+        if (col < 0) continue;
+        for (int i = 0; i < 3; ++i)
+          if (rows[i] >= 0) A[(int64_t)col * ld + rows[i]] = B[i][j];
+      }
+    });
+  }
+}
+
+size_t elem_record_bytes() { return sizeof(ElemRec); }
+
+void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int64_t* d_conn,
+                               int64_t ld_conn, int64_t n_el, double beta, void* d_elem,
+                               cudaStream_t s) {
+  gl_host_init(s);
+  const int bs = 128;
+  ++g_launches;
+  element_precompute_kernel<<<(unsigned)((n_el + bs - 1) / bs), bs, 0, s>>>(
+      d_nods, ld_nods, d_conn, ld_conn, n_el, beta, static_cast<ElemRec*>(d_elem));
+}
+
+void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                     int is_dd_local, double* d_a, int64_t ld, int* d_status, cudaStream_t s) {
+  gl_host_init(s);
+  const size_t smem = sizeof(AsmSmem);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(assemble_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(assemble_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
+  const dim3 grid((unsigned)((6 * n_el + kTile - 1) / kTile), (unsigned)n_el);
+  const ElemRec* e = static_cast<const ElemRec*>(d_elem);
+  ++g_launches;
+  assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_status);
+  ++g_launches;
+  assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_status);
+}
+
+// ----------------------------------------------------------- VC border
+// system_assembly.cpp:495-555: volume row (shape-function integral x normal
+// component, or x e3 for local DD) and pressure column (-normal).  The
+// integrals of quadratic Lagrange shape functions over a flat triangle are 0
+// for vertex nodes and area/3 for edge nodes.
+__global__ void vc_border_kernel(const ElemRec* __restrict__ elems, int64_t n_el,
+                                 const int32_t* __restrict__ dof, int64_t n_dof, int is_dd_local,
+                                 double* __restrict__ A, int64_t ld) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i == 0) A[n_dof + ld * n_dof] = 0.0;
+  if (i >= 18 * n_el) return;
+  const int64_t el = i / 18;
+  const int l = (int)(i - 18 * el), ns = l / 3, j = l % 3;
+  const int32_t sd = dof[el + n_el * l];
+  if (sd < 0) return;
+  const ElemRec& E = elems[el];
+  const double sfi = ns < 3 ? 0.0 : E.area / 3.0;
+  A[n_dof + ld * (int64_t)sd] = is_dd_local ? (j == 2 ? sfi : 0.0) : sfi * E.r[6 + j];
+  A[sd + ld * n_dof] = -E.r[6 + j];
+}
+
+void launch_vc_border(const void* d_elem, int64_t n_el, const int32_t* d_dof, int64_t n_dof,
+                      int is_dd_local, double* d_a, int64_t ld, cudaStream_t s) {
+  const int bs = 256;
+  ++g_launches;
+  vc_border_kernel<<<(unsigned)((18 * n_el + bs - 1) / bs), bs, 0, s>>>(
+      static_cast<const ElemRec*>(d_elem), n_el, d_dof, n_dof, is_dd_local, d_a, ld);
+}
+
+// ------------------------------------------------------------------ RHS
+// system_assembly.cpp:222-274: rhs[dof] -= (n . s_inf)_l, per load case.
+__global__ void rhs_kernel(const ElemRec* __restrict__ elems, int64_t n_el,
+                           const int32_t* __restrict__ dof, const double* __restrict__ sinf,
+                           int64_t n_rhs, double* __restrict__ rhs, int64_t ld) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 18 * n_el * n_rhs) return;
+  const int64_t c = i / (18 * n_el), rem = i - c * 18 * n_el;
+  const int64_t el = rem / 18;
+  const int l18 = (int)(rem - 18 * el), l = l18 % 3;
+  const int32_t d = dof[el + n_el * l18];
+  if (d < 0) return;
+  const double* n = elems[el].nrm;
+  const double* si = sinf + 6 * c;
+  double t;
+  if (l == 0) t = n[0] * si[0] + n[1] * si[3] + n[2] * si[4];
+  else if (l == 1) t = n[1] * si[1] + n[0] * si[3] + n[2] * si[5];
+  else t = n[2] * si[2] + n[0] * si[4] + n[1] * si[5];
+  rhs[d + ld * c] -= t;
+}
+
+void launch_rhs(const void* d_elem, int64_t n_el, const int32_t* d_dof, const double* d_sinf,
+                int64_t n_rhs, double* d_rhs, int64_t ld_rhs, cudaStream_t s) {
+  const int bs = 256;
+  const int64_t n = 18 * n_el * n_rhs;
+  ++g_launches;
+  rhs_kernel<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(static_cast<const ElemRec*>(d_elem), n_el,
+                                                        d_dof, d_sinf, n_rhs, d_rhs, ld_rhs);
+}
+
+// --------------------------------------------------------------- stress
+// system_assembly.cpp:279-455: one CTA per observation point, threads over
+// source elements, fixed-order tree reduction (deterministic).
+constexpr int kStressThreads = 128;
+
+__global__ void __launch_bounds__(kStressThreads) stress_kernel(
+    const ElemRec* __restrict__ elems, int64_t n_el, double G, double nu, int is_dd_local,
+    const double* __restrict__ dd, const double* __restrict__ pts, int64_t n_pts,
+    const double* __restrict__ sinf, double* __restrict__ out) {
+  __shared__ double red[6][kStressThreads];
+  const int64_t p = blockIdx.x;
+  const int tid = threadIdx.x;
+  const double pt[3] = {pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]};
+  const double scale = -G / (4.0 * kPi * (1.0 - nu));
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t s = tid; s < n_el; s += kStressThreads) {
+    const ElemRec& S = elems[s];
+    double h;
+    cplx z;
+    point_hz(S, pt, h, z);
+    const double* r = S.r;
+    auto sink = [&](int a, const double Sx[6][3]) {
+      // rotate_sim (tensor_utilities.cpp:57-91): sigma_g = R^T sigma R per DD column
+      double Sg[6][3];
+      for (int k = 0; k < 3; ++k) {
+        const double m[3][3] = {{Sx[0][k], Sx[3][k], Sx[4][k]},
+                                {Sx[3][k], Sx[1][k], Sx[5][k]},
+                                {Sx[4][k], Sx[5][k], Sx[2][k]}};
+        double tt[3][3], gg[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) tt[i][j] = m[i][0] * r[j] + m[i][1] * r[3 + j] + m[i][2] * r[6 + j];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) gg[i][j] = r[i] * tt[0][j] + r[3 + i] * tt[1][j] + r[6 + i] * tt[2][j];
+        Sg[0][k] = gg[0][0]; Sg[1][k] = gg[1][1]; Sg[2][k] = gg[2][2];
+        Sg[3][k] = gg[0][1]; Sg[4][k] = gg[0][2]; Sg[5][k] = gg[1][2];
+      }
+      double ddv[3];
+      for (int j = 0; j < 3; ++j) ddv[j] = dd[(6 * s + a) + 6 * n_el * j];
+      for (int c = 0; c < 6; ++c) {
+        double w0 = Sg[c][0], w1 = Sg[c][1], w2 = Sg[c][2];
+        if (!is_dd_local) {
+          const double g0 = w0 * r[0] + w1 * r[3] + w2 * r[6];
+          const double g1 = w0 * r[1] + w1 * r[4] + w2 * r[7];
+          const double g2 = w0 * r[2] + w1 * r[5] + w2 * r[8];
+          w0 = g0; w1 = g1; w2 = g2;
+        }
+        acc[c] += w0 * ddv[0] + w1 * ddv[1] + w2 * ddv[2];
+      }
+    };
+    if (fabs(h) < kHTol) {
+      cplx P[6], Q[6];
+      inplane_moments(S, z, P, Q);
+      inplane_nodes(S, z, P, Q, nu, scale, sink);
+    } else {
+      cplx smon[72];
+      offplane_smon(S, z, h, nu, smon);
+      contract_nodes(S.sfm, z, smon, scale, sink);
+    }
+  }
+  for (int c = 0; c < 6; ++c) red[c][tid] = acc[c];
+  __syncthreads();
+  for (int w = kStressThreads / 2; w > 0; w >>= 1) {
+    if (tid < w)
+      for (int c = 0; c < 6; ++c) red[c][tid] += red[c][tid + w];
+    __syncthreads();
+  }
+  if (tid < 6) out[p + n_pts * tid] = red[tid][0] + sinf[tid];
+}
+
+void launch_stress(const void* d_elem, int64_t n_el, double G, double nu, int is_dd_local,
+                   const double* d_dd, const double* d_pts, int64_t n_pts, const double* d_sinf,
+                   double* d_out, cudaStream_t s) {
+  gl_host_init(s);
+  ++g_launches;
+  stress_kernel<<<(unsigned)n_pts, kStressThreads, 0, s>>>(static_cast<const ElemRec*>(d_elem), n_el, G,
+                                                          nu, is_dd_local, d_dd, d_pts, n_pts, d_sinf,
+                                                          d_out);
+}
+
+// --------------------------------------------------------- single block
+__global__ void local_block_kernel(double G, double nu, double h, double zr, double zi,
+                                   const double* __restrict__ tau, const double* __restrict__ sfm,
+                                   double* __restrict__ out) {
+  ElemRec S;
+  for (int i = 0; i < 6; ++i) S.tau[i] = tau[i];
+  for (int i = 0; i < 72; ++i) S.sfm[i] = sfm[i];
+  const cplx z = mk(zr, zi);
+  const double scale = -G / (4.0 * kPi * (1.0 - nu));
+  auto sink = [&](int a, const double Sx[6][3]) {
+    for (int c = 0; c < 6; ++c)
+      for (int k = 0; k < 3; ++k) out[18 * c + 3 * a + k] = Sx[c][k];
+  };
+  if (fabs(h) < kHTol) {
+    cplx P[6], Q[6];
+    inplane_moments(S, z, P, Q);
+    inplane_nodes(S, z, P, Q, nu, scale, sink);
+  } else {
+    cplx smon[72];
+    offplane_smon(S, z, h, nu, smon);
+    contract_nodes(S.sfm, z, smon, scale, sink);
+  }
+}
+
+void launch_local_block(double G, double nu, double h, double zr, double zi, const double* d_tau,
+                        const double* d_sfm, double* d_out, cudaStream_t s) {
+  gl_host_init(s);
+  ++g_launches;
+  local_block_kernel<<<1, 1, 0, s>>>(G, nu, h, zr, zi, d_tau, d_sfm, d_out);
+}
+
+// ------------------------------------------------------- FP64 -> FP32 copy
+__global__ void convert_f32_kernel(const double* __restrict__ a, int64_t ld, int64_t n,
+                                   float* __restrict__ f) {
+  const int64_t col = blockIdx.y;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    f[r + ld * col] = (float)a[r + ld * col];
+}
+
+void launch_convert_f32(const double* d_a, int64_t ld, int64_t n, float* d_f, cudaStream_t s) {
+  const dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)n);
+  ++g_launches;
+  convert_f32_kernel<<<grid, 256, 0, s>>>(d_a, ld, n, d_f);
+}
+
+}  // namespace hfpx

@@ -1,0 +1,483 @@
+// C-ABI of the engine (include/hfpx_engine.h): objects, argument checks,
+// host<->device copies around the kernels of assembly.cu and lu.cu.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include "engine_internal.h"
+
+namespace hfpx {
+
+std::atomic<long long> g_launches{0};
+
+int set_error(hfpx_ctx* c, int code, const std::string& msg) {
+  if (c) c->last_error = msg;
+  return code;
+}
+
+int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HFPX_OK;
+  return set_error(c, e == cudaErrorMemoryAllocation ? HFPX_ERR_NOMEM : HFPX_ERR_CUDA,
+                   std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// RAII device buffer for per-call temporaries.
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t bytes) { return cudaMalloc(&p, bytes ? bytes : 16); }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+static int upload_dof(hfpx_ctx* c, const int64_t* dof_h, int64_t n_el, int64_t n_dof, DevBuf& d) {
+  std::vector<int32_t> tmp(18 * n_el);
+  for (int64_t i = 0; i < 18 * n_el; ++i) {
+    const int64_t v = dof_h[i];
+    if (v < -1 || v >= n_dof) return set_error(c, HFPX_ERR_ARG, "dof_h entry out of range");
+    tmp[i] = (int32_t)v;
+  }
+  int rc = check_cuda(c, d.alloc(sizeof(int32_t) * tmp.size()), "dof_h alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(d.p, tmp.data(), sizeof(int32_t) * tmp.size(), cudaMemcpyHostToDevice, c->stream), "dof_h copy");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "dof_h copy");
+  return rc;
+}
+
+static int64_t round_ld(int64_t n) { return ((n + 31) / 32) * 32; }
+
+}  // namespace hfpx
+
+using namespace hfpx;
+
+extern "C" {
+
+int hfpx_ctx_create(int device, hfpx_ctx** out) {
+  if (!out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return HFPX_ERR_CUDA;
+  hfpx_ctx* c = new (std::nothrow) hfpx_ctx;
+  if (!c) return HFPX_ERR_NOMEM;
+  c->device = device;
+  int rc = check_cuda(c, cudaSetDevice(device), "cudaSetDevice");
+  if (!rc) rc = check_cuda(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  if (!rc) rc = check_cuda(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&c->d_flags, 16 * sizeof(int)), "flags");
+  if (!rc) {
+    cublasHandle_t h = nullptr;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) rc = HFPX_ERR_CUDA;
+    else {
+      cublasSetStream(h, c->stream);
+      c->cublas = h;
+    }
+  }
+  if (rc) {
+    hfpx_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return HFPX_OK;
+}
+
+int hfpx_ctx_destroy(hfpx_ctx* c) {
+  if (!c) return HFPX_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
+  if (c->d_flags) cudaFree(c->d_flags);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return HFPX_OK;
+}
+
+const char* hfpx_ctx_last_error(const hfpx_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+int hfpx_ctx_stream(hfpx_ctx* c, void** stream) {
+  if (!c || !stream) return HFPX_ERR_ARG;
+  *stream = c->stream;
+  return HFPX_OK;
+}
+
+int hfpx_ctx_synchronize(hfpx_ctx* c) {
+  if (!c) return HFPX_ERR_ARG;
+  return check_cuda(c, cudaStreamSynchronize(c->stream), "synchronize");
+}
+
+// surface_mesh_utilities.cpp:28-112 (make_dof_h_crack, approximation order 2).
+int64_t hfpx_dof_handle(const double* nods, int64_t ld_nods, int64_t n_nodes, const int64_t* conn,
+                        int64_t ld_conn, int64_t n_el, int tip_type, int64_t* dof_h) {
+  if (!nods || !conn || !dof_h || ld_nods < 3 || ld_conn < 3 || n_el < 1 || n_nodes < 3) return -HFPX_ERR_ARG;
+  const bool ext = ld_nods >= 5 && ld_conn >= 5;
+  int64_t n_dof = 18 * n_el, dec = 0;
+  for (int64_t el = 0; el < n_el; ++el)
+    for (int l = 0; l < 18; ++l) dof_h[el + n_el * l] = 18 * el + l;
+  for (int64_t el = 0; el < n_el; ++el) {
+    bool tip[3] = {false, false, false};
+    if (ext && conn[3 + ld_conn * el] == conn[4 + ld_conn * el])
+      for (int v = 0; v < 3; ++v) {
+        const int64_t n = conn[v + ld_conn * el];
+        if (n < 0 || n >= n_nodes) return -HFPX_ERR_ARG;
+        tip[v] = nods[3 + ld_nods * n] == 1.0 && nods[4 + ld_nods * n] == 1.0;
+      }
+    for (int v = 0; v < 6; ++v) {
+      // act: 0 shift by the running count, 1 fix, 2 keep (the reference leaves
+      // non-tip edge nodes unshifted when tip_type == 2)
+      int act = 0;
+      if (tip_type >= 1 && v < 3 && tip[v]) act = 1;
+      else if (tip_type == 2 && v >= 3) {
+        const int a = (v - 3 + 1) % 3, b = (a + 1) % 3;
+        act = (tip[a] && tip[b]) ? 1 : 2;
+      }
+      for (int l = 0; l < 3; ++l) {
+        int64_t& d = dof_h[el + n_el * (3 * v + l)];
+        if (act == 1) { --n_dof; ++dec; d = -1; }
+        else if (act == 0) d -= dec;
+      }
+    }
+  }
+  return n_dof;
+}
+
+int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n_nodes, const int64_t* conn,
+                     int64_t ld_conn, int64_t n_el, double beta, hfpx_mesh** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  if (!nods || !conn || ld_nods < 3 || ld_conn < 3 || n_el < 1 || n_nodes < 3)
+    return set_error(c, HFPX_ERR_ARG, "mesh needs >= 3 coordinate rows, >= 3 nodes and >= 1 element");
+  for (int64_t e = 0; e < n_el; ++e)
+    for (int j = 0; j < 3; ++j) {
+      const int64_t n = conn[j + ld_conn * e];
+      if (n < 0 || n >= n_nodes) return set_error(c, HFPX_ERR_ARG, "connectivity refers to a missing node");
+    }
+  for (int64_t n = 0; n < n_nodes; ++n)
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(nods[k + ld_nods * n])) return set_error(c, HFPX_ERR_ARG, "non-finite node coordinate");
+  cudaSetDevice(c->device);
+  DevBuf dn, dc;
+  int rc = check_cuda(c, dn.alloc(sizeof(double) * ld_nods * n_nodes), "nods alloc");
+  if (!rc) rc = check_cuda(c, dc.alloc(sizeof(int64_t) * ld_conn * n_el), "conn alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dn.p, nods, sizeof(double) * ld_nods * n_nodes, cudaMemcpyHostToDevice, c->stream), "nods copy");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dc.p, conn, sizeof(int64_t) * ld_conn * n_el, cudaMemcpyHostToDevice, c->stream), "conn copy");
+  hfpx_mesh* m = new (std::nothrow) hfpx_mesh;
+  if (!m) return HFPX_ERR_NOMEM;
+  m->n_el = n_el;
+  if (!rc) rc = check_cuda(c, cudaMalloc(&m->d_elem, elem_record_bytes() * n_el), "element records");
+  if (!rc) launch_element_precompute(dn.as<double>(), ld_nods, dc.as<int64_t>(), ld_conn, n_el, beta, m->d_elem, c->stream);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "element precompute");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "element precompute");
+  if (rc) {
+    hfpx_mesh_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
+}
+
+int hfpx_mesh_destroy(hfpx_mesh* m) {
+  if (!m) return HFPX_OK;
+  if (m->d_elem) cudaFree(m->d_elem);
+  delete m;
+  return HFPX_OK;
+}
+
+static int new_matrix(hfpx_ctx* c, int64_t n, hfpx_matrix** out) {
+  hfpx_matrix* m = new (std::nothrow) hfpx_matrix;
+  if (!m) return HFPX_ERR_NOMEM;
+  m->n = n;
+  m->ld = round_ld(n);
+  int rc = check_cuda(c, cudaMalloc(&m->d_a, sizeof(double) * (size_t)m->ld * n), "matrix alloc");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&m->d_piv, sizeof(int32_t) * n), "pivot alloc");
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
+}
+
+static int check_assembly_args(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G,
+                               double nu) {
+  if (!mesh || !dof_h) return set_error(c, HFPX_ERR_ARG, "null mesh or dof handle");
+  if (n_dof < 1 || n_dof > 18 * mesh->n_el) return set_error(c, HFPX_ERR_ARG, "n_dof out of range");
+  if (!(G > 0) || !(nu > -1.0 && nu < 0.5))
+    return set_error(c, HFPX_ERR_ARG, "shear modulus must be > 0 and Poisson ratio in (-1, 0.5)");
+  return HFPX_OK;
+}
+
+static int assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
+                         int is_dd_local, int vc_border, hfpx_matrix* m) {
+  DevBuf dd;
+  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, dd);
+  if (rc) return rc;
+  m->factored = 0;
+  m->info = 0;
+  launch_assemble(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), G, nu, is_dd_local, m->d_a, m->ld, c->d_flags, c->stream);
+  if (vc_border) launch_vc_border(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), n_dof, is_dd_local, m->d_a, m->ld, c->stream);
+  rc = check_cuda(c, cudaGetLastError(), "assembly launch");
+  int flags[2] = {0, 0};
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(flags, c->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream), "flags");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "assembly");
+  if (!rc && (flags[0] & 1)) rc = set_error(c, HFPX_ERR_CUDA, "element staging copy timed out");
+  return rc;
+}
+
+int hfpx_assemble(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
+                  int is_dd_local, int vc_border, hfpx_matrix** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  hfpx_matrix* m = nullptr;
+  rc = new_matrix(c, n_dof + (vc_border ? 1 : 0), &m);
+  if (!rc) rc = assemble_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, vc_border, m);
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
+}
+
+int hfpx_assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
+                       int is_dd_local, int vc_border, hfpx_matrix* m) {
+  if (!c) return HFPX_ERR_ARG;
+  int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
+  if (rc) return rc;
+  if (!m || m->n != n_dof + (vc_border ? 1 : 0)) return set_error(c, HFPX_ERR_ARG, "matrix size does not match n_dof");
+  cudaSetDevice(c->device);
+  return assemble_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, vc_border, m);
+}
+
+int hfpx_matrix_upload(hfpx_ctx* c, const double* a, int64_t n, int64_t ld_host, hfpx_matrix** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  if (!a || n < 1 || ld_host < n) return set_error(c, HFPX_ERR_ARG, "bad matrix dimensions");
+  cudaSetDevice(c->device);
+  hfpx_matrix* m = nullptr;
+  int rc = new_matrix(c, n, &m);
+  if (rc) return rc;
+  rc = check_cuda(c, cudaMemcpy2DAsync(m->d_a, m->ld * sizeof(double), a, ld_host * sizeof(double), n * sizeof(double), n,
+                                       cudaMemcpyHostToDevice, c->stream),
+                  "matrix upload");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "matrix upload");
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
+}
+
+int hfpx_matrix_dims(const hfpx_matrix* m, int64_t* n, int64_t* ld) {
+  if (!m) return HFPX_ERR_ARG;
+  if (n) *n = m->n;
+  if (ld) *ld = m->ld;
+  return HFPX_OK;
+}
+
+int hfpx_matrix_download(hfpx_ctx* c, const hfpx_matrix* m, double* a, int64_t ld_host) {
+  if (!c || !m || !a || ld_host < m->n) return set_error(c, HFPX_ERR_ARG, "bad download arguments");
+  cudaSetDevice(c->device);
+  int rc = check_cuda(c, cudaMemcpy2DAsync(a, ld_host * sizeof(double), m->d_a, m->ld * sizeof(double), m->n * sizeof(double),
+                                           m->n, cudaMemcpyDeviceToHost, c->stream),
+                      "matrix download");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "matrix download");
+  return rc;
+}
+
+int hfpx_matrix_destroy(hfpx_matrix* m) {
+  if (!m) return HFPX_OK;
+  if (m->d_a) cudaFree(m->d_a);
+  if (m->d_f) cudaFree(m->d_f);
+  if (m->d_piv) cudaFree(m->d_piv);
+  delete m;
+  return HFPX_OK;
+}
+
+int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, const double* s_inf,
+                  int64_t n_rhs, double* rhs, int64_t ld_rhs) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!mesh || !dof_h || !s_inf || !rhs || n_rhs < 1 || ld_rhs < n_dof || n_dof < 1)
+    return set_error(c, HFPX_ERR_ARG, "bad rhs arguments");
+  cudaSetDevice(c->device);
+  DevBuf dd, ds, dr;
+  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, dd);
+  if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 6 * n_rhs), "s_inf alloc");
+  if (!rc) rc = check_cuda(c, dr.alloc(sizeof(double) * ld_rhs * n_rhs), "rhs alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ds.p, s_inf, sizeof(double) * 6 * n_rhs, cudaMemcpyHostToDevice, c->stream), "s_inf");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dr.p, rhs, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyHostToDevice, c->stream), "rhs");
+  if (!rc) launch_rhs(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), ds.as<double>(), n_rhs, dr.as<double>(), ld_rhs, c->stream);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "rhs launch");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(rhs, dr.p, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyDeviceToHost, c->stream), "rhs back");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "rhs");
+  return rc;
+}
+
+int hfpx_lu_factor(hfpx_ctx* c, hfpx_matrix* m, int mode, int64_t* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m) return set_error(c, HFPX_ERR_ARG, "null matrix");
+  if (mode != HFPX_LU_FP64 && mode != HFPX_LU_MIXED) return set_error(c, HFPX_ERR_ARG, "unknown LU mode");
+  if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "matrix already factored in place");
+  cudaSetDevice(c->device);
+  int rc = mode == HFPX_LU_FP64 ? lu_factor_fp64(c, m) : lu_factor_fp32(c, m);
+  if (info) *info = m->info;
+  return rc;
+}
+
+int hfpx_lu_solve(hfpx_ctx* c, const hfpx_matrix* m, double* b, int64_t nrhs, int64_t ld_b, double tol, int max_iter,
+                  hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !b || nrhs < 1 || ld_b < m->n) return set_error(c, HFPX_ERR_ARG, "bad solve arguments");
+  if (m->factored == 0) return set_error(c, HFPX_ERR_STATE, "solve before factor");
+  if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
+  cudaSetDevice(c->device);
+  DevBuf db;
+  int rc = check_cuda(c, db.alloc(sizeof(double) * m->ld * nrhs), "rhs alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpy2DAsync(db.p, m->ld * sizeof(double), b, ld_b * sizeof(double), m->n * sizeof(double),
+                                                nrhs, cudaMemcpyHostToDevice, c->stream),
+                           "rhs upload");
+  if (!rc) {
+    if (m->factored == 1) {
+      rc = lu_solve_fp64(c, m, db.as<double>(), nrhs, m->ld);
+      if (info) { info->iterations = 0; info->residual = 0.0; info->converged = 1; }
+    } else {
+      rc = refine_solve(c, m, db.as<double>(), nrhs, m->ld, tol > 0 ? tol : 1e-12, max_iter > 0 ? max_iter : 30, info);
+    }
+  }
+  if (!rc || rc == HFPX_ERR_NOT_CONVERGED) {
+    int rc2 = check_cuda(c, cudaMemcpy2DAsync(b, ld_b * sizeof(double), db.p, m->ld * sizeof(double), m->n * sizeof(double),
+                                              nrhs, cudaMemcpyDeviceToHost, c->stream),
+                         "solution download");
+    if (!rc2) rc2 = check_cuda(c, cudaStreamSynchronize(c->stream), "solution download");
+    if (rc2) rc = rc2;
+  }
+  return rc;
+}
+
+int hfpx_lu_solve_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ld_b, double tol,
+                         int max_iter, hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !d_b || nrhs < 1 || ld_b < m->n) return set_error(c, HFPX_ERR_ARG, "bad solve arguments");
+  if (m->factored == 0) return set_error(c, HFPX_ERR_STATE, "solve before factor");
+  if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
+  cudaSetDevice(c->device);
+  if (m->factored == 1) {
+    if (info) { info->iterations = 0; info->residual = 0.0; info->converged = 1; }
+    return lu_solve_fp64(c, m, d_b, nrhs, ld_b);
+  }
+  return refine_solve(c, m, d_b, nrhs, ld_b, tol > 0 ? tol : 1e-12, max_iter > 0 ? max_iter : 30, info);
+}
+
+int64_t hfpx_ctx_launch_count(const hfpx_ctx* c) { return c ? (int64_t)g_launches.load() : -1; }
+
+int hfpx_stress(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, int is_dd_local, const double* dd,
+                const double* pts, int64_t n_pts, const double* s_inf, double* out) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!mesh || !dd || !pts || !s_inf || !out || n_pts < 1) return set_error(c, HFPX_ERR_ARG, "bad stress arguments");
+  if (!(G > 0) || !(nu > -1.0 && nu < 0.5)) return set_error(c, HFPX_ERR_ARG, "bad elastic constants");
+  cudaSetDevice(c->device);
+  DevBuf ddd, dp, ds, dout;
+  const int64_t ne = mesh->n_el;
+  int rc = check_cuda(c, ddd.alloc(sizeof(double) * 18 * ne), "dd alloc");
+  if (!rc) rc = check_cuda(c, dp.alloc(sizeof(double) * 3 * n_pts), "pts alloc");
+  if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 6), "s_inf alloc");
+  if (!rc) rc = check_cuda(c, dout.alloc(sizeof(double) * 6 * n_pts), "out alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ddd.p, dd, sizeof(double) * 18 * ne, cudaMemcpyHostToDevice, c->stream), "dd");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dp.p, pts, sizeof(double) * 3 * n_pts, cudaMemcpyHostToDevice, c->stream), "pts");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ds.p, s_inf, sizeof(double) * 6, cudaMemcpyHostToDevice, c->stream), "s_inf");
+  if (!rc) launch_stress(mesh->d_elem, ne, G, nu, is_dd_local, ddd.as<double>(), dp.as<double>(), n_pts, ds.as<double>(),
+                         dout.as<double>(), c->stream);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "stress launch");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(out, dout.p, sizeof(double) * 6 * n_pts, cudaMemcpyDeviceToHost, c->stream), "out");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "stress");
+  return rc;
+}
+
+int hfpx_local_submatrix(hfpx_ctx* c, double G, double nu, double h, double zr, double zi, const double* tau,
+                         const double* sfm, double* out) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!tau || !sfm || !out) return set_error(c, HFPX_ERR_ARG, "null argument");
+  cudaSetDevice(c->device);
+  DevBuf dt, ds, dout;
+  int rc = check_cuda(c, dt.alloc(sizeof(double) * 6), "alloc");
+  if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 72), "alloc");
+  if (!rc) rc = check_cuda(c, dout.alloc(sizeof(double) * 108), "alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dt.p, tau, sizeof(double) * 6, cudaMemcpyHostToDevice, c->stream), "tau");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ds.p, sfm, sizeof(double) * 72, cudaMemcpyHostToDevice, c->stream), "sfm");
+  if (!rc) launch_local_block(G, nu, h, zr, zi, dt.as<double>(), ds.as<double>(), dout.as<double>(), c->stream);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "local block launch");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(out, dout.p, sizeof(double) * 108, cudaMemcpyDeviceToHost, c->stream), "out");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "local block");
+  return rc;
+}
+
+// element_utilities.cpp:62-238 on the host, same arithmetic as the device
+// precompute (round-to-nearest, no contraction).
+int hfpx_element_frame(const double* vert, double* r, double* tau_out, double* sfm_out) {
+  if (!vert || !r || !tau_out || !sfm_out) return HFPX_ERR_ARG;
+  typedef std::complex<double> C;
+  double v[3][3];
+  for (int j = 0; j < 3; ++j)
+    for (int k = 0; k < 3; ++k) v[j][k] = vert[k + 3 * j];
+  auto dot = [](const double* a, const double* b) {
+    volatile double t = a[0] * b[0];
+    volatile double u = a[1] * b[1];
+    volatile double w = a[2] * b[2];
+    double s = t + u;
+    return s + w;
+  };
+  double a1[3], a2[3], e1[3], a3[3], e3[3], a4[3];
+  for (int k = 0; k < 3; ++k) { a1[k] = v[1][k] - v[0][k]; a2[k] = v[2][k] - v[0][k]; }
+  const double n1 = std::sqrt(dot(a1, a1));
+  for (int k = 0; k < 3; ++k) e1[k] = a1[k] / n1;
+  a3[0] = e1[1] * a2[2] - e1[2] * a2[1];
+  a3[1] = e1[2] * a2[0] - e1[0] * a2[2];
+  a3[2] = e1[0] * a2[1] - e1[1] * a2[0];
+  const double n3 = std::sqrt(dot(a3, a3));
+  for (int k = 0; k < 3; ++k) e3[k] = a3[k] / n3;
+  a4[0] = e3[1] * e1[2] - e3[2] * e1[1];
+  a4[1] = e3[2] * e1[0] - e3[0] * e1[2];
+  a4[2] = e3[0] * e1[1] - e3[1] * e1[0];
+  const double n4 = std::sqrt(dot(a4, a4));
+  for (int k = 0; k < 3; ++k) { r[k] = e1[k]; r[3 + k] = a4[k] / n4; r[6 + k] = e3[k]; }
+  C tau[3];
+  for (int j = 0; j < 3; ++j) {
+    double b[3];
+    for (int k = 0; k < 3; ++k) b[k] = v[j][k] - v[0][k];
+    tau[j] = C(dot(r, b), dot(r + 3, b));
+    tau_out[2 * j] = tau[j].real();
+    tau_out[2 * j + 1] = tau[j].imag();
+  }
+  const C det = tau[1] * std::conj(tau[2]) - tau[2] * std::conj(tau[1]);
+  C L[3][3];
+  L[1][0] = 0.0; L[1][1] = std::conj(tau[2]) / det; L[1][2] = -tau[2] / det;
+  L[2][0] = 0.0; L[2][1] = -std::conj(tau[1]) / det; L[2][2] = tau[1] / det;
+  for (int i = 0; i < 3; ++i) L[0][i] = -(L[1][i] + L[2][i]);
+  L[0][0] += 1.0;
+  C sf[6][6] = {};
+  auto prod = [](C* P, const C* A, const C* B, double s) {
+    P[0] += s * (A[0] * B[0]);
+    P[1] += s * (A[0] * B[1] + A[1] * B[0]);
+    P[2] += s * (A[0] * B[2] + A[2] * B[0]);
+    P[3] += s * (A[1] * B[1]);
+    P[4] += s * (A[2] * B[2]);
+    P[5] += s * (A[1] * B[2] + A[2] * B[1]);
+  };
+  for (int vx = 0; vx < 3; ++vx) {
+    prod(sf[vx], L[vx], L[vx], 2.0);
+    for (int i = 0; i < 3; ++i) sf[vx][i] -= L[vx][i];
+    prod(sf[3 + vx], L[(vx + 1) % 3], L[(vx + 2) % 3], 4.0);
+  }
+  for (int a = 0; a < 6; ++a)
+    for (int j = 0; j < 6; ++j) {
+      sfm_out[2 * (6 * a + j)] = sf[a][j].real();
+      sfm_out[2 * (6 * a + j) + 1] = sf[a][j].imag();
+    }
+  return HFPX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/hfpx_engine.h"
+
+struct hfpx_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  void* cublas = nullptr;          // cublasHandle_t
+  std::string last_error;
+  int* d_flags = nullptr;          // device status words (see kernels)
+};
+
+struct hfpx_mesh {
+  int64_t n_el = 0;
+  void* d_elem = nullptr;          // ElemRec[n_el]
+};
+
+struct hfpx_matrix {
+  int64_t n = 0, ld = 0;
+  double* d_a = nullptr;           // FP64 n x n column-major (ld)
+  float* d_f = nullptr;            // FP32 working copy (mixed mode), ld
+  int32_t* d_piv = nullptr;        // pivots (0-based global rows), n
+  int factored = 0;                // 0 none, 1 fp64 in place, 2 fp32 copy
+  int64_t info = 0;
+};
+
+namespace hfpx {
+// launches of this engine's own kernels in this process (library kernels excluded)
+extern std::atomic<long long> g_launches;
+int set_error(hfpx_ctx* c, int code, const std::string& msg);
+int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what);
+
+// assembly.cu
+size_t elem_record_bytes();
+void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int64_t* d_conn,
+                               int64_t ld_conn, int64_t n_el, double beta, void* d_elem,
+                               cudaStream_t s);
+void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                     int is_dd_local, double* d_a, int64_t ld, int* d_general_count,
+                     cudaStream_t s);
+void launch_vc_border(const void* d_elem, int64_t n_el, const int32_t* d_dof, int64_t n_dof,
+                      int is_dd_local, double* d_a, int64_t ld, cudaStream_t s);
+void launch_rhs(const void* d_elem, int64_t n_el, const int32_t* d_dof, const double* d_sinf,
+                int64_t n_rhs, double* d_rhs, int64_t ld_rhs, cudaStream_t s);
+void launch_stress(const void* d_elem, int64_t n_el, double G, double nu, int is_dd_local,
+                   const double* d_dd, const double* d_pts, int64_t n_pts, const double* d_sinf,
+                   double* d_out, cudaStream_t s);
+void launch_local_block(double G, double nu, double h, double zr, double zi, const double* d_tau,
+                        const double* d_sfm, double* d_out, cudaStream_t s);
+void launch_convert_f32(const double* d_a, int64_t ld, int64_t n, float* d_f, cudaStream_t s);
+
+// lu.cu
+int lu_factor_fp64(hfpx_ctx* c, hfpx_matrix* m);
+int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m);
+int lu_solve_fp64(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb);
+int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, int64_t ldb);
+int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb,
+                 double tol, int max_iter, hfpx_solve_info* info);
+}  // namespace hfpx

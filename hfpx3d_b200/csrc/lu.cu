@@ -1,0 +1,458 @@
+// Dense LU with partial pivoting (the work of il::LU / LAPACK dgetrf+dgetrs,
+// il/linear_algebra/dense/factorization/LU.h:79-120) and the mixed-precision
+// solve.
+//
+// Blocked right-looking LU, block nb = 256:
+//   panel  (n-k) x nb : recursive halving; the <=32-column base case is one
+//          cooperative kernel that keeps the whole tall panel resident in the
+//          shared memory of all SMs (one CTA per SM) and takes one grid
+//          barrier per column: local arg-max + candidate row -> barrier ->
+//          every CTA picks the same pivot, swaps, scales and updates its rows.
+//   swaps  applied to the columns left and right of the panel;
+//   U12 = L11^-1 A12 (triangular solve), A22 -= L21 U12 (trailing update).
+// FP64 mode factors the FP64 matrix in place (trailing update and triangular
+// solves: cuBLAS FP64, i.e. FP64 tensor cores).  Mixed mode factors an FP32
+// copy with TF32 tensor-core trailing updates and recovers FP64 accuracy by
+// iterative refinement against the untouched FP64 matrix.
+#include <cooperative_groups.h>
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <vector>
+#include "engine_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace hfpx {
+
+constexpr int kNb = 256;
+constexpr int kBaseW = 32;
+constexpr int kPanelThreads = 512;
+
+// ------------------------------------------------------ panel base kernel
+template <class T>
+struct PanelScratch {
+  T* cand;        // [2][grid][kBaseW] candidate pivot rows
+  double* cmax;   // [2][grid]
+  int* cidx;      // [2][grid]
+  T* rowj;        // [2][kBaseW] old row j
+};
+
+template <class T>
+__global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
+    T* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
+    PanelScratch<T> sc, int64_t* __restrict__ info, int64_t col_offset) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* chunk = reinterpret_cast<T*>(smem_raw);               // [w][rpc]
+  T* prow = chunk + (size_t)w * rpc;                        // [kBaseW]
+  __shared__ double rmax[kPanelThreads / 32];
+  __shared__ int ridx[kPanelThreads / 32];
+  __shared__ int s_p;
+  cg::grid_group grid = cg::this_grid();
+  const int b = blockIdx.x, G = gridDim.x, tid = threadIdx.x;
+  const int64_t r0 = (int64_t)b * rpc;
+  const int nrow = (int)std::max<int64_t>(0, std::min<int64_t>(rpc, m - r0));
+  for (int c = 0; c < w; ++c)
+    for (int i = tid; i < nrow; i += kPanelThreads) chunk[(size_t)c * rpc + i] = A[(r0 + i) + lda * c];
+  __syncthreads();
+  for (int j = 0; j < w; ++j) {
+    const int buf = j & 1;
+    // local arg-max of |a(i,j)| over owned rows i >= j (first index on ties)
+    double best = -1.0;
+    int bidx = INT32_MAX;
+    for (int i = tid; i < nrow; i += kPanelThreads) {
+      if (r0 + i < j) continue;
+      const double v = fabs((double)chunk[(size_t)j * rpc + i]);
+      if (v > best) { best = v; bidx = (int)(r0 + i); }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bidx, o);
+      if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+    }
+    if ((tid & 31) == 0) { rmax[tid >> 5] = best; ridx[tid >> 5] = bidx; }
+    __syncthreads();
+    if (tid == 0) {
+      for (int q = 1; q < kPanelThreads / 32; ++q)
+        if (rmax[q] > best || (rmax[q] == best && ridx[q] < bidx)) { best = rmax[q]; bidx = ridx[q]; }
+      sc.cmax[buf * G + b] = best;
+      sc.cidx[buf * G + b] = bidx;
+      s_p = bidx;
+    }
+    __syncthreads();
+    const int li = s_p - (int)r0;
+    if (li >= 0 && li < nrow && tid < w) sc.cand[((size_t)buf * G + b) * kBaseW + tid] = chunk[(size_t)tid * rpc + li];
+    const int lj = j - (int)r0;
+    if (lj >= 0 && lj < nrow && tid < w) sc.rowj[buf * kBaseW + tid] = chunk[(size_t)tid * rpc + lj];
+    grid.sync();
+    // global pivot, identical in every CTA
+    if (tid == 0) {
+      double gb = -1.0;
+      int gi = INT32_MAX, gw = 0;
+      for (int q = 0; q < G; ++q) {
+        const double v = sc.cmax[buf * G + q];
+        const int ix = sc.cidx[buf * G + q];
+        if (v > gb || (v == gb && ix < gi)) { gb = v; gi = ix; gw = q; }
+      }
+      s_p = gi;
+      rmax[0] = gb;
+      ridx[0] = gw;
+    }
+    __syncthreads();
+    const int p = s_p, win = ridx[0];
+    if (tid < w) prow[tid] = sc.cand[((size_t)buf * G + win) * kBaseW + tid];
+    if (b == 0 && tid == 0) {
+      piv[j] = p;
+      if (rmax[0] == 0.0 && info && *info == 0) *info = col_offset + j + 1;
+    }
+    __syncthreads();
+    // swap rows j and p
+    if (p != j) {
+      const int lp = p - (int)r0;
+      if (lp >= 0 && lp < nrow && tid < w) chunk[(size_t)tid * rpc + lp] = sc.rowj[buf * kBaseW + tid];
+      if (lj >= 0 && lj < nrow && tid < w) chunk[(size_t)tid * rpc + lj] = prow[tid];
+    }
+    __syncthreads();
+    // scale column j and rank-1 update of columns j+1..w-1, rows i > j
+    const T pv = prow[j];
+    if (pv != (T)0) {
+      const T inv = (T)1 / pv;
+      for (int i = tid; i < nrow; i += kPanelThreads) {
+        if (r0 + i <= j) continue;
+        const T l = chunk[(size_t)j * rpc + i] * inv;
+        chunk[(size_t)j * rpc + i] = l;
+        for (int c = j + 1; c < w; ++c) chunk[(size_t)c * rpc + i] -= l * prow[c];
+      }
+    }
+    __syncthreads();
+  }
+  for (int c = 0; c < w; ++c)
+    for (int i = tid; i < nrow; i += kPanelThreads) A[(r0 + i) + lda * c] = chunk[(size_t)c * rpc + i];
+}
+
+// -------------------------------------------------------------- row swaps
+// Apply interchanges piv[0..k) (rows relative to A's top, piv relative too)
+// to columns [0, ncols) of A; one thread per column, swaps in order.
+template <class T>
+__global__ void laswp_kernel(T* __restrict__ A, int64_t lda, int64_t ncols,
+                             const int32_t* __restrict__ piv, int k, int piv_base) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  T* col = A + lda * c;
+  for (int i = 0; i < k; ++i) {
+    const int p = piv[i] - piv_base;
+    if (p != i) {
+      const T t = col[i];
+      col[i] = col[p];
+      col[p] = t;
+    }
+  }
+}
+
+__global__ void offset_piv_kernel(int32_t* piv, int k, int off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < k) piv[i] += off;
+}
+
+// --------------------------------------------------------------- BLAS glue
+static inline cublasHandle_t H(hfpx_ctx* c) { return static_cast<cublasHandle_t>(c->cublas); }
+
+static void trsm_llu(hfpx_ctx* c, int64_t m, int64_t n, const double* L, int64_t ldl, double* B, int64_t ldb) {
+  const double one = 1.0;
+  cublasDtrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
+              L, (int)ldl, B, (int)ldb);
+}
+static void trsm_llu(hfpx_ctx* c, int64_t m, int64_t n, const float* L, int64_t ldl, float* B, int64_t ldb) {
+  const float one = 1.0f;
+  cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
+              L, (int)ldl, B, (int)ldb);
+}
+static void gemm_sub(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+                     int64_t ldb, double* C, int64_t ldc) {
+  const double mone = -1.0, one = 1.0;
+  cublasDgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
+              (int)ldc);
+}
+static void gemm_sub(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const float* A, int64_t lda, const float* B,
+                     int64_t ldb, float* C, int64_t ldc) {
+  const float mone = -1.0f, one = 1.0f;
+  cublasSgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
+              (int)ldc);
+}
+
+// --------------------------------------------------------------- driver
+template <class T>
+struct LuWork {
+  PanelScratch<T> sc{};
+  int64_t* d_info = nullptr;
+  int grid = 0;
+};
+
+template <class T>
+static int panel_base(hfpx_ctx* c, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
+                      int64_t col_offset) {
+  int G = std::min<int64_t>(c->num_sms, std::max<int64_t>(1, (m + 31) / 32));
+  int rpc = (int)((m + G - 1) / G);
+  size_t smem = (size_t)w * rpc * sizeof(T) + kBaseW * sizeof(T);
+  if (smem > 200 * 1024) return set_error(c, HFPX_ERR_ARG, "panel too tall for shared memory");
+  static bool attr_d = false, attr_f = false;
+  bool& attr = sizeof(T) == 8 ? attr_d : attr_f;
+  if (!attr) {
+    cudaFuncSetAttribute(panel_base_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  void* args[] = {&A, &lda, &m, &w, &rpc, &piv, &wk.sc, &wk.d_info, &col_offset};
+  ++g_launches;
+  cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_base_kernel<T>, dim3(G), dim3(kPanelThreads), args, smem,
+                                              c->stream);
+  return check_cuda(c, e, "panel_base_kernel launch");
+}
+
+template <class T>
+static void laswp(hfpx_ctx* c, T* A, int64_t lda, int64_t ncols, const int32_t* piv, int k, int base) {
+  if (ncols <= 0 || k <= 0) return;
+  ++g_launches;
+  laswp_kernel<T><<<(unsigned)((ncols + 127) / 128), 128, 0, c->stream>>>(A, lda, ncols, piv, k, base);
+}
+
+// dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
+template <class T>
+static int panel_rec(hfpx_ctx* c, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
+                     int64_t col_offset) {
+  if (w <= kBaseW) return panel_base(c, wk, A, lda, m, w, piv, col_offset);
+  const int w1 = w / 2, w2 = w - w1;
+  int rc = panel_rec(c, wk, A, lda, m, w1, piv, col_offset);
+  if (rc) return rc;
+  laswp(c, A + lda * w1, lda, w2, piv, w1, 0);
+  trsm_llu(c, w1, w2, A, lda, A + lda * w1, lda);
+  gemm_sub(c, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
+  rc = panel_rec(c, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1);
+  if (rc) return rc;
+  ++g_launches;
+  offset_piv_kernel<<<(w2 + 127) / 128, 128, 0, c->stream>>>(piv + w1, w2, w1);
+  laswp(c, A + w1, lda, w1, piv + w1, w2, w1);
+  return 0;
+}
+
+template <class T>
+static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, int64_t* info_out) {
+  LuWork<T> wk;
+  const int G = c->num_sms;
+  std::vector<void*> allocs;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return p;
+  };
+  wk.sc.cand = (T*)alloc(sizeof(T) * 2 * G * kBaseW);
+  wk.sc.cmax = (double*)alloc(sizeof(double) * 2 * G);
+  wk.sc.cidx = (int*)alloc(sizeof(int) * 2 * G);
+  wk.sc.rowj = (T*)alloc(sizeof(T) * 2 * kBaseW);
+  wk.d_info = (int64_t*)alloc(sizeof(int64_t));
+  int rc = 0;
+  if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info) rc = set_error(c, HFPX_ERR_NOMEM, "LU scratch");
+  if (!rc) cudaMemsetAsync(wk.d_info, 0, sizeof(int64_t), c->stream);
+  for (int64_t k = 0; k < n && !rc; k += kNb) {
+    const int kb = (int)std::min<int64_t>(kNb, n - k);
+    T* Akk = A + k + lda * k;
+    rc = panel_rec(c, wk, Akk, lda, n - k, kb, piv + k, k);
+    if (rc) break;
+    laswp(c, A + k, lda, k, piv + k, kb, 0);                                   // left columns
+    laswp(c, A + k + lda * (k + kb), lda, n - k - kb, piv + k, kb, 0);          // right columns
+    ++g_launches;
+    offset_piv_kernel<<<(kb + 127) / 128, 128, 0, c->stream>>>(piv + k, kb, (int)k);
+    if (k + kb < n) {
+      trsm_llu(c, kb, n - k - kb, Akk, lda, Akk + lda * kb, lda);
+      gemm_sub(c, n - k - kb, n - k - kb, kb, Akk + kb, lda, Akk + lda * kb, lda, Akk + kb + lda * kb, lda);
+    }
+  }
+  int64_t info = 0;
+  if (!rc) {
+    rc = check_cuda(c, cudaMemcpyAsync(&info, wk.d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream), "info");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "LU factorisation");
+  }
+  for (void* p : allocs) cudaFree(p);
+  *info_out = info;
+  if (!rc && info != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "matrix is singular: zero pivot at column " + std::to_string(info));
+  return rc;
+}
+
+int lu_factor_fp64(hfpx_ctx* c, hfpx_matrix* m) {
+  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  int rc = lu_factor<double>(c, m->d_a, m->ld, m->n, m->d_piv, &m->info);
+  m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 1 : 0;
+  return rc;
+}
+
+int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
+  if (!m->d_f) {
+    if (cudaMalloc(&m->d_f, sizeof(float) * (size_t)m->ld * m->n) != cudaSuccess) {
+      m->d_f = nullptr;
+      return set_error(c, HFPX_ERR_NOMEM, "FP32 working copy");
+    }
+  }
+  launch_convert_f32(m->d_a, m->ld, m->n, m->d_f, c->stream);
+  cublasSetMathMode(H(c), CUBLAS_TF32_TENSOR_OP_MATH);
+  int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info);
+  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
+  return rc;
+}
+
+// ----------------------------------------------------------------- solves
+template <class T>
+__global__ void permute_rows_kernel(const T* __restrict__ src, T* __restrict__ dst, const int32_t* __restrict__ perm,
+                                    int64_t n, int64_t nrhs, int64_t ld) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * nrhs) return;
+  const int64_t c = i / n, r = i - c * n;
+  dst[r + ld * c] = src[perm[r] + ld * c];
+}
+
+__global__ void d2f_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n, int64_t nrhs, int64_t lda,
+                           int64_t ldb) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * nrhs) return;
+  const int64_t c = i / n, r = i - c * n;
+  b[r + ldb * c] = (float)a[r + lda * c];
+}
+
+__global__ void axpy_f2d_kernel(const float* __restrict__ d, double* __restrict__ x, int64_t n, int64_t nrhs,
+                                int64_t ldd, int64_t ldx) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * nrhs) return;
+  const int64_t c = i / n, r = i - c * n;
+  x[r + ldx * c] += (double)d[r + ldd * c];
+}
+
+// Row permutation from the sequential interchanges (host: O(n)).
+static int build_perm(hfpx_ctx* c, const hfpx_matrix* m, int32_t** d_perm) {
+  std::vector<int32_t> piv(m->n), perm(m->n);
+  int rc = check_cuda(c, cudaMemcpyAsync(piv.data(), m->d_piv, sizeof(int32_t) * m->n, cudaMemcpyDeviceToHost, c->stream),
+                      "pivots");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "pivots");
+  if (rc) return rc;
+  for (int64_t i = 0; i < m->n; ++i) perm[i] = (int32_t)i;
+  for (int64_t i = 0; i < m->n; ++i) std::swap(perm[i], perm[piv[i]]);
+  if (cudaMalloc(d_perm, sizeof(int32_t) * m->n) != cudaSuccess) return set_error(c, HFPX_ERR_NOMEM, "perm");
+  return check_cuda(c, cudaMemcpyAsync(*d_perm, perm.data(), sizeof(int32_t) * m->n, cudaMemcpyHostToDevice, c->stream),
+                    "perm");
+}
+
+template <class T>
+static int solve_factored(hfpx_ctx* c, const hfpx_matrix* m, const T* LU, T* d_b, int64_t nrhs, int64_t ldb,
+                          const int32_t* d_perm) {
+  const int64_t n = m->n;
+  T* tmp = nullptr;
+  if (cudaMalloc(&tmp, sizeof(T) * (size_t)ldb * nrhs) != cudaSuccess) return set_error(c, HFPX_ERR_NOMEM, "solve tmp");
+  const int64_t tot = n * nrhs;
+  ++g_launches;
+  permute_rows_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(d_b, tmp, d_perm, n, nrhs, ldb);
+  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  const T one = 1;
+  if constexpr (sizeof(T) == 8) {
+    cublasDtrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)n, (int)nrhs, &one,
+                (const double*)LU, (int)m->ld, (double*)tmp, (int)ldb);
+    cublasDtrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, (int)nrhs,
+                &one, (const double*)LU, (int)m->ld, (double*)tmp, (int)ldb);
+  } else {
+    cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)n, (int)nrhs, &one,
+                (const float*)LU, (int)m->ld, (float*)tmp, (int)ldb);
+    cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, (int)nrhs,
+                &one, (const float*)LU, (int)m->ld, (float*)tmp, (int)ldb);
+  }
+  int rc = check_cuda(c, cudaMemcpy2DAsync(d_b, ldb * sizeof(T), tmp, ldb * sizeof(T), n * sizeof(T), nrhs,
+                                           cudaMemcpyDeviceToDevice, c->stream),
+                      "solve copy");
+  cudaStreamSynchronize(c->stream);
+  cudaFree(tmp);
+  return rc;
+}
+
+int lu_solve_fp64(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb) {
+  int32_t* d_perm = nullptr;
+  int rc = build_perm(c, m, &d_perm);
+  if (!rc) rc = solve_factored<double>(c, m, m->d_a, d_b, nrhs, ldb, d_perm);
+  cudaFree(d_perm);
+  return rc;
+}
+
+int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, int64_t ldb) {
+  int32_t* d_perm = nullptr;
+  int rc = build_perm(c, m, &d_perm);
+  if (!rc) rc = solve_factored<float>(c, m, m->d_f, d_b, nrhs, ldb, d_perm);
+  cudaFree(d_perm);
+  return rc;
+}
+
+// Iterative refinement: x += LU32^-1 r, r = b - A x in FP64.
+int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb, double tol, int max_iter,
+                 hfpx_solve_info* info) {
+  const int64_t n = m->n;
+  double *x = nullptr, *r = nullptr;
+  float* rf = nullptr;
+  int32_t* d_perm = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&x, sizeof(double) * ldb * nrhs) != cudaSuccess || cudaMalloc(&r, sizeof(double) * ldb * nrhs) != cudaSuccess ||
+      cudaMalloc(&rf, sizeof(float) * ldb * nrhs) != cudaSuccess)
+    rc = set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
+  if (!rc) rc = build_perm(c, m, &d_perm);
+  std::vector<double> bnorm(nrhs, 0.0), rnorm(nrhs, 0.0);
+  const int64_t tot = n * nrhs;
+  const unsigned nb = (unsigned)((tot + 255) / 256);
+  int it = 0;
+  double worst = INFINITY;
+  if (!rc) {
+    cudaMemsetAsync(x, 0, sizeof(double) * ldb * nrhs, c->stream);
+    cudaMemcpyAsync(r, d_b, sizeof(double) * ldb * nrhs, cudaMemcpyDeviceToDevice, c->stream);
+    for (int64_t j = 0; j < nrhs; ++j) {
+      int idx = 0;
+      cublasSetPointerMode(H(c), CUBLAS_POINTER_MODE_HOST);
+      cublasIdamax(H(c), (int)n, d_b + ldb * j, 1, &idx);
+      double v = 0.0;
+      cudaMemcpyAsync(&v, d_b + ldb * j + (idx - 1), sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+      cudaStreamSynchronize(c->stream);
+      bnorm[j] = std::fabs(v) > 0 ? std::fabs(v) : 1.0;
+    }
+    for (it = 1; it <= max_iter; ++it) {
+      ++g_launches;
+      d2f_kernel<<<nb, 256, 0, c->stream>>>(r, rf, n, nrhs, ldb, ldb);
+      rc = solve_factored<float>(c, m, m->d_f, rf, nrhs, ldb, d_perm);
+      if (rc) break;
+      ++g_launches;
+      axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(rf, x, n, nrhs, ldb, ldb);
+      cudaMemcpyAsync(r, d_b, sizeof(double) * ldb * nrhs, cudaMemcpyDeviceToDevice, c->stream);
+      const double mone = -1.0, one = 1.0;
+      cublasDgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)nrhs, (int)n, &mone, m->d_a, (int)m->ld, x, (int)ldb,
+                  &one, r, (int)ldb);
+      worst = 0.0;
+      for (int64_t j = 0; j < nrhs; ++j) {
+        int idx = 0;
+        cublasIdamax(H(c), (int)n, r + ldb * j, 1, &idx);
+        double v = 0.0;
+        cudaMemcpyAsync(&v, r + ldb * j + (idx - 1), sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        cudaStreamSynchronize(c->stream);
+        rnorm[j] = std::fabs(v) / bnorm[j];
+        worst = std::max(worst, rnorm[j]);
+      }
+      if (worst <= tol) break;
+    }
+    if (!rc) cudaMemcpyAsync(d_b, x, sizeof(double) * ldb * nrhs, cudaMemcpyDeviceToDevice, c->stream);
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "refinement");
+  }
+  if (info) {
+    info->iterations = std::min(it, max_iter);
+    info->residual = worst;
+    info->converged = worst <= tol;
+  }
+  cudaFree(x);
+  cudaFree(r);
+  cudaFree(rf);
+  cudaFree(d_perm);
+  if (!rc && !(worst <= tol)) rc = set_error(c, HFPX_ERR_NOT_CONVERGED, "refinement did not reach the tolerance");
+  return rc;
+}
+
+}  // namespace hfpx

@@ -1,0 +1,345 @@
+"""ctypes bindings of libhfpx_engine.so (include/hfpx_engine.h) and a Python
+mirror of the reference's call surface for the assembly -> solve -> stress path.
+
+The functions below keep the reference's names and argument meaning
+(namespace hfp3d in src/Solvers/system_assembly.h:35-71,
+src/Core/surface_mesh_utilities.h, and il::LU in
+il/linear_algebra/dense/factorization/LU.h:46-61).  Every call goes through
+the C-ABI; there is no CPU fallback: if the CUDA library is missing or no GPU
+is present the calls raise EngineError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libhfpx_engine.so')
+
+HFPX_OK, HFPX_ERR_ARG, HFPX_ERR_CUDA, HFPX_ERR_SINGULAR, HFPX_ERR_NOMEM, HFPX_ERR_STATE, \
+    HFPX_ERR_NOT_CONVERGED = range(7)
+HFPX_LU_FP64, HFPX_LU_MIXED = 0, 1
+_STATUS_NAMES = {0: 'HFPX_OK', 1: 'HFPX_ERR_ARG', 2: 'HFPX_ERR_CUDA', 3: 'HFPX_ERR_SINGULAR',
+                 4: 'HFPX_ERR_NOMEM', 5: 'HFPX_ERR_STATE', 6: 'HFPX_ERR_NOT_CONVERGED'}
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f'{_STATUS_NAMES.get(code, code)}: {msg}')
+        self.code = code
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [('iterations', ctypes.c_int), ('residual', ctypes.c_double), ('converged', ctypes.c_int)]
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_L = ctypes.POINTER(ctypes.c_int64)
+_V = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_f64 = ctypes.c_double
+_int = ctypes.c_int
+
+# name -> (restype, argtypes): the whole exported surface of include/hfpx_engine.h
+SIGNATURES = {
+    'hfpx_ctx_create': (_int, [_int, ctypes.POINTER(_V)]),
+    'hfpx_ctx_destroy': (_int, [_V]),
+    'hfpx_ctx_last_error': (ctypes.c_char_p, [_V]),
+    'hfpx_ctx_stream': (_int, [_V, ctypes.POINTER(_V)]),
+    'hfpx_ctx_synchronize': (_int, [_V]),
+    'hfpx_dof_handle': (_i64, [_D, _i64, _i64, _L, _i64, _i64, _int, _L]),
+    'hfpx_mesh_create': (_int, [_V, _D, _i64, _i64, _L, _i64, _i64, _f64, ctypes.POINTER(_V)]),
+    'hfpx_mesh_destroy': (_int, [_V]),
+    'hfpx_assemble': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, _int, ctypes.POINTER(_V)]),
+    'hfpx_assemble_into': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, _int, _V]),
+    'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
+    'hfpx_matrix_dims': (_int, [_V, _L, _L]),
+    'hfpx_matrix_download': (_int, [_V, _V, _D, _i64]),
+    'hfpx_matrix_destroy': (_int, [_V]),
+    'hfpx_rhs_sinf': (_int, [_V, _V, _L, _i64, _D, _i64, _D, _i64]),
+    'hfpx_lu_factor': (_int, [_V, _V, _int, _L]),
+    'hfpx_lu_solve': (_int, [_V, _V, _D, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_lu_solve_device': (_int, [_V, _V, _V, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_ctx_launch_count': (_i64, [_V]),
+    'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
+    'hfpx_local_submatrix': (_int, [_V, _f64, _f64, _f64, _f64, _f64, _D, _D, _D]),
+    'hfpx_element_frame': (_int, [_D, _D, _D, _D]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the engine library (fails loudly when it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EngineError(HFPX_ERR_STATE, f'{LIB_PATH} not built (python -m hfpx3d_b200.build)')
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def _lp(a):
+    return a.ctypes.data_as(_L)
+
+
+def _f(a, dtype=np.float64):
+    return np.asfortranarray(a, dtype=dtype)
+
+
+class Context:
+    """One GPU, one CUDA stream (hfpx_ctx)."""
+
+    def __init__(self, device=0):
+        self.h = _V()
+        rc = lib().hfpx_ctx_create(device, ctypes.byref(self.h))
+        if rc != HFPX_OK:
+            raise EngineError(rc, f'cannot create a context on device {device}')
+        self.device = device
+
+    def check(self, rc):
+        if rc != HFPX_OK:
+            raise EngineError(rc, lib().hfpx_ctx_last_error(self.h).decode())
+
+    @property
+    def stream(self):
+        s = _V()
+        self.check(lib().hfpx_ctx_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def synchronize(self):
+        self.check(lib().hfpx_ctx_synchronize(self.h))
+
+    def close(self):
+        if self.h:
+            lib().hfpx_ctx_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class MeshGeom:
+    """Mesh_Geom_T (src/Core/surface_mesh_utilities.h:25-31): nods >=3 x Nn,
+    conn >=3 x Ne (0-based), both column-major; rows 3,4 carry tip flags."""
+    nods: np.ndarray
+    conn: np.ndarray
+
+    def __post_init__(self):
+        self.nods = _f(self.nods)
+        self.conn = _f(self.conn, np.int64)
+
+    @property
+    def n_el(self):
+        return self.conn.shape[1]
+
+
+@dataclass
+class NumParam:
+    """Num_Param_T (src/Core/model_parameters.h:75-95)."""
+    beta: float = 0.125
+    tip_type: int = 1
+    is_dd_local: bool = False
+
+
+def make_dof_h_crack(mesh: MeshGeom, tip_type: int):
+    """surface_mesh_utilities.cpp:28-112 -> (dof_h n_el x 18 int64 F-order, n_dof)."""
+    ne = mesh.n_el
+    dof = np.zeros((ne, 18), dtype=np.int64, order='F')
+    n = lib().hfpx_dof_handle(_dp(mesh.nods), mesh.nods.shape[0], mesh.nods.shape[1], _lp(mesh.conn),
+                              mesh.conn.shape[0], ne, tip_type, _lp(dof))
+    if n < 0:
+        raise EngineError(-n, 'bad mesh for the DoF handle')
+    return dof, int(n)
+
+
+class DeviceMesh:
+    """Mesh uploaded with its per-element precompute (hfpx_mesh)."""
+
+    def __init__(self, ctx: Context, mesh: MeshGeom, beta=0.125):
+        self.ctx, self.h = ctx, _V()
+        ctx.check(lib().hfpx_mesh_create(ctx.h, _dp(mesh.nods), mesh.nods.shape[0], mesh.nods.shape[1],
+                                         _lp(mesh.conn), mesh.conn.shape[0], mesh.n_el, beta,
+                                         ctypes.byref(self.h)))
+        self.n_el = mesh.n_el
+
+    def close(self):
+        if self.h:
+            lib().hfpx_mesh_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceMatrix:
+    """Dense column-major matrix resident in HBM (hfpx_matrix)."""
+
+    def __init__(self, ctx, handle):
+        self.ctx, self.h = ctx, handle
+        n, ld = _i64(), _i64()
+        lib().hfpx_matrix_dims(self.h, ctypes.byref(n), ctypes.byref(ld))
+        self.n, self.ld = n.value, ld.value
+
+    @classmethod
+    def upload(cls, ctx, a):
+        a = _f(a)
+        h = _V()
+        ctx.check(lib().hfpx_matrix_upload(ctx.h, _dp(a), a.shape[0], a.shape[0], ctypes.byref(h)))
+        return cls(ctx, h)
+
+    def download(self):
+        out = np.empty((self.n, self.n), order='F')
+        self.ctx.check(lib().hfpx_matrix_download(self.ctx.h, self.h, _dp(out), self.n))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().hfpx_matrix_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def assemble(ctx, dmesh: DeviceMesh, dof_h, n_dof, G, nu, is_dd_local=False, vc=False) -> DeviceMatrix:
+    h = _V()
+    dof_h = _f(dof_h, np.int64)
+    ctx.check(lib().hfpx_assemble(ctx.h, dmesh.h, _lp(dof_h), n_dof, G, nu, int(is_dd_local), int(vc),
+                                  ctypes.byref(h)))
+    return DeviceMatrix(ctx, h)
+
+
+def assemble_into(ctx, dmesh: DeviceMesh, dof_h, n_dof, G, nu, matrix: DeviceMatrix, is_dd_local=False, vc=False):
+    """Re-assemble into an existing device matrix (storage reused)."""
+    dof_h = _f(dof_h, np.int64)
+    ctx.check(lib().hfpx_assemble_into(ctx.h, dmesh.h, _lp(dof_h), n_dof, G, nu, int(is_dd_local), int(vc),
+                                       matrix.h))
+    return matrix
+
+
+def make_3dbem_matrix_s(ctx, shear_m, poiss_r, mesh: MeshGeom, n_par: NumParam, dof_h=None):
+    """system_assembly.cpp:30-219 -> (host matrix, dof_h, n_dof)."""
+    if dof_h is None:
+        dof_h, n_dof = make_dof_h_crack(mesh, n_par.tip_type)
+    else:
+        n_dof = int(dof_h.max()) + 1
+    dm = DeviceMesh(ctx, mesh, n_par.beta)
+    m = assemble(ctx, dm, dof_h, n_dof, shear_m, poiss_r, n_par.is_dd_local, vc=False)
+    return m.download(), dof_h, n_dof
+
+
+def make_3dbem_matrix_vc(ctx, shear_m, poiss_r, mesh: MeshGeom, n_par: NumParam, dof_h=None):
+    """system_assembly.cpp:458-557 (corner defined as 0) -> (host matrix, dof_h, n_dof)."""
+    if dof_h is None:
+        dof_h, n_dof = make_dof_h_crack(mesh, n_par.tip_type)
+    else:
+        n_dof = int(dof_h.max()) + 1
+    dm = DeviceMesh(ctx, mesh, n_par.beta)
+    m = assemble(ctx, dm, dof_h, n_dof, shear_m, poiss_r, n_par.is_dd_local, vc=True)
+    return m.download(), dof_h, n_dof
+
+
+def add_s_inf_to_3dbem_rhs(ctx, dmesh: DeviceMesh, dof_h, n_dof, s_inf, rhs=None):
+    """system_assembly.cpp:222-274; s_inf is (6,) or 6 x n_rhs."""
+    s = _f(np.asarray(s_inf, dtype=np.float64).reshape(6, -1))
+    nr = s.shape[1]
+    if rhs is None:
+        rhs = np.zeros((n_dof, nr), order='F')
+    rhs = _f(rhs.reshape(n_dof, nr) if rhs.ndim == 1 else rhs)
+    dof_h = _f(dof_h, np.int64)
+    ctx.check(lib().hfpx_rhs_sinf(ctx.h, dmesh.h, _lp(dof_h), n_dof, _dp(s), nr, _dp(rhs), rhs.shape[0]))
+    return rhs[:, 0].copy() if nr == 1 else rhs
+
+
+class LU:
+    """il::LU<il::Array2D<double>> (LU.h:46-120) on the device: factor on
+    construction (dgetrf), solve(y) (dgetrs).  mode HFPX_LU_MIXED factors an
+    FP32 copy on TF32 tensor cores and refines in FP64."""
+
+    def __init__(self, ctx, matrix: DeviceMatrix, mode=HFPX_LU_FP64):
+        self.ctx, self.matrix, self.mode = ctx, matrix, mode
+        info = _i64()
+        rc = lib().hfpx_lu_factor(ctx.h, matrix.h, mode, ctypes.byref(info))
+        self.info = info.value
+        ctx.check(rc)
+
+    def solve(self, y, tol=0.0, max_iter=0):
+        b = _f(np.array(y, dtype=np.float64, copy=True))
+        one = b.ndim == 1
+        if one:
+            b = b.reshape(-1, 1, order='F')
+        info = SolveInfo()
+        rc = lib().hfpx_lu_solve(self.ctx.h, self.matrix.h, _dp(b), b.shape[1], b.shape[0], tol, max_iter,
+                                 ctypes.byref(info))
+        self.last_info = info
+        self.ctx.check(rc)
+        return b[:, 0].copy() if one else b
+
+
+def make_3dbem_stress_f_s(ctx, dmesh: DeviceMesh, shear_m, poiss_r, dd, pts, s_inf, is_dd_local=False):
+    """system_assembly.cpp:279-455: dd (6 Ne) x 3, pts 3 x P -> P x 6."""
+    dd = _f(dd)
+    pts = _f(pts)
+    s = np.ascontiguousarray(np.asarray(s_inf, dtype=np.float64).reshape(6))
+    P = pts.shape[1]
+    out = np.empty((P, 6), order='F')
+    ctx.check(lib().hfpx_stress(ctx.h, dmesh.h, shear_m, poiss_r, int(is_dd_local), _dp(dd), _dp(pts), P,
+                                _dp(s), _dp(out)))
+    return out
+
+
+def make_local_3dbem_submatrix(ctx, shear_m, poiss_r, h, z, tau, sfm):
+    """elasticity_kernel_integration.cpp:34-205 (kernel 1) -> 6 x 18."""
+    tau = np.ascontiguousarray(np.column_stack([np.real(tau), np.imag(tau)]).reshape(-1))
+    sfm = np.asarray(sfm)
+    sfm = np.ascontiguousarray(np.stack([sfm.real, sfm.imag], axis=-1).reshape(-1))
+    out = np.empty(108)
+    ctx.check(lib().hfpx_local_submatrix(ctx.h, shear_m, poiss_r, h, complex(z).real, complex(z).imag,
+                                         _dp(tau), _dp(sfm), _dp(out)))
+    return out.reshape(6, 18)
+
+
+def element_frame(vert):
+    """make_el_sfm_uniform + make_el_tau_crd (element_utilities.cpp:89-238) on
+    the host: vert is 3 x 3 (column j = vertex j) -> (r 3x3, tau (3,), sfm 6x6)."""
+    v = np.ascontiguousarray(np.asarray(vert, dtype=np.float64).T)
+    r, tau, sfm = np.empty(9), np.empty(6), np.empty(72)
+    rc = lib().hfpx_element_frame(_dp(v), _dp(r), _dp(tau), _dp(sfm))
+    if rc != HFPX_OK:
+        raise EngineError(rc, 'element_frame')
+    return r.reshape(3, 3), tau[0::2] + 1j * tau[1::2], (sfm[0::2] + 1j * sfm[1::2]).reshape(6, 6)
+
+
+def write_dd_vector_to_md(sol, dof_h, n_el):
+    """surface_mesh_utilities.cpp:256-328 -> nodal DD (6 n_el) x 3."""
+    dd = np.zeros((6 * n_el, 3), order='F')
+    d = np.asarray(dof_h)
+    for j in range(18):
+        rows = 6 * np.arange(n_el) + j // 3
+        g = d[:, j]
+        ok = g >= 0
+        dd[rows[ok], j % 3] = sol[g[ok]]
+    return dd

@@ -1,0 +1,144 @@
+/* hfpx_engine.h -- C-ABI of the B200 engine for HFPx3D's
+ * assembly -> dense solve -> stress path.
+ *
+ * Every entry point replaces one function of the reference's C++ call surface
+ * (namespace hfp3d, plus il::LU); the comment above each declaration names it
+ * by file:line inside the HFPx3D project.  Plain pointers and sizes only:
+ *   - all host arrays are column-major with the leading dimension given;
+ *   - mesh: nods is ld_nods x n_nodes (rows 0..2 coordinates, rows 3..4 the
+ *     tip flags the DoF handle reads), conn is ld_conn x n_el int64 0-based;
+ *   - dof_h is n_el x 18 int64 column-major, -1 marks a fixed DoF;
+ *   - device objects (context, mesh, matrix) are opaque engine-owned handles;
+ *     host buffers stay caller-owned.
+ * Every function returns an hfpx_status; no exception crosses the boundary.
+ * hfpx_ctx_last_error() gives the message of the last failure on a context.
+ * A context owns one CUDA stream and is not shared across host threads.
+ */
+#ifndef HFPX_ENGINE_H
+#define HFPX_ENGINE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hfpx_ctx hfpx_ctx;
+typedef struct hfpx_mesh hfpx_mesh;
+typedef struct hfpx_matrix hfpx_matrix;
+
+typedef enum {
+  HFPX_OK = 0,
+  HFPX_ERR_ARG = 1,          /* bad argument (the reference aborts via IL_EXPECT_FAST) */
+  HFPX_ERR_CUDA = 2,         /* CUDA runtime / library failure */
+  HFPX_ERR_SINGULAR = 3,     /* zero pivot; info holds the 1-based column (LU.h:92-99) */
+  HFPX_ERR_NOMEM = 4,        /* device allocation failed */
+  HFPX_ERR_STATE = 5,        /* object in the wrong state (e.g. solve before factor) */
+  HFPX_ERR_NOT_CONVERGED = 6 /* refinement did not reach the tolerance */
+} hfpx_status;
+
+typedef enum {
+  HFPX_LU_FP64 = 0,   /* FP64 LU in place, FP64 triangular solves */
+  HFPX_LU_MIXED = 1   /* FP32 LU of a copy (TF32 tensor-core trailing updates),
+                         FP64 iterative refinement against the FP64 matrix */
+} hfpx_lu_mode;
+
+typedef struct {
+  int iterations;          /* refinement steps taken (0 for FP64 mode) */
+  double residual;         /* final max_j ||b_j - A x_j||_inf / ||b_j||_inf */
+  int converged;
+} hfpx_solve_info;
+
+/* ---- context ---------------------------------------------------------- */
+int hfpx_ctx_create(int device, hfpx_ctx **ctx);
+int hfpx_ctx_destroy(hfpx_ctx *ctx);
+const char *hfpx_ctx_last_error(const hfpx_ctx *ctx);
+/* The context's cudaStream_t, for callers that time or order work around it. */
+int hfpx_ctx_stream(hfpx_ctx *ctx, void **stream);
+int hfpx_ctx_synchronize(hfpx_ctx *ctx);
+
+/* ---- DoF handle: make_dof_h_crack, src/Core/surface_mesh_utilities.cpp:28-112
+ * (approximation order 2).  Host-only; writes dof_h and returns n_dof (< 0 on
+ * a bad argument). */
+int64_t hfpx_dof_handle(const double *nods, int64_t ld_nods, int64_t n_nodes,
+                        const int64_t *conn, int64_t ld_conn, int64_t n_el,
+                        int tip_type, int64_t *dof_h);
+
+/* ---- mesh: uploads the mesh and computes, once per element, what
+ * make_el_r_tensor / make_el_tau_crd / make_el_sfm_uniform / el_cp_uniform
+ * (src/Core/element_utilities.cpp:62-238, 364-395) give; the reference
+ * recomputes these inside its pair loops (system_assembly.cpp:64-113). */
+int hfpx_mesh_create(hfpx_ctx *ctx, const double *nods, int64_t ld_nods, int64_t n_nodes,
+                     const int64_t *conn, int64_t ld_conn, int64_t n_el, double beta,
+                     hfpx_mesh **mesh);
+int hfpx_mesh_destroy(hfpx_mesh *mesh);
+
+/* ---- assembly: make_3dbem_matrix_s, src/Solvers/system_assembly.cpp:30-219
+ * (vc_border == 0), or make_3dbem_matrix_vc, :458-557 (vc_border != 0: one
+ * extra row of shape-function-weighted normals, one extra column of -normals,
+ * corner 0).  The matrix stays in device memory. */
+int hfpx_assemble(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, int64_t n_dof,
+                  double shear_m, double poiss_r, int is_dd_local, int vc_border,
+                  hfpx_matrix **matrix);
+/* Same as hfpx_assemble into an existing matrix of matching size (n_dof, or
+ * n_dof + 1 with vc_border), reusing its device storage; clears any
+ * factorisation it held. */
+int hfpx_assemble_into(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, int64_t n_dof,
+                       double shear_m, double poiss_r, int is_dd_local, int vc_border,
+                       hfpx_matrix *matrix);
+/* Upload a caller matrix (n x n, column-major, ld_host) for il::LU use. */
+int hfpx_matrix_upload(hfpx_ctx *ctx, const double *a, int64_t n, int64_t ld_host,
+                       hfpx_matrix **matrix);
+int hfpx_matrix_dims(const hfpx_matrix *matrix, int64_t *n, int64_t *ld);
+/* Copy the FP64 matrix (or, after an FP64 factorisation, its LU factors) to host. */
+int hfpx_matrix_download(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *a, int64_t ld_host);
+int hfpx_matrix_destroy(hfpx_matrix *matrix);
+
+/* ---- right-hand side: add_s_inf_to_3dbem_rhs, system_assembly.cpp:222-274.
+ * s_inf is 6 x n_rhs (Voigt xx,yy,zz,xy,xz,yz, tension positive); rhs is
+ * ld_rhs x n_rhs on the host; rhs[dof] -= (n . s_inf)_l is added to what the
+ * caller passes in. */
+int hfpx_rhs_sinf(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, int64_t n_dof,
+                  const double *s_inf, int64_t n_rhs, double *rhs, int64_t ld_rhs);
+
+/* ---- dense LU: il::LU<il::Array2D<double>>(A, il::io, status),
+ * il/linear_algebra/dense/factorization/LU.h:79-99 (LAPACK dgetrf).  Partial
+ * pivoting by rows.  info = 0, or the 1-based column of a zero pivot
+ * (HFPX_ERR_SINGULAR). */
+int hfpx_lu_factor(hfpx_ctx *ctx, hfpx_matrix *matrix, int mode, int64_t *info);
+/* lu.solve(y), LU.h:106-120 (LAPACK dgetrs), for nrhs columns of b (host,
+ * ld_b x nrhs) overwritten with x.  In mixed mode x is refined in FP64 until
+ * the relative residual is below tol (<= 0 selects 1e-12) or max_iter steps. */
+int hfpx_lu_solve(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *b, int64_t nrhs,
+                  int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
+
+/* Same as hfpx_lu_solve with b already in device memory (ld_b >= n). */
+int hfpx_lu_solve_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, int64_t nrhs,
+                         int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
+
+/* Number of this engine's own kernels launched on the context so far
+ * (library kernels such as cuBLAS are not counted). */
+int64_t hfpx_ctx_launch_count(const hfpx_ctx *ctx);
+
+/* ---- stress: make_3dbem_stress_f_s, system_assembly.cpp:279-455.
+ * dd is (6 n_el) x 3 nodal DD (row 6 e + node), pts 3 x n_pts, out n_pts x 6
+ * [Sxx,Syy,Szz,Sxy,Sxz,Syz]; s_inf (6) is added.  Deterministic (no atomics). */
+int hfpx_stress(hfpx_ctx *ctx, const hfpx_mesh *mesh, double shear_m, double poiss_r,
+                int is_dd_local, const double *dd, const double *pts, int64_t n_pts,
+                const double *s_inf, double *out);
+
+/* ---- one element at one point: make_local_3dbem_submatrix,
+ * src/Elasticity/elasticity_kernel_integration.cpp:34-205 (kernel 1).
+ * tau: 3 complex (re,im), sfm: 6x6 complex row-major (re,im); out 6x18
+ * row-major local stress influence.  Runs the device kernel once. */
+int hfpx_local_submatrix(hfpx_ctx *ctx, double shear_m, double poiss_r, double h, double zr,
+                         double zi, const double *tau, const double *sfm, double *out);
+
+/* ---- element frame on the host (same arithmetic as the device precompute):
+ * make_el_sfm_uniform + make_el_tau_crd, element_utilities.cpp:89-238.
+ * vert[k + 3 j] = coordinate k of vertex j; r row-major 3x3. */
+int hfpx_element_frame(const double *vert, double *r, double *tau, double *sfm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

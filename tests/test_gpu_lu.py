@@ -1,0 +1,87 @@
+"""Dense LU (il::LU / LAPACK dgetrf+dgetrs semantics) on the GPU: FP64 and mixed
+(TF32 tensor-core factorisation + FP64 refinement), against LAPACK (numpy)."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fp64_solution_matches_lapack(ctx):
+    from hfpx3d_b200 import engine
+    g = golden('ref_p24')
+    m = engine.DeviceMatrix.upload(ctx, g['A'])
+    lu = engine.LU(ctx, m, engine.HFPX_LU_FP64)
+    x = lu.solve(g['rhs'])
+    assert np.abs(x - g['x']).max() / np.abs(g['x']).max() < 1e-12
+
+
+@pytest.mark.parametrize('n', [300, 1000, 2500])
+def test_fp64_random_and_factors(ctx, n):
+    from hfpx3d_b200 import engine
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)) + n ** 0.5 * np.eye(n)
+    B = rng.standard_normal((n, 3))
+    m = engine.DeviceMatrix.upload(ctx, A)
+    lu = engine.LU(ctx, m)
+    X = lu.solve(B)
+    assert np.abs(A @ X - B).max() < 1e-10 * np.abs(B).max()
+    # factors reproduce A under the row permutation LAPACK-style
+    F = m.download()
+    L = np.tril(F, -1) + np.eye(n)
+    U = np.triu(F)
+    PA = L @ U
+    assert np.abs(np.sort(PA, axis=None) - np.sort(A, axis=None)).max() < 1e-9 * np.abs(A).max()
+
+
+def test_mixed_refinement_reaches_fp64(ctx):
+    from hfpx3d_b200 import engine
+    g = golden('ref_c1')
+    from hfpx3d_b200 import meshgen  # noqa: F401
+    mesh = engine.MeshGeom(g['nods'], g['conn'])
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh)
+    A = engine.assemble(ctx, dm, dof, n, 1.0, 0.35)
+    lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+    x = lu.solve(g['rhs'], tol=1e-12, max_iter=30)
+    assert lu.last_info.converged and lu.last_info.residual <= 1e-12
+    assert np.abs(x - g['x']).max() / np.abs(g['x']).max() < 1e-9
+
+
+def test_vc_bordered_system(ctx, ora):
+    from hfpx3d_b200 import engine
+    g = golden('ref_c1')
+    mesh = engine.MeshGeom(g['nods'], g['conn'])
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh)
+    A = engine.assemble(ctx, dm, dof, n, 1.0, 0.35, vc=True)
+    Ah = A.download()
+    rhs = np.concatenate([g['rhs'], [1.0]])
+    x_ref = np.linalg.solve(Ah, rhs)
+    for mode in (engine.HFPX_LU_FP64, engine.HFPX_LU_MIXED):
+        A2 = engine.DeviceMatrix.upload(ctx, Ah)
+        x = engine.LU(ctx, A2, mode).solve(rhs, tol=1e-12)
+        assert np.abs(x - x_ref).max() / np.abs(x_ref).max() < 1e-9
+
+
+def test_singular_matrix_reports_column(ctx):
+    from hfpx3d_b200 import engine
+    A = np.eye(50)
+    A[:, 17] = 0.0
+    m = engine.DeviceMatrix.upload(ctx, A)
+    with pytest.raises(engine.EngineError) as e:
+        engine.LU(ctx, m)
+    assert e.value.code == engine.HFPX_ERR_SINGULAR
+    b = np.ones(50)
+    with pytest.raises(engine.EngineError):
+        engine.lib()  # library still usable
+        engine.LU.solve(type('X', (), {'ctx': ctx, 'matrix': m})(), b)
+
+
+def test_solve_before_factor_is_refused(ctx):
+    from hfpx3d_b200 import engine
+    m = engine.DeviceMatrix.upload(ctx, np.eye(10))
+    b = np.ones((10, 1), order='F')
+    rc = engine.lib().hfpx_lu_solve(ctx.h, m.h, engine._dp(b), 1, 10, 0.0, 0, None)
+    assert rc == engine.HFPX_ERR_STATE
