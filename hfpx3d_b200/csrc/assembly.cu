@@ -619,15 +619,16 @@ void launch_local_block(double G, double nu, double h, double zr, double zi, con
 }
 
 // ------------------------------------------------------- FP64 -> FP32 copy
+// Whole columns (ld entries each, padding rows included) as a flat range.
 __global__ void convert_f32_kernel(const double* __restrict__ a, int64_t ld, int64_t n,
                                    float* __restrict__ f) {
-  const int64_t col = blockIdx.y;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
-    f[r + ld * col] = (float)a[r + ld * col];
+  const int64_t total = ld * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+    f[i] = (float)a[i];
 }
 
 void launch_convert_f32(const double* d_a, int64_t ld, int64_t n, float* d_f, cudaStream_t s) {
-  const dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 64), (unsigned)n);
+  const dim3 grid(148 * 16);
   ++g_launches;
   convert_f32_kernel<<<grid, 256, 0, s>>>(d_a, ld, n, d_f);
 }

@@ -202,6 +202,7 @@ static int check_assembly_args(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t
                                double nu) {
   if (!mesh || !dof_h) return set_error(c, HFPX_ERR_ARG, "null mesh or dof handle");
   if (n_dof < 1 || n_dof > 18 * mesh->n_el) return set_error(c, HFPX_ERR_ARG, "n_dof out of range");
+  if (mesh->n_el > 65535) return set_error(c, HFPX_ERR_ARG, "more than 65535 elements (grid limit of the assembly launch)");
   if (!(G > 0) || !(nu > -1.0 && nu < 0.5))
     return set_error(c, HFPX_ERR_ARG, "shear modulus must be > 0 and Poisson ratio in (-1, 0.5)");
   return HFPX_OK;

@@ -70,27 +70,38 @@ __device__ __forceinline__ void lim_moments_diff(double chi_m, double chi_n, cpl
   const cplx e = mk(ce, se), e2 = e * e, e3 = e2 * e, e4 = e2 * e2;
   const cplx ec = conj(e), e2c = conj(e2);
   const double iD = 1.0 / D;
-#pragma unroll
-  for (int side = 0; side < 2; ++side) {
+  // Both ends go through the same code into separate arrays and are
+  // subtracted explicitly: for an edge whose two ends are seen under the same
+  // angle (the point on the edge line) the terms, of size 1/|d|, cancel
+  // exactly instead of leaving a contraction residue.
+  cplx E[2][12];
+#pragma unroll 1
+  for (int side = 0; side < 2; ++side) {  // one instruction sequence for both ends
     const double chi = side ? chi_n : chi_m;
-    const double sg = side ? 1.0 : -1.0;
     double s, c;
     sincos(chi, &s, &c);
     const cplx u = mk(c, s), u3 = u * u * u;
     const double at = atanh(s);
     const cplx iu = mul_i(u), iu3 = mul_i(u3);
-    P[0] += mk(sg * (-s * iD));
-    P[1] += (sg * -at) * e;
-    P[2] += (sg * -at) * ec;
-    P[3] += (sg * -D) * (e2 * (mk(at) + 2.0 * iu));
-    P[4] += (sg * -D) * (e2c * (mk(at) - 2.0 * mul_i(conj(u))));
-    P[5] += mk(sg * D * at);
-    Q[0] += (sg * iD / 6.0) * mul_i(e2 * (u3 + 3.0 * u));
-    Q[1] += sg * (e3 * (mk(at / 3.0) + (2.0 / 3.0) * iu + iu3 * (1.0 / 12.0)));
-    Q[2] += (-sg) * (e * (mk(at) + (5.0 / 12.0) * iu));
-    Q[3] += (sg * D) * (e4 * (mk(at) + 2.0 * iu - (2.0 / 3.0) * iu3));
-    Q[4] += mk(sg * D * at);
-    Q[5] += (sg * -D) * (e2 * (mk(at) + 2.0 * iu));
+    cplx* V = E[side];
+    V[0] = mk(-s * iD);
+    V[1] = -at * e;
+    V[2] = -at * ec;
+    V[3] = -D * (e2 * (mk(at) + 2.0 * iu));
+    V[4] = -D * (e2c * (mk(at) - 2.0 * mul_i(conj(u))));
+    V[5] = mk(D * at);
+    V[6] = (iD / 6.0) * mul_i(e2 * (u3 + 3.0 * u));
+    V[7] = e3 * (mk(at / 3.0) + (2.0 / 3.0) * iu + iu3 * (1.0 / 12.0));
+    V[8] = -(e * (mk(at) + (5.0 / 12.0) * iu));
+    V[9] = D * (e4 * (mk(at) + 2.0 * iu - (2.0 / 3.0) * iu3));
+    V[10] = mk(D * at);
+    V[11] = -D * (e2 * (mk(at) + 2.0 * iu));
+  }
+#pragma unroll
+  for (int j = 0; j < 12; ++j) {
+    const cplx dlt = mk(__dsub_rn(E[1][j].re, E[0][j].re), __dsub_rn(E[1][j].im, E[0][j].im));
+    cplx& T = j < 6 ? P[j] : Q[j - 6];
+    T = mk(__dadd_rn(T.re, dlt.re), __dadd_rn(T.im, dlt.im));
   }
 }
 
@@ -186,6 +197,31 @@ struct EdgeSet {
   bool use[3];
 };
 
+// Complex product and quotient without fused multiply-adds (round-to-nearest
+// products and sums in the order of the textbook formulas).  The quotient is
+// Smith's algorithm (Smith 1962, CACM Algorithm 116).  Foot vectors of points
+// that lie exactly on an edge line come out as rounding noise whose size
+// decides the |d| < 2.221e-16 branch, so this arithmetic is kept identical to
+// an IEEE-double host computation of the same formulas.
+__device__ __forceinline__ cplx mul_rn(cplx x, cplx y) {
+  return {__dsub_rn(__dmul_rn(x.re, y.re), __dmul_rn(x.im, y.im)),
+          __dadd_rn(__dmul_rn(x.re, y.im), __dmul_rn(x.im, y.re))};
+}
+
+__device__ __forceinline__ cplx div_smith(cplx x, cplx y) {
+  const double a = x.re, b = x.im, c = y.re, d = y.im;
+  if (fabs(c) < fabs(d)) {
+    const double r = __ddiv_rn(c, d), den = __dadd_rn(__dmul_rn(c, r), d);
+    return {__ddiv_rn(__dadd_rn(__dmul_rn(a, r), b), den), __ddiv_rn(__dsub_rn(__dmul_rn(b, r), a), den)};
+  }
+  const double r = __ddiv_rn(d, c), den = __dadd_rn(__dmul_rn(d, r), c);
+  if (fabs(r) > 2.2250738585072014e-308)
+    return {__ddiv_rn(__dadd_rn(__dmul_rn(b, r), a), den), __ddiv_rn(__dsub_rn(b, __dmul_rn(a, r)), den)};
+  // r underflowed (d == 0): divide b and a by c first
+  return {__ddiv_rn(__dadd_rn(a, __dmul_rn(d, __ddiv_rn(b, c))), den),
+          __ddiv_rn(__dsub_rn(b, __dmul_rn(d, __ddiv_rn(a, c))), den)};
+}
+
 __device__ __forceinline__ void edge_setup(const double* tau6, cplx z, EdgeSet& E) {
   cplx tz[3];
   double phi[3], psi[3];
@@ -193,12 +229,11 @@ __device__ __forceinline__ void edge_setup(const double* tau6, cplx z, EdgeSet& 
   for (int j = 0; j < 3; ++j) {
     const int q = (j + 1) % 3;
     const cplx tj = mk(tau6[2 * j], tau6[2 * j + 1]), tq = mk(tau6[2 * q], tau6[2 * q + 1]);
-    tz[j] = tj - z;
-    const cplx dt = tq - tj;
-    // dt / conj(dt) = dt^2 / |dt|^2
-    const double n2 = dt.re * dt.re + dt.im * dt.im;
-    const cplx nt2 = (1.0 / n2) * (dt * dt);
-    E.d[j] = 0.5 * (tz[j] - nt2 * conj(tz[j]));
+    tz[j] = mk(__dsub_rn(tj.re, z.re), __dsub_rn(tj.im, z.im));
+    const cplx dt = mk(__dsub_rn(tq.re, tj.re), __dsub_rn(tq.im, tj.im));
+    const cplx nt2 = div_smith(dt, conj(dt));
+    const cplx pr = mul_rn(nt2, conj(tz[j]));
+    E.d[j] = mk(__dmul_rn(0.5, __dsub_rn(tz[j].re, pr.re)), __dmul_rn(0.5, __dsub_rn(tz[j].im, pr.im)));
   }
   E.span = 0.0;
 #pragma unroll

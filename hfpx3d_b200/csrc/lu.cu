@@ -28,7 +28,7 @@ namespace hfpx {
 
 constexpr int kNb = 256;
 constexpr int kBaseW = 32;
-constexpr int kPanelThreads = 512;
+constexpr int kPanelThreads = 256;
 
 // ------------------------------------------------------ panel base kernel
 template <class T>
@@ -56,77 +56,96 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
   for (int c = 0; c < w; ++c)
     for (int i = tid; i < nrow; i += kPanelThreads) chunk[(size_t)c * rpc + i] = A[(r0 + i) + lda * c];
   __syncthreads();
-  for (int j = 0; j < w; ++j) {
-    const int buf = j & 1;
-    // local arg-max of |a(i,j)| over owned rows i >= j (first index on ties)
-    double best = -1.0;
-    int bidx = INT32_MAX;
-    for (int i = tid; i < nrow; i += kPanelThreads) {
-      if (r0 + i < j) continue;
-      const double v = fabs((double)chunk[(size_t)j * rpc + i]);
-      if (v > best) { best = v; bidx = (int)(r0 + i); }
-    }
+  const int lane = tid & 31, warp = tid >> 5;
+  // (max, first index) pair reduction within a warp
+  auto warp_argmax = [&](double& best, int& bidx) {
     for (int o = 16; o > 0; o >>= 1) {
       const double ov = __shfl_down_sync(0xffffffffu, best, o);
       const int oi = __shfl_down_sync(0xffffffffu, bidx, o);
       if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
     }
-    if ((tid & 31) == 0) { rmax[tid >> 5] = best; ridx[tid >> 5] = bidx; }
-    __syncthreads();
-    if (tid == 0) {
-      for (int q = 1; q < kPanelThreads / 32; ++q)
-        if (rmax[q] > best || (rmax[q] == best && ridx[q] < bidx)) { best = rmax[q]; bidx = ridx[q]; }
-      sc.cmax[buf * G + b] = best;
-      sc.cidx[buf * G + b] = bidx;
-      s_p = bidx;
-    }
-    __syncthreads();
-    const int li = s_p - (int)r0;
-    if (li >= 0 && li < nrow && tid < w) sc.cand[((size_t)buf * G + b) * kBaseW + tid] = chunk[(size_t)tid * rpc + li];
+  };
+  // thread-local arg-max of |a(i,0)|
+  double best = -1.0;
+  int bidx = INT32_MAX;
+  for (int i = tid; i < nrow; i += kPanelThreads) {
+    const double v = fabs((double)chunk[i]);
+    if (v > best) { best = v; bidx = (int)(r0 + i); }
+  }
+  for (int j = 0; j < w; ++j) {
+    const int buf = j & 1;
     const int lj = j - (int)r0;
-    if (lj >= 0 && lj < nrow && tid < w) sc.rowj[buf * kBaseW + tid] = chunk[(size_t)tid * rpc + lj];
+    // CTA arg-max of |a(i,j)|, i >= j (first index on ties); warp 0 publishes
+    // it with the candidate row and, in the owner of row j, the old row j
+    warp_argmax(best, bidx);
+    if (lane == 0) { rmax[warp] = best; ridx[warp] = bidx; }
+    __syncthreads();
+    if (warp == 0) {
+      best = lane < kPanelThreads / 32 ? rmax[lane] : -1.0;
+      bidx = lane < kPanelThreads / 32 ? ridx[lane] : INT32_MAX;
+      warp_argmax(best, bidx);
+      best = __shfl_sync(0xffffffffu, best, 0);
+      bidx = __shfl_sync(0xffffffffu, bidx, 0);
+      if (lane == 0) { sc.cmax[buf * G + b] = best; sc.cidx[buf * G + b] = bidx; }
+      const int li = bidx - (int)r0;
+      if (li >= 0 && li < nrow && lane < w) sc.cand[((size_t)buf * G + b) * kBaseW + lane] = chunk[(size_t)lane * rpc + li];
+      if (lj >= 0 && lj < nrow && lane < w) sc.rowj[buf * kBaseW + lane] = chunk[(size_t)lane * rpc + lj];
+    }
     grid.sync();
-    // global pivot, identical in every CTA
-    if (tid == 0) {
+    // global pivot, identical in every CTA (warp 0 scans the CTAs' candidates)
+    if (warp == 0) {
       double gb = -1.0;
       int gi = INT32_MAX, gw = 0;
-      for (int q = 0; q < G; ++q) {
+      for (int q = lane; q < G; q += 32) {
         const double v = sc.cmax[buf * G + q];
         const int ix = sc.cidx[buf * G + q];
         if (v > gb || (v == gb && ix < gi)) { gb = v; gi = ix; gw = q; }
       }
-      s_p = gi;
-      rmax[0] = gb;
-      ridx[0] = gw;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, gb, o);
+        const int oi = __shfl_down_sync(0xffffffffu, gi, o);
+        const int ow = __shfl_down_sync(0xffffffffu, gw, o);
+        if (ov > gb || (ov == gb && oi < gi)) { gb = ov; gi = oi; gw = ow; }
+      }
+      if (lane == 0) { s_p = gi; rmax[0] = gb; ridx[0] = gw; }
     }
     __syncthreads();
     const int p = s_p, win = ridx[0];
-    if (tid < w) prow[tid] = sc.cand[((size_t)buf * G + win) * kBaseW + tid];
+    if (tid < w) {
+      const T pr = sc.cand[((size_t)buf * G + win) * kBaseW + tid];
+      prow[tid] = pr;
+      if (p != j) {  // swap rows j and p
+        const int lp = p - (int)r0;
+        if (lp >= 0 && lp < nrow) chunk[(size_t)tid * rpc + lp] = sc.rowj[buf * kBaseW + tid];
+        if (lj >= 0 && lj < nrow) chunk[(size_t)tid * rpc + lj] = pr;
+      }
+    }
     if (b == 0 && tid == 0) {
       piv[j] = p;
       if (rmax[0] == 0.0 && info && *info == 0) *info = col_offset + j + 1;
     }
     __syncthreads();
-    // swap rows j and p
-    if (p != j) {
-      const int lp = p - (int)r0;
-      if (lp >= 0 && lp < nrow && tid < w) chunk[(size_t)tid * rpc + lp] = sc.rowj[buf * kBaseW + tid];
-      if (lj >= 0 && lj < nrow && tid < w) chunk[(size_t)tid * rpc + lj] = prow[tid];
-    }
-    __syncthreads();
-    // scale column j and rank-1 update of columns j+1..w-1, rows i > j
+    // scale column j and rank-1 update of columns j+1..w-1 for rows i > j,
+    // tracking the arg-max of the updated column j+1 for the next step
+    best = -1.0;
+    bidx = INT32_MAX;
     const T pv = prow[j];
-    if (pv != (T)0) {
-      const T inv = (T)1 / pv;
-      for (int i = tid; i < nrow; i += kPanelThreads) {
-        if (r0 + i <= j) continue;
-        const T l = chunk[(size_t)j * rpc + i] * inv;
+    const T inv = pv != (T)0 ? (T)1 / pv : (T)0;
+    for (int i = tid; i < nrow; i += kPanelThreads) {
+      if (r0 + i <= j) continue;
+      T l = chunk[(size_t)j * rpc + i];
+      if (pv != (T)0) {
+        l *= inv;
         chunk[(size_t)j * rpc + i] = l;
         for (int c = j + 1; c < w; ++c) chunk[(size_t)c * rpc + i] -= l * prow[c];
       }
+      if (j + 1 < w) {
+        const double v = fabs((double)chunk[(size_t)(j + 1) * rpc + i]);
+        if (v > best) { best = v; bidx = (int)(r0 + i); }
+      }
     }
-    __syncthreads();
   }
+  __syncthreads();
   for (int c = 0; c < w; ++c)
     for (int i = tid; i < nrow; i += kPanelThreads) A[(r0 + i) + lda * c] = chunk[(size_t)c * rpc + i];
 }
@@ -267,6 +286,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       trsm_llu(c, kb, n - k - kb, Akk, lda, Akk + lda * kb, lda);
       gemm_sub(c, n - k - kb, n - k - kb, kb, Akk + kb, lda, Akk + lda * kb, lda, Akk + kb + lda * kb, lda);
     }
+    rc = check_cuda(c, cudaGetLastError(), "LU step launch");
   }
   int64_t info = 0;
   if (!rc) {
