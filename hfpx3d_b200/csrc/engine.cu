@@ -375,6 +375,13 @@ int hfpx_lu_solve_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t
 
 int64_t hfpx_ctx_launch_count(const hfpx_ctx* c) { return c ? (int64_t)g_launches.load() : -1; }
 
+int hfpx_lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
+                                 int64_t* info) {
+  if (!c) return HFPX_ERR_ARG;
+  cudaSetDevice(c->device);
+  return lu_panel_factor_noalloc(c, d_a, lda, m, w, d_piv, info);
+}
+
 int hfpx_stress(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, int is_dd_local, const double* dd,
                 const double* pts, int64_t n_pts, const double* s_inf, double* out) {
   if (!c) return HFPX_ERR_ARG;

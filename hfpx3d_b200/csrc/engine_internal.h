@@ -62,4 +62,6 @@ int lu_solve_fp64(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, 
 int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, int64_t ldb);
 int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb,
                  double tol, int max_iter, hfpx_solve_info* info);
+int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
+                            int64_t* info);
 }  // namespace hfpx

@@ -475,4 +475,74 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
   return rc;
 }
 
+// ------------------------------------------------- allocation-free panel LU
+// For callers that cannot allocate device memory: code running while a CUDA
+// stream is being captured into a graph (cudaMalloc is illegal there), hosts
+// whose device memory belongs to an arena or pool they manage themselves, and
+// embedded or real-time callers that forbid allocation after start-up.  The
+// pivot search scratch of the panel kernel lives in this file-scope array
+// instead of in cudaMalloc'd buffers.  Every GPU that loads the library holds
+// it until the process exits; all calls share it, so calls that overlap on the
+// GPU (other streams, other host threads) race and must be serialised by the
+// caller.
+constexpr int kNoAllocMaxCtas = 256;
+constexpr size_t kNoAllocCand = sizeof(double) * 2 * kNoAllocMaxCtas * kBaseW;
+constexpr size_t kNoAllocCmax = sizeof(double) * 2 * kNoAllocMaxCtas;
+constexpr size_t kNoAllocCidx = sizeof(int) * 2 * kNoAllocMaxCtas;
+constexpr size_t kNoAllocRowj = sizeof(double) * 2 * kBaseW;
+constexpr size_t kNoAllocBytes = kNoAllocCand + kNoAllocCmax + kNoAllocCidx + kNoAllocRowj + sizeof(int64_t);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of the array, looked up once per device with that device
+// current.  In host code the symbol's name is a host-side stand-in, not a
+// device address, so only the looked-up pointer is passed to kernels.
+static unsigned char* noalloc_scratch(hfpx_ctx* c) {
+  static unsigned char* addr[64] = {nullptr};
+  if (c->device < 0 || c->device >= 64) return nullptr;
+  if (!addr[c->device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+    if (cudaFuncSetAttribute(panel_base_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+        cudaSuccess)
+      return nullptr;
+    addr[c->device] = static_cast<unsigned char*>(p);
+  }
+  return addr[c->device];
+}
+
+int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
+                            int64_t* info) {
+  if (!d_a || !d_piv || !info) return set_error(c, HFPX_ERR_ARG, "null argument");
+  if (w < 1 || w > kBaseW) return set_error(c, HFPX_ERR_ARG, "panel width must be 1..32 columns");
+  if (m < w || lda < m) return set_error(c, HFPX_ERR_ARG, "need m >= w and lda >= m");
+  const int G = (int)std::min<int64_t>(std::min<int64_t>(c->num_sms, kNoAllocMaxCtas), std::max<int64_t>(1, (m + 31) / 32));
+  const int rpc = (int)((m + G - 1) / G);
+  const size_t smem = (size_t)w * rpc * sizeof(double) + kBaseW * sizeof(double);
+  if (smem > 200 * 1024)
+    return set_error(c, HFPX_ERR_ARG, "panel too tall: at most " + std::to_string((long long)G * (200 * 1024 / 8 - kBaseW) / w) +
+                                          " rows for this width on this GPU");
+  unsigned char* base = noalloc_scratch(c);
+  if (!base) return set_error(c, HFPX_ERR_CUDA, "cannot resolve the device address of the scratch array");
+  PanelScratch<double> sc;
+  sc.cand = reinterpret_cast<double*>(base);
+  sc.cmax = reinterpret_cast<double*>(base + kNoAllocCand);
+  sc.cidx = reinterpret_cast<int*>(base + kNoAllocCand + kNoAllocCmax);
+  sc.rowj = reinterpret_cast<double*>(base + kNoAllocCand + kNoAllocCmax + kNoAllocCidx);
+  int64_t* d_info = reinterpret_cast<int64_t*>(base + kNoAllocCand + kNoAllocCmax + kNoAllocCidx + kNoAllocRowj);
+  // the array keeps the previous call's contents: the zero-pivot word starts at 0
+  int rc = check_cuda(c, cudaMemsetAsync(d_info, 0, sizeof(int64_t), c->stream), "clear info");
+  int64_t col_offset = 0;
+  void* args[] = {&d_a, &lda, &m, &w, const_cast<int*>(&rpc), &d_piv, &sc, &d_info, &col_offset};
+  if (!rc) {
+    ++g_launches;
+    rc = check_cuda(c, cudaLaunchCooperativeKernel((void*)panel_base_kernel<double>, dim3(G), dim3(kPanelThreads), args,
+                                                   smem, c->stream),
+                    "panel launch");
+  }
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(info, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream), "info");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "panel factorisation");
+  if (!rc && *info != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "zero pivot at column " + std::to_string(*info));
+  return rc;
+}
+
 }  // namespace hfpx

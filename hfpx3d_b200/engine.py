@@ -64,6 +64,7 @@ SIGNATURES = {
     'hfpx_lu_solve': (_int, [_V, _V, _D, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_lu_solve_device': (_int, [_V, _V, _V, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
+    'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
     'hfpx_local_submatrix': (_int, [_V, _f64, _f64, _f64, _f64, _f64, _D, _D, _D]),
     'hfpx_element_frame': (_int, [_D, _D, _D, _D]),

@@ -115,6 +115,23 @@ int hfpx_lu_solve(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *b, int64_t n
 int hfpx_lu_solve_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, int64_t nrhs,
                          int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
 
+/* Partial-pivoting LU of one tall panel already in device memory, in place,
+ * without allocating anything: no counterpart in the reference.  For callers
+ * that cannot call cudaMalloc (inside a stream capture, under a
+ * caller-managed memory arena, or in allocation-free real-time code).
+ * d_a: m x w column-major (lda >= m, 1 <= w <= 32, m >= w), overwritten with
+ * L (unit lower, below the diagonal) and U; d_piv: w int32 pivot rows
+ * (0-based, relative to the panel's first row, applied in order as LAPACK
+ * dgetf2's ipiv); info (host): 0, or the 1-based column of the first zero
+ * pivot (HFPX_ERR_SINGULAR).  Taller panels than the shared memory of all SMs
+ * can hold (about 118000 rows at w = 32 on a B200) are rejected with
+ * HFPX_ERR_ARG.  Its pivot-search scratch is one static device array of
+ * about 138 KB shared by every call: the first call on a device looks up its
+ * address (make that call before any stream capture), and calls that overlap
+ * on the GPU race. */
+int hfpx_lu_panel_factor_noalloc(hfpx_ctx *ctx, double *d_a, int64_t lda, int64_t m, int w,
+                                 int32_t *d_piv, int64_t *info);
+
 /* Number of this engine's own kernels launched on the context so far
  * (library kernels such as cuBLAS are not counted). */
 int64_t hfpx_ctx_launch_count(const hfpx_ctx *ctx);

@@ -1,0 +1,102 @@
+"""The allocation-free panel LU (hfpx_lu_panel_factor_noalloc) through the C-ABI.
+
+It is for callers that cannot allocate device memory: code running while a
+stream is captured into a CUDA graph, hosts that hand all device memory to
+their own arena, allocation-free real-time loops.  The caller passes device
+buffers (made here with torch); the entry point itself allocates nothing and
+keeps its pivot-search scratch in one static device array.  Its results are
+checked against the existing entry point (hfpx_lu_factor), within the
+tolerance the other LU tests use, on two calls in a row."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def factor_existing(ctx, A):
+    from hfpx3d_b200 import engine
+    m = engine.DeviceMatrix.upload(ctx, A)
+    info = ctypes.c_int64()
+    ctx.check(engine.lib().hfpx_lu_factor(ctx.h, m.h, engine.HFPX_LU_FP64, ctypes.byref(info)))
+    return m.download(), m
+
+
+def factor_noalloc(ctx, A):
+    import torch
+    from hfpx3d_b200 import engine
+    m, w = A.shape
+    # a (w, m) row-major tensor is the (m, w) column-major panel, lda = m
+    d = torch.from_numpy(np.ascontiguousarray(A.T)).to('cuda:0')
+    piv = torch.full((w,), -7, dtype=torch.int32, device='cuda:0')
+    info = ctypes.c_int64(-1)
+    torch.cuda.synchronize()
+    rc = engine.lib().hfpx_lu_panel_factor_noalloc(ctx.h, ctypes.c_void_p(d.data_ptr()), m, m, w,
+                                                   ctypes.c_void_p(piv.data_ptr()), ctypes.byref(info))
+    torch.cuda.synchronize()
+    return rc, d.cpu().numpy().T.copy(), piv.cpu().numpy(), info.value
+
+
+def apply_pivots(A, piv):
+    P = A.copy()
+    for i, p in enumerate(piv):
+        P[[i, p]] = P[[p, i]]
+    return P
+
+
+@pytest.mark.parametrize('n', [5, 17, 32])
+def test_matches_existing_entry_point_on_two_calls(ctx, n):
+    from hfpx3d_b200 import engine
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n))
+    F_ref, m = factor_existing(ctx, A)
+    b = rng.standard_normal(n)
+    x_ref = engine.LU.solve(type('L', (), {'ctx': ctx, 'matrix': m, 'mode': 0})(), b)
+    for _ in range(2):
+        rc, F, piv, info = factor_noalloc(ctx, A)
+        assert rc == engine.HFPX_OK and info == 0
+        assert np.abs(F - F_ref).max() <= 1e-12 * np.abs(F_ref).max()
+        L = np.tril(F, -1) + np.eye(n)
+        U = np.triu(F)
+        y = np.linalg.solve(L, apply_pivots(b[:, None], piv)[:, 0])
+        x = np.linalg.solve(U, y)
+        assert np.abs(x - x_ref).max() <= 1e-10 * np.abs(x_ref).max()
+
+
+def test_tall_panel_two_calls(ctx):
+    from hfpx3d_b200 import engine
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((6000, 32))
+    out = [factor_noalloc(ctx, A) for _ in range(2)]
+    for rc, F, piv, info in out:
+        assert rc == engine.HFPX_OK and info == 0
+        L = np.tril(F, -1)
+        L[:32] += np.eye(32)
+        U = np.triu(F[:32])
+        assert np.abs(L @ U - apply_pivots(A, piv)).max() <= 1e-12 * np.abs(A).max()
+        assert np.abs(L).max() <= 1.0 + 1e-15     # partial pivoting bound
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+
+
+def test_rejects_sizes_beyond_the_limit(ctx):
+    import torch
+    from hfpx3d_b200 import engine
+    d = torch.zeros(64, dtype=torch.float64, device='cuda:0')
+    piv = torch.zeros(64, dtype=torch.int32, device='cuda:0')
+    info = ctypes.c_int64()
+    L = engine.lib()
+    for m, w in ((64, 33), (10, 32), (1_000_000, 32)):
+        rc = L.hfpx_lu_panel_factor_noalloc(ctx.h, ctypes.c_void_p(d.data_ptr()), m, m, w,
+                                            ctypes.c_void_p(piv.data_ptr()), ctypes.byref(info))
+        assert rc == engine.HFPX_ERR_ARG, (m, w)
+
+
+def test_zero_pivot_reported(ctx):
+    from hfpx3d_b200 import engine
+    A = np.random.default_rng(4).standard_normal((300, 12))
+    A[:, 7] = 0.0
+    rc, F, piv, info = factor_noalloc(ctx, A)
+    assert rc == engine.HFPX_ERR_SINGULAR and info == 8
+    rc, F, piv, info = factor_noalloc(ctx, np.eye(40, 20))   # scratch reused: info cleared again
+    assert rc == engine.HFPX_OK and info == 0
