@@ -74,6 +74,18 @@ int hfpx_ctx_create(int device, hfpx_ctx** out) {
       c->cublas = h;
     }
   }
+  if (!rc) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    rc = check_cuda(c, cudaStreamCreateWithPriority(&c->stream_panel, cudaStreamNonBlocking, hi), "panel stream");
+    if (!rc) rc = check_cuda(c, cudaStreamCreateWithFlags(&c->stream_left, cudaStreamNonBlocking), "swap stream");
+    cublasHandle_t h = nullptr;
+    if (!rc && cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) rc = HFPX_ERR_CUDA;
+    if (!rc) {
+      cublasSetStream(h, c->stream_panel);
+      c->cublas_panel = h;
+    }
+  }
   if (rc) {
     hfpx_ctx_destroy(c);
     return rc;
@@ -86,9 +98,14 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   if (!c) return HFPX_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream_panel) cudaStreamSynchronize(c->stream_panel);
+  if (c->stream_left) cudaStreamSynchronize(c->stream_left);
   if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
+  if (c->cublas_panel) cublasDestroy(static_cast<cublasHandle_t>(c->cublas_panel));
   if (c->d_flags) cudaFree(c->d_flags);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream_panel) cudaStreamDestroy(c->stream_panel);
+  if (c->stream_left) cudaStreamDestroy(c->stream_left);
   delete c;
   return HFPX_OK;
 }

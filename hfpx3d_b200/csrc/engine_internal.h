@@ -12,6 +12,10 @@ struct hfpx_ctx {
   int num_sms = 0;
   cudaStream_t stream = nullptr;
   void* cublas = nullptr;          // cublasHandle_t
+  // LU look-ahead: panels on a high-priority stream with their own cuBLAS
+  // handle, deferred left-side row swaps on a third stream
+  cudaStream_t stream_panel = nullptr, stream_left = nullptr;
+  void* cublas_panel = nullptr;
   std::string last_error;
   int* d_flags = nullptr;          // device status words (see kernels)
 };

@@ -19,6 +19,9 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 #include "engine_internal.h"
 
@@ -26,8 +29,19 @@ namespace cg = cooperative_groups;
 
 namespace hfpx {
 
-constexpr int kNb = 256;
 constexpr int kBaseW = 32;
+// Block size of the right-looking LU: each trailing update reads and writes
+// the remaining matrix once, so HBM traffic ~ N^3 / (3 nb) x 8 bytes (FP32);
+// larger blocks move work into the (overlapped) panel.  HFPX_LU_NB overrides
+// the default (multiple of 32 in [64, 1024]).
+static int lu_block_size() {
+  static const int nb = [] {
+    const char* e = std::getenv("HFPX_LU_NB");
+    const int v = e ? std::atoi(e) : 0;
+    return (v >= 64 && v <= 1024 && v % kBaseW == 0) ? v : 768;
+  }();
+  return nb;
+}
 constexpr int kPanelThreads = 256;
 
 // ------------------------------------------------------ panel base kernel
@@ -177,27 +191,83 @@ __global__ void offset_piv_kernel(int32_t* piv, int k, int off) {
 // --------------------------------------------------------------- BLAS glue
 static inline cublasHandle_t H(hfpx_ctx* c) { return static_cast<cublasHandle_t>(c->cublas); }
 
-static void trsm_llu(hfpx_ctx* c, int64_t m, int64_t n, const double* L, int64_t ldl, double* B, int64_t ldb) {
+// A stream with the cuBLAS handle bound to it.
+struct Lane {
+  cudaStream_t s;
+  cublasHandle_t h;
+};
+static Lane main_lane(hfpx_ctx* c) { return {c->stream, H(c)}; }
+static Lane panel_lane(hfpx_ctx* c) { return {c->stream_panel, static_cast<cublasHandle_t>(c->cublas_panel)}; }
+
+static void trsm_llu(Lane l, int64_t m, int64_t n, const double* L, int64_t ldl, double* B, int64_t ldb) {
+  if (m <= 0 || n <= 0) return;
   const double one = 1.0;
-  cublasDtrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
+  cublasDtrsm(l.h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
               L, (int)ldl, B, (int)ldb);
 }
-static void trsm_llu(hfpx_ctx* c, int64_t m, int64_t n, const float* L, int64_t ldl, float* B, int64_t ldb) {
+static void trsm_llu(Lane l, int64_t m, int64_t n, const float* L, int64_t ldl, float* B, int64_t ldb) {
+  if (m <= 0 || n <= 0) return;
   const float one = 1.0f;
-  cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
+  cublasStrsm(l.h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)m, (int)n, &one,
               L, (int)ldl, B, (int)ldb);
 }
-static void gemm_sub(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
+static void gemm_sub(Lane l, int64_t m, int64_t n, int64_t k, const double* A, int64_t lda, const double* B,
                      int64_t ldb, double* C, int64_t ldc) {
+  if (m <= 0 || n <= 0 || k <= 0) return;
   const double mone = -1.0, one = 1.0;
-  cublasDgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
+  cublasDgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
               (int)ldc);
 }
-static void gemm_sub(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const float* A, int64_t lda, const float* B,
+static void gemm_sub(Lane l, int64_t m, int64_t n, int64_t k, const float* A, int64_t lda, const float* B,
                      int64_t ldb, float* C, int64_t ldc) {
+  if (m <= 0 || n <= 0 || k <= 0) return;
   const float mone = -1.0f, one = 1.0f;
-  cublasSgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
+  cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
               (int)ldc);
+}
+
+// ------------------------------------------------------------- profiling
+// HFPX_PROFILE=1 in the environment: every LU phase is synchronised and
+// timed on the host, and a per-phase summary goes to stderr after each
+// factorisation / solve.  Off by default (no synchronisation, no cost).
+struct PhaseProfile {
+  bool on = false;
+  double t[8] = {0};
+  int n[8] = {0};
+  const char* name[8] = {"panel", "laswp", "trsm", "gemm", "convert", "trsv", "residual", "other"};
+  std::chrono::steady_clock::time_point t0;
+  cudaStream_t s = nullptr;
+  void begin(cudaStream_t st) {
+    if (!on) return;
+    s = st;
+    cudaDeviceSynchronize();
+    t0 = std::chrono::steady_clock::now();
+  }
+  void end(int k) {
+    if (!on) return;
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    t[k] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    n[k] += 1;
+    t0 = t1;
+  }
+  void report(const char* what) {
+    if (!on) return;
+    std::fprintf(stderr, "[hfpx profile] %s:", what);
+    for (int k = 0; k < 8; ++k)
+      if (n[k]) std::fprintf(stderr, " %s %.1f ms (%d)", name[k], t[k], n[k]);
+    std::fprintf(stderr, "\n");
+    for (int k = 0; k < 8; ++k) { t[k] = 0; n[k] = 0; }
+  }
+};
+static PhaseProfile& prof() {
+  static PhaseProfile p = [] {
+    PhaseProfile q;
+    const char* e = std::getenv("HFPX_PROFILE");
+    q.on = e && *e == '1';
+    return q;
+  }();
+  return p;
 }
 
 // --------------------------------------------------------------- driver
@@ -208,52 +278,91 @@ struct LuWork {
   int grid = 0;
 };
 
+// CTAs for a panel of m rows: enough for the panel to fit in shared memory,
+// at least kPanelCtas when there are rows for them, never more than the SMs.
+// Fewer CTAs than SMs leave room for the trailing update running beside it
+// and make the per-column grid barrier cheaper.
+constexpr int kPanelCtas = 48;
+constexpr size_t kPanelSmemCap = 200 * 1024;
+
 template <class T>
-static int panel_base(hfpx_ctx* c, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
+static int panel_ctas(hfpx_ctx* c, int64_t m, int w) {
+  const int64_t per_cta_rows = (int64_t)((kPanelSmemCap - kBaseW * sizeof(T)) / (w * sizeof(T)));
+  const int64_t need = (m + per_cta_rows - 1) / per_cta_rows;
+  const int64_t want = std::min<int64_t>(kPanelCtas, std::max<int64_t>(1, (m + 31) / 32));
+  return (int)std::min<int64_t>(c->num_sms, std::max(need, want));
+}
+
+template <class T>
+static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
                       int64_t col_offset) {
-  int G = std::min<int64_t>(c->num_sms, std::max<int64_t>(1, (m + 31) / 32));
+  int G = panel_ctas<T>(c, m, w);
   int rpc = (int)((m + G - 1) / G);
   size_t smem = (size_t)w * rpc * sizeof(T) + kBaseW * sizeof(T);
-  if (smem > 200 * 1024) return set_error(c, HFPX_ERR_ARG, "panel too tall for shared memory");
+  if (smem > kPanelSmemCap) return set_error(c, HFPX_ERR_ARG, "panel too tall for shared memory");
   static bool attr_d = false, attr_f = false;
   bool& attr = sizeof(T) == 8 ? attr_d : attr_f;
   if (!attr) {
-    cudaFuncSetAttribute(panel_base_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(panel_base_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemCap);
     attr = true;
   }
   void* args[] = {&A, &lda, &m, &w, &rpc, &piv, &wk.sc, &wk.d_info, &col_offset};
   ++g_launches;
-  cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_base_kernel<T>, dim3(G), dim3(kPanelThreads), args, smem,
-                                              c->stream);
+  cudaError_t e =
+      cudaLaunchCooperativeKernel((void*)panel_base_kernel<T>, dim3(G), dim3(kPanelThreads), args, smem, l.s);
   return check_cuda(c, e, "panel_base_kernel launch");
 }
 
 template <class T>
-static void laswp(hfpx_ctx* c, T* A, int64_t lda, int64_t ncols, const int32_t* piv, int k, int base) {
+static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, const int32_t* piv, int k, int base) {
   if (ncols <= 0 || k <= 0) return;
   ++g_launches;
-  laswp_kernel<T><<<(unsigned)((ncols + 127) / 128), 128, 0, c->stream>>>(A, lda, ncols, piv, k, base);
+  laswp_kernel<T><<<(unsigned)((ncols + 127) / 128), 128, 0, l.s>>>(A, lda, ncols, piv, k, base);
 }
 
 // dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
 template <class T>
-static int panel_rec(hfpx_ctx* c, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
+static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
                      int64_t col_offset) {
-  if (w <= kBaseW) return panel_base(c, wk, A, lda, m, w, piv, col_offset);
+  PhaseProfile& P = prof();
+  if (w <= kBaseW) {
+    P.begin(l.s);
+    const int rc = panel_base(c, l, wk, A, lda, m, w, piv, col_offset);
+    P.end(0);
+    return rc;
+  }
   const int w1 = w / 2, w2 = w - w1;
-  int rc = panel_rec(c, wk, A, lda, m, w1, piv, col_offset);
+  int rc = panel_rec(c, l, wk, A, lda, m, w1, piv, col_offset);
   if (rc) return rc;
-  laswp(c, A + lda * w1, lda, w2, piv, w1, 0);
-  trsm_llu(c, w1, w2, A, lda, A + lda * w1, lda);
-  gemm_sub(c, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
-  rc = panel_rec(c, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1);
+  P.begin(l.s);
+  laswp(l, A + lda * w1, lda, w2, piv, w1, 0);
+  P.end(1);
+  trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
+  P.end(2);
+  gemm_sub(l, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
+  P.end(3);
+  rc = panel_rec(c, l, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1);
   if (rc) return rc;
+  P.begin(l.s);
   ++g_launches;
-  offset_piv_kernel<<<(w2 + 127) / 128, 128, 0, c->stream>>>(piv + w1, w2, w1);
-  laswp(c, A + w1, lda, w1, piv + w1, w2, w1);
+  offset_piv_kernel<<<(w2 + 127) / 128, 128, 0, l.s>>>(piv + w1, w2, w1);
+  laswp(l, A + w1, lda, w1, piv + w1, w2, w1);
+  P.end(1);
   return 0;
 }
 
+// Pivots of block b are relative to the block's first row until the end.
+__global__ void globalise_piv_kernel(int32_t* piv, int64_t n, int nb) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) piv[i] += (int32_t)((i / nb) * nb);
+}
+
+// Right-looking blocked LU with depth-1 look-ahead.  Step k on the main
+// stream: swaps of panel k on the columns to its right, U12 = L11^-1 A12, the
+// update of the next block column only, then (while the panel stream
+// factors that next block column) the update of everything right of it.
+// Swaps on the columns left of each panel wait for the step that last read
+// those columns and run on a third stream.
 template <class T>
 static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, int64_t* info_out) {
   LuWork<T> wk;
@@ -272,35 +381,86 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   wk.d_info = (int64_t*)alloc(sizeof(int64_t));
   int rc = 0;
   if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info) rc = set_error(c, HFPX_ERR_NOMEM, "LU scratch");
-  if (!rc) cudaMemsetAsync(wk.d_info, 0, sizeof(int64_t), c->stream);
+  const Lane M = main_lane(c), Pn = panel_lane(c);
+  const cudaStream_t S = c->stream_left;
+  const int kNb = lu_block_size();
+  cudaEvent_t ev_panel = nullptr, ev_next = nullptr, ev_rest = nullptr, ev_left = nullptr, ev_start = nullptr;
+  for (cudaEvent_t* e : {&ev_panel, &ev_next, &ev_rest, &ev_left, &ev_start})
+    if (!rc) rc = check_cuda(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "LU events");
+  PhaseProfile& P = prof();
+  if (!rc) {
+    cudaMemsetAsync(wk.d_info, 0, sizeof(int64_t), c->stream);
+    // the panel and swap streams start after everything queued on the main stream
+    cudaEventRecord(ev_start, M.s);
+    cudaStreamWaitEvent(Pn.s, ev_start, 0);
+    cudaStreamWaitEvent(S, ev_start, 0);
+    const int kb0 = (int)std::min<int64_t>(kNb, n);
+    rc = panel_rec(c, Pn, wk, A, lda, n, kb0, piv, 0);
+    cudaEventRecord(ev_panel, Pn.s);
+  }
   for (int64_t k = 0; k < n && !rc; k += kNb) {
     const int kb = (int)std::min<int64_t>(kNb, n - k);
     T* Akk = A + k + lda * k;
-    rc = panel_rec(c, wk, Akk, lda, n - k, kb, piv + k, k);
-    if (rc) break;
-    laswp(c, A + k, lda, k, piv + k, kb, 0);                                   // left columns
-    laswp(c, A + k + lda * (k + kb), lda, n - k - kb, piv + k, kb, 0);          // right columns
-    ++g_launches;
-    offset_piv_kernel<<<(kb + 127) / 128, 128, 0, c->stream>>>(piv + k, kb, (int)k);
+    cudaStreamWaitEvent(M.s, ev_panel, 0);
+    // left swaps of panel k, after the step that read those columns last
+    cudaStreamWaitEvent(S, ev_panel, 0);
+    if (k > 0) cudaStreamWaitEvent(S, ev_rest, 0);
+    laswp(Lane{S, nullptr}, A + k, lda, k, piv + k, kb, 0);
+    P.begin(M.s);
+    laswp(M, A + k + lda * (k + kb), lda, n - k - kb, piv + k, kb, 0);
+    P.end(1);
     if (k + kb < n) {
-      trsm_llu(c, kb, n - k - kb, Akk, lda, Akk + lda * kb, lda);
-      gemm_sub(c, n - k - kb, n - k - kb, kb, Akk + kb, lda, Akk + lda * kb, lda, Akk + kb + lda * kb, lda);
+      const int64_t rest = n - k - kb;
+      const int kn = (int)std::min<int64_t>(kNb, rest);
+      trsm_llu(M, kb, rest, Akk, lda, Akk + lda * kb, lda);
+      P.end(2);
+      gemm_sub(M, rest, kn, kb, Akk + kb, lda, Akk + lda * kb, lda, Akk + kb + lda * kb, lda);
+      P.end(3);
+      cudaEventRecord(ev_next, M.s);
+      cudaStreamWaitEvent(Pn.s, ev_next, 0);
+      rc = panel_rec(c, Pn, wk, Akk + kb + lda * kb, lda, rest, kn, piv + k + kb, k + kb);
+      cudaEventRecord(ev_panel, Pn.s);
+      if (rc) break;
+      P.begin(M.s);
+      gemm_sub(M, rest, rest - kn, kb, Akk + kb, lda, Akk + lda * (kb + kn), lda, Akk + kb + lda * (kb + kn), lda);
+      P.end(3);
+      cudaEventRecord(ev_rest, M.s);
     }
-    rc = check_cuda(c, cudaGetLastError(), "LU step launch");
+    if (!rc) rc = check_cuda(c, cudaGetLastError(), "LU step launch");
   }
+  if (ev_left) {
+    cudaEventRecord(ev_left, S);
+    cudaStreamWaitEvent(M.s, ev_left, 0);
+    cudaEventRecord(ev_panel, Pn.s);
+    cudaStreamWaitEvent(M.s, ev_panel, 0);
+  }
+  if (!rc) {
+    ++g_launches;
+    globalise_piv_kernel<<<(unsigned)((n + 255) / 256), 256, 0, M.s>>>(piv, n, kNb);
+  }
+  P.report(sizeof(T) == 8 ? "LU fp64" : "LU fp32");
   int64_t info = 0;
   if (!rc) {
-    rc = check_cuda(c, cudaMemcpyAsync(&info, wk.d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream), "info");
-    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "LU factorisation");
+    rc = check_cuda(c, cudaMemcpyAsync(&info, wk.d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, M.s), "info");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(M.s), "LU factorisation");
   }
+  cudaStreamSynchronize(Pn.s);
+  cudaStreamSynchronize(S);
+  for (cudaEvent_t e : {ev_panel, ev_next, ev_rest, ev_left, ev_start})
+    if (e) cudaEventDestroy(e);
   for (void* p : allocs) cudaFree(p);
   *info_out = info;
   if (!rc && info != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "matrix is singular: zero pivot at column " + std::to_string(info));
   return rc;
 }
 
+static void set_math(hfpx_ctx* c, cublasMath_t mode) {
+  cublasSetMathMode(H(c), mode);
+  cublasSetMathMode(static_cast<cublasHandle_t>(c->cublas_panel), mode);
+}
+
 int lu_factor_fp64(hfpx_ctx* c, hfpx_matrix* m) {
-  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  set_math(c, CUBLAS_DEFAULT_MATH);
   int rc = lu_factor<double>(c, m->d_a, m->ld, m->n, m->d_piv, &m->info);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 1 : 0;
   return rc;
@@ -314,9 +474,9 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
     }
   }
   launch_convert_f32(m->d_a, m->ld, m->n, m->d_f, c->stream);
-  cublasSetMathMode(H(c), CUBLAS_TF32_TENSOR_OP_MATH);
+  set_math(c, CUBLAS_TF32_TENSOR_OP_MATH);
   int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info);
-  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  set_math(c, CUBLAS_DEFAULT_MATH);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
   return rc;
 }
