@@ -164,6 +164,273 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
     for (int i = tid; i < nrow; i += kPanelThreads) A[(r0 + i) + lda * c] = chunk[(size_t)c * rpc + i];
 }
 
+// ------------------------------------------ register-resident FP32 panel
+// Same factorisation as panel_base_kernel<float> (same pivots, same
+// arithmetic per element, so the same bits), restructured for latency:
+//  * each thread keeps kLLRows whole rows of the <= 32-column panel in
+//    registers, so the rank-1 update touches no shared memory;
+//  * the pivot search is exchanged through L2 in "LL" words: 8 bytes holding
+//    4 bytes of data and a 4-byte tag naming the launch and column.  A word
+//    is written and read as one 8-byte access, so a reader that sees the
+//    expected tag holds the data: no grid barrier and no fence.  Every CTA
+//    publishes its arg-max (value, row, the candidate row) and the owner of
+//    row j the old row j; every CTA then polls all of them in one L2 round
+//    trip and picks the same pivot.
+// Words of column j sit in buffer j & 1: a CTA can only write column j + 2
+// after all CTAs published column j + 1, i.e. after all finished reading j.
+// Tags are unique within one factorisation and the buffers are zeroed before
+// it (tag 0 is never used), so stale words never match.  Every poll gives up
+// after kLLTimeoutNs, records the failure and ends the kernel.
+constexpr int kLLThreads = 256;
+constexpr int kLLRows = 6;
+constexpr int kLLCap = kLLThreads * kLLRows;  // panel rows per CTA
+constexpr int kLLSlot = 2 + 2 * kBaseW;       // words per CTA per column
+constexpr int kLLUnits = 8;                   // words each thread polls
+constexpr int kLLMaxCtas = (kLLThreads * kLLUnits - kBaseW) / (2 + kBaseW);
+constexpr unsigned long long kLLTimeoutNs = 200ull * 1000 * 1000;
+
+__device__ __forceinline__ void ll_store(uint64_t* p, uint32_t data, uint32_t tag) {
+  const uint64_t v = ((uint64_t)tag << 32) | data;
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ll_load(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// (max, first index) over the warp, result in every lane
+__device__ __forceinline__ void warp_argmax_all(float& v, int& i) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+  }
+}
+
+// a[k][c] if c == j else keep, by bit masks: a plain "if (c == j) x =
+// a[k][c]" over an unrolled c is folded back into a[k][j] with a run-time j,
+// which moves the whole register array to local memory.
+__device__ __forceinline__ float pick(float x, float cand, bool take) {
+  const int msk = -(int)take;
+  return __int_as_float((__float_as_int(cand) & msk) | (__float_as_int(x) & ~msk));
+}
+
+// Scale column j and update columns j+1..31 of this thread's rows below row
+// j (j in [C0, C0 + 8)); columns below C0 are not touched.  One FMA per
+// element: rows that take no update get multiplier 0 and columns c <= j a
+// zero pivot-row entry, so the FMA leaves them unchanged (up to the sign of
+// a zero); column j is then set by selects over the 8 columns of its group.
+// nxt gets |a(., j+1)| for the next arg-max.
+template <int C0>
+__device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], int g0, int nrow_left, int j, float inv,
+                                          bool nonzero, const float* __restrict__ prow, float (&nxt)[kLLRows]) {
+  float l[kLLRows], lz[kLLRows];
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    const bool below = nonzero && k * kLLThreads < nrow_left && g0 + k * kLLThreads > j;
+    float v = 0.f;
+#pragma unroll
+    for (int c = C0; c < C0 + 8; ++c) v = pick(v, a[k][c], c == j);
+    l[k] = below ? v * inv : v;  // rows not below keep their column-j value
+    lz[k] = below ? l[k] : 0.f;
+  }
+#pragma unroll
+  for (int c = C0; c < kBaseW; ++c) {
+    const float pc = c > j ? prow[c] : 0.f;
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) a[k][c] = fmaf(-lz[k], pc, a[k][c]);
+  }
+#pragma unroll
+  for (int c = C0; c < C0 + 8; ++c) {
+    const bool eq = c == j;
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) a[k][c] = eq ? l[k] : a[k][c];
+  }
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    const bool below = k * kLLThreads < nrow_left && g0 + k * kLLThreads > j;
+    float x = 0.f;
+#pragma unroll
+    for (int c = C0 + 1; c < C0 + 9 && c < kBaseW; ++c) x = pick(x, a[k][c], c == j + 1);
+    nxt[k] = below ? fabsf(x) : -1.f;
+  }
+}
+
+// Row k of this thread's registers to 32 LL words / from shared memory.  The
+// if-chain over compile-time K keeps every register index static.
+template <int K = 0>
+__device__ __forceinline__ void ll_row_store(const float (&a)[kLLRows][kBaseW], int k, uint64_t* dst, int w,
+                                             uint32_t tag) {
+  if (k == K) {
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c)
+      if (c < w) ll_store(dst + c, __float_as_uint(a[K][c]), tag);
+  } else if constexpr (K + 1 < kLLRows) {
+    ll_row_store<K + 1>(a, k, dst, w, tag);
+  }
+}
+template <int K = 0>
+__device__ __forceinline__ void ll_row_load(float (&a)[kLLRows][kBaseW], int k, const float* src) {
+  if (k == K) {
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c) a[K][c] = src[c];
+  } else if constexpr (K + 1 < kLLRows) {
+    ll_row_load<K + 1>(a, k, src);
+  }
+}
+
+__global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
+    float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
+    uint64_t* __restrict__ slots, int64_t* __restrict__ info, int64_t col_offset, uint32_t tag0,
+    int* __restrict__ err) {
+  __shared__ float s_cand[2][kLLMaxCtas][kBaseW];
+  __shared__ float s_rowj[2][kBaseW];
+  __shared__ float s_val[2][kLLMaxCtas];
+  __shared__ int s_idx[2][kLLMaxCtas];
+  __shared__ float s_wv[kLLThreads / 32];
+  __shared__ int s_wi[kLLThreads / 32];
+  __shared__ int s_fail;
+  const int b = blockIdx.x, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t r0 = (int64_t)b * rpc;
+  const int nrow = (int)max((int64_t)0, min((int64_t)rpc, m - r0));
+  const int g0 = (int)r0 + tid;       // panel row of a[0]; a[k] is row g0 + k * kLLThreads
+  const int nrow_left = nrow - tid;   // a[k] holds a row iff k * kLLThreads < nrow_left
+  float a[kLLRows][kBaseW];
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k)
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c)
+      a[k][c] = (k * kLLThreads < nrow_left && c < w) ? A[(int64_t)(g0 + k * kLLThreads) + lda * c] : 0.f;
+  // candidate rows past column w stay zero
+  for (int i = tid; i < 2 * kLLMaxCtas * kBaseW; i += kLLThreads) (&s_cand[0][0][0])[i] = 0.f;
+  if (tid < 2 * kBaseW) (&s_rowj[0][0])[tid] = 0.f;
+  if (tid == 0) s_fail = 0;
+  // words this thread polls: CTA q's (value, row, candidate row) or the old row j
+  const int per = 2 + w, nmain = G * per, units = nmain + w;
+  int off[kLLUnits];
+#pragma unroll
+  for (int u = 0; u < kLLUnits; ++u) {
+    const int x = tid + u * kLLThreads;
+    off[u] = x < nmain ? (x / per) * kLLSlot + x % per : (x < units ? -1 - (x - nmain) : INT32_MIN);
+  }
+  float nxt[kLLRows];
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) nxt[k] = k * kLLThreads < nrow_left ? fabsf(a[k][0]) : -1.f;
+  for (int j = 0; j < w; ++j) {
+    const int buf = j & 1;
+    const uint32_t tag = tag0 + (uint32_t)j + 1u;
+    // CTA arg-max of |a(i, j)|, i >= j, first row on ties
+    float best = -1.f;
+    int bidx = INT32_MAX;
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k)
+      if (nxt[k] > best) { best = nxt[k]; bidx = g0 + k * kLLThreads; }
+    warp_argmax_all(best, bidx);
+    if (lane == 0) { s_wv[warp] = best; s_wi[warp] = bidx; }
+    __syncthreads();
+    best = lane < kLLThreads / 32 ? s_wv[lane] : -1.f;
+    bidx = lane < kLLThreads / 32 ? s_wi[lane] : INT32_MAX;
+    warp_argmax_all(best, bidx);
+    // publish
+    uint64_t* mine = slots + ((size_t)buf * G + b) * kLLSlot;
+    if (tid == 0) {
+      ll_store(mine, __float_as_uint(best), tag);
+      ll_store(mine + 1, (uint32_t)bidx, tag);
+    }
+    {
+      const int dc = bidx - g0, dj = j - g0;
+      if (dc >= 0 && dc % kLLThreads == 0 && dc < nrow_left) ll_row_store(a, dc / kLLThreads, mine + 2, w, tag);
+      if (dj >= 0 && dj % kLLThreads == 0 && dj < nrow_left)
+        ll_row_store(a, dj / kLLThreads, mine + 2 + kBaseW, w, tag);
+    }
+    // poll every CTA's words for this column
+    const uint64_t* xb = slots + (size_t)buf * G * kLLSlot;
+    const int rowj_off = (j / rpc) * kLLSlot + 2 + kBaseW;
+    bool need[kLLUnits];
+#pragma unroll
+    for (int u = 0; u < kLLUnits; ++u) need[u] = off[u] != INT32_MIN;
+    uint64_t t_start = 0;
+    bool failed = false;
+    for (;;) {
+      uint64_t v[kLLUnits];
+#pragma unroll
+      for (int u = 0; u < kLLUnits; ++u)
+        v[u] = need[u] ? ll_load(xb + (off[u] >= 0 ? off[u] : rowj_off + (-1 - off[u]))) : 0;
+      bool pending = false;
+#pragma unroll
+      for (int u = 0; u < kLLUnits; ++u) {
+        if (!need[u]) continue;
+        if ((uint32_t)(v[u] >> 32) != tag) { pending = true; continue; }
+        need[u] = false;
+        const uint32_t d = (uint32_t)v[u];
+        if (off[u] < 0) {
+          s_rowj[buf][-1 - off[u]] = __uint_as_float(d);
+        } else {
+          const int q = off[u] / kLLSlot, o = off[u] - q * kLLSlot;
+          if (o == 0) s_val[buf][q] = __uint_as_float(d);
+          else if (o == 1) s_idx[buf][q] = (int)d;
+          else s_cand[buf][q][o - 2] = __uint_as_float(d);
+        }
+      }
+      if (!pending) break;
+      const uint64_t now = global_ns();
+      if (t_start == 0) t_start = now;
+      else if (now - t_start > kLLTimeoutNs) { failed = true; break; }
+    }
+    if (failed) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      if (tid == 0) atomicExch(err, 1);
+      break;
+    }
+    // global pivot, identical in every warp of every CTA
+    float gv = -1.f;
+    int gix = INT32_MAX, gw = 0;
+    for (int q = lane; q < G; q += 32) {
+      const float vq = s_val[buf][q];
+      const int iq = s_idx[buf][q];
+      if (vq > gv || (vq == gv && iq < gix)) { gv = vq; gix = iq; gw = q; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, gv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, gix, o);
+      const int ow = __shfl_xor_sync(0xffffffffu, gw, o);
+      if (ov > gv || (ov == gv && oi < gix)) { gv = ov; gix = oi; gw = ow; }
+    }
+    const int p = gix;
+    const float* prow = s_cand[buf][gw];
+    if (b == 0 && tid == 0) {
+      piv[j] = p;
+      if (gv == 0.f && info && *info == 0) *info = col_offset + j + 1;
+    }
+    // swap rows j and p
+    if (p != j) {
+      const int dj = j - g0, dp = p - g0;
+      if (dj >= 0 && dj % kLLThreads == 0 && dj < nrow_left) ll_row_load(a, dj / kLLThreads, prow);
+      if (dp >= 0 && dp % kLLThreads == 0 && dp < nrow_left) ll_row_load(a, dp / kLLThreads, s_rowj[buf]);
+    }
+    const float pv = prow[j];
+    const bool nz = pv != 0.f;
+    const float inv = nz ? 1.f / pv : 0.f;
+    if (j < 8) ll_update<0>(a, g0, nrow_left, j, inv, nz, prow, nxt);
+    else if (j < 16) ll_update<8>(a, g0, nrow_left, j, inv, nz, prow, nxt);
+    else if (j < 24) ll_update<16>(a, g0, nrow_left, j, inv, nz, prow, nxt);
+    else ll_update<24>(a, g0, nrow_left, j, inv, nz, prow, nxt);
+  }
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k)
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c)
+      if (k * kLLThreads < nrow_left && c < w) A[(int64_t)(g0 + k * kLLThreads) + lda * c] = a[k][c];
+}
+
 // -------------------------------------------------------------- row swaps
 // Apply interchanges piv[0..k) (rows relative to A's top, piv relative too)
 // to columns [0, ncols) of A; one thread per column, swaps in order.
@@ -276,7 +543,21 @@ struct LuWork {
   PanelScratch<T> sc{};
   int64_t* d_info = nullptr;
   int grid = 0;
+  // register-resident FP32 panel: exchange words [2][kLLMaxCtas][kLLSlot]
+  // (zeroed), failure word, launches so far (names the tags)
+  uint64_t* ll_slots = nullptr;
+  int* ll_err = nullptr;
+  uint32_t ll_launches = 0;
 };
+
+// HFPX_LU_PANEL=smem selects the shared-memory panel kernel for FP32 too.
+static bool ll_panel_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_LU_PANEL");
+    return !(e && std::string(e) == "smem");
+  }();
+  return on;
+}
 
 // CTAs for a panel of m rows: enough for the panel to fit in shared memory,
 // at least kPanelCtas when there are rows for them, never more than the SMs.
@@ -296,6 +577,18 @@ static int panel_ctas(hfpx_ctx* c, int64_t m, int w) {
 template <class T>
 static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
                       int64_t col_offset) {
+  if constexpr (sizeof(T) == 4) {
+    const int64_t g_ll = (m + kLLCap - 1) / kLLCap;
+    if (wk.ll_slots && g_ll <= kLLMaxCtas && ll_panel_enabled()) {
+      int G = (int)g_ll;
+      int rpc = (int)((m + G - 1) / G);
+      uint32_t tag0 = (++wk.ll_launches) << 6;
+      void* args[] = {&A, &lda, &m, &w, &rpc, &piv, &wk.ll_slots, &wk.d_info, &col_offset, &tag0, &wk.ll_err};
+      ++g_launches;
+      return check_cuda(c, cudaLaunchCooperativeKernel((void*)panel_ll_kernel, dim3(G), dim3(kLLThreads), args, 0, l.s),
+                        "panel_ll_kernel launch");
+    }
+  }
   int G = panel_ctas<T>(c, m, w);
   int rpc = (int)((m + G - 1) / G);
   size_t smem = (size_t)w * rpc * sizeof(T) + kBaseW * sizeof(T);
@@ -331,7 +624,9 @@ static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int6
     P.end(0);
     return rc;
   }
-  const int w1 = w / 2, w2 = w - w1;
+  // left half rounded up to whole base panels (768 -> 384 -> 192 -> 96 ->
+  // 64 + 32), so every base panel but a ragged last one is 32 wide
+  const int w1 = (w / 2 + kBaseW - 1) / kBaseW * kBaseW, w2 = w - w1;
   int rc = panel_rec(c, l, wk, A, lda, m, w1, piv, col_offset);
   if (rc) return rc;
   P.begin(l.s);
@@ -379,8 +674,19 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   wk.sc.cidx = (int*)alloc(sizeof(int) * 2 * G);
   wk.sc.rowj = (T*)alloc(sizeof(T) * 2 * kBaseW);
   wk.d_info = (int64_t*)alloc(sizeof(int64_t));
+  const size_t ll_bytes = sizeof(uint64_t) * 2 * kLLMaxCtas * kLLSlot;
+  if (sizeof(T) == 4) {
+    wk.ll_slots = (uint64_t*)alloc(ll_bytes);
+    wk.ll_err = (int*)alloc(sizeof(int));
+  }
   int rc = 0;
-  if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info) rc = set_error(c, HFPX_ERR_NOMEM, "LU scratch");
+  if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info ||
+      (sizeof(T) == 4 && (!wk.ll_slots || !wk.ll_err)))
+    rc = set_error(c, HFPX_ERR_NOMEM, "LU scratch");
+  if (!rc && wk.ll_slots) {
+    cudaMemsetAsync(wk.ll_slots, 0, ll_bytes, c->stream);
+    cudaMemsetAsync(wk.ll_err, 0, sizeof(int), c->stream);
+  }
   const Lane M = main_lane(c), Pn = panel_lane(c);
   const cudaStream_t S = c->stream_left;
   const int kNb = lu_block_size();
@@ -440,12 +746,16 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   }
   P.report(sizeof(T) == 8 ? "LU fp64" : "LU fp32");
   int64_t info = 0;
+  int ll_err = 0;
   if (!rc) {
     rc = check_cuda(c, cudaMemcpyAsync(&info, wk.d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, M.s), "info");
+    if (!rc && wk.ll_err)
+      rc = check_cuda(c, cudaMemcpyAsync(&ll_err, wk.ll_err, sizeof(int), cudaMemcpyDeviceToHost, M.s), "panel status");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(M.s), "LU factorisation");
   }
   cudaStreamSynchronize(Pn.s);
   cudaStreamSynchronize(S);
+  if (!rc && ll_err) rc = set_error(c, HFPX_ERR_CUDA, "panel pivot exchange timed out");
   for (cudaEvent_t e : {ev_panel, ev_next, ev_rest, ev_left, ev_start})
     if (e) cudaEventDestroy(e);
   for (void* p : allocs) cudaFree(p);

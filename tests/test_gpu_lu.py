@@ -85,3 +85,54 @@ def test_solve_before_factor_is_refused(ctx):
     b = np.ones((10, 1), order='F')
     rc = engine.lib().hfpx_lu_solve(ctx.h, m.h, engine._dp(b), 1, 10, 0.0, 0, None)
     assert rc == engine.HFPX_ERR_STATE
+
+
+_PANEL_RUN = r'''
+import sys
+import numpy as np
+from hfpx3d_b200 import engine, meshgen
+ctx = engine.Context(0)
+nods, conn = meshgen.penny(int(sys.argv[1]), seed=3)
+mesh = engine.MeshGeom(nods, conn)
+dof, n = engine.make_dof_h_crack(mesh, 1)
+dm = engine.DeviceMesh(ctx, mesh)
+A = engine.assemble(ctx, dm, dof, n, 1.0, 0.35)
+rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, [0, 0, 1.0, 0, 0, 0])
+lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+x = lu.solve(rhs, tol=1e-12)
+np.save(sys.argv[2], np.concatenate([x, [lu.last_info.iterations, lu.last_info.residual]]))
+'''
+
+
+@pytest.mark.parametrize('n_el', [300, 1200])
+def test_fp32_panel_kernels_agree_bitwise(tmp_path, n_el):
+    # the register-resident FP32 panel (L2 word exchange) and the shared-memory
+    # panel (grid barrier per column) take the same pivots and do the same
+    # arithmetic per element: the mixed solutions match bit for bit.  1200
+    # elements (21 600 rows) spread the first panels over 15 CTAs.
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for kind in ('', 'smem'):
+        env = dict(os.environ, HFPX_LU_PANEL=kind, PYTHONPATH=root)
+        f = tmp_path / ('x_%s.npy' % (kind or 'll'))
+        r = subprocess.run([sys.executable, '-c', _PANEL_RUN, str(n_el), str(f)], env=env, cwd=root,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[kind] = np.load(f)
+    assert np.array_equal(out[''], out['smem'])
+    assert out[''][-1] <= 1e-12
+
+
+def test_mixed_singular_reports_column(ctx):
+    from hfpx3d_b200 import engine
+    for n, col in ((50, 17), (3000, 1234)):
+        A = np.eye(n) + 0.01 * np.random.default_rng(n).standard_normal((n, n))
+        A[:, col] = 0.0
+        m = engine.DeviceMatrix.upload(ctx, A)
+        with pytest.raises(engine.EngineError) as e:
+            engine.LU(ctx, m, engine.HFPX_LU_MIXED)
+        assert e.value.code == engine.HFPX_ERR_SINGULAR
+        assert str(col + 1) in str(e.value)

@@ -174,6 +174,7 @@ def test_driver_default_output_precision(tmp_path, driver):
     r = subprocess.run([driver, str(cfg)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     text = (tmp_path / 'Out' / 'test_solution.csv').read_text().splitlines()
-    assert all(len(c.lstrip('-').replace('.', '').split('e')[0]) <= 6 for c in text[0].split(','))
+    digits = [c.lstrip('-').split('e')[0].replace('.', '').lstrip('0') for line in text for c in line.split(',')]
+    assert max(len(d) for d in digits) == 6
     sol = np.loadtxt(tmp_path / 'Out' / 'test_solution.csv', delimiter=',')
     assert np.abs(sol[:, 4:] - g['dd']).max() / np.abs(g['dd']).max() < 1e-5
