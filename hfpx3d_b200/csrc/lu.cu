@@ -16,6 +16,7 @@
 // iterative refinement against the untouched FP64 matrix.
 #include <cooperative_groups.h>
 #include <cublas_v2.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -432,27 +433,97 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
 }
 
 // -------------------------------------------------------------- row swaps
-// Apply interchanges piv[0..k) (rows relative to A's top, piv relative too)
-// to columns [0, ncols) of A; one thread per column, swaps in order.
-template <class T>
-__global__ void laswp_kernel(T* __restrict__ A, int64_t lda, int64_t ncols,
-                             const int32_t* __restrict__ piv, int k, int piv_base) {
-  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= ncols) return;
-  T* col = A + lda * c;
-  for (int i = 0; i < k; ++i) {
-    const int p = piv[i] - piv_base;
-    if (p != i) {
-      const T t = col[i];
-      col[i] = col[p];
-      col[p] = t;
+// The interchanges piv[0..k) (LAPACK dlaswp order: row i <-> row piv[i] -
+// base, i = 0, 1, ...) are turned once into the permutation they make of the
+// rows they touch (a "plan": new row dst[e] = old row src[e]), then applied
+// to every column as one gather: contiguous reads of the leading rows
+// instead of k dependent strided swaps per column.
+constexpr int kSwapMax = 1024;                  // interchanges per plan (block size cap)
+constexpr int kSwapHash = 4096;                 // rows >= k touched, open addressing
+constexpr int kSwapPlanInts = 1 + 4 * kSwapMax; // count, src[2 kSwapMax], dst[2 kSwapMax]
+constexpr int kSwapThreads = 256;
+constexpr int kSwapPer = 2 * kSwapMax / kSwapThreads;
+constexpr int kSwapCols = 4;                    // columns per gather pass
+
+// add != 0: piv[i] += add afterwards (pivots of a sub-panel made relative to
+// the enclosing panel).
+__global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __restrict__ piv, int k, int base,
+                                                                  int32_t* __restrict__ plan, int add) {
+  __shared__ int32_t content[kSwapMax], spiv[kSwapMax], hkey[kSwapHash], hval[kSwapHash];
+  __shared__ int moved;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < k; i += kSwapThreads) {
+    content[i] = i;
+    spiv[i] = piv[i] - base;
+    if (add) piv[i] += add;
+  }
+  for (int i = tid; i < kSwapHash; i += kSwapThreads) hkey[i] = -1;
+  if (tid == 0) moved = 0;
+  __syncthreads();
+  if (tid == 0) {
+    // content[x]: original row now at position x (x < k; rows >= k in the hash)
+    for (int i = 0; i < k; ++i) {
+      const int p = spiv[i];
+      if (p == i) continue;
+      int* slot;
+      if (p < k) {
+        slot = &content[p];
+      } else {
+        unsigned h = ((unsigned)p * 2654435761u) >> 20;
+        while (hkey[h] != -1 && hkey[h] != p) h = (h + 1) & (kSwapHash - 1);
+        if (hkey[h] == -1) { hkey[h] = p; hval[h] = p; }
+        slot = &hval[h];
+      }
+      const int t = content[i];
+      content[i] = *slot;
+      *slot = t;
     }
   }
+  __syncthreads();
+  // all k leading rows in order (contiguous writes, near-contiguous reads),
+  // then the rows below k that changed, in any order
+  int32_t* src = plan + 1;
+  int32_t* dst = plan + 1 + 2 * kSwapMax;
+  for (int i = tid; i < k; i += kSwapThreads) {
+    src[i] = content[i];
+    dst[i] = i;
+  }
+  for (int h = tid; h < kSwapHash; h += kSwapThreads)
+    if (hkey[h] >= 0 && hval[h] != hkey[h]) {
+      const int e = k + atomicAdd(&moved, 1);
+      src[e] = hval[h];
+      dst[e] = hkey[h];
+    }
+  __syncthreads();
+  if (tid == 0) plan[0] = k + moved;
 }
 
-__global__ void offset_piv_kernel(int32_t* piv, int k, int off) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < k) piv[i] += off;
+template <class T>
+__global__ void __launch_bounds__(kSwapThreads) swap_apply_kernel(T* __restrict__ A, int64_t lda, int64_t ncols,
+                                                                   const int32_t* __restrict__ plan) {
+  const int cnt = plan[0];
+  const int tid = threadIdx.x;
+  int s[kSwapPer], d[kSwapPer];
+#pragma unroll
+  for (int r = 0; r < kSwapPer; ++r) {
+    const int e = tid + r * kSwapThreads;
+    s[r] = e < cnt ? plan[1 + e] : -1;
+    d[r] = e < cnt ? plan[1 + 2 * kSwapMax + e] : -1;
+  }
+  for (int64_t c0 = (int64_t)blockIdx.x * kSwapCols; c0 < ncols; c0 += (int64_t)gridDim.x * kSwapCols) {
+    T v[kSwapCols][kSwapPer];
+#pragma unroll
+    for (int q = 0; q < kSwapCols; ++q)
+#pragma unroll
+      for (int r = 0; r < kSwapPer; ++r)
+        if (s[r] >= 0 && c0 + q < ncols) v[q][r] = A[s[r] + lda * (c0 + q)];
+    __syncthreads();  // every read of these columns before any write
+#pragma unroll
+    for (int q = 0; q < kSwapCols; ++q)
+#pragma unroll
+      for (int r = 0; r < kSwapPer; ++r)
+        if (s[r] >= 0 && c0 + q < ncols) A[d[r] + lda * (c0 + q)] = v[q][r];
+  }
 }
 
 // --------------------------------------------------------------- BLAS glue
@@ -491,6 +562,77 @@ static void gemm_sub(Lane l, int64_t m, int64_t n, int64_t k, const float* A, in
   const float mone = -1.0f, one = 1.0f;
   cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, &mone, A, (int)lda, B, (int)ldb, &one, C,
               (int)ldc);
+}
+
+// ------------------------------------------------- FP16 trailing update
+// The FP32 factorisation's trailing update C -= L21 U12 runs on FP16 tensor
+// cores with FP32 accumulation.  FP16 and TF32 both keep 11 significant
+// bits, so the factor keeps TF32 quality at twice the tensor throughput.
+// L21 holds multipliers (|l| <= 1 under partial pivoting) and converts as
+// is; U12 is scaled by a power of two, from its largest magnitude, to put
+// that entry in [2^14, 2^15), and the GEMM's alpha (read from device memory)
+// undoes the scale exactly.
+__global__ void amax_kernel(const float* __restrict__ a, int64_t lda, int64_t rows, int64_t cols,
+                            unsigned* __restrict__ amax) {
+  __shared__ float wmax[8];
+  float m = 0.f;
+  const int64_t tot = rows * cols;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / rows, r = i - c * rows;
+    m = fmaxf(m, fabsf(a[r + lda * c]));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+    atomicMax(amax, __float_as_uint(m));  // non-negative floats order as their bits
+  }
+}
+
+// h = a * 2^(15 - e), amax = f 2^e with f in [0.5, 1); no scaling when amax
+// is null.  coef (if given) = {-2^(e - 15), 1}: alpha and beta of the update.
+__global__ void to_half_kernel(const float* __restrict__ a, int64_t lda, int64_t rows, int64_t cols,
+                               __half* __restrict__ h, int64_t ldh, const unsigned* __restrict__ amax,
+                               float* __restrict__ coef) {
+  int e = 15;
+  if (amax) {
+    const float m = __uint_as_float(*amax);
+    if (m > 0.f) frexpf(m, &e);
+  }
+  const float sc = ldexpf(1.f, 15 - e);
+  if (coef && blockIdx.x == 0 && threadIdx.x == 0) {
+    coef[0] = -ldexpf(1.f, e - 15);
+    coef[1] = 1.f;
+  }
+  const int64_t tot = rows * cols;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / rows, r = i - c * rows;
+    h[r + ldh * c] = __float2half_rn(a[r + lda * c] * sc);
+  }
+}
+
+static unsigned grid_for(int64_t tot) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, 148 * 16));
+}
+
+// C = coef[0] A B + coef[1] C, FP16 A and B, FP32 C, FP32 accumulation.
+static void gemm16(Lane l, int64_t m, int64_t n, int64_t k, const __half* A, int64_t lda, const __half* B,
+                   int64_t ldb, float* C, int64_t ldc, const float* d_coef) {
+  if (m <= 0 || n <= 0 || k <= 0) return;
+  cublasSetPointerMode(l.h, CUBLAS_POINTER_MODE_DEVICE);
+  cublasGemmEx(l.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, d_coef, A, CUDA_R_16F, (int)lda, B, CUDA_R_16F,
+               (int)ldb, d_coef + 1, C, CUDA_R_32F, (int)ldc, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
+  cublasSetPointerMode(l.h, CUBLAS_POINTER_MODE_HOST);
+}
+
+// HFPX_LU_UPDATE=tf32 keeps the trailing update on TF32 tensor cores.
+static bool fp16_update_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_LU_UPDATE");
+    return !(e && std::string(e) == "tf32");
+  }();
+  return on;
 }
 
 // ------------------------------------------------------------- profiling
@@ -548,7 +690,75 @@ struct LuWork {
   uint64_t* ll_slots = nullptr;
   int* ll_err = nullptr;
   uint32_t ll_launches = 0;
+  // FP32: L11^-1 (nb x nb) and a copy of A12 (nb x n) for U12 = L11^-1 A12
+  // as one TF32 GEMM
+  T* linv = nullptr;
+  T* a12 = nullptr;
+  // row-swap plans: one for the panel stream's own swaps, one per block
+  // (read by the right and left swaps of that block on two streams)
+  int32_t* plan_panel = nullptr;
+  int32_t* plans = nullptr;
+  // FP32 with the FP16 trailing update: L21 (rest x nb) and scaled U12
+  // (nb x rest) in FP16, U12's largest magnitude and the update's alpha/beta
+  __half* l16 = nullptr;
+  __half* u16 = nullptr;
+  unsigned* amax = nullptr;
+  float* coef = nullptr;
 };
+
+__global__ void identity_kernel(float* a, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i < n) a[i + (int64_t)n * j] = i == j ? 1.f : 0.f;
+}
+
+// U12 = L11^-1 A12 for the trailing block row.  FP32: invert the unit lower
+// L11 (kb x kb triangular solve on the identity), then one TF32 GEMM over the
+// whole block row; the triangular solve over the block row (kb x rest) is
+// the slow path it replaces.  FP64: triangular solve.
+template <class T>
+static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L, int64_t lda, T* B) {
+  if constexpr (sizeof(T) == 4) {
+    if (wk.linv && wk.a12) {
+      ++g_launches;
+      identity_kernel<<<dim3((kb + 127) / 128, kb), 128, 0, l.s>>>(wk.linv, kb);
+      trsm_llu(l, kb, kb, L, lda, wk.linv, kb);
+      cudaMemcpy2DAsync(wk.a12, sizeof(T) * kb, B, sizeof(T) * lda, sizeof(T) * kb, rest, cudaMemcpyDeviceToDevice, l.s);
+      const float one = 1.f, zero = 0.f;
+      cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, kb, (int)rest, kb, &one, wk.linv, kb, wk.a12, kb, &zero, B, (int)lda);
+      return;
+    }
+  }
+  trsm_llu(l, kb, rest, L, lda, B, lda);
+}
+
+// Trailing update of step k: FP16 copies of L21 and U12 (FP32 with the FP16
+// update), then C -= L21 U12[:, c0:c0+nc] for one range of columns.
+template <class T>
+static void update_prepare(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L21, const T* U12, int64_t lda) {
+  if constexpr (sizeof(T) == 4) {
+    if (wk.l16) {
+      ++g_launches;
+      to_half_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(L21, lda, rest, kb, wk.l16, rest, nullptr, nullptr);
+      cudaMemsetAsync(wk.amax, 0, sizeof(unsigned), l.s);
+      ++g_launches;
+      amax_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(U12, lda, kb, rest, wk.amax);
+      ++g_launches;
+      to_half_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(U12, lda, kb, rest, wk.u16, kb, wk.amax, wk.coef);
+    }
+  }
+}
+
+template <class T>
+static void update_gemm(Lane l, LuWork<T>& wk, int kb, int64_t rest, int64_t c0, int64_t nc, const T* L21,
+                        const T* U12, T* C, int64_t lda) {
+  if constexpr (sizeof(T) == 4) {
+    if (wk.l16) {
+      gemm16(l, rest, nc, kb, wk.l16, rest, wk.u16 + (size_t)kb * c0, kb, C, lda, wk.coef);
+      return;
+    }
+  }
+  gemm_sub(l, rest, nc, kb, L21, lda, U12 + lda * c0, lda, C, lda);
+}
 
 // HFPX_LU_PANEL=smem selects the shared-memory panel kernel for FP32 too.
 static bool ll_panel_enabled() {
@@ -606,11 +816,27 @@ static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int
   return check_cuda(c, e, "panel_base_kernel launch");
 }
 
-template <class T>
-static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, const int32_t* piv, int k, int base) {
-  if (ncols <= 0 || k <= 0) return;
+static void swap_plan(Lane l, int32_t* piv, int k, int base, int32_t* plan, int add = 0) {
+  if (k <= 0) return;
   ++g_launches;
-  laswp_kernel<T><<<(unsigned)((ncols + 127) / 128), 128, 0, l.s>>>(A, lda, ncols, piv, k, base);
+  swap_plan_kernel<<<1, kSwapThreads, 0, l.s>>>(piv, k, base, plan, add);
+}
+
+template <class T>
+static void swap_apply(Lane l, T* A, int64_t lda, int64_t ncols, const int32_t* plan) {
+  if (ncols <= 0) return;
+  const int64_t blocks = std::min<int64_t>((ncols + kSwapCols - 1) / kSwapCols, 148 * 8);
+  ++g_launches;
+  swap_apply_kernel<T><<<(unsigned)blocks, kSwapThreads, 0, l.s>>>(A, lda, ncols, plan);
+}
+
+// dlaswp: interchanges piv[0..k) (minus base) on columns [0, ncols) of A,
+// through the plan buffer.
+template <class T>
+static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, int32_t* piv, int k, int base, int32_t* plan) {
+  if (ncols <= 0 || k <= 0) return;
+  swap_plan(l, piv, k, base, plan);
+  swap_apply(l, A, lda, ncols, plan);
 }
 
 // dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
@@ -630,7 +856,7 @@ static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int6
   int rc = panel_rec(c, l, wk, A, lda, m, w1, piv, col_offset);
   if (rc) return rc;
   P.begin(l.s);
-  laswp(l, A + lda * w1, lda, w2, piv, w1, 0);
+  laswp(l, A + lda * w1, lda, w2, piv, w1, 0, wk.plan_panel);
   P.end(1);
   trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
   P.end(2);
@@ -639,9 +865,10 @@ static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int6
   rc = panel_rec(c, l, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1);
   if (rc) return rc;
   P.begin(l.s);
-  ++g_launches;
-  offset_piv_kernel<<<(w2 + 127) / 128, 128, 0, l.s>>>(piv + w1, w2, w1);
-  laswp(l, A + w1, lda, w1, piv + w1, w2, w1);
+  // the right half's interchanges on the left half's columns; its pivots
+  // become relative to this panel's top
+  swap_plan(l, piv + w1, w2, 0, wk.plan_panel, w1);
+  swap_apply(l, A + w1, lda, w1, wk.plan_panel);
   P.end(1);
   return 0;
 }
@@ -674,13 +901,35 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   wk.sc.cidx = (int*)alloc(sizeof(int) * 2 * G);
   wk.sc.rowj = (T*)alloc(sizeof(T) * 2 * kBaseW);
   wk.d_info = (int64_t*)alloc(sizeof(int64_t));
+  const int64_t n_blocks = (n + lu_block_size() - 1) / lu_block_size();
+  wk.plan_panel = (int32_t*)alloc(sizeof(int32_t) * kSwapPlanInts);
+  wk.plans = (int32_t*)alloc(sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
   const size_t ll_bytes = sizeof(uint64_t) * 2 * kLLMaxCtas * kLLSlot;
   if (sizeof(T) == 4) {
     wk.ll_slots = (uint64_t*)alloc(ll_bytes);
     wk.ll_err = (int*)alloc(sizeof(int));
+    // optional: without room for them the block row takes the triangular solve
+    const size_t nb = (size_t)lu_block_size();
+    wk.linv = (T*)alloc(sizeof(T) * nb * nb);
+    wk.a12 = (T*)alloc(sizeof(T) * nb * (size_t)n);
+    if (!wk.linv || !wk.a12) {
+      wk.linv = wk.a12 = nullptr;
+      cudaGetLastError();
+    }
+    // optional too: without them the update stays on TF32
+    if (fp16_update_enabled()) {
+      wk.l16 = (__half*)alloc(sizeof(__half) * nb * (size_t)n);
+      wk.u16 = (__half*)alloc(sizeof(__half) * nb * (size_t)n);
+      wk.amax = (unsigned*)alloc(sizeof(unsigned));
+      wk.coef = (float*)alloc(2 * sizeof(float));
+      if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) {
+        wk.l16 = wk.u16 = nullptr;
+        cudaGetLastError();
+      }
+    }
   }
   int rc = 0;
-  if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info ||
+  if (!wk.sc.cand || !wk.sc.cmax || !wk.sc.cidx || !wk.sc.rowj || !wk.d_info || !wk.plan_panel || !wk.plans ||
       (sizeof(T) == 4 && (!wk.ll_slots || !wk.ll_err)))
     rc = set_error(c, HFPX_ERR_NOMEM, "LU scratch");
   if (!rc && wk.ll_slots) {
@@ -702,6 +951,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     cudaStreamWaitEvent(S, ev_start, 0);
     const int kb0 = (int)std::min<int64_t>(kNb, n);
     rc = panel_rec(c, Pn, wk, A, lda, n, kb0, piv, 0);
+    if (!rc) swap_plan(Pn, piv, kb0, 0, wk.plans);
     cudaEventRecord(ev_panel, Pn.s);
   }
   for (int64_t k = 0; k < n && !rc; k += kNb) {
@@ -711,24 +961,27 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     // left swaps of panel k, after the step that read those columns last
     cudaStreamWaitEvent(S, ev_panel, 0);
     if (k > 0) cudaStreamWaitEvent(S, ev_rest, 0);
-    laswp(Lane{S, nullptr}, A + k, lda, k, piv + k, kb, 0);
+    const int32_t* plan_k = wk.plans + (size_t)(k / kNb) * kSwapPlanInts;
+    swap_apply(Lane{S, nullptr}, A + k, lda, k, plan_k);
     P.begin(M.s);
-    laswp(M, A + k + lda * (k + kb), lda, n - k - kb, piv + k, kb, 0);
+    swap_apply(M, A + k + lda * (k + kb), lda, n - k - kb, plan_k);
     P.end(1);
     if (k + kb < n) {
       const int64_t rest = n - k - kb;
       const int kn = (int)std::min<int64_t>(kNb, rest);
-      trsm_llu(M, kb, rest, Akk, lda, Akk + lda * kb, lda);
+      block_row_solve(M, wk, kb, rest, Akk, lda, Akk + lda * kb);
       P.end(2);
-      gemm_sub(M, rest, kn, kb, Akk + kb, lda, Akk + lda * kb, lda, Akk + kb + lda * kb, lda);
+      update_prepare(M, wk, kb, rest, Akk + kb, Akk + lda * kb, lda);
+      update_gemm(M, wk, kb, rest, 0, kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * kb, lda);
       P.end(3);
       cudaEventRecord(ev_next, M.s);
       cudaStreamWaitEvent(Pn.s, ev_next, 0);
       rc = panel_rec(c, Pn, wk, Akk + kb + lda * kb, lda, rest, kn, piv + k + kb, k + kb);
+      if (!rc) swap_plan(Pn, piv + k + kb, kn, 0, wk.plans + (size_t)((k + kb) / kNb) * kSwapPlanInts);
       cudaEventRecord(ev_panel, Pn.s);
       if (rc) break;
       P.begin(M.s);
-      gemm_sub(M, rest, rest - kn, kb, Akk + kb, lda, Akk + lda * (kb + kn), lda, Akk + kb + lda * (kb + kn), lda);
+      update_gemm(M, wk, kb, rest, kn, rest - kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * (kb + kn), lda);
       P.end(3);
       cudaEventRecord(ev_rest, M.s);
     }
