@@ -197,13 +197,14 @@ def run_engine(args, rank, world, local_rank):
     line = {
         'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'f64+tf32' if mode == engine.HFPX_LU_MIXED else 'f64',
+        'vs_baseline': None, 'dtype': 'f64+f32+f16' if mode == engine.HFPX_LU_MIXED else 'f64',
         'data': 'synthetic (seeded 4000-triangle penny mesh, pressure 1)',
         'config': {'workload': f'penny crack {args.n_el} el, N={n} DoF, assembly + LU + solve to rel residual '
                                f'{args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'mode': args.mode,
                    'parallelism': f'replicas x{world}',
                    'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
         'phases_ms': {'assembly': asm_ms, 'factor': statistics.mean(t_fac), 'solve': statistics.mean(t_sol)},
+        'steps_ms': {'factor': [round(t, 2) for t in t_fac], 'solve': [round(t, 2) for t in t_sol]},
         'refinement': {'iterations': iters_main, 'residual': res_main},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,

@@ -14,6 +14,30 @@ namespace hfpx {
 
 std::atomic<long long> g_launches{0};
 
+void* ctx_scratch(hfpx_ctx* c, int slot, size_t bytes) {
+  static_assert(kScrCount <= hfpx_ctx::kScratchSlots, "scratch slots");
+  if (slot < 0 || slot >= hfpx_ctx::kScratchSlots) return nullptr;
+  if (bytes == 0) bytes = 1;
+  if (c->scratch[slot] && c->scratch_bytes[slot] >= bytes) return c->scratch[slot];
+  if (c->scratch[slot]) {
+    // earlier work queued on the context's streams may still read it
+    cudaStreamSynchronize(c->stream);
+    cudaStreamSynchronize(c->stream_panel);
+    cudaStreamSynchronize(c->stream_left);
+    cudaFree(c->scratch[slot]);
+    c->scratch[slot] = nullptr;
+    c->scratch_bytes[slot] = 0;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  c->scratch[slot] = p;
+  c->scratch_bytes[slot] = bytes;
+  return p;
+}
+
 int set_error(hfpx_ctx* c, int code, const std::string& msg) {
   if (c) c->last_error = msg;
   return code;
@@ -33,15 +57,17 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
-static int upload_dof(hfpx_ctx* c, const int64_t* dof_h, int64_t n_el, int64_t n_dof, DevBuf& d) {
+// dof_h (int64, n_el x 18) to int32 in the context's dof buffer.
+static int upload_dof(hfpx_ctx* c, const int64_t* dof_h, int64_t n_el, int64_t n_dof, int32_t** d) {
   std::vector<int32_t> tmp(18 * n_el);
   for (int64_t i = 0; i < 18 * n_el; ++i) {
     const int64_t v = dof_h[i];
     if (v < -1 || v >= n_dof) return set_error(c, HFPX_ERR_ARG, "dof_h entry out of range");
     tmp[i] = (int32_t)v;
   }
-  int rc = check_cuda(c, d.alloc(sizeof(int32_t) * tmp.size()), "dof_h alloc");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(d.p, tmp.data(), sizeof(int32_t) * tmp.size(), cudaMemcpyHostToDevice, c->stream), "dof_h copy");
+  *d = (int32_t*)ctx_scratch(c, kScrDof, sizeof(int32_t) * tmp.size());
+  if (!*d) return set_error(c, HFPX_ERR_NOMEM, "dof_h alloc");
+  int rc = check_cuda(c, cudaMemcpyAsync(*d, tmp.data(), sizeof(int32_t) * tmp.size(), cudaMemcpyHostToDevice, c->stream), "dof_h copy");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "dof_h copy");
   return rc;
 }
@@ -103,6 +129,8 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
   if (c->cublas_panel) cublasDestroy(static_cast<cublasHandle_t>(c->cublas_panel));
   if (c->d_flags) cudaFree(c->d_flags);
+  for (void* p : c->scratch)
+    if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->stream_panel) cudaStreamDestroy(c->stream_panel);
   if (c->stream_left) cudaStreamDestroy(c->stream_left);
@@ -227,13 +255,13 @@ static int check_assembly_args(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t
 
 static int assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
                          int is_dd_local, int vc_border, hfpx_matrix* m) {
-  DevBuf dd;
-  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, dd);
+  int32_t* dd = nullptr;
+  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, &dd);
   if (rc) return rc;
   m->factored = 0;
   m->info = 0;
-  launch_assemble(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), G, nu, is_dd_local, m->d_a, m->ld, c->d_flags, c->stream);
-  if (vc_border) launch_vc_border(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), n_dof, is_dd_local, m->d_a, m->ld, c->stream);
+  launch_assemble(mesh->d_elem, mesh->n_el, dd, G, nu, is_dd_local, m->d_a, m->ld, c->d_flags, c->stream);
+  if (vc_border) launch_vc_border(mesh->d_elem, mesh->n_el, dd, n_dof, is_dd_local, m->d_a, m->ld, c->stream);
   rc = check_cuda(c, cudaGetLastError(), "assembly launch");
   int flags[2] = {0, 0};
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(flags, c->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream), "flags");
@@ -322,13 +350,14 @@ int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   if (!mesh || !dof_h || !s_inf || !rhs || n_rhs < 1 || ld_rhs < n_dof || n_dof < 1)
     return set_error(c, HFPX_ERR_ARG, "bad rhs arguments");
   cudaSetDevice(c->device);
-  DevBuf dd, ds, dr;
-  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, dd);
+  DevBuf ds, dr;
+  int32_t* dd = nullptr;
+  int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, &dd);
   if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 6 * n_rhs), "s_inf alloc");
   if (!rc) rc = check_cuda(c, dr.alloc(sizeof(double) * ld_rhs * n_rhs), "rhs alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ds.p, s_inf, sizeof(double) * 6 * n_rhs, cudaMemcpyHostToDevice, c->stream), "s_inf");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dr.p, rhs, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyHostToDevice, c->stream), "rhs");
-  if (!rc) launch_rhs(mesh->d_elem, mesh->n_el, dd.as<int32_t>(), ds.as<double>(), n_rhs, dr.as<double>(), ld_rhs, c->stream);
+  if (!rc) launch_rhs(mesh->d_elem, mesh->n_el, dd, ds.as<double>(), n_rhs, dr.as<double>(), ld_rhs, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "rhs launch");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(rhs, dr.p, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyDeviceToHost, c->stream), "rhs back");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "rhs");

@@ -18,6 +18,11 @@ struct hfpx_ctx {
   void* cublas_panel = nullptr;
   std::string last_error;
   int* d_flags = nullptr;          // device status words (see kernels)
+  // device work buffers kept between calls (grown on demand, freed with the
+  // context), so repeated factorisations and solves allocate nothing
+  static constexpr int kScratchSlots = 24;
+  void* scratch[kScratchSlots] = {};
+  size_t scratch_bytes[kScratchSlots] = {};
 };
 
 struct hfpx_mesh {
@@ -39,6 +44,16 @@ namespace hfpx {
 extern std::atomic<long long> g_launches;
 int set_error(hfpx_ctx* c, int code, const std::string& msg);
 int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what);
+// Work buffer `slot` of the context with at least `bytes` bytes (null when
+// the device is out of memory; the CUDA error state is cleared).  A slot
+// that grows is reallocated after the context's streams finish with it.
+void* ctx_scratch(hfpx_ctx* c, int slot, size_t bytes);
+// scratch slots
+enum : int {
+  kScrPanelCand, kScrPanelMax, kScrPanelIdx, kScrPanelRowj, kScrInfo, kScrPlanPanel, kScrPlans, kScrLLSlots,
+  kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
+  kScrRefR, kScrRefRf, kScrDof, kScrCount
+};
 
 // assembly.cu
 size_t elem_record_bytes();

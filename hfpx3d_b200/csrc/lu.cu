@@ -174,9 +174,13 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
 //    4 bytes of data and a 4-byte tag naming the launch and column.  A word
 //    is written and read as one 8-byte access, so a reader that sees the
 //    expected tag holds the data: no grid barrier and no fence.  Every CTA
-//    publishes its arg-max (value, row, the candidate row) and the owner of
-//    row j the old row j; every CTA then polls all of them in one L2 round
-//    trip and picks the same pivot.
+//    publishes its arg-max (key, row, the candidate row); every CTA then
+//    polls all of them in one L2 round trip and picks the same pivot;
+//  * rows are interchanged by relabelling, not by moving data: each register
+//    row carries the panel row it currently stands for.  Swapping rows j and
+//    p swaps the two labels; the pivot row's data stays where it is and, now
+//    labelled j, takes no further updates.  The write-back stores every row
+//    at its final label.
 // Words of column j sit in buffer j & 1: a CTA can only write column j + 2
 // after all CTAs published column j + 1, i.e. after all finished reading j.
 // Tags are unique within one factorisation and the buffers are zeroed before
@@ -185,9 +189,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
 constexpr int kLLThreads = 256;
 constexpr int kLLRows = 6;
 constexpr int kLLCap = kLLThreads * kLLRows;  // panel rows per CTA
-constexpr int kLLSlot = 2 + 2 * kBaseW;       // words per CTA per column
+constexpr int kLLSlot = 2 + kBaseW;           // words per CTA per column
 constexpr int kLLUnits = 8;                   // words each thread polls
-constexpr int kLLMaxCtas = (kLLThreads * kLLUnits - kBaseW) / (2 + kBaseW);
+constexpr int kLLMaxCtas = kLLThreads * kLLUnits / kLLSlot;
 constexpr unsigned long long kLLTimeoutNs = 200ull * 1000 * 1000;
 
 __device__ __forceinline__ void ll_store(uint64_t* p, uint32_t data, uint32_t tag) {
@@ -204,16 +208,6 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// (max, first index) over the warp, result in every lane
-__device__ __forceinline__ void warp_argmax_all(float& v, int& i) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
-  }
-}
-
 // a[k][c] if c == j else keep, by bit masks: a plain "if (c == j) x =
 // a[k][c]" over an unrolled c is folded back into a[k][j] with a run-time j,
 // which moves the whole register array to local memory.
@@ -222,19 +216,20 @@ __device__ __forceinline__ float pick(float x, float cand, bool take) {
   return __int_as_float((__float_as_int(cand) & msk) | (__float_as_int(x) & ~msk));
 }
 
-// Scale column j and update columns j+1..31 of this thread's rows below row
-// j (j in [C0, C0 + 8)); columns below C0 are not touched.  One FMA per
-// element: rows that take no update get multiplier 0 and columns c <= j a
-// zero pivot-row entry, so the FMA leaves them unchanged (up to the sign of
-// a zero); column j is then set by selects over the 8 columns of its group.
-// nxt gets |a(., j+1)| for the next arg-max.
+// Scale column j and update columns j+1..31 of this thread's rows labelled
+// below row j (j in [C0, C0 + 8); label -1: no row); columns below C0 are
+// not touched.  One FMA per element: rows that take no update get
+// multiplier 0 and columns c <= j a zero pivot-row entry, so the FMA leaves
+// them unchanged (up to the sign of a zero); column j is then set by selects
+// over the 8 columns of its group.  nxt gets |a(., j+1)| for the next
+// arg-max (-1: not a candidate).
 template <int C0>
-__device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], int g0, int nrow_left, int j, float inv,
+__device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], const int (&lab)[kLLRows], int j, float inv,
                                           bool nonzero, const float* __restrict__ prow, float (&nxt)[kLLRows]) {
   float l[kLLRows], lz[kLLRows];
 #pragma unroll
   for (int k = 0; k < kLLRows; ++k) {
-    const bool below = nonzero && k * kLLThreads < nrow_left && g0 + k * kLLThreads > j;
+    const bool below = nonzero && lab[k] > j;
     float v = 0.f;
 #pragma unroll
     for (int c = C0; c < C0 + 8; ++c) v = pick(v, a[k][c], c == j);
@@ -255,7 +250,7 @@ __device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], int g0, i
   }
 #pragma unroll
   for (int k = 0; k < kLLRows; ++k) {
-    const bool below = k * kLLThreads < nrow_left && g0 + k * kLLThreads > j;
+    const bool below = lab[k] > j;
     float x = 0.f;
 #pragma unroll
     for (int c = C0 + 1; c < C0 + 9 && c < kBaseW; ++c) x = pick(x, a[k][c], c == j + 1);
@@ -263,26 +258,15 @@ __device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], int g0, i
   }
 }
 
-// Row k of this thread's registers to 32 LL words / from shared memory.  The
-// if-chain over compile-time K keeps every register index static.
+// Register row k of this thread to shared memory.  The if-chain over
+// compile-time K keeps every register index static.
 template <int K = 0>
-__device__ __forceinline__ void ll_row_store(const float (&a)[kLLRows][kBaseW], int k, uint64_t* dst, int w,
-                                             uint32_t tag) {
+__device__ __forceinline__ void ll_row_to_smem(const float (&a)[kLLRows][kBaseW], int k, float* dst) {
   if (k == K) {
 #pragma unroll
-    for (int c = 0; c < kBaseW; ++c)
-      if (c < w) ll_store(dst + c, __float_as_uint(a[K][c]), tag);
+    for (int c = 0; c < kBaseW; ++c) dst[c] = a[K][c];
   } else if constexpr (K + 1 < kLLRows) {
-    ll_row_store<K + 1>(a, k, dst, w, tag);
-  }
-}
-template <int K = 0>
-__device__ __forceinline__ void ll_row_load(float (&a)[kLLRows][kBaseW], int k, const float* src) {
-  if (k == K) {
-#pragma unroll
-    for (int c = 0; c < kBaseW; ++c) a[K][c] = src[c];
-  } else if constexpr (K + 1 < kLLRows) {
-    ll_row_load<K + 1>(a, k, src);
+    ll_row_to_smem<K + 1>(a, k, dst);
   }
 }
 
@@ -290,79 +274,97 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
     uint64_t* __restrict__ slots, int64_t* __restrict__ info, int64_t col_offset, uint32_t tag0,
     int* __restrict__ err) {
+  // arg-max candidates travel as keys: |a| bits + 1 (non-negative floats
+  // order as their bits), 0 for "no row"; ties go to the lower row
   __shared__ float s_cand[2][kLLMaxCtas][kBaseW];
-  __shared__ float s_rowj[2][kBaseW];
-  __shared__ float s_val[2][kLLMaxCtas];
-  __shared__ int s_idx[2][kLLMaxCtas];
-  __shared__ float s_wv[kLLThreads / 32];
-  __shared__ int s_wi[kLLThreads / 32];
+  __shared__ unsigned s_key[2][kLLMaxCtas];
+  __shared__ unsigned s_idx[2][kLLMaxCtas];
+  __shared__ unsigned s_wk[kLLThreads / 32];
+  __shared__ unsigned s_wi[kLLThreads / 32];
+  __shared__ float s_stage[kLLThreads / 32][kBaseW];
   __shared__ int s_fail;
   const int b = blockIdx.x, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t r0 = (int64_t)b * rpc;
   const int nrow = (int)max((int64_t)0, min((int64_t)rpc, m - r0));
-  const int g0 = (int)r0 + tid;       // panel row of a[0]; a[k] is row g0 + k * kLLThreads
+  const int g0 = (int)r0 + tid;       // panel row first held in a[k]: g0 + k * kLLThreads
   const int nrow_left = nrow - tid;   // a[k] holds a row iff k * kLLThreads < nrow_left
   float a[kLLRows][kBaseW];
+  int lab[kLLRows];                   // panel row a[k] stands for, -1: none
 #pragma unroll
-  for (int k = 0; k < kLLRows; ++k)
+  for (int k = 0; k < kLLRows; ++k) {
+    lab[k] = k * kLLThreads < nrow_left ? g0 + k * kLLThreads : -1;
 #pragma unroll
     for (int c = 0; c < kBaseW; ++c)
-      a[k][c] = (k * kLLThreads < nrow_left && c < w) ? A[(int64_t)(g0 + k * kLLThreads) + lda * c] : 0.f;
+      a[k][c] = (lab[k] >= 0 && c < w) ? A[(int64_t)lab[k] + lda * c] : 0.f;
+  }
   // candidate rows past column w stay zero
   for (int i = tid; i < 2 * kLLMaxCtas * kBaseW; i += kLLThreads) (&s_cand[0][0][0])[i] = 0.f;
-  if (tid < 2 * kBaseW) (&s_rowj[0][0])[tid] = 0.f;
   if (tid == 0) s_fail = 0;
-  // words this thread polls: CTA q's (value, row, candidate row) or the old row j
-  const int per = 2 + w, nmain = G * per, units = nmain + w;
+  // words this thread polls: CTA q's (key, row, candidate row)
+  const int per = 2 + w, units = G * per;
   int off[kLLUnits];
 #pragma unroll
   for (int u = 0; u < kLLUnits; ++u) {
     const int x = tid + u * kLLThreads;
-    off[u] = x < nmain ? (x / per) * kLLSlot + x % per : (x < units ? -1 - (x - nmain) : INT32_MIN);
+    off[u] = x < units ? (x / per) * kLLSlot + x % per : -1;
   }
   float nxt[kLLRows];
 #pragma unroll
-  for (int k = 0; k < kLLRows; ++k) nxt[k] = k * kLLThreads < nrow_left ? fabsf(a[k][0]) : -1.f;
+  for (int k = 0; k < kLLRows; ++k) nxt[k] = lab[k] >= 0 ? fabsf(a[k][0]) : -1.f;
   for (int j = 0; j < w; ++j) {
     const int buf = j & 1;
     const uint32_t tag = tag0 + (uint32_t)j + 1u;
-    // CTA arg-max of |a(i, j)|, i >= j, first row on ties
-    float best = -1.f;
-    int bidx = INT32_MAX;
+    // CTA arg-max of |a(i, j)| over rows labelled >= j, lowest label on ties
+    unsigned bkey = 0u, bidx = 0xFFFFFFFFu;
 #pragma unroll
-    for (int k = 0; k < kLLRows; ++k)
-      if (nxt[k] > best) { best = nxt[k]; bidx = g0 + k * kLLThreads; }
-    warp_argmax_all(best, bidx);
-    if (lane == 0) { s_wv[warp] = best; s_wi[warp] = bidx; }
-    __syncthreads();
-    best = lane < kLLThreads / 32 ? s_wv[lane] : -1.f;
-    bidx = lane < kLLThreads / 32 ? s_wi[lane] : INT32_MAX;
-    warp_argmax_all(best, bidx);
-    // publish
-    uint64_t* mine = slots + ((size_t)buf * G + b) * kLLSlot;
-    if (tid == 0) {
-      ll_store(mine, __float_as_uint(best), tag);
-      ll_store(mine + 1, (uint32_t)bidx, tag);
+    for (int k = 0; k < kLLRows; ++k) {
+      const unsigned kk = nxt[k] >= 0.f ? __float_as_uint(nxt[k]) + 1u : 0u;
+      if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) { bkey = kk; bidx = (unsigned)lab[k]; }
     }
     {
-      const int dc = bidx - g0, dj = j - g0;
-      if (dc >= 0 && dc % kLLThreads == 0 && dc < nrow_left) ll_row_store(a, dc / kLLThreads, mine + 2, w, tag);
-      if (dj >= 0 && dj % kLLThreads == 0 && dj < nrow_left)
-        ll_row_store(a, dj / kLLThreads, mine + 2 + kBaseW, w, tag);
+      const unsigned wm = __reduce_max_sync(0xffffffffu, bkey);
+      const unsigned wi = __reduce_min_sync(0xffffffffu, bkey == wm ? bidx : 0xFFFFFFFFu);
+      if (lane == 0) { s_wk[warp] = wm; s_wi[warp] = wi; }
+    }
+    __syncthreads();
+    {
+      const unsigned k2 = lane < kLLThreads / 32 ? s_wk[lane] : 0u;
+      const unsigned i2 = lane < kLLThreads / 32 ? s_wi[lane] : 0xFFFFFFFFu;
+      bkey = __reduce_max_sync(0xffffffffu, k2);
+      bidx = __reduce_min_sync(0xffffffffu, k2 == bkey ? i2 : 0xFFFFFFFFu);
+    }
+    // publish: thread 0 the key and row; the warp holding the candidate row
+    // (staged through shared memory by its lane) that row, one word per
+    // lane; a CTA without candidates publishes zeros
+    uint64_t* mine = slots + ((size_t)buf * G + b) * kLLSlot;
+    if (tid == 0) {
+      ll_store(mine, bkey, tag);
+      ll_store(mine + 1, bidx, tag);
+    }
+    {
+      int kc = -1;
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) kc = ((unsigned)lab[k] == bidx && bkey != 0u) ? k : kc;
+      const unsigned hit = __ballot_sync(0xffffffffu, kc >= 0);
+      if (hit) {
+        if (kc >= 0) ll_row_to_smem(a, kc, s_stage[warp]);
+        __syncwarp();
+        if (lane < w) ll_store(mine + 2 + lane, __float_as_uint(s_stage[warp][lane]), tag);
+      } else if (bkey == 0u && warp == 0 && lane < w) {
+        ll_store(mine + 2 + lane, 0u, tag);
+      }
     }
     // poll every CTA's words for this column
     const uint64_t* xb = slots + (size_t)buf * G * kLLSlot;
-    const int rowj_off = (j / rpc) * kLLSlot + 2 + kBaseW;
     bool need[kLLUnits];
 #pragma unroll
-    for (int u = 0; u < kLLUnits; ++u) need[u] = off[u] != INT32_MIN;
+    for (int u = 0; u < kLLUnits; ++u) need[u] = off[u] >= 0;
     uint64_t t_start = 0;
     bool failed = false;
     for (;;) {
       uint64_t v[kLLUnits];
 #pragma unroll
-      for (int u = 0; u < kLLUnits; ++u)
-        v[u] = need[u] ? ll_load(xb + (off[u] >= 0 ? off[u] : rowj_off + (-1 - off[u]))) : 0;
+      for (int u = 0; u < kLLUnits; ++u) v[u] = need[u] ? ll_load(xb + off[u]) : 0;
       bool pending = false;
 #pragma unroll
       for (int u = 0; u < kLLUnits; ++u) {
@@ -370,14 +372,10 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
         if ((uint32_t)(v[u] >> 32) != tag) { pending = true; continue; }
         need[u] = false;
         const uint32_t d = (uint32_t)v[u];
-        if (off[u] < 0) {
-          s_rowj[buf][-1 - off[u]] = __uint_as_float(d);
-        } else {
-          const int q = off[u] / kLLSlot, o = off[u] - q * kLLSlot;
-          if (o == 0) s_val[buf][q] = __uint_as_float(d);
-          else if (o == 1) s_idx[buf][q] = (int)d;
-          else s_cand[buf][q][o - 2] = __uint_as_float(d);
-        }
+        const int q = off[u] / kLLSlot, o = off[u] - q * kLLSlot;
+        if (o == 0) s_key[buf][q] = d;
+        else if (o == 1) s_idx[buf][q] = d;
+        else s_cand[buf][q][o - 2] = __uint_as_float(d);
       }
       if (!pending) break;
       const uint64_t now = global_ns();
@@ -391,45 +389,38 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
       break;
     }
     // global pivot, identical in every warp of every CTA
-    float gv = -1.f;
-    int gix = INT32_MAX, gw = 0;
+    unsigned gk = 0u, gi = 0xFFFFFFFFu, gq = 0u;
     for (int q = lane; q < G; q += 32) {
-      const float vq = s_val[buf][q];
-      const int iq = s_idx[buf][q];
-      if (vq > gv || (vq == gv && iq < gix)) { gv = vq; gix = iq; gw = q; }
+      const unsigned kq = s_key[buf][q], iq = s_idx[buf][q];
+      if (kq > gk || (kq == gk && iq < gi)) { gk = kq; gi = iq; gq = (unsigned)q; }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, gv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, gix, o);
-      const int ow = __shfl_xor_sync(0xffffffffu, gw, o);
-      if (ov > gv || (ov == gv && oi < gix)) { gv = ov; gix = oi; gw = ow; }
-    }
-    const int p = gix;
-    const float* prow = s_cand[buf][gw];
+    const unsigned gmax = __reduce_max_sync(0xffffffffu, gk);
+    const unsigned pu = __reduce_min_sync(0xffffffffu, gk == gmax ? gi : 0xFFFFFFFFu);
+    const int p = (int)pu;
+    const float* prow = s_cand[buf][__reduce_max_sync(0xffffffffu, (gk == gmax && gi == pu) ? gq : 0u)];
     if (b == 0 && tid == 0) {
       piv[j] = p;
-      if (gv == 0.f && info && *info == 0) *info = col_offset + j + 1;
+      if (gmax == 1u && info && *info == 0) *info = col_offset + j + 1;  // |pivot| == 0
     }
-    // swap rows j and p
+    // interchange rows j and p: swap the labels
     if (p != j) {
-      const int dj = j - g0, dp = p - g0;
-      if (dj >= 0 && dj % kLLThreads == 0 && dj < nrow_left) ll_row_load(a, dj / kLLThreads, prow);
-      if (dp >= 0 && dp % kLLThreads == 0 && dp < nrow_left) ll_row_load(a, dp / kLLThreads, s_rowj[buf]);
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) lab[k] = lab[k] == j ? p : (lab[k] == p ? j : lab[k]);
     }
     const float pv = prow[j];
     const bool nz = pv != 0.f;
     const float inv = nz ? 1.f / pv : 0.f;
-    if (j < 8) ll_update<0>(a, g0, nrow_left, j, inv, nz, prow, nxt);
-    else if (j < 16) ll_update<8>(a, g0, nrow_left, j, inv, nz, prow, nxt);
-    else if (j < 24) ll_update<16>(a, g0, nrow_left, j, inv, nz, prow, nxt);
-    else ll_update<24>(a, g0, nrow_left, j, inv, nz, prow, nxt);
+    if (j < 8) ll_update<0>(a, lab, j, inv, nz, prow, nxt);
+    else if (j < 16) ll_update<8>(a, lab, j, inv, nz, prow, nxt);
+    else if (j < 24) ll_update<16>(a, lab, j, inv, nz, prow, nxt);
+    else ll_update<24>(a, lab, j, inv, nz, prow, nxt);
   }
+  // every row to the panel row it stands for
 #pragma unroll
   for (int k = 0; k < kLLRows; ++k)
 #pragma unroll
     for (int c = 0; c < kBaseW; ++c)
-      if (k * kLLThreads < nrow_left && c < w) A[(int64_t)(g0 + k * kLLThreads) + lda * c] = a[k][c];
+      if (lab[k] >= 0 && c < w) A[(int64_t)lab[k] + lda * c] = a[k][c];
 }
 
 // -------------------------------------------------------------- row swaps
@@ -679,6 +670,59 @@ static PhaseProfile& prof() {
   return p;
 }
 
+// HFPX_PROFILE=2: no synchronisation; timing events around every wait of the
+// look-ahead show which stream is on the critical path.  Per step: the main
+// stream's stall waiting for the panel, the panel stream's stall waiting for
+// the next block column, the panel's own duration, and the main stream's
+// work; summary to stderr after each factorisation.
+struct StepTimeline {
+  bool on = false;
+  struct Step {
+    int64_t rest;
+    cudaEvent_t m_idle, m_go, p_idle, p_go, p_done, m_done;
+  };
+  std::vector<Step> steps;
+  void add(int64_t rest) {
+    Step s{rest, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    for (cudaEvent_t* e : {&s.m_idle, &s.m_go, &s.p_idle, &s.p_go, &s.p_done, &s.m_done}) cudaEventCreate(e);
+    steps.push_back(s);
+  }
+  void report() {
+    if (!on || steps.empty()) return;
+    auto el = [](cudaEvent_t a, cudaEvent_t b) {
+      float ms = 0.f;
+      return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? (double)ms : 0.0;
+    };
+    double m_stall = 0, p_stall = 0, panel = 0, main = 0;
+    std::fprintf(stderr, "[hfpx timeline] step rest panel_ms main_ms main_wait_ms panel_wait_ms\n");
+    for (size_t i = 0; i < steps.size(); ++i) {
+      const Step& s = steps[i];
+      const double ms = el(s.m_idle, s.m_go), ps = el(s.p_idle, s.p_go), pd = el(s.p_go, s.p_done),
+                   md = el(s.m_go, s.m_done);
+      m_stall += ms;
+      p_stall += ps;
+      panel += pd;
+      main += md;
+      if (i % std::max<size_t>(1, steps.size() / 8) == 0 || i + 1 == steps.size())
+        std::fprintf(stderr, "[hfpx timeline] %4zu %7lld %8.3f %8.3f %8.3f %8.3f\n", i, (long long)s.rest, pd, md, ms, ps);
+    }
+    std::fprintf(stderr, "[hfpx timeline] total: panel %.1f ms, main %.1f ms, main waiting %.1f ms, panel waiting %.1f ms\n",
+                 panel, main, m_stall, p_stall);
+    for (Step& s : steps)
+      for (cudaEvent_t e : {s.m_idle, s.m_go, s.p_idle, s.p_go, s.p_done, s.m_done}) cudaEventDestroy(e);
+    steps.clear();
+  }
+};
+static StepTimeline& timeline() {
+  static StepTimeline t = [] {
+    StepTimeline q;
+    const char* e = std::getenv("HFPX_PROFILE");
+    q.on = e && *e == '2';
+    return q;
+  }();
+  return t;
+}
+
 // --------------------------------------------------------------- driver
 template <class T>
 struct LuWork {
@@ -889,43 +933,32 @@ template <class T>
 static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, int64_t* info_out) {
   LuWork<T> wk;
   const int G = c->num_sms;
-  std::vector<void*> allocs;
-  auto alloc = [&](size_t bytes) -> void* {
-    void* p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
-    allocs.push_back(p);
-    return p;
-  };
-  wk.sc.cand = (T*)alloc(sizeof(T) * 2 * G * kBaseW);
-  wk.sc.cmax = (double*)alloc(sizeof(double) * 2 * G);
-  wk.sc.cidx = (int*)alloc(sizeof(int) * 2 * G);
-  wk.sc.rowj = (T*)alloc(sizeof(T) * 2 * kBaseW);
-  wk.d_info = (int64_t*)alloc(sizeof(int64_t));
+  // work buffers live in the context and are reused by later factorisations
+  auto alloc = [&](int slot, size_t bytes) -> void* { return ctx_scratch(c, slot, bytes); };
+  wk.sc.cand = (T*)alloc(kScrPanelCand, sizeof(T) * 2 * G * kBaseW);
+  wk.sc.cmax = (double*)alloc(kScrPanelMax, sizeof(double) * 2 * G);
+  wk.sc.cidx = (int*)alloc(kScrPanelIdx, sizeof(int) * 2 * G);
+  wk.sc.rowj = (T*)alloc(kScrPanelRowj, sizeof(T) * 2 * kBaseW);
+  wk.d_info = (int64_t*)alloc(kScrInfo, sizeof(int64_t));
   const int64_t n_blocks = (n + lu_block_size() - 1) / lu_block_size();
-  wk.plan_panel = (int32_t*)alloc(sizeof(int32_t) * kSwapPlanInts);
-  wk.plans = (int32_t*)alloc(sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
+  wk.plan_panel = (int32_t*)alloc(kScrPlanPanel, sizeof(int32_t) * kSwapPlanInts);
+  wk.plans = (int32_t*)alloc(kScrPlans, sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
   const size_t ll_bytes = sizeof(uint64_t) * 2 * kLLMaxCtas * kLLSlot;
   if (sizeof(T) == 4) {
-    wk.ll_slots = (uint64_t*)alloc(ll_bytes);
-    wk.ll_err = (int*)alloc(sizeof(int));
+    wk.ll_slots = (uint64_t*)alloc(kScrLLSlots, ll_bytes);
+    wk.ll_err = (int*)alloc(kScrLLErr, sizeof(int));
     // optional: without room for them the block row takes the triangular solve
     const size_t nb = (size_t)lu_block_size();
-    wk.linv = (T*)alloc(sizeof(T) * nb * nb);
-    wk.a12 = (T*)alloc(sizeof(T) * nb * (size_t)n);
-    if (!wk.linv || !wk.a12) {
-      wk.linv = wk.a12 = nullptr;
-      cudaGetLastError();
-    }
+    wk.linv = (T*)alloc(kScrLinv, sizeof(T) * nb * nb);
+    wk.a12 = (T*)alloc(kScrA12, sizeof(T) * nb * (size_t)n);
+    if (!wk.linv || !wk.a12) wk.linv = wk.a12 = nullptr;
     // optional too: without them the update stays on TF32
     if (fp16_update_enabled()) {
-      wk.l16 = (__half*)alloc(sizeof(__half) * nb * (size_t)n);
-      wk.u16 = (__half*)alloc(sizeof(__half) * nb * (size_t)n);
-      wk.amax = (unsigned*)alloc(sizeof(unsigned));
-      wk.coef = (float*)alloc(2 * sizeof(float));
-      if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) {
-        wk.l16 = wk.u16 = nullptr;
-        cudaGetLastError();
-      }
+      wk.l16 = (__half*)alloc(kScrL16, sizeof(__half) * nb * (size_t)n);
+      wk.u16 = (__half*)alloc(kScrU16, sizeof(__half) * nb * (size_t)n);
+      wk.amax = (unsigned*)alloc(kScrAmax, sizeof(unsigned));
+      wk.coef = (float*)alloc(kScrCoef, 2 * sizeof(float));
+      if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) wk.l16 = wk.u16 = nullptr;
     }
   }
   int rc = 0;
@@ -957,7 +990,15 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   for (int64_t k = 0; k < n && !rc; k += kNb) {
     const int kb = (int)std::min<int64_t>(kNb, n - k);
     T* Akk = A + k + lda * k;
+    StepTimeline& TL = timeline();
+    StepTimeline::Step* ts = nullptr;
+    if (TL.on) {
+      TL.add(n - k - kb);
+      ts = &TL.steps.back();
+      cudaEventRecord(ts->m_idle, M.s);
+    }
     cudaStreamWaitEvent(M.s, ev_panel, 0);
+    if (ts) cudaEventRecord(ts->m_go, M.s);
     // left swaps of panel k, after the step that read those columns last
     cudaStreamWaitEvent(S, ev_panel, 0);
     if (k > 0) cudaStreamWaitEvent(S, ev_rest, 0);
@@ -975,15 +1016,19 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       update_gemm(M, wk, kb, rest, 0, kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * kb, lda);
       P.end(3);
       cudaEventRecord(ev_next, M.s);
+      if (ts) cudaEventRecord(ts->p_idle, Pn.s);
       cudaStreamWaitEvent(Pn.s, ev_next, 0);
+      if (ts) cudaEventRecord(ts->p_go, Pn.s);
       rc = panel_rec(c, Pn, wk, Akk + kb + lda * kb, lda, rest, kn, piv + k + kb, k + kb);
       if (!rc) swap_plan(Pn, piv + k + kb, kn, 0, wk.plans + (size_t)((k + kb) / kNb) * kSwapPlanInts);
+      if (ts) cudaEventRecord(ts->p_done, Pn.s);
       cudaEventRecord(ev_panel, Pn.s);
       if (rc) break;
       P.begin(M.s);
       update_gemm(M, wk, kb, rest, kn, rest - kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * (kb + kn), lda);
       P.end(3);
       cudaEventRecord(ev_rest, M.s);
+      if (ts) cudaEventRecord(ts->m_done, M.s);
     }
     if (!rc) rc = check_cuda(c, cudaGetLastError(), "LU step launch");
   }
@@ -1008,10 +1053,10 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   }
   cudaStreamSynchronize(Pn.s);
   cudaStreamSynchronize(S);
+  timeline().report();
   if (!rc && ll_err) rc = set_error(c, HFPX_ERR_CUDA, "panel pivot exchange timed out");
   for (cudaEvent_t e : {ev_panel, ev_next, ev_rest, ev_left, ev_start})
     if (e) cudaEventDestroy(e);
-  for (void* p : allocs) cudaFree(p);
   *info_out = info;
   if (!rc && info != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "matrix is singular: zero pivot at column " + std::to_string(info));
   return rc;
@@ -1079,17 +1124,20 @@ static int build_perm(hfpx_ctx* c, const hfpx_matrix* m, int32_t** d_perm) {
   if (rc) return rc;
   for (int64_t i = 0; i < m->n; ++i) perm[i] = (int32_t)i;
   for (int64_t i = 0; i < m->n; ++i) std::swap(perm[i], perm[piv[i]]);
-  if (cudaMalloc(d_perm, sizeof(int32_t) * m->n) != cudaSuccess) return set_error(c, HFPX_ERR_NOMEM, "perm");
-  return check_cuda(c, cudaMemcpyAsync(*d_perm, perm.data(), sizeof(int32_t) * m->n, cudaMemcpyHostToDevice, c->stream),
-                    "perm");
+  *d_perm = (int32_t*)ctx_scratch(c, kScrPerm, sizeof(int32_t) * m->n);
+  if (!*d_perm) return set_error(c, HFPX_ERR_NOMEM, "perm");
+  // the host vector goes out of scope: copy synchronously with the stream
+  rc = check_cuda(c, cudaMemcpyAsync(*d_perm, perm.data(), sizeof(int32_t) * m->n, cudaMemcpyHostToDevice, c->stream),
+                  "perm");
+  return rc ? rc : check_cuda(c, cudaStreamSynchronize(c->stream), "perm");
 }
 
 template <class T>
 static int solve_factored(hfpx_ctx* c, const hfpx_matrix* m, const T* LU, T* d_b, int64_t nrhs, int64_t ldb,
                           const int32_t* d_perm) {
   const int64_t n = m->n;
-  T* tmp = nullptr;
-  if (cudaMalloc(&tmp, sizeof(T) * (size_t)ldb * nrhs) != cudaSuccess) return set_error(c, HFPX_ERR_NOMEM, "solve tmp");
+  T* tmp = (T*)ctx_scratch(c, kScrSolveTmp, sizeof(T) * (size_t)ldb * nrhs);
+  if (!tmp) return set_error(c, HFPX_ERR_NOMEM, "solve tmp");
   const int64_t tot = n * nrhs;
   ++g_launches;
   permute_rows_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(d_b, tmp, d_perm, n, nrhs, ldb);
@@ -1106,19 +1154,15 @@ static int solve_factored(hfpx_ctx* c, const hfpx_matrix* m, const T* LU, T* d_b
     cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, (int)nrhs,
                 &one, (const float*)LU, (int)m->ld, (float*)tmp, (int)ldb);
   }
-  int rc = check_cuda(c, cudaMemcpy2DAsync(d_b, ldb * sizeof(T), tmp, ldb * sizeof(T), n * sizeof(T), nrhs,
-                                           cudaMemcpyDeviceToDevice, c->stream),
-                      "solve copy");
-  cudaStreamSynchronize(c->stream);
-  cudaFree(tmp);
-  return rc;
+  return check_cuda(c, cudaMemcpy2DAsync(d_b, ldb * sizeof(T), tmp, ldb * sizeof(T), n * sizeof(T), nrhs,
+                                         cudaMemcpyDeviceToDevice, c->stream),
+                    "solve copy");
 }
 
 int lu_solve_fp64(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb) {
   int32_t* d_perm = nullptr;
   int rc = build_perm(c, m, &d_perm);
   if (!rc) rc = solve_factored<double>(c, m, m->d_a, d_b, nrhs, ldb, d_perm);
-  cudaFree(d_perm);
   return rc;
 }
 
@@ -1126,7 +1170,6 @@ int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, i
   int32_t* d_perm = nullptr;
   int rc = build_perm(c, m, &d_perm);
   if (!rc) rc = solve_factored<float>(c, m, m->d_f, d_b, nrhs, ldb, d_perm);
-  cudaFree(d_perm);
   return rc;
 }
 
@@ -1134,13 +1177,12 @@ int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, i
 int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb, double tol, int max_iter,
                  hfpx_solve_info* info) {
   const int64_t n = m->n;
-  double *x = nullptr, *r = nullptr;
-  float* rf = nullptr;
+  double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * ldb * nrhs);
+  double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * ldb * nrhs);
+  float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * ldb * nrhs);
   int32_t* d_perm = nullptr;
   int rc = 0;
-  if (cudaMalloc(&x, sizeof(double) * ldb * nrhs) != cudaSuccess || cudaMalloc(&r, sizeof(double) * ldb * nrhs) != cudaSuccess ||
-      cudaMalloc(&rf, sizeof(float) * ldb * nrhs) != cudaSuccess)
-    rc = set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
+  if (!x || !r || !rf) rc = set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
   if (!rc) rc = build_perm(c, m, &d_perm);
   std::vector<double> bnorm(nrhs, 0.0), rnorm(nrhs, 0.0);
   const int64_t tot = n * nrhs;
@@ -1190,10 +1232,6 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
     info->residual = worst;
     info->converged = worst <= tol;
   }
-  cudaFree(x);
-  cudaFree(r);
-  cudaFree(rf);
-  cudaFree(d_perm);
   if (!rc && !(worst <= tol)) rc = set_error(c, HFPX_ERR_NOT_CONVERGED, "refinement did not reach the tolerance");
   return rc;
 }
