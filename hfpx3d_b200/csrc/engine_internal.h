@@ -52,7 +52,7 @@ void* ctx_scratch(hfpx_ctx* c, int slot, size_t bytes);
 enum : int {
   kScrPanelCand, kScrPanelMax, kScrPanelIdx, kScrPanelRowj, kScrInfo, kScrPlanPanel, kScrPlans, kScrLLSlots,
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
-  kScrRefR, kScrRefRf, kScrDof, kScrCount
+  kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrCount
 };
 
 // assembly.cu

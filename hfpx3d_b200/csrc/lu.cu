@@ -270,10 +270,12 @@ __device__ __forceinline__ void ll_row_to_smem(const float (&a)[kLLRows][kBaseW]
   }
 }
 
+// piv[j] = pivot row + piv_add; left/right: columns of the enclosing block
+// panel on either side that take the interchanges too (see the end).
 __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
     uint64_t* __restrict__ slots, int64_t* __restrict__ info, int64_t col_offset, uint32_t tag0,
-    int* __restrict__ err) {
+    int* __restrict__ err, int left, int right, float* __restrict__ xtmp, int piv_add) {
   // arg-max candidates travel as keys: |a| bits + 1 (non-negative floats
   // order as their bits), 0 for "no row"; ties go to the lower row
   __shared__ float s_cand[2][kLLMaxCtas][kBaseW];
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const int p = (int)pu;
     const float* prow = s_cand[buf][__reduce_max_sync(0xffffffffu, (gk == gmax && gi == pu) ? gq : 0u)];
     if (b == 0 && tid == 0) {
-      piv[j] = p;
+      piv[j] = p + piv_add;
       if (gmax == 1u && info && *info == 0) *info = col_offset + j + 1;  // |pivot| == 0
     }
     // interchange rows j and p: swap the labels
@@ -421,6 +423,66 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
 #pragma unroll
     for (int c = 0; c < kBaseW; ++c)
       if (lab[k] >= 0 && c < w) A[(int64_t)lab[k] + lda * c] = a[k][c];
+  if (left + right == 0) return;
+  // The same interchanges on the enclosing block panel's other columns
+  // (left: [-left, 0), right: [w, w + right)), in place of the row swaps a
+  // recursive panel makes between its halves.  A moved row's old values go to
+  // xtmp first, at slot = its final label if < w, else w + its first row
+  // (a row starting at w or below only ever moves to a label < w, so the
+  // slots are distinct); then a barrier over the CTAs; then to the final row.
+  __shared__ int s_nmv;
+  __shared__ int s_src[2 * kBaseW], s_dst[2 * kBaseW], s_slot[2 * kBaseW];
+  if (tid == 0) s_nmv = 0;
+  __syncthreads();
+  if (!s_fail) {
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+      const int phys = g0 + k * kLLThreads;
+      if (lab[k] >= 0 && lab[k] != phys) {
+        const int q = atomicAdd(&s_nmv, 1);
+        s_src[q] = phys;
+        s_dst[q] = lab[k];
+        s_slot[q] = lab[k] < w ? lab[k] : w + phys;
+      }
+    }
+  }
+  __syncthreads();
+  const int nmv = s_nmv, ncol = left + right;
+  for (int i = tid; i < nmv * ncol; i += kLLThreads) {
+    const int q = i / ncol, cc = i - q * ncol;
+    const int64_t col = cc < left ? (int64_t)(cc - left) : (int64_t)(w + cc - left);
+    xtmp[(size_t)s_slot[q] * ncol + cc] = A[(int64_t)s_src[q] + lda * col];
+  }
+  // barrier: each CTA publishes one word with tag tag0 + 63 after its copies
+  // (release fence), every CTA waits for all (acquire fence after)
+  __syncthreads();
+  uint64_t* bar = slots + (size_t)2 * kLLMaxCtas * kLLSlot;
+  const uint32_t btag = tag0 + 63u;
+  if (tid == 0) {
+    __threadfence();
+    ll_store(bar + b, 0u, btag);
+  }
+  if (tid < G) {
+    const uint64_t t0 = global_ns();
+    while ((uint32_t)(ll_load(bar + tid) >> 32) != btag) {
+      if (global_ns() - t0 > kLLTimeoutNs) {
+        s_fail = 1;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  __threadfence();
+  for (int i = tid; i < nmv * ncol; i += kLLThreads) {
+    const int q = i / ncol, cc = i - q * ncol;
+    const int64_t col = cc < left ? (int64_t)(cc - left) : (int64_t)(w + cc - left);
+    A[(int64_t)s_dst[q] + lda * col] = xtmp[(size_t)s_slot[q] * ncol + cc];
+  }
 }
 
 // -------------------------------------------------------------- row swaps
@@ -711,6 +773,7 @@ struct StepTimeline {
     for (Step& s : steps)
       for (cudaEvent_t e : {s.m_idle, s.m_go, s.p_idle, s.p_go, s.p_done, s.m_done}) cudaEventDestroy(e);
     steps.clear();
+    cudaGetLastError();  // elapsed times of the last step's unrecorded events
   }
 };
 static StepTimeline& timeline() {
@@ -748,6 +811,28 @@ struct LuWork {
   __half* u16 = nullptr;
   unsigned* amax = nullptr;
   float* coef = nullptr;
+  // moved rows of one base panel across the block panel: [2 kBaseW][nb]
+  float* xtmp = nullptr;
+};
+
+// HFPX_LU_PANEL=smem selects the shared-memory panel kernel for FP32 too.
+static bool ll_panel_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_LU_PANEL");
+    return !(e && std::string(e) == "smem");
+  }();
+  return on;
+}
+
+// The register-resident panel takes m rows.
+template <class T>
+static bool ll_fits(const LuWork<T>& wk, int64_t m) {
+  return sizeof(T) == 4 && wk.ll_slots && (m + kLLCap - 1) / kLLCap <= kLLMaxCtas && ll_panel_enabled();
+}
+
+struct PanelSpan {
+  int c0 = 0, bw = 0;
+  bool eager = false;
 };
 
 __global__ void identity_kernel(float* a, int n) {
@@ -804,15 +889,6 @@ static void update_gemm(Lane l, LuWork<T>& wk, int kb, int64_t rest, int64_t c0,
   gemm_sub(l, rest, nc, kb, L21, lda, U12 + lda * c0, lda, C, lda);
 }
 
-// HFPX_LU_PANEL=smem selects the shared-memory panel kernel for FP32 too.
-static bool ll_panel_enabled() {
-  static const bool on = [] {
-    const char* e = std::getenv("HFPX_LU_PANEL");
-    return !(e && std::string(e) == "smem");
-  }();
-  return on;
-}
-
 // CTAs for a panel of m rows: enough for the panel to fit in shared memory,
 // at least kPanelCtas when there are rows for them, never more than the SMs.
 // Fewer CTAs than SMs leave room for the trailing update running beside it
@@ -830,14 +906,15 @@ static int panel_ctas(hfpx_ctx* c, int64_t m, int w) {
 
 template <class T>
 static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
-                      int64_t col_offset) {
+                      int64_t col_offset, const PanelSpan& sp) {
   if constexpr (sizeof(T) == 4) {
-    const int64_t g_ll = (m + kLLCap - 1) / kLLCap;
-    if (wk.ll_slots && g_ll <= kLLMaxCtas && ll_panel_enabled()) {
-      int G = (int)g_ll;
+    if (ll_fits(wk, m)) {
+      int G = (int)((m + kLLCap - 1) / kLLCap);
       int rpc = (int)((m + G - 1) / G);
       uint32_t tag0 = (++wk.ll_launches) << 6;
-      void* args[] = {&A, &lda, &m, &w, &rpc, &piv, &wk.ll_slots, &wk.d_info, &col_offset, &tag0, &wk.ll_err};
+      int left = sp.eager ? sp.c0 : 0, right = sp.eager ? sp.bw - sp.c0 - w : 0, piv_add = sp.eager ? sp.c0 : 0;
+      void* args[] = {&A,  &lda,       &m,           &w,    &rpc,  &piv,    &wk.ll_slots, &wk.d_info,
+                      &col_offset, &tag0, &wk.ll_err, &left, &right, &wk.xtmp, &piv_add};
       ++g_launches;
       return check_cuda(c, cudaLaunchCooperativeKernel((void*)panel_ll_kernel, dim3(G), dim3(kLLThreads), args, 0, l.s),
                         "panel_ll_kernel launch");
@@ -884,37 +961,54 @@ static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, int32_t* piv, int k,
 }
 
 // dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
+// sp.c0: column (and row) offset of this sub-panel inside its block panel of
+// sp.bw columns.  sp.eager: every base panel applies its own interchanges to
+// the whole block panel, so the recursion swaps nothing between its halves.
 template <class T>
 static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
-                     int64_t col_offset) {
+                     int64_t col_offset, PanelSpan sp) {
   PhaseProfile& P = prof();
   if (w <= kBaseW) {
     P.begin(l.s);
-    const int rc = panel_base(c, l, wk, A, lda, m, w, piv, col_offset);
+    const int rc = panel_base(c, l, wk, A, lda, m, w, piv, col_offset, sp);
     P.end(0);
     return rc;
   }
   // left half rounded up to whole base panels (768 -> 384 -> 192 -> 96 ->
   // 64 + 32), so every base panel but a ragged last one is 32 wide
   const int w1 = (w / 2 + kBaseW - 1) / kBaseW * kBaseW, w2 = w - w1;
-  int rc = panel_rec(c, l, wk, A, lda, m, w1, piv, col_offset);
+  int rc = panel_rec(c, l, wk, A, lda, m, w1, piv, col_offset, sp);
   if (rc) return rc;
   P.begin(l.s);
-  laswp(l, A + lda * w1, lda, w2, piv, w1, 0, wk.plan_panel);
+  if (!sp.eager) laswp(l, A + lda * w1, lda, w2, piv, w1, 0, wk.plan_panel);
   P.end(1);
   trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
   P.end(2);
   gemm_sub(l, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
   P.end(3);
-  rc = panel_rec(c, l, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1);
+  PanelSpan sr = sp;
+  sr.c0 += w1;
+  rc = panel_rec(c, l, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1, sr);
   if (rc) return rc;
-  P.begin(l.s);
-  // the right half's interchanges on the left half's columns; its pivots
-  // become relative to this panel's top
-  swap_plan(l, piv + w1, w2, 0, wk.plan_panel, w1);
-  swap_apply(l, A + w1, lda, w1, wk.plan_panel);
-  P.end(1);
+  if (!sp.eager) {
+    P.begin(l.s);
+    // the right half's interchanges on the left half's columns; its pivots
+    // become relative to this panel's top
+    swap_plan(l, piv + w1, w2, 0, wk.plan_panel, w1);
+    swap_apply(l, A + w1, lda, w1, wk.plan_panel);
+    P.end(1);
+  }
   return 0;
+}
+
+// Factor block panel [0, w) of A (m rows), pivots relative to its top.
+template <class T>
+static int block_panel(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int64_t m, int w, int32_t* piv,
+                       int64_t col_offset) {
+  PanelSpan sp;
+  sp.bw = w;
+  sp.eager = wk.xtmp != nullptr && ll_fits(wk, m);
+  return panel_rec(c, l, wk, A, lda, m, w, piv, col_offset, sp);
 }
 
 // Pivots of block b are relative to the block's first row until the end.
@@ -943,12 +1037,14 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   const int64_t n_blocks = (n + lu_block_size() - 1) / lu_block_size();
   wk.plan_panel = (int32_t*)alloc(kScrPlanPanel, sizeof(int32_t) * kSwapPlanInts);
   wk.plans = (int32_t*)alloc(kScrPlans, sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
-  const size_t ll_bytes = sizeof(uint64_t) * 2 * kLLMaxCtas * kLLSlot;
+  // two column buffers of per-CTA words, then one barrier word per CTA
+  const size_t ll_bytes = sizeof(uint64_t) * (2 * kLLMaxCtas * kLLSlot + kLLMaxCtas);
   if (sizeof(T) == 4) {
     wk.ll_slots = (uint64_t*)alloc(kScrLLSlots, ll_bytes);
     wk.ll_err = (int*)alloc(kScrLLErr, sizeof(int));
     // optional: without room for them the block row takes the triangular solve
     const size_t nb = (size_t)lu_block_size();
+    wk.xtmp = (float*)alloc(kScrXtmp, sizeof(float) * 2 * kBaseW * nb);
     wk.linv = (T*)alloc(kScrLinv, sizeof(T) * nb * nb);
     wk.a12 = (T*)alloc(kScrA12, sizeof(T) * nb * (size_t)n);
     if (!wk.linv || !wk.a12) wk.linv = wk.a12 = nullptr;
@@ -983,7 +1079,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     cudaStreamWaitEvent(Pn.s, ev_start, 0);
     cudaStreamWaitEvent(S, ev_start, 0);
     const int kb0 = (int)std::min<int64_t>(kNb, n);
-    rc = panel_rec(c, Pn, wk, A, lda, n, kb0, piv, 0);
+    rc = block_panel(c, Pn, wk, A, lda, n, kb0, piv, 0);
     if (!rc) swap_plan(Pn, piv, kb0, 0, wk.plans);
     cudaEventRecord(ev_panel, Pn.s);
   }
@@ -1019,7 +1115,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       if (ts) cudaEventRecord(ts->p_idle, Pn.s);
       cudaStreamWaitEvent(Pn.s, ev_next, 0);
       if (ts) cudaEventRecord(ts->p_go, Pn.s);
-      rc = panel_rec(c, Pn, wk, Akk + kb + lda * kb, lda, rest, kn, piv + k + kb, k + kb);
+      rc = block_panel(c, Pn, wk, Akk + kb + lda * kb, lda, rest, kn, piv + k + kb, k + kb);
       if (!rc) swap_plan(Pn, piv + k + kb, kn, 0, wk.plans + (size_t)((k + kb) / kNb) * kSwapPlanInts);
       if (ts) cudaEventRecord(ts->p_done, Pn.s);
       cudaEventRecord(ev_panel, Pn.s);
