@@ -43,11 +43,18 @@ UNIT = 's'
 
 
 def peaks():
+    """(HBM GB/s, dense BF16/FP16 tensor TFLOP/s sustained, source)."""
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get('hbm_gbs', 6650.0), 'measured'
-    return 6650.0, 'fallback'
+        return d.get('hbm_gbs', 6650.0), d.get('bf16_tflops_sustained', 1400.0), 'measured'
+    return 6650.0, 1400.0, 'fallback'
+
+
+# DRAM bytes per matrix entry written by the in-plane assembly kernel, from
+# the ncu capture of profiles/assemble_kernel_penny1000.md (3.4297 GB for an
+# 18 000 x 18 000 fill; traffic grows with the entries, so it scales by N^2)
+ASM_DRAM_BYTES_PER_ENTRY = 3.429715e9 / 18000 ** 2
 
 
 class Clocks:
@@ -98,6 +105,19 @@ class Clocks:
 def workload(n_el, seed=2026):
     from hfpx3d_b200 import meshgen
     return meshgen.penny(n_el, seed=seed)
+
+
+def replica_max(x, world, local_rank):
+    """Max of x over the replicas: every rank's time, so the job's time is the
+    slowest replica's (NCCL on the GPUs; gloo when the group runs on CPU)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = 'cpu' if dist.get_backend() == 'gloo' else f'cuda:{local_rank}'
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 # ---------------------------------------------------------------- engine arm
@@ -166,10 +186,7 @@ def run_engine(args, rank, world, local_rank):
     ms = total_ms / args.steps
     x_main = d_x.cpu().numpy()
     res_main, iters_main = info.residual, info.iterations
-    if world > 1:
-        t = torch.tensor([ms], device=f'cuda:{local_rank}')
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replica_max(ms, world, local_rank)
 
     # the other precision, once, for the speed-up and the opening error
     other_s, rel_err = None, None
@@ -191,9 +208,11 @@ def run_engine(args, rank, world, local_rank):
 
     if rank != 0:
         return None
-    hbm, peak_src = peaks()
+    hbm, tensor_peak, peak_src = peaks()
     asm_ms = statistics.mean(t_asm)
+    fac_ms = statistics.mean(t_fac)
     bytes_asm = float(n) * n * 8
+    flops_lu = 2.0 / 3.0 * float(n) ** 3
     line = {
         'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
@@ -208,10 +227,19 @@ def run_engine(args, rank, world, local_rank):
         'refinement': {'iterations': iters_main, 'residual': res_main},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,
-        'roofline': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
-                     'achieved': bytes_asm / (asm_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
-                     'frac': bytes_asm / (asm_ms / 1e3) / 1e9 / hbm, 'traffic': None,
-                     'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm},
+        # the factorisation is ~80 % of the step: 2/3 N^3 flop over its CUDA-event time on the
+        # engine's stream, against the sustained dense tensor peak (the FP16 update and the
+        # BF16 GEMM of the peak run on the same pipe); the panel chain keeps it latency-bound
+        'roofline': {'kernel': 'LU factorisation (panel_ll_kernel chain + FP16/TF32 tensor-core updates)',
+                     'bound': 'tensor', 'achieved': flops_lu / (fac_ms / 1e3) / 1e12, 'peak': tensor_peak,
+                     'unit': 'TFLOP/s', 'frac': flops_lu / (fac_ms / 1e3) / 1e12 / tensor_peak,
+                     'traffic': None, 'peak_source': f'{peak_src} bf16_tflops_sustained',
+                     'algorithmic_flops': flops_lu},
+        'roofline_assembly': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
+                              'achieved': bytes_asm / (asm_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
+                              'frac': bytes_asm / (asm_ms / 1e3) / 1e9 / hbm,
+                              'traffic': ASM_DRAM_BYTES_PER_ENTRY * float(n) * n,
+                              'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm},
         'gpu_launches': int(launches),
         'clocks': clk.summary(),
         'e2e': e2e,

@@ -2,18 +2,19 @@
 // il/linear_algebra/dense/factorization/LU.h:79-120) and the mixed-precision
 // solve.
 //
-// Blocked right-looking LU, block nb = 256:
-//   panel  (n-k) x nb : recursive halving; the <=32-column base case is one
-//          cooperative kernel that keeps the whole tall panel resident in the
-//          shared memory of all SMs (one CTA per SM) and takes one grid
-//          barrier per column: local arg-max + candidate row -> barrier ->
-//          every CTA picks the same pivot, swaps, scales and updates its rows.
-//   swaps  applied to the columns left and right of the panel;
-//   U12 = L11^-1 A12 (triangular solve), A22 -= L21 U12 (trailing update).
+// Blocked right-looking LU, block nb = 768 (HFPX_LU_NB), depth-1 look-ahead:
+//   panel  (n-k) x nb : recursive halving (dgetrf2 order); the <=32-column
+//          base case is one cooperative kernel: for FP32 the rows sit in
+//          registers and the pivot search is exchanged through L2 words
+//          (panel_ll_kernel), for FP64 the panel sits in shared memory with
+//          one grid barrier per column (panel_base_kernel);
+//   swaps  applied to the columns left and right of the panel as gathers;
+//   U12 = L11^-1 A12, A22 -= L21 U12 (trailing update).
 // FP64 mode factors the FP64 matrix in place (trailing update and triangular
 // solves: cuBLAS FP64, i.e. FP64 tensor cores).  Mixed mode factors an FP32
-// copy with TF32 tensor-core trailing updates and recovers FP64 accuracy by
-// iterative refinement against the untouched FP64 matrix.
+// copy (U12 by an inverse-L11 TF32 GEMM, FP16 tensor-core trailing updates
+// with FP32 accumulation) and recovers FP64 accuracy by iterative refinement
+// against the untouched FP64 matrix.
 #include <cooperative_groups.h>
 #include <cublas_v2.h>
 #include <cuda_fp16.h>

@@ -158,5 +158,13 @@ Array2D<double> load_crd_from_csv(const std::string& dir, const std::string& f);
 Array2D<double> load_crd_from_numpy(const std::string& dir, const std::string& f);
 // precision 0: the reference's default stream precision (6 significant digits)
 bool save_data_to_csv(const Array2D<double>& a, const std::string& dir, const std::string& name, int precision = 0);
+// NumPy .npy (format 1.0, Fortran order), float32 (bits 32) or float64 (64):
+// the npy32/npy64 output formats the reference's driver leaves unwritten
+// (main.cpp:131-136, 218-222, 271-275).
+bool save_data_to_npy(const Array2D<double>& a, const std::string& dir, const std::string& name, int bits);
+// save_data_to_npy for output_format "npy32"/"npy64" (".csv" in name becomes
+// ".npy"), else save_data_to_csv; returns the file name written.
+std::string save_output(const Array2D<double>& a, const IO_param_T& io, const std::string& name, int precision,
+                        bool* ok);
 
 }  // namespace hfpx

@@ -427,4 +427,48 @@ bool save_data_to_csv(const Array2D<double>& a, const std::string& dir, const st
   return true;
 }
 
+bool save_data_to_npy(const Array2D<double>& a, const std::string& dir, const std::string& name, int bits) {
+  std::string p = dir;
+  if (p.empty() || p.back() != '/') p += '/';
+  p += name;
+  std::ofstream o(p, std::ios::binary);
+  if (!o) {
+    std::cout << "Can't open the file (" << p << ")" << std::endl;
+    return false;
+  }
+  std::string hdr = std::string("{'descr': '") + (bits == 32 ? "<f4" : "<f8") +
+                    "', 'fortran_order': True, 'shape': (" + std::to_string(a.size(0)) + ", " +
+                    std::to_string(a.size(1)) + "), }";
+  // magic (6) + version (2) + length (2) + header, padded with spaces to a
+  // multiple of 64 bytes and ended by a newline
+  const size_t total = ((10 + hdr.size() + 1 + 63) / 64) * 64;
+  hdr.append(total - 10 - hdr.size() - 1, ' ');
+  hdr.push_back('\n');
+  const uint16_t hlen = (uint16_t)hdr.size();
+  o.write("\x93NUMPY\x01\x00", 8);
+  o.write(reinterpret_cast<const char*>(&hlen), 2);
+  o.write(hdr.data(), (std::streamsize)hdr.size());
+  const size_t n = (size_t)(a.size(0) * a.size(1));
+  if (bits == 32) {
+    std::vector<float> f(n);
+    for (size_t i = 0; i < n; ++i) f[i] = (float)a.data()[i];
+    o.write(reinterpret_cast<const char*>(f.data()), (std::streamsize)(n * sizeof(float)));
+  } else {
+    o.write(reinterpret_cast<const char*>(a.data()), (std::streamsize)(n * sizeof(double)));
+  }
+  return (bool)o;
+}
+
+std::string save_output(const Array2D<double>& a, const IO_param_T& io, const std::string& name, int precision,
+                        bool* ok) {
+  if (io.out_f_format == "npy32" || io.out_f_format == "npy64") {
+    std::string f = name;
+    if (f.size() >= 4 && f.compare(f.size() - 4, 4, ".csv") == 0) f.replace(f.size() - 4, 4, ".npy");
+    *ok = save_data_to_npy(a, io.output_dir, f, io.out_f_format == "npy32" ? 32 : 64);
+    return f;
+  }
+  *ok = save_data_to_csv(a, io.output_dir, name, precision);
+  return name;
+}
+
 }  // namespace hfpx

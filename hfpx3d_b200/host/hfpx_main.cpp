@@ -12,6 +12,8 @@
 // (precision = "fp64" | "mixed"), the refinement tolerance of the mixed mode
 // (refine_tol = 1e-12) and csv output with 17 significant digits
 // (full_precision_output = true) in place of the reference's 6.
+// output_format = "npy32" | "npy64" writes .npy files, which the reference's
+// driver leaves unwritten.
 #include <chrono>
 #include <iostream>
 
@@ -79,8 +81,9 @@ int main(int argc, char* argv[]) {
     std::cout << 18 * ne - md.dof_h_dd.n_dof << " Fixed DoF" << std::endl;
 
     if (sim.do_save_matrix) {
-      const bool ok = save_data_to_csv(a->download(), io.output_dir, io.matr_f_name, prec);
-      if (ok) std::cout << "Matrix saved to " << io.output_dir << "/" << io.matr_f_name << std::endl;
+      bool ok = false;
+      const std::string f = save_output(a->download(), io, io.matr_f_name, prec, &ok);
+      if (ok) std::cout << "Matrix saved to " << io.output_dir << "/" << f << std::endl;
       else std::cout << "Cannot save the matrix" << std::endl;
     }
 
@@ -113,8 +116,9 @@ int main(int argc, char* argv[]) {
         for (int k = 0; k < 6; ++k)
           for (int l = 0; l < 3; ++l) out(6 * j + k, l + 4) = md.dd(6 * j + k, l);
       }
-      const bool ok = save_data_to_csv(out, io.output_dir, io.out_f_name, prec);
-      if (ok) std::cout << "Solution (nodes + DD) saved to " << io.output_dir << "/" << io.out_f_name << std::endl;
+      bool ok = false;
+      const std::string f = save_output(out, io, io.out_f_name, prec, &ok);
+      if (ok) std::cout << "Solution (nodes + DD) saved to " << io.output_dir << "/" << f << std::endl;
       else std::cout << "Cannot save the solution" << std::endl;
     }
 
@@ -127,8 +131,9 @@ int main(int argc, char* argv[]) {
       t0 = std::chrono::steady_clock::now();
       const Array2D<double> s = make_3dbem_stress_f_s(props.shear_m, props.poiss_r, dmesh, md, load, np, pts);
       std::cout << ": " << seconds_since(t0) << "s" << std::endl;
-      const bool ok = save_data_to_csv(s, io.output_dir, io.strs_f_name, prec);
-      if (ok) std::cout << "Stresses at given points saved to " << io.output_dir << "/" << io.strs_f_name << std::endl;
+      bool ok = false;
+      const std::string f = save_output(s, io, io.strs_f_name, prec, &ok);
+      if (ok) std::cout << "Stresses at given points saved to " << io.output_dir << "/" << f << std::endl;
       else std::cout << "Cannot save the stresses" << std::endl;
     }
   } catch (const Error& e) {

@@ -178,3 +178,23 @@ def test_driver_default_output_precision(tmp_path, driver):
     assert max(len(d) for d in digits) == 6
     sol = np.loadtxt(tmp_path / 'Out' / 'test_solution.csv', delimiter=',')
     assert np.abs(sol[:, 4:] - g['dd']).max() / np.abs(g['dd']).max() < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('fmt,tol', [('npy64', 1e-10), ('npy32', 1e-6)])
+def test_driver_npy_output(tmp_path, driver, fmt, tol):
+    # npy32/npy64 outputs (left unwritten by the reference's driver); with
+    # these formats the observation points are read as .npy, as there
+    g = golden('ref_p24')
+    extra = ('do_save_solution = true\ndo_postprocess = true\nobserv_crd_fname = "pts.npy"\n'
+             'output_format = "%s"\nfix_tip = %d\nPoisson_ratio = 0.35\n' % (fmt, int(g['tip'])))
+    cfg = write_case(tmp_path, g['nods'], g['conn'], extra, s_cfg=s_config(g['s_inf']))
+    np.save(tmp_path / 'Mesh_Files' / 'pts.npy', np.asfortranarray(g['pts']))
+    r = subprocess.run([driver, str(cfg)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert 'test_solution.npy' in r.stdout and 'test_stresses.npy' in r.stdout
+    sol = np.load(tmp_path / 'Out' / 'test_solution.npy')
+    assert sol.dtype == (np.float32 if fmt == 'npy32' else np.float64) and sol.shape == (144, 7)
+    assert np.abs(sol[:, 4:] - g['dd']).max() / np.abs(g['dd']).max() < tol
+    st = np.load(tmp_path / 'Out' / 'test_stresses.npy')
+    assert np.abs(st - g['stress']).max() / np.abs(g['stress']).max() < max(tol, 1e-9)
