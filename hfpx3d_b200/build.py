@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 OUT = os.path.join(HERE, 'libhfpx_engine.so')
 HOST_LIB = os.path.join(HERE, 'libhfpx_host.so')
 MAIN = os.path.join(HERE, 'bin', 'hfpx_main')
-SOURCES = ['engine.cu', 'assembly.cu', 'lu.cu']
+SOURCES = ['engine.cu', 'assembly.cu', 'lu.cu', 'solve.cu']
 CUDA = os.environ.get('CUDA_HOME', '/usr/local/cuda')
 NVCC = os.path.join(CUDA, 'bin', 'nvcc')
 CXX = os.environ.get('CXX', 'g++')

@@ -339,6 +339,7 @@ int hfpx_matrix_destroy(hfpx_matrix* m) {
   if (!m) return HFPX_OK;
   if (m->d_a) cudaFree(m->d_a);
   if (m->d_f) cudaFree(m->d_f);
+  if (m->d_dinv) cudaFree(m->d_dinv);
   if (m->d_piv) cudaFree(m->d_piv);
   delete m;
   return HFPX_OK;

@@ -20,9 +20,14 @@ struct hfpx_ctx {
   int* d_flags = nullptr;          // device status words (see kernels)
   // device work buffers kept between calls (grown on demand, freed with the
   // context), so repeated factorisations and solves allocate nothing
-  static constexpr int kScratchSlots = 24;
+  static constexpr int kScratchSlots = 28;
   void* scratch[kScratchSlots] = {};
   size_t scratch_bytes[kScratchSlots] = {};
+  // tile triangular solves: tiles the flag array covers, epoch of the last
+  // solve, tickets handed out so far
+  int64_t trsv_cap = 0;
+  int trsv_epoch = 0;
+  unsigned long long trsv_base = 0;
 };
 
 struct hfpx_mesh {
@@ -37,6 +42,10 @@ struct hfpx_matrix {
   int32_t* d_piv = nullptr;        // pivots (0-based global rows), n
   int factored = 0;                // 0 none, 1 fp64 in place, 2 fp32 copy
   int64_t info = 0;
+  // inverses of the FP32 factors' 128 x 128 diagonal blocks (L, then U),
+  // made by the first single-right-hand-side solve after a factorisation
+  mutable float* d_dinv = nullptr;
+  mutable int dinv_valid = 0;
 };
 
 namespace hfpx {
@@ -52,7 +61,8 @@ void* ctx_scratch(hfpx_ctx* c, int slot, size_t bytes);
 enum : int {
   kScrPanelCand, kScrPanelMax, kScrPanelIdx, kScrPanelRowj, kScrInfo, kScrPlanPanel, kScrPlans, kScrLLSlots,
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
-  kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrCount
+  kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
+  kScrTrsvErr, kScrCount
 };
 
 // assembly.cu
@@ -83,4 +93,14 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
                  double tol, int max_iter, hfpx_solve_info* info);
 int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
                             int64_t* info);
+
+// solve.cu: one right-hand side of the refinement
+int trsv_tiles(int64_t n);
+int tri_inverses(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, float* dinv_lower, float* dinv_upper);
+int trsv_f32(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const float* dinv, float* x, bool upper);
+int trsv_status(hfpx_ctx* c);
+int resid_chunks(int64_t n);
+int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
+                 double* part, unsigned long long* d_max);
+int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max);
 }  // namespace hfpx

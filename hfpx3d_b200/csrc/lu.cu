@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 #include "engine_internal.h"
 
@@ -1183,6 +1184,7 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
   int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info);
   set_math(c, CUBLAS_DEFAULT_MATH);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
+  m->dinv_valid = 0;
   return rc;
 }
 
@@ -1270,9 +1272,114 @@ int lu_solve_fp32(hfpx_ctx* c, const hfpx_matrix* m, float* d_b, int64_t nrhs, i
   return rc;
 }
 
+// HFPX_SOLVE=cublas keeps the single right-hand side on cuBLAS solves.
+static bool own_solve_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_SOLVE");
+    return !(e && std::string(e) == "cublas");
+  }();
+  return on;
+}
+
+// The single right-hand side uses the engine's tile-sweep triangular solves
+// (solve.cu: 5.9-6.1 ms per triangle at N = 72 000, a little under cuBLAS);
+// HFPX_TRSV=cublas selects cuBLAS instead.
+static bool own_trsv_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_TRSV");
+    return !(e && std::string(e) == "cublas");
+  }();
+  return on;
+}
+
+// One right-hand side: the engine's residual (solve.cu; |r|_inf comes back
+// as one 8-byte copy per step) and triangular solves.
+static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int max_iter, hfpx_solve_info* info) {
+  const int64_t n = m->n;
+  double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * n);
+  double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * n);
+  float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * n);
+  float* y = (float*)ctx_scratch(c, kScrSolveTmp, sizeof(float) * n);
+  double* part = (double*)ctx_scratch(c, kScrResidPart, sizeof(double) * n * resid_chunks(n));
+  unsigned long long* dmax = (unsigned long long*)ctx_scratch(c, kScrResidMax, sizeof(unsigned long long));
+  if (!x || !r || !rf || !y || !part || !dmax) return set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
+  int32_t* d_perm = nullptr;
+  int rc = build_perm(c, m, &d_perm);
+  if (rc) return rc;
+  auto read_max = [&](double* v) {
+    unsigned long long bits = 0;
+    int e = check_cuda(c, cudaMemcpyAsync(&bits, dmax, sizeof(bits), cudaMemcpyDeviceToHost, c->stream), "max");
+    if (!e) e = check_cuda(c, cudaStreamSynchronize(c->stream), "max");
+    std::memcpy(v, &bits, sizeof(double));
+    return e;
+  };
+  double bnorm = 0.0, worst = INFINITY;
+  rc = absmax_f64(c, d_b, n, dmax);
+  if (!rc) rc = read_max(&bnorm);
+  if (!(bnorm > 0.0)) bnorm = 1.0;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  int it = 0;
+  if (!rc) {
+    cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream);
+    cudaMemcpyAsync(r, d_b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+    for (it = 1; it <= max_iter; ++it) {
+      ++g_launches;
+      d2f_kernel<<<nb, 256, 0, c->stream>>>(r, rf, n, 1, n, n);
+      ++g_launches;
+      permute_rows_kernel<float><<<nb, 256, 0, c->stream>>>(rf, y, d_perm, n, 1, n);
+      if (own_trsv_enabled()) {
+        const size_t blk = (size_t)trsv_tiles(n) * 128 * 128;
+        if (!m->dinv_valid) {
+          if (!m->d_dinv && cudaMalloc(&m->d_dinv, sizeof(float) * 2 * blk) != cudaSuccess) {
+            m->d_dinv = nullptr;
+            cudaGetLastError();
+            rc = set_error(c, HFPX_ERR_NOMEM, "diagonal block inverses");
+            break;
+          }
+          rc = tri_inverses(c, m->d_f, m->ld, n, m->d_dinv, m->d_dinv + blk);
+          if (rc) break;
+          m->dinv_valid = 1;
+        }
+        rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv, y, false);
+        if (!rc) rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv + blk, y, true);
+      } else {
+        // cuBLAS strsm with one column measured faster than strsv here
+        const float one = 1.f;
+        cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+        cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)n, 1, &one,
+                    m->d_f, (int)m->ld, y, (int)n);
+        cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
+                    m->d_f, (int)m->ld, y, (int)n);
+      }
+      if (rc) break;
+      ++g_launches;
+      axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(y, x, n, 1, n, n);
+      rc = residual_f64(c, m->d_a, m->ld, n, x, d_b, r, part, dmax);
+      double rmax = 0.0;
+      if (!rc) rc = read_max(&rmax);
+      if (rc) break;
+      worst = rmax / bnorm;
+      if (worst <= tol) break;
+    }
+  }
+  if (!rc) rc = trsv_status(c);
+  if (!rc) {
+    cudaMemcpyAsync(d_b, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+    rc = check_cuda(c, cudaStreamSynchronize(c->stream), "refinement");
+  }
+  if (info) {
+    info->iterations = std::min(it, max_iter);
+    info->residual = worst;
+    info->converged = worst <= tol;
+  }
+  if (!rc && !(worst <= tol)) rc = set_error(c, HFPX_ERR_NOT_CONVERGED, "refinement did not reach the tolerance");
+  return rc;
+}
+
 // Iterative refinement: x += LU32^-1 r, r = b - A x in FP64.
 int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb, double tol, int max_iter,
                  hfpx_solve_info* info) {
+  if (nrhs == 1 && own_solve_enabled()) return refine_one(c, m, d_b, tol, max_iter, info);
   const int64_t n = m->n;
   double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * ldb * nrhs);
   double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * ldb * nrhs);

@@ -1,0 +1,381 @@
+// The mixed-precision refinement's memory-bound pieces, one right-hand side:
+//   * triangular solves with the FP32 factors (forward with unit L, backward
+//     with U) as one persistent sweep over 128-row tiles;
+//   * the FP64 residual r = b - A x and its largest magnitude.
+// Both replace cuBLAS calls of the refinement (dgetrs-style solve at
+// il/linear_algebra/dense/factorization/LU.h:106-120 applied to FP32 factors,
+// and the FP64 residual of the refinement loop), with fixed summation orders
+// so repeated solves give the same bits.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+#include "engine_internal.h"
+
+namespace hfpx {
+
+// ------------------------------------------------------ triangular solves
+// Solve order s = 0 .. T-1 over the 128-row tiles (tile s forward, tile
+// T-1-s backward).  One CTA per SM, launched cooperatively; CTA g owns the
+// solves s = g, g + G, ... and keeps their right-hand sides in shared
+// memory.  For each s in turn, every CTA
+//   * takes x_s: its owner computes x_s = D_s^-1 y_s with the inverse of the
+//     diagonal block (precomputed once per factorisation) and publishes it
+//     as 128 8-byte words (value + the solve's epoch); the others poll those
+//     words (one L2 round trip, no flag, no fence);
+//   * subtracts A(t', t_s) x_s from its owned tiles t' later in solve order,
+//     the next solve's tile first, with that tile and the next inverse
+//     loaded before the wait.
+// The critical path per tile: one word exchange and two 128 x 128 products.
+// Every wait gives up after kTrsvTimeoutNs and records the failure.
+constexpr int kTb = 128;
+constexpr int kSwThreads = 256;
+constexpr int kSwMaxOwn = 16;  // solves per CTA: n <= 16 * 148 * 128 rows
+constexpr unsigned long long kTrsvTimeoutNs = 200ull * 1000 * 1000;
+constexpr size_t kSwSmem = sizeof(float) * (2 * kTb * kTb + kSwMaxOwn * kTb + 6 * kTb);
+
+__device__ __forceinline__ unsigned long long trsv_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void xw_store(uint64_t* p, float v, uint32_t tag) {
+  const uint64_t w = ((uint64_t)tag << 32) | __float_as_uint(v);
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ uint64_t xw_load(const uint64_t* p) {
+  uint64_t w;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+  return w;
+}
+
+template <bool UPPER>
+__global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* __restrict__ A, int64_t lda, int n,
+                                                                   const float* __restrict__ dinv,
+                                                                   float* __restrict__ x, uint64_t* __restrict__ xw,
+                                                                   uint32_t epoch, int* __restrict__ err) {
+  extern __shared__ float sm[];
+  float* s_dinv = sm;                       // [2][kTb * kTb], column-major blocks
+  float* s_y = s_dinv + 2 * kTb * kTb;      // [kSwMaxOwn][kTb]
+  float* s_x = s_y + kSwMaxOwn * kTb;       // [kTb] x of the strip being applied
+  float* s_xo = s_x + kTb;                  // [kTb] x of this CTA's latest solve
+  float* s_red = s_xo + kTb;                // [2][kTb]
+  float* s_red2 = s_red + 2 * kTb;          // [2][kTb]
+  __shared__ int s_fail;
+  const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x;
+  const int T = (n + kTb - 1) / kTb;
+  const int r = tid & (kTb - 1), half = tid >> 7;
+  constexpr int kHalf = kTb / 2;
+  auto tile_of = [&](int s) { return UPPER ? T - 1 - s : s; };
+  auto rows_of = [&](int t) { return min(kTb, n - t * kTb); };
+  auto load_dinv = [&](float* dst, int t) {
+    const float* src = dinv + (size_t)t * kTb * kTb;
+    for (int i = tid; i < kTb * kTb; i += kSwThreads) dst[i] = src[i];
+  };
+  const int nown = g < T ? (T - 1 - g) / G + 1 : 0;
+  for (int i = 0; i < nown; ++i) {
+    const int t = tile_of(g + i * G);
+    if (tid < kTb) s_y[i * kTb + tid] = tid < rows_of(t) ? x[(int64_t)t * kTb + tid] : 0.f;
+  }
+  if (tid == 0) s_fail = 0;
+  if (nown > 0) load_dinv(s_dinv + (g & 1) * kTb * kTb, tile_of(g));
+  __syncthreads();
+  // y_s holds every update from earlier solves: x_s = D_s^-1 y_s into s_xo,
+  // published at once (words + the caller's x)
+  auto solve_own = [&](int s) {
+    const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
+    const float* D = s_dinv + (s & 1) * kTb * kTb;
+    const float* ys = s_y + (s / G) * kTb;
+    float acc = 0.f;
+#pragma unroll 16
+    for (int u = 0; u < kHalf; ++u) {
+      const int c = half * kHalf + u;
+      acc = fmaf(D[r + kTb * c], ys[c], acc);
+    }
+    s_red[half * kTb + r] = acc;
+    __syncthreads();
+    if (tid < kTb) {
+      const float v = tid < cols ? s_red[tid] + s_red[kTb + tid] : 0.f;
+      s_xo[tid] = v;
+      xw_store(xw + (size_t)s * kTb + tid, v, epoch);
+      if (tid < cols) x[(int64_t)c0 + tid] = v;
+    }
+    __syncthreads();
+  };
+  if (g == 0) solve_own(0);
+  for (int s = 0; s < T; ++s) {
+    const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
+    const bool mine = s % G == g;
+    const bool mine_next = s + 1 < T && (s + 1) % G == g;
+    // the next owned solve: its tile of this strip and its inverse, early
+    float pa[kHalf];
+    if (mine_next) {
+      const int tn = tile_of(s + 1), rn = rows_of(tn);
+#pragma unroll
+      for (int u = 0; u < kHalf; ++u) {
+        const int c = half * kHalf + u;
+        pa[u] = (r < rn && c < cols) ? A[(int64_t)tn * kTb + r + lda * (c0 + c)] : 0.f;
+      }
+      load_dinv(s_dinv + ((s + 1) & 1) * kTb * kTb, tn);
+    }
+    if (mine) {
+      if (tid < kTb) s_x[tid] = s_xo[tid];
+    } else if (tid < kTb) {
+      const uint64_t* p = xw + (size_t)s * kTb + tid;
+      uint64_t w = xw_load(p);
+      if ((uint32_t)(w >> 32) != epoch) {
+        const unsigned long long t0 = trsv_ns();
+        do {
+          w = xw_load(p);
+          if (trsv_ns() - t0 > kTrsvTimeoutNs) { s_fail = 1; break; }
+        } while ((uint32_t)(w >> 32) != epoch);
+      }
+      s_x[tid] = __uint_as_float((uint32_t)w);
+    }
+    __syncthreads();
+    if (s_fail) break;
+    // the critical path: the next solve's last update, its solve, publish
+    if (mine_next) {
+      float acc = 0.f;
+#pragma unroll
+      for (int u = 0; u < kHalf; ++u) acc = fmaf(pa[u], s_x[half * kHalf + u], acc);
+      s_red[half * kTb + r] = acc;
+      __syncthreads();
+      if (tid < kTb) s_y[((s + 1) / G) * kTb + tid] -= s_red[tid] + s_red[kTb + tid];
+      __syncthreads();
+      solve_own(s + 1);
+    }
+    // the other owned tiles later in solve order, two at a time with all
+    // their loads in flight together
+    for (int i = 0; i < nown; i += 2) {
+      const int sa = g + i * G, sb = g + (i + 1) * G;
+      const bool ua = sa > s + 1, ub = i + 1 < nown && sb > s + 1;
+      if (!ua && !ub) continue;
+      const int ta = ua ? tile_of(sa) : 0, tb = ub ? tile_of(sb) : 0;
+      const int rna = ua ? rows_of(ta) : 0, rnb = ub ? rows_of(tb) : 0;
+      float va[kHalf], vb[kHalf];
+#pragma unroll
+      for (int u = 0; u < kHalf; ++u) {
+        const int c = half * kHalf + u;
+        va[u] = (r < rna && c < cols) ? A[(int64_t)ta * kTb + r + lda * (c0 + c)] : 0.f;
+        vb[u] = (r < rnb && c < cols) ? A[(int64_t)tb * kTb + r + lda * (c0 + c)] : 0.f;
+      }
+      float acca = 0.f, accb = 0.f;
+#pragma unroll
+      for (int u = 0; u < kHalf; ++u) {
+        const float xv = s_x[half * kHalf + u];
+        acca = fmaf(va[u], xv, acca);
+        accb = fmaf(vb[u], xv, accb);
+      }
+      s_red[half * kTb + r] = acca;
+      s_red2[half * kTb + r] = accb;
+      __syncthreads();
+      if (tid < kTb) {
+        if (ua) s_y[i * kTb + tid] -= s_red[tid] + s_red[kTb + tid];
+        if (ub) s_y[(i + 1) * kTb + tid] -= s_red2[tid] + s_red2[kTb + tid];
+      }
+      __syncthreads();
+    }
+  }
+  if (s_fail && tid == 0) atomicExch(err, 1);
+}
+
+// Inverses of the 128 x 128 diagonal blocks of the factors: unit lower L
+// (forward) or upper U (backward), by substitution on the identity, one
+// column per thread; the ragged last block is padded with the identity.
+template <bool UPPER>
+__global__ void __launch_bounds__(kTb) tri_inverse_kernel(const float* __restrict__ A, int64_t lda, int n,
+                                                          float* __restrict__ dinv) {
+  extern __shared__ float sm[];
+  float* s_a = sm;                     // [kTb][kTb + 1] row-major
+  float* s_v = s_a + kTb * (kTb + 1);  // [kTb][kTb + 1]: s_v[i][j] = inverse (i, j)
+  const int t = blockIdx.x, r0 = t * kTb, rows = min(kTb, n - r0), j = threadIdx.x;
+  for (int i = 0; i < kTb; ++i)
+    s_a[i * (kTb + 1) + j] = (i < rows && j < rows) ? A[(int64_t)r0 + i + lda * (r0 + j)] : (i == j ? 1.f : 0.f);
+  __syncthreads();
+  if (!UPPER) {
+    for (int i = 0; i < kTb; ++i) {
+      float v = i == j ? 1.f : 0.f;
+      for (int k = j; k < i; ++k) v = fmaf(-s_a[i * (kTb + 1) + k], s_v[k * (kTb + 1) + j], v);
+      s_v[i * (kTb + 1) + j] = i < j ? 0.f : v;
+    }
+  } else {
+    for (int i = kTb - 1; i >= 0; --i) {
+      float v = i == j ? 1.f : 0.f;
+      for (int k = i + 1; k <= j; ++k) v = fmaf(-s_a[i * (kTb + 1) + k], s_v[k * (kTb + 1) + j], v);
+      s_v[i * (kTb + 1) + j] = i > j ? 0.f : v / s_a[i * (kTb + 1) + i];
+    }
+  }
+  __syncthreads();
+  float* out = dinv + (size_t)t * kTb * kTb;
+  for (int i = 0; i < kTb; ++i) out[i + (size_t)kTb * j] = s_v[i * (kTb + 1) + j];
+}
+
+int trsv_tiles(int64_t n) { return (int)((n + kTb - 1) / kTb); }
+
+int tri_inverses(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, float* dinv_lower, float* dinv_upper) {
+  static bool attr = false;
+  const size_t smem = sizeof(float) * 2 * kTb * (kTb + 1);
+  if (!attr) {
+    cudaFuncSetAttribute(tri_inverse_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(tri_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  const unsigned T = (unsigned)trsv_tiles(n);
+  ++g_launches;
+  tri_inverse_kernel<false><<<T, kTb, smem, c->stream>>>(A, lda, (int)n, dinv_lower);
+  ++g_launches;
+  tri_inverse_kernel<true><<<T, kTb, smem, c->stream>>>(A, lda, (int)n, dinv_upper);
+  return check_cuda(c, cudaGetLastError(), "diagonal block inverses");
+}
+
+// x (n) holds the right-hand side on entry, the solution on return.  The
+// exchange words and the failure word live in the context; the epoch tags
+// each solve, so the words need no clearing between solves.
+int trsv_f32(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const float* dinv, float* x, bool upper) {
+  if (n <= 0) return 0;
+  const int64_t T = trsv_tiles(n);
+  const int G = std::min(c->num_sms, (int)T);
+  if ((T + G - 1) / G > kSwMaxOwn) return set_error(c, HFPX_ERR_ARG, "matrix too large for the tile solve");
+  auto* xw = (uint64_t*)ctx_scratch(c, kScrTrsvFlags, sizeof(uint64_t) * T * kTb);
+  int* err = (int*)ctx_scratch(c, kScrTrsvErr, sizeof(int));
+  if (!xw || !err) return set_error(c, HFPX_ERR_NOMEM, "trsv state");
+  if (c->trsv_cap < T) {
+    // (re)allocated: words and failure word start at zero (epoch 0 unused)
+    cudaMemsetAsync(xw, 0, sizeof(uint64_t) * T * kTb, c->stream);
+    cudaMemsetAsync(err, 0, sizeof(int), c->stream);
+    c->trsv_cap = T;
+    c->trsv_epoch = 0;
+  }
+  if (++c->trsv_epoch <= 0) c->trsv_epoch = 1;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(trsv_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwSmem);
+    cudaFuncSetAttribute(trsv_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwSmem);
+    attr = true;
+  }
+  int nn = (int)n;
+  uint32_t ep = (uint32_t)c->trsv_epoch;
+  void* args[] = {&A, &lda, &nn, &dinv, &x, &xw, &ep, &err};
+  ++g_launches;
+  cudaError_t e = cudaLaunchCooperativeKernel(upper ? (void*)trsv_sweep_kernel<true> : (void*)trsv_sweep_kernel<false>,
+                                              dim3(G), dim3(kSwThreads), args, kSwSmem, c->stream);
+  return check_cuda(c, e, "triangular solve launch");
+}
+
+int trsv_status(hfpx_ctx* c) {
+  if (c->trsv_cap == 0) return 0;  // no solve has run (the word is set up by the first)
+  int* err = (int*)ctx_scratch(c, kScrTrsvErr, sizeof(int));
+  if (!err) return 0;
+  int e = 0;
+  int rc = check_cuda(c, cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "trsv status");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "trsv status");
+  if (!rc && e) rc = set_error(c, HFPX_ERR_CUDA, "triangular solve wait timed out");
+  return rc;
+}
+
+// ---------------------------------------------------------- FP64 residual
+// r = b - A x: blocks of 512 rows (two per thread, 16-byte loads) times
+// column chunks; the chunks' partial sums are added in chunk order by a
+// second kernel, which also records max |r| (non-negative doubles order as
+// their bits).
+constexpr int kGvThreads = 256;
+constexpr int kGvRows = 2 * kGvThreads;
+constexpr int kGvChunk = 4096;
+
+__global__ void __launch_bounds__(kGvThreads) resid_partial_kernel(const double* __restrict__ A, int64_t lda, int n,
+                                                                   const double* __restrict__ x,
+                                                                   double* __restrict__ part) {
+  __shared__ double s_x[kGvChunk];
+  const int nch = gridDim.y;
+  const int per = (n + nch - 1) / nch;
+  const int c_lo = blockIdx.y * per, c_hi = min(n, c_lo + per);
+  for (int j = c_lo + threadIdx.x; j < c_hi; j += kGvThreads) s_x[j - c_lo] = x[j];
+  __syncthreads();
+  const int i0 = blockIdx.x * kGvRows + 2 * threadIdx.x;
+  double a0 = 0.0, a1 = 0.0;
+  if (i0 + 1 < n) {
+    const double* col = A + i0;
+    int j = c_lo;
+    for (; j + 4 <= c_hi; j += 4) {
+      const double2 v0 = *reinterpret_cast<const double2*>(col + lda * j);
+      const double2 v1 = *reinterpret_cast<const double2*>(col + lda * (j + 1));
+      const double2 v2 = *reinterpret_cast<const double2*>(col + lda * (j + 2));
+      const double2 v3 = *reinterpret_cast<const double2*>(col + lda * (j + 3));
+      const double x0 = s_x[j - c_lo], x1 = s_x[j + 1 - c_lo], x2 = s_x[j + 2 - c_lo], x3 = s_x[j + 3 - c_lo];
+      a0 = fma(v0.x, x0, a0);
+      a1 = fma(v0.y, x0, a1);
+      a0 = fma(v1.x, x1, a0);
+      a1 = fma(v1.y, x1, a1);
+      a0 = fma(v2.x, x2, a0);
+      a1 = fma(v2.y, x2, a1);
+      a0 = fma(v3.x, x3, a0);
+      a1 = fma(v3.y, x3, a1);
+    }
+    for (; j < c_hi; ++j) {
+      const double2 v = *reinterpret_cast<const double2*>(col + lda * j);
+      a0 = fma(v.x, s_x[j - c_lo], a0);
+      a1 = fma(v.y, s_x[j - c_lo], a1);
+    }
+  } else if (i0 < n) {
+    for (int j = c_lo; j < c_hi; ++j) a0 = fma(A[i0 + lda * j], s_x[j - c_lo], a0);
+  }
+  if (i0 < n) part[(int64_t)blockIdx.y * n + i0] = a0;
+  if (i0 + 1 < n) part[(int64_t)blockIdx.y * n + i0 + 1] = a1;
+}
+
+__global__ void resid_finish_kernel(const double* __restrict__ b, const double* __restrict__ part, int n, int nch,
+                                    double* __restrict__ r, unsigned long long* __restrict__ rmax) {
+  __shared__ double s_m[8];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (i < n) {
+    double s = 0.0;
+    for (int k = 0; k < nch; ++k) s += part[(int64_t)k * n + i];
+    const double v = b[i] - s;
+    r[i] = v;
+    m = fabs(v);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_m[w]);
+    atomicMax(rmax, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+__global__ void absmax_kernel(const double* __restrict__ v, int n, unsigned long long* __restrict__ out) {
+  __shared__ double s_m[8];
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, fabs(v[i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_m[w]);
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+int resid_chunks(int64_t n) { return (int)std::max<int64_t>(16, (n + kGvChunk - 1) / kGvChunk); }
+
+int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
+                 double* part, unsigned long long* d_max) {
+  const int nch = resid_chunks(n);
+  cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
+  ++g_launches;
+  resid_partial_kernel<<<dim3((unsigned)((n + kGvRows - 1) / kGvRows), (unsigned)nch), kGvThreads, 0, c->stream>>>(
+      A, lda, (int)n, x, part);
+  ++g_launches;
+  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max);
+  return check_cuda(c, cudaGetLastError(), "residual launch");
+}
+
+int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max) {
+  cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
+  ++g_launches;
+  absmax_kernel<<<(unsigned)std::min<int64_t>(148 * 4, (n + 255) / 256), 256, 0, c->stream>>>(v, (int)n, d_max);
+  return check_cuda(c, cudaGetLastError(), "absmax launch");
+}
+
+}  // namespace hfpx

@@ -136,3 +136,23 @@ def test_mixed_singular_reports_column(ctx):
             engine.LU(ctx, m, engine.HFPX_LU_MIXED)
         assert e.value.code == engine.HFPX_ERR_SINGULAR
         assert str(col + 1) in str(e.value)
+
+
+def test_tile_sweep_triangular_solves(tmp_path):
+    # the engine's tile-sweep triangular solves (default) and cuBLAS's
+    # (HFPX_TRSV=cublas) reach the same refined solution
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for kind in ('', 'cublas'):
+        env = dict(os.environ, HFPX_TRSV=kind, PYTHONPATH=root)
+        f = tmp_path / ('x_%s.npy' % (kind or 'own'))
+        r = subprocess.run([sys.executable, '-c', _PANEL_RUN, '700', str(f)], env=env, cwd=root,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[kind] = np.load(f)
+    x0, x1 = out['cublas'][:-2], out[''][:-2]
+    assert out[''][-1] <= 1e-12
+    assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
