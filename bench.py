@@ -287,7 +287,7 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
             times.append(e0.elapsed_time(e1))
     h2d = hn.nbytes + hc.nbytes + 2 * hd.nbytes + hr.nbytes + s.nbytes  # dof_h goes up twice
     return {'value': statistics.mean(times) / 1e3, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
-            'd2h_bytes_per_step': int(hr.nbytes), 'steps': len(times)}
+            'd2h_bytes_per_step': int(hr.nbytes), 'steps': len(times), 'steps_ms': [round(t, 2) for t in times]}
 
 
 # ------------------------------------------------------------- CPU reference
