@@ -587,6 +587,107 @@ void launch_stress(const void* d_elem, int64_t n_el, double G, double nu, int is
                                                           d_out);
 }
 
+// ----------------------------------------------------- stress influence
+// The same per-(point, element) blocks as stress_kernel, stored instead of
+// summed: M (6 n_pts x 18 n_el, column-major, ldm) with row 6 p + c (stress
+// component c at point p) and column 18 s + 3 a + j (DD component j of node
+// a of element s).  Threads run over points for one element, so each column
+// segment is written contiguously.
+__global__ void __launch_bounds__(kStressThreads) stress_influence_kernel(
+    const ElemRec* __restrict__ elems, int64_t n_el, double G, double nu, int is_dd_local,
+    const double* __restrict__ pts, int64_t n_pts, double* __restrict__ M, int64_t ldm) {
+  const int64_t s = blockIdx.y;
+  const int64_t p = (int64_t)blockIdx.x * kStressThreads + threadIdx.x;
+  if (p >= n_pts) return;
+  const double pt[3] = {pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]};
+  const double scale = -G / (4.0 * kPi * (1.0 - nu));
+  const ElemRec& S = elems[s];
+  double h;
+  cplx z;
+  point_hz(S, pt, h, z);
+  const double* r = S.r;
+  auto sink = [&](int a, const double Sx[6][3]) {
+    double Sg[6][3];
+    for (int k = 0; k < 3; ++k) {
+      const double m[3][3] = {{Sx[0][k], Sx[3][k], Sx[4][k]},
+                              {Sx[3][k], Sx[1][k], Sx[5][k]},
+                              {Sx[4][k], Sx[5][k], Sx[2][k]}};
+      double tt[3][3], gg[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) tt[i][j] = m[i][0] * r[j] + m[i][1] * r[3 + j] + m[i][2] * r[6 + j];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) gg[i][j] = r[i] * tt[0][j] + r[3 + i] * tt[1][j] + r[6 + i] * tt[2][j];
+      Sg[0][k] = gg[0][0]; Sg[1][k] = gg[1][1]; Sg[2][k] = gg[2][2];
+      Sg[3][k] = gg[0][1]; Sg[4][k] = gg[0][2]; Sg[5][k] = gg[1][2];
+    }
+    for (int c = 0; c < 6; ++c) {
+      double w0 = Sg[c][0], w1 = Sg[c][1], w2 = Sg[c][2];
+      if (!is_dd_local) {
+        const double g0 = w0 * r[0] + w1 * r[3] + w2 * r[6];
+        const double g1 = w0 * r[1] + w1 * r[4] + w2 * r[7];
+        const double g2 = w0 * r[2] + w1 * r[5] + w2 * r[8];
+        w0 = g0; w1 = g1; w2 = g2;
+      }
+      double* col = M + (6 * p + c) + ldm * (18 * s + 3 * a);
+      col[0] = w0;
+      col[ldm] = w1;
+      col[2 * ldm] = w2;
+    }
+  };
+  if (fabs(h) < kHTol) {
+    cplx P[6], Q[6];
+    inplane_moments(S, z, P, Q);
+    inplane_nodes(S, z, P, Q, nu, scale, sink);
+  } else {
+    cplx smon[72];
+    offplane_smon(S, z, h, nu, smon);
+    contract_nodes(S.sfm, z, smon, scale, sink);
+  }
+}
+
+// DD of n_cases load cases, (6 n_el) x 3 each, to the vectors of the
+// influence matrix's columns: D[18 s + 3 a + j, case].
+__global__ void dd_to_vec_kernel(const double* __restrict__ dd, int64_t n_el, int64_t n_cases,
+                                 double* __restrict__ D) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 18 * n_el * n_cases) return;
+  const int64_t cs = i / (18 * n_el), e = i - cs * 18 * n_el;
+  const int64_t s = e / 18, a = (e % 18) / 3, j = e % 3;
+  D[i] = dd[cs * 18 * n_el + (6 * s + a) + 6 * n_el * j];
+}
+
+// S (6 n_pts x n_cases) + s_inf to out: n_cases blocks of n_pts x 6.
+__global__ void stress_out_kernel(const double* __restrict__ S, int64_t n_pts, int64_t n_cases,
+                                  const double* __restrict__ sinf, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 6 * n_pts * n_cases) return;
+  const int64_t cs = i / (6 * n_pts), e = i - cs * 6 * n_pts;
+  const int64_t c = e / n_pts, p = e - c * n_pts;
+  out[i] = S[(6 * p + c) + 6 * n_pts * cs] + sinf[c + 6 * cs];
+}
+
+void launch_stress_influence(const void* d_elem, int64_t n_el, double G, double nu, int is_dd_local,
+                             const double* d_pts, int64_t n_pts, double* d_M, int64_t ldm, cudaStream_t s) {
+  gl_host_init(s);
+  ++g_launches;
+  stress_influence_kernel<<<dim3((unsigned)((n_pts + kStressThreads - 1) / kStressThreads), (unsigned)n_el),
+                            kStressThreads, 0, s>>>(static_cast<const ElemRec*>(d_elem), n_el, G, nu, is_dd_local,
+                                                    d_pts, n_pts, d_M, ldm);
+}
+
+void launch_dd_to_vec(const double* d_dd, int64_t n_el, int64_t n_cases, double* d_D, cudaStream_t s) {
+  const int64_t tot = 18 * n_el * n_cases;
+  ++g_launches;
+  dd_to_vec_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(d_dd, n_el, n_cases, d_D);
+}
+
+void launch_stress_out(const double* d_S, int64_t n_pts, int64_t n_cases, const double* d_sinf, double* d_out,
+                       cudaStream_t s) {
+  const int64_t tot = 6 * n_pts * n_cases;
+  ++g_launches;
+  stress_out_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(d_S, n_pts, n_cases, d_sinf, d_out);
+}
+
 // --------------------------------------------------------- single block
 __global__ void local_block_kernel(double G, double nu, double h, double zr, double zi,
                                    const double* __restrict__ tau, const double* __restrict__ sfm,

@@ -452,6 +452,44 @@ int hfpx_stress(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, int is_
   return rc;
 }
 
+int hfpx_stress_batch(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, int is_dd_local, const double* dd,
+                      int64_t n_cases, const double* pts, int64_t n_pts, const double* s_inf, double* out) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!mesh || !dd || !pts || !s_inf || !out || n_pts < 1 || n_cases < 1)
+    return set_error(c, HFPX_ERR_ARG, "bad stress arguments");
+  if (!(G > 0) || !(nu > -1.0 && nu < 0.5)) return set_error(c, HFPX_ERR_ARG, "bad elastic constants");
+  if (n_cases == 1) return hfpx_stress(c, mesh, G, nu, is_dd_local, dd, pts, n_pts, s_inf, out);
+  cudaSetDevice(c->device);
+  const int64_t ne = mesh->n_el, rows = 6 * n_pts, cols = 18 * ne;
+  DevBuf dm, ddd, dvec, dp, ds, dS, dout;
+  int rc = check_cuda(c, dm.alloc(sizeof(double) * rows * cols), "influence matrix alloc");
+  if (!rc) rc = check_cuda(c, ddd.alloc(sizeof(double) * cols * n_cases), "dd alloc");
+  if (!rc) rc = check_cuda(c, dvec.alloc(sizeof(double) * cols * n_cases), "dd vectors alloc");
+  if (!rc) rc = check_cuda(c, dp.alloc(sizeof(double) * 3 * n_pts), "pts alloc");
+  if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 6 * n_cases), "s_inf alloc");
+  if (!rc) rc = check_cuda(c, dS.alloc(sizeof(double) * rows * n_cases), "stress alloc");
+  if (!rc) rc = check_cuda(c, dout.alloc(sizeof(double) * rows * n_cases), "out alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ddd.p, dd, sizeof(double) * cols * n_cases, cudaMemcpyHostToDevice, c->stream), "dd");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dp.p, pts, sizeof(double) * 3 * n_pts, cudaMemcpyHostToDevice, c->stream), "pts");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(ds.p, s_inf, sizeof(double) * 6 * n_cases, cudaMemcpyHostToDevice, c->stream), "s_inf");
+  if (!rc) {
+    launch_stress_influence(mesh->d_elem, ne, G, nu, is_dd_local, dp.as<double>(), n_pts, dm.as<double>(), rows,
+                            c->stream);
+    launch_dd_to_vec(ddd.as<double>(), ne, n_cases, dvec.as<double>(), c->stream);
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
+    cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)rows, (int)n_cases, (int)cols, &one, dm.as<double>(), (int)rows,
+                    dvec.as<double>(), (int)cols, &zero, dS.as<double>(), (int)rows) != CUBLAS_STATUS_SUCCESS)
+      rc = set_error(c, HFPX_ERR_CUDA, "stress GEMM");
+  }
+  if (!rc) launch_stress_out(dS.as<double>(), n_pts, n_cases, ds.as<double>(), dout.as<double>(), c->stream);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "stress launch");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(out, dout.p, sizeof(double) * rows * n_cases, cudaMemcpyDeviceToHost, c->stream), "out");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "stress");
+  return rc;
+}
+
 int hfpx_local_submatrix(hfpx_ctx* c, double G, double nu, double h, double zr, double zi, const double* tau,
                          const double* sfm, double* out) {
   if (!c) return HFPX_ERR_ARG;

@@ -80,6 +80,11 @@ void launch_rhs(const void* d_elem, int64_t n_el, const int32_t* d_dof, const do
 void launch_stress(const void* d_elem, int64_t n_el, double G, double nu, int is_dd_local,
                    const double* d_dd, const double* d_pts, int64_t n_pts, const double* d_sinf,
                    double* d_out, cudaStream_t s);
+void launch_stress_influence(const void* d_elem, int64_t n_el, double G, double nu, int is_dd_local,
+                             const double* d_pts, int64_t n_pts, double* d_M, int64_t ldm, cudaStream_t s);
+void launch_dd_to_vec(const double* d_dd, int64_t n_el, int64_t n_cases, double* d_D, cudaStream_t s);
+void launch_stress_out(const double* d_S, int64_t n_pts, int64_t n_cases, const double* d_sinf, double* d_out,
+                       cudaStream_t s);
 void launch_local_block(double G, double nu, double h, double zr, double zi, const double* d_tau,
                         const double* d_sfm, double* d_out, cudaStream_t s);
 void launch_convert_f32(const double* d_a, int64_t ld, int64_t n, float* d_f, cudaStream_t s);

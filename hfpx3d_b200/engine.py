@@ -66,6 +66,7 @@ SIGNATURES = {
     'hfpx_ctx_launch_count': (_i64, [_V]),
     'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
+    'hfpx_stress_batch': (_int, [_V, _V, _f64, _f64, _int, _D, _i64, _D, _i64, _D, _D]),
     'hfpx_local_submatrix': (_int, [_V, _f64, _f64, _f64, _f64, _f64, _D, _D, _D]),
     'hfpx_element_frame': (_int, [_D, _D, _D, _D]),
 }
@@ -310,6 +311,24 @@ def make_3dbem_stress_f_s(ctx, dmesh: DeviceMesh, shear_m, poiss_r, dd, pts, s_i
     ctx.check(lib().hfpx_stress(ctx.h, dmesh.h, shear_m, poiss_r, int(is_dd_local), _dp(dd), _dp(pts), P,
                                 _dp(s), _dp(out)))
     return out
+
+
+def make_3dbem_stress_f_s_batch(ctx, dmesh: DeviceMesh, shear_m, poiss_r, dd_cases, pts, s_inf_cases,
+                                is_dd_local=False):
+    """make_3dbem_stress_f_s for many load cases: dd_cases (n_cases, 6 Ne, 3),
+    s_inf_cases 6 x n_cases -> (n_cases, P, 6); one influence matrix and one
+    FP64 GEMM on the device (hfpx_stress_batch)."""
+    dd = np.asarray(dd_cases, dtype=np.float64)
+    nc = dd.shape[0]
+    # each case's (6 Ne) x 3 block column-major, blocks one after another
+    flat = np.ascontiguousarray(np.stack([np.asfortranarray(dd[k]).reshape(-1, order='F') for k in range(nc)]))
+    pts = _f(pts)
+    s = _f(np.asarray(s_inf_cases, dtype=np.float64).reshape(6, nc))
+    P = pts.shape[1]
+    out = np.empty(nc * P * 6)
+    ctx.check(lib().hfpx_stress_batch(ctx.h, dmesh.h, shear_m, poiss_r, int(is_dd_local), _dp(flat), nc, _dp(pts), P,
+                                      _dp(s), _dp(out)))
+    return np.stack([out[k * 6 * P:(k + 1) * 6 * P].reshape(P, 6, order='F') for k in range(nc)])
 
 
 def make_local_3dbem_submatrix(ctx, shear_m, poiss_r, h, z, tau, sfm):

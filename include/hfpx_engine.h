@@ -143,6 +143,17 @@ int hfpx_stress(hfpx_ctx *ctx, const hfpx_mesh *mesh, double shear_m, double poi
                 int is_dd_local, const double *dd, const double *pts, int64_t n_pts,
                 const double *s_inf, double *out);
 
+/* ---- stress for many load cases at once (the batched workload's
+ * postprocessing): the 6 n_pts x 18 n_el influence matrix of the points
+ * (the blocks make_3dbem_stress_f_s sums, system_assembly.cpp:306-437) is
+ * formed once on the device and applied to all cases with one FP64 GEMM.
+ * dd: n_cases blocks of (6 n_el) x 3 as for hfpx_stress (block k at
+ * dd + 18 n_el k); s_inf: 6 x n_cases; out: n_cases blocks of n_pts x 6.
+ * n_cases == 1 runs hfpx_stress. */
+int hfpx_stress_batch(hfpx_ctx *ctx, const hfpx_mesh *mesh, double shear_m, double poiss_r,
+                      int is_dd_local, const double *dd, int64_t n_cases, const double *pts,
+                      int64_t n_pts, const double *s_inf, double *out);
+
 /* ---- one element at one point: make_local_3dbem_submatrix,
  * src/Elasticity/elasticity_kernel_integration.cpp:34-205 (kernel 1).
  * tau: 3 complex (re,im), sfm: 6x6 complex row-major (re,im); out 6x18
