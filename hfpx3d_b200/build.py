@@ -18,6 +18,7 @@ HOST = os.path.join(HERE, 'host')
 INCLUDE = os.path.join(os.path.dirname(HERE), 'include')
 OUT = os.path.join(HERE, 'libhfpx_engine.so')
 HOST_LIB = os.path.join(HERE, 'libhfpx_host.so')
+LAPACKE_LIB = os.path.join(HERE, 'libhfpx_lapacke.so')
 MAIN = os.path.join(HERE, 'bin', 'hfpx_main')
 SOURCES = ['engine.cu', 'assembly.cu', 'lu.cu', 'solve.cu']
 CUDA = os.environ.get('CUDA_HOME', '/usr/local/cuda')
@@ -26,7 +27,9 @@ CXX = os.environ.get('CXX', 'g++')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3', '-std=c++17',
          '-Xcompiler', '-fPIC', '-shared', '--expt-relaxed-constexpr', '-I' + INCLUDE]
 LIBS = ['-L' + os.path.join(CUDA, 'lib64'), '-lcublas', '-Xlinker', '-rpath=' + os.path.join(CUDA, 'lib64')]
-HOST_FLAGS = ['-O2', '-std=c++17', '-Wall', '-I' + INCLUDE, '-I' + HOST]
+# --exclude-libs: a toolchain that links its C++ runtime statically must not
+# re-export it from these libraries into the programs that load them
+HOST_FLAGS = ['-O2', '-std=c++17', '-Wall', '-I' + INCLUDE, '-I' + HOST, '-Wl,--exclude-libs,ALL']
 
 
 def _stale(out, deps):
@@ -59,6 +62,9 @@ def build_host(force=False, verbose=False):
         os.makedirs(os.path.dirname(MAIN), exist_ok=True)
         _run([CXX] + HOST_FLAGS + [os.path.join(HOST, 'hfpx_main.cpp'), '-o', MAIN, '-L' + HERE, '-lhfpx_host',
                                    '-lhfpx_engine', '-Wl,-rpath,$ORIGIN/..'], verbose)
+    if force or _stale(LAPACKE_LIB, deps):
+        _run([CXX] + HOST_FLAGS + ['-fPIC', '-shared', os.path.join(HOST, 'lapacke_shim.cpp'), '-o', LAPACKE_LIB,
+                                   '-L' + HERE, '-lhfpx_engine', '-Wl,-rpath,$ORIGIN'], verbose)
     return MAIN
 
 

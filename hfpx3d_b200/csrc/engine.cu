@@ -318,6 +318,38 @@ int hfpx_matrix_upload(hfpx_ctx* c, const double* a, int64_t n, int64_t ld_host,
   return HFPX_OK;
 }
 
+int hfpx_matrix_pivots(hfpx_ctx* c, const hfpx_matrix* m, int32_t* ipiv) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !ipiv) return set_error(c, HFPX_ERR_ARG, "null argument");
+  if (m->factored != 1) return set_error(c, HFPX_ERR_STATE, "no FP64 factorisation");
+  cudaSetDevice(c->device);
+  int rc = check_cuda(c, cudaMemcpyAsync(ipiv, m->d_piv, sizeof(int32_t) * m->n, cudaMemcpyDeviceToHost, c->stream),
+                      "pivots");
+  return rc ? rc : check_cuda(c, cudaStreamSynchronize(c->stream), "pivots");
+}
+
+int hfpx_matrix_upload_lu(hfpx_ctx* c, const double* lu, int64_t n, int64_t ld_host, const int32_t* ipiv,
+                          hfpx_matrix** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  if (!ipiv) return set_error(c, HFPX_ERR_ARG, "null pivots");
+  for (int64_t i = 0; i < n; ++i)
+    if (ipiv[i] < i || ipiv[i] >= n) return set_error(c, HFPX_ERR_ARG, "pivot out of range");
+  hfpx_matrix* m = nullptr;
+  int rc = hfpx_matrix_upload(c, lu, n, ld_host, &m);
+  if (rc) return rc;
+  rc = check_cuda(c, cudaMemcpyAsync(m->d_piv, ipiv, sizeof(int32_t) * n, cudaMemcpyHostToDevice, c->stream), "pivots");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "pivots");
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  m->factored = 1;
+  m->info = 0;
+  *out = m;
+  return HFPX_OK;
+}
+
 int hfpx_matrix_dims(const hfpx_matrix* m, int64_t* n, int64_t* ld) {
   if (!m) return HFPX_ERR_ARG;
   if (n) *n = m->n;

@@ -67,6 +67,8 @@ SIGNATURES = {
     'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
     'hfpx_stress_batch': (_int, [_V, _V, _f64, _f64, _int, _D, _i64, _D, _i64, _D, _D]),
+    'hfpx_matrix_pivots': (_int, [_V, _V, ctypes.POINTER(ctypes.c_int32)]),
+    'hfpx_matrix_upload_lu': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(_V)]),
     'hfpx_local_submatrix': (_int, [_V, _f64, _f64, _f64, _f64, _f64, _D, _D, _D]),
     'hfpx_element_frame': (_int, [_D, _D, _D, _D]),
 }

@@ -111,6 +111,15 @@ int hfpx_lu_factor(hfpx_ctx *ctx, hfpx_matrix *matrix, int mode, int64_t *info);
 int hfpx_lu_solve(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *b, int64_t nrhs,
                   int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
 
+/* The row interchanges of an FP64 factorisation (dgetrf's ipiv, 0-based:
+ * row i was interchanged with row ipiv[i], i = 0 .. n-1 in order). */
+int hfpx_matrix_pivots(hfpx_ctx *ctx, const hfpx_matrix *matrix, int32_t *ipiv);
+/* A matrix holding FP64 LU factors made elsewhere (dgetrf layout: unit L
+ * below the diagonal, U on and above; ipiv 0-based as above), ready for
+ * hfpx_lu_solve: the dgetrs of LU.h:106-120 given a caller's factors. */
+int hfpx_matrix_upload_lu(hfpx_ctx *ctx, const double *lu, int64_t n, int64_t ld_host,
+                          const int32_t *ipiv, hfpx_matrix **matrix);
+
 /* Same as hfpx_lu_solve with b already in device memory (ld_b >= n). */
 int hfpx_lu_solve_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, int64_t nrhs,
                          int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
