@@ -28,6 +28,8 @@ def shim():
     lib.LAPACKE_dgetrf.restype = _I
     lib.LAPACKE_dgetrs.argtypes = [_I, ctypes.c_char, _I, _I, _D, _I, _IP, _D, _I]
     lib.LAPACKE_dgetrs.restype = _I
+    lib.LAPACKE_dgesv.argtypes = [_I, _I, _I, _D, _I, _IP, _D, _I]
+    lib.LAPACKE_dgesv.restype = _I
     return lib
 
 
@@ -47,6 +49,37 @@ def test_exports_and_argument_checks():
     b = np.zeros(4)
     assert lib.LAPACKE_dgetrs(102, b'T', 4, 1, dp(a), 4, ipp, dp(b), 4) == -2   # transposed
     assert lib.LAPACKE_dgetrs(102, b'N', 4, 1, dp(a), 4, ipp, dp(b), 2) == -9   # ldb < n
+    assert lib.LAPACKE_dgesv(100, 4, 1, dp(a), 4, ipp, dp(b), 4) == -1          # unknown layout
+    assert lib.LAPACKE_dgesv(102, 4, -1, dp(a), 4, ipp, dp(b), 4) == -3
+    assert lib.LAPACKE_dgesv(102, 4, 1, dp(a), 3, ipp, dp(b), 4) == -5
+    assert lib.LAPACKE_dgesv(102, 4, 1, dp(a), 4, ipp, dp(b), 3) == -8          # col-major: ldb < n
+    assert lib.LAPACKE_dgesv(101, 4, 2, dp(a), 4, ipp, dp(b), 1) == -8          # row-major: ldb < nrhs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize('layout', [102, 101])
+def test_dgesv_matches_lapack(layout):
+    # il::linearSolve (linearSolve.h:28-76): column-major Array2D, row-major Array2C
+    import scipy.linalg as sl
+    lib = shim()
+    rng = np.random.default_rng(5)
+    n, nrhs = 300, 2
+    A = rng.standard_normal((n, n)) + np.diag(np.linspace(1, 3, n))
+    B = rng.standard_normal((n, nrhs))
+    order = 'F' if layout == 102 else 'C'
+    a, b = np.array(A, order=order), np.array(B, order=order)
+    ip = np.zeros(n, dtype=np.int32)
+    ld_b = n if layout == 102 else nrhs
+    assert lib.LAPACKE_dgesv(layout, n, nrhs, dp(a), n, ip.ctypes.data_as(_IP), dp(b), ld_b) == 0
+    lu, piv = sl.lu_factor(A)
+    assert np.array_equal(ip - 1, piv)
+    assert np.abs(a - lu).max() <= 1e-12 * np.abs(lu).max()
+    assert np.abs(b - np.linalg.solve(A, B)).max() <= 1e-11 * np.abs(b).max()
+    # a zero column: info = its 1-based index, B untouched
+    A[:, 7] = 0.0
+    a, b = np.array(A, order=order), np.array(B, order=order)
+    assert lib.LAPACKE_dgesv(layout, n, nrhs, dp(a), n, ip.ctypes.data_as(_IP), dp(b), ld_b) == 8
+    assert np.array_equal(b, B)
 
 
 @pytest.mark.gpu
