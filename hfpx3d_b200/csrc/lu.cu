@@ -171,7 +171,13 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
 // Same factorisation as panel_base_kernel<float> (same pivots, same
 // arithmetic per element, so the same bits), restructured for latency:
 //  * each thread keeps kLLRows whole rows of the <= 32-column panel in
-//    registers, so the rank-1 update touches no shared memory;
+//    registers, so the rank-1 update touches no shared memory.  The rows are
+//    kept shifted: at column j register column c holds panel column j + c,
+//    so every register index is a compile-time constant (no selects, one
+//    compact loop body: an unrolled per-column variant of this loop ran out
+//    of the instruction cache).  The rank-1 update writes into the shifted
+//    place, a(c) <- a(c + 1) - l p(c + 1), and column j, final once step j is
+//    done, goes to the row's slot in A;
 //  * the pivot search is exchanged through L2 in "LL" words: 8 bytes holding
 //    4 bytes of data and a 4-byte tag naming the launch and column.  A word
 //    is written and read as one 8-byte access, so a reader that sees the
@@ -181,8 +187,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
 //  * rows are interchanged by relabelling, not by moving data: each register
 //    row carries the panel row it currently stands for.  Swapping rows j and
 //    p swaps the two labels; the pivot row's data stays where it is and, now
-//    labelled j, takes no further updates.  The write-back stores every row
-//    at its final label.
+//    labelled j, takes no further updates.  At the end the rows whose label
+//    is not their slot (<= 2 w of them) move to it with all of the block
+//    panel's columns (ll_finish).
 // Words of column j sit in buffer j & 1: a CTA can only write column j + 2
 // after all CTAs published column j + 1, i.e. after all finished reading j.
 // Tags are unique within one factorisation and the buffers are zeroed before
@@ -210,56 +217,6 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// a[k][c] if c == j else keep, by bit masks: a plain "if (c == j) x =
-// a[k][c]" over an unrolled c is folded back into a[k][j] with a run-time j,
-// which moves the whole register array to local memory.
-__device__ __forceinline__ float pick(float x, float cand, bool take) {
-  const int msk = -(int)take;
-  return __int_as_float((__float_as_int(cand) & msk) | (__float_as_int(x) & ~msk));
-}
-
-// Scale column j and update columns j+1..31 of this thread's rows labelled
-// below row j (j in [C0, C0 + 8); label -1: no row); columns below C0 are
-// not touched.  One FMA per element: rows that take no update get
-// multiplier 0 and columns c <= j a zero pivot-row entry, so the FMA leaves
-// them unchanged (up to the sign of a zero); column j is then set by selects
-// over the 8 columns of its group.  nxt gets |a(., j+1)| for the next
-// arg-max (-1: not a candidate).
-template <int C0>
-__device__ __forceinline__ void ll_update(float (&a)[kLLRows][kBaseW], const int (&lab)[kLLRows], int j, float inv,
-                                          bool nonzero, const float* __restrict__ prow, float (&nxt)[kLLRows]) {
-  float l[kLLRows], lz[kLLRows];
-#pragma unroll
-  for (int k = 0; k < kLLRows; ++k) {
-    const bool below = nonzero && lab[k] > j;
-    float v = 0.f;
-#pragma unroll
-    for (int c = C0; c < C0 + 8; ++c) v = pick(v, a[k][c], c == j);
-    l[k] = below ? v * inv : v;  // rows not below keep their column-j value
-    lz[k] = below ? l[k] : 0.f;
-  }
-#pragma unroll
-  for (int c = C0; c < kBaseW; ++c) {
-    const float pc = c > j ? prow[c] : 0.f;
-#pragma unroll
-    for (int k = 0; k < kLLRows; ++k) a[k][c] = fmaf(-lz[k], pc, a[k][c]);
-  }
-#pragma unroll
-  for (int c = C0; c < C0 + 8; ++c) {
-    const bool eq = c == j;
-#pragma unroll
-    for (int k = 0; k < kLLRows; ++k) a[k][c] = eq ? l[k] : a[k][c];
-  }
-#pragma unroll
-  for (int k = 0; k < kLLRows; ++k) {
-    const bool below = lab[k] > j;
-    float x = 0.f;
-#pragma unroll
-    for (int c = C0 + 1; c < C0 + 9 && c < kBaseW; ++c) x = pick(x, a[k][c], c == j + 1);
-    nxt[k] = below ? fabsf(x) : -1.f;
-  }
-}
-
 // Register row k of this thread to shared memory.  The if-chain over
 // compile-time K keeps every register index static.
 template <int K = 0>
@@ -272,8 +229,100 @@ __device__ __forceinline__ void ll_row_to_smem(const float (&a)[kLLRows][kBaseW]
   }
 }
 
+// Waits until every CTA of the grid has stored tag in its word of bar (one
+// word per CTA), bounded by kLLTimeoutNs; release fence before the store,
+// acquire fence after.  Returns false (and sets s_fail) on a timeout.
+__device__ bool ll_grid_barrier(uint64_t* bar, uint32_t tag, int& s_fail) {
+  const int tid = threadIdx.x;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    ll_store(bar + blockIdx.x, 0u, tag);
+  }
+  if (tid < (int)gridDim.x) {
+    const uint64_t t0 = global_ns();
+    while ((uint32_t)(ll_load(bar + tid) >> 32) != tag) {
+      if (global_ns() - t0 > kLLTimeoutNs) {
+        s_fail = 1;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return !s_fail;
+}
+
+// Rows of a register-resident panel that end at another row (lab[k] !=
+// g0 + k kLLThreads, the slot register row k came from) take their values to
+// it on the enclosing block panel's columns [-left, w + right): with mid = w
+// all of them, with mid = 0 the columns outside the panel only (left:
+// [-left, 0), right: [w, w + right); the recursive panel's halves then need
+// no row swaps between them).  A moved row's old values go to xtmp first
+// (ll_moves_stash), at slot = its final label if < w, else w + its first row
+// (a row starting at w or below only ever moves to a label < w, so the slots
+// are distinct); after a barrier over the CTAs they go to the final row
+// (ll_moves_apply).
+struct MoveShared {
+  int nmv;
+  int src[2 * kBaseW], dst[2 * kBaseW], slot[2 * kBaseW];
+};
+
+__device__ __forceinline__ int64_t ll_move_col(int cc, int left, int mid, int w) {
+  return cc < left + mid ? (int64_t)(cc - left) : (int64_t)(w + cc - left - mid);
+}
+
+__device__ void ll_moves_stash(MoveShared& ms, const float* __restrict__ A, int64_t lda, int w,
+                               const int (&lab)[kLLRows], int g0, int left, int mid, int right,
+                               float* __restrict__ xtmp, const int& s_fail) {
+  const int tid = threadIdx.x;
+  if (tid == 0) ms.nmv = 0;
+  __syncthreads();
+  if (!s_fail && left + mid + right > 0) {
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+      const int phys = g0 + k * kLLThreads;
+      if (lab[k] >= 0 && lab[k] != phys) {
+        const int q = atomicAdd(&ms.nmv, 1);
+        ms.src[q] = phys;
+        ms.dst[q] = lab[k];
+        ms.slot[q] = lab[k] < w ? lab[k] : w + phys;
+      }
+    }
+  }
+  __syncthreads();
+  const int nmv = ms.nmv, ncol = left + mid + right;
+  for (int i = tid; i < nmv * ncol; i += kLLThreads) {
+    const int q = i / ncol, cc = i - q * ncol;
+    xtmp[(size_t)ms.slot[q] * ncol + cc] = A[(int64_t)ms.src[q] + lda * ll_move_col(cc, left, mid, w)];
+  }
+}
+
+__device__ void ll_moves_apply(const MoveShared& ms, float* __restrict__ A, int64_t lda, int w, int left, int mid,
+                               int right, const float* __restrict__ xtmp) {
+  const int nmv = ms.nmv, ncol = left + mid + right;
+  for (int i = threadIdx.x; i < nmv * ncol; i += kLLThreads) {
+    const int q = i / ncol, cc = i - q * ncol;
+    A[(int64_t)ms.dst[q] + lda * ll_move_col(cc, left, mid, w)] = xtmp[(size_t)ms.slot[q] * ncol + cc];
+  }
+}
+
+// End of panel_ll_kernel, whose rows are in their slots: the moved rows to
+// their labels on all block-panel columns (barrier words bar, tag btag).
+__device__ void ll_finish(MoveShared& ms, float* __restrict__ A, int64_t lda, int w, const int (&lab)[kLLRows],
+                          int g0, int left, int right, float* __restrict__ xtmp, uint64_t* bar, uint32_t btag,
+                          int* err, int& s_fail) {
+  ll_moves_stash(ms, A, lda, w, lab, g0, left, w, right, xtmp, s_fail);
+  if (!ll_grid_barrier(bar, btag, s_fail)) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    return;
+  }
+  __threadfence();
+  ll_moves_apply(ms, A, lda, w, left, w, right, xtmp);
+}
+
 // piv[j] = pivot row + piv_add; left/right: columns of the enclosing block
-// panel on either side that take the interchanges too (see the end).
+// panel on either side that take the interchanges too (ll_finish).
 __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
     uint64_t* __restrict__ slots, int64_t* __restrict__ info, int64_t col_offset, uint32_t tag0,
@@ -312,17 +361,15 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const int x = tid + u * kLLThreads;
     off[u] = x < units ? (x / per) * kLLSlot + x % per : -1;
   }
-  float nxt[kLLRows];
-#pragma unroll
-  for (int k = 0; k < kLLRows; ++k) nxt[k] = lab[k] >= 0 ? fabsf(a[k][0]) : -1.f;
   for (int j = 0; j < w; ++j) {
     const int buf = j & 1;
     const uint32_t tag = tag0 + (uint32_t)j + 1u;
-    // CTA arg-max of |a(i, j)| over rows labelled >= j, lowest label on ties
+    // CTA arg-max of |a(i, j)| (register column 0) over rows labelled >= j,
+    // lowest label on ties
     unsigned bkey = 0u, bidx = 0xFFFFFFFFu;
 #pragma unroll
     for (int k = 0; k < kLLRows; ++k) {
-      const unsigned kk = nxt[k] >= 0.f ? __float_as_uint(nxt[k]) + 1u : 0u;
+      const unsigned kk = lab[k] >= j ? __float_as_uint(fabsf(a[k][0])) + 1u : 0u;
       if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) { bkey = kk; bidx = (unsigned)lab[k]; }
     }
     {
@@ -411,80 +458,432 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
 #pragma unroll
       for (int k = 0; k < kLLRows; ++k) lab[k] = lab[k] == j ? p : (lab[k] == p ? j : lab[k]);
     }
-    const float pv = prow[j];
+    const float pv = prow[0];
     const bool nz = pv != 0.f;
     const float inv = nz ? 1.f / pv : 0.f;
-    if (j < 8) ll_update<0>(a, lab, j, inv, nz, prow, nxt);
-    else if (j < 16) ll_update<8>(a, lab, j, inv, nz, prow, nxt);
-    else if (j < 24) ll_update<16>(a, lab, j, inv, nz, prow, nxt);
-    else ll_update<24>(a, lab, j, inv, nz, prow, nxt);
-  }
-  // every row to the panel row it stands for
-#pragma unroll
-  for (int k = 0; k < kLLRows; ++k)
-#pragma unroll
-    for (int c = 0; c < kBaseW; ++c)
-      if (lab[k] >= 0 && c < w) A[(int64_t)lab[k] + lda * c] = a[k][c];
-  if (left + right == 0) return;
-  // The same interchanges on the enclosing block panel's other columns
-  // (left: [-left, 0), right: [w, w + right)), in place of the row swaps a
-  // recursive panel makes between its halves.  A moved row's old values go to
-  // xtmp first, at slot = its final label if < w, else w + its first row
-  // (a row starting at w or below only ever moves to a label < w, so the
-  // slots are distinct); then a barrier over the CTAs; then to the final row.
-  __shared__ int s_nmv;
-  __shared__ int s_src[2 * kBaseW], s_dst[2 * kBaseW], s_slot[2 * kBaseW];
-  if (tid == 0) s_nmv = 0;
-  __syncthreads();
-  if (!s_fail) {
+    // Column j of every row is final after this step (the multiplier of a
+    // row below, U of the pivot and of earlier pivots): it goes to the row's
+    // slot in A, and the registers shift left by one as the rows below take
+    // the rank-1 update (multiplier 0 for the others: a plain shift).
 #pragma unroll
     for (int k = 0; k < kLLRows; ++k) {
-      const int phys = g0 + k * kLLThreads;
-      if (lab[k] >= 0 && lab[k] != phys) {
-        const int q = atomicAdd(&s_nmv, 1);
-        s_src[q] = phys;
-        s_dst[q] = lab[k];
-        s_slot[q] = lab[k] < w ? lab[k] : w + phys;
+      const bool below = nz && lab[k] > j;
+      const float l = below ? a[k][0] * inv : a[k][0];
+      const float lz = below ? l : 0.f;
+      if (lab[k] >= 0) A[(int64_t)(g0 + k * kLLThreads) + lda * j] = l;
+#pragma unroll
+      for (int c = 0; c + 1 < kBaseW; ++c) a[k][c] = fmaf(-lz, prow[c + 1], a[k][c + 1]);
+      a[k][kBaseW - 1] = 0.f;
+    }
+  }
+  __shared__ MoveShared ms;
+  ll_finish(ms, A, lda, w, lab, g0, left, right, xtmp, slots + (size_t)2 * kLLMaxCtas * kLLSlot, tag0 + 63u, err,
+            s_fail);
+}
+
+// ------------------------------------------ tournament-pivoting FP32 panel
+// For the mixed-precision factorisation only (FP64 keeps LAPACK's partial
+// pivoting).  Same register layout as panel_ll_kernel, but the pivots of all
+// w columns are chosen with one exchange over the grid instead of one per
+// column: TSLU, the panel step of communication-avoiding LU (Grigori, Demmel
+// and Xiang, "CALU: a communication optimal LU factorization algorithm",
+// SIAM J. Matrix Anal. Appl. 32 (2011) 1317-1350), with a flat tournament:
+//  1. each CTA runs partial pivoting on its own rows, exchanging through
+//     shared memory only, and publishes the original values of the <= w rows
+//     it chose;
+//  2. after one grid barrier every CTA loads all G w candidates (<= 1536, one
+//     per register row) and runs partial pivoting on them.  The same inputs
+//     and the same arithmetic in every CTA give every CTA the same w pivot
+//     rows and the same rows of U, with no broadcast;
+//  3. each CTA turns the pivots into LAPACK interchanges (row j <-> row
+//     piv[j], in order), reloads its rows and, after a second barrier (other
+//     CTAs' rows move onto rows this CTA reloads), eliminates them with the
+//     known U, writing each row at its final place.
+// With one CTA step 2 is skipped: step 1 is partial pivoting on the whole panel.
+//
+// The partial pivoting of steps 1 and 2 is blocked, kLeaf columns at a time,
+// so that every register index is a compile-time constant: the leaf's columns
+// sit in register columns [0, kLeaf) and take the rank-1 steps; the leaf's
+// pivot rows give U12 = L11^-1 A12 (one small forward substitution in shared
+// memory); the other rows take A22 -= L21 U12; then the registers shift left
+// by kLeaf.  Step 3 runs the same elimination with U from step 2 (a pivot row
+// stops at its own column), so each pivot row ends bit-identical to its U row.
+// Zero pivots are reported as partial pivoting does: info = first column
+// whose chosen pivot is 0.  The refinement against the FP64 matrix, not the
+// pivot sequence, pins the mixed solution.
+constexpr int kTsluMaxCtas = kLLCap / kBaseW;  // candidates fill one CTA's registers: 48
+constexpr int kLeaf = 8;
+constexpr int kTrail = kBaseW - kLeaf;
+constexpr int kLLWarps = kLLThreads / 32;
+
+struct TsluShared {
+  float stage[kLeaf][kLLWarps][kLeaf];  // leaf step s: each warp's arg-max row, leaf columns
+  unsigned key[kLeaf][kLLWarps];
+  unsigned idx[kLeaf][kLLWarps];
+  int win[kLeaf];                       // warp whose row won leaf step s
+  float u12[kLeaf][kTrail];             // the leaf's pivot rows, trailing columns -> U12
+  int sel[kBaseW];                      // label chosen at column j, -1: none left
+  float fin[kBaseW][kBaseW];            // row j: U(j, c) for c >= j
+  int pos[kLLCap];                      // own row -> pivot column, then -> final label
+  int zero;                             // first column with a zero pivot (kBaseW: none)
+};
+
+// Register row k's leaf columns to shared memory (if-chain: static indices).
+template <int K = 0>
+__device__ __forceinline__ void leaf_row_to_smem(const float (&a)[kLLRows][kBaseW], int k, float* dst) {
+  if (k == K) {
+#pragma unroll
+    for (int c = 0; c < kLeaf; ++c) dst[c] = a[K][c];
+  } else if constexpr (K + 1 < kLLRows) {
+    leaf_row_to_smem<K + 1>(a, k, dst);
+  }
+}
+
+// Blocked partial pivoting over columns [0, w) of the rows this CTA holds
+// (lab[k] >= 0); ties go to the lower label, as in panel_ll_kernel.
+// sh.sel[j] <- label chosen at column j, sh.zero <- first zero pivot, and
+// with want_fin sh.fin[j] <- U(j, c >= j).  The registers are consumed.
+__device__ __forceinline__ void tslu_gepp(float (&a)[kLLRows][kBaseW], const int (&lab)[kLLRows], int w,
+                                          bool want_fin, TsluShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  bool act[kLLRows];
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) act[k] = lab[k] >= 0;
+  if (tid == 0) sh.zero = kBaseW;
+#pragma unroll 1
+  for (int j0 = 0; j0 < w; j0 += kLeaf) {
+    const int lw = min(kLeaf, w - j0);
+    int cs[kLLRows];  // leaf step at which register row k was chosen, -1: not in this leaf
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) cs[k] = -1;
+#pragma unroll
+    for (int s = 0; s < kLeaf; ++s) {
+      if (s >= lw) break;
+      unsigned bkey = 0u, bidx = 0xFFFFFFFFu;
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) {
+        const unsigned kk = act[k] ? __float_as_uint(fabsf(a[k][s])) + 1u : 0u;
+        if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) {
+          bkey = kk;
+          bidx = (unsigned)lab[k];
+        }
+      }
+      const unsigned wm = __reduce_max_sync(0xffffffffu, bkey);
+      const unsigned wi = __reduce_min_sync(0xffffffffu, bkey == wm ? bidx : 0xFFFFFFFFu);
+      if (wm != 0u) {
+        int kc = -1;
+#pragma unroll
+        for (int k = 0; k < kLLRows; ++k) kc = (act[k] && (unsigned)lab[k] == wi) ? k : kc;
+        if (kc >= 0) leaf_row_to_smem(a, kc, sh.stage[s][warp]);
+      }
+      if (lane == 0) {
+        sh.key[s][warp] = wm;
+        sh.idx[s][warp] = wi;
+      }
+      __syncthreads();
+      const unsigned k2 = lane < kLLWarps ? sh.key[s][lane] : 0u;
+      const unsigned i2 = lane < kLLWarps ? sh.idx[s][lane] : 0xFFFFFFFFu;
+      const unsigned gk = __reduce_max_sync(0xffffffffu, k2);
+      const unsigned gi = __reduce_min_sync(0xffffffffu, k2 == gk ? i2 : 0xFFFFFFFFu);
+      const unsigned gw = __reduce_max_sync(0xffffffffu, (k2 == gk && i2 == gi) ? (unsigned)lane : 0u);
+      if (tid == 0) {
+        sh.sel[j0 + s] = gk != 0u ? (int)gi : -1;
+        sh.win[s] = (int)gw;
+        if (gk <= 1u) sh.zero = min(sh.zero, j0 + s);  // no row left, or |pivot| == 0
+      }
+      if (gk == 0u) continue;
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) {
+        if (act[k] && (unsigned)lab[k] == gi) {
+          act[k] = false;
+          cs[k] = s;
+        }
+      }
+      const float* prow = sh.stage[s][gw];
+      const float pv = prow[s];
+      if (pv == 0.f) continue;
+      const float inv = 1.f / pv;
+      float pc[kLeaf];
+#pragma unroll
+      for (int c = s + 1; c < kLeaf; ++c) pc[c] = prow[c];
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) {
+        if (!act[k]) continue;
+        const float l = a[k][s] * inv;
+        a[k][s] = l;
+#pragma unroll
+        for (int c = s + 1; c < kLeaf; ++c) a[k][c] = fmaf(-l, pc[c], a[k][c]);
+      }
+    }
+    // the leaf's pivot rows, trailing columns as at the leaf's start
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+      if (cs[k] < 0) continue;
+      float* d = sh.u12[cs[k]];
+#pragma unroll
+      for (int c = 0; c < kTrail; ++c) d[c] = a[k][kLeaf + c];
+    }
+    __syncthreads();
+    // U12 = L11^-1 A12; L11(i, i2) = multiplier of the pivot row of step i at leaf column i2
+    if (tid < kTrail) {
+      float u[kLeaf];
+#pragma unroll
+      for (int i = 0; i < kLeaf; ++i) {
+        const bool ok = i < lw && sh.sel[j0 + i] >= 0;
+        u[i] = ok ? sh.u12[i][tid] : 0.f;
+        if (ok) {
+          const float* li = sh.stage[i][sh.win[i]];
+#pragma unroll
+          for (int i2 = 0; i2 < i; ++i2) u[i] = fmaf(-li[i2], u[i2], u[i]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kLeaf; ++i) sh.u12[i][tid] = u[i];
+    }
+    __syncthreads();
+    if (want_fin) {
+      for (int e = tid; e < kLeaf * kBaseW; e += kLLThreads) {
+        const int i = e / kBaseW, col = e - i * kBaseW, j = j0 + i;
+        if (i < lw && col >= j && sh.sel[j] >= 0)
+          sh.fin[j][col] = col < j0 + kLeaf ? sh.stage[i][sh.win[i]][col - j0] : sh.u12[i][col - j0 - kLeaf];
+      }
+    }
+    // A22 -= L21 U12 on the rows still in play (kLeaf trailing columns at a
+    // time, to bound the registers), then the registers shift by a leaf
+#pragma unroll
+    for (int cb = 0; cb < kTrail; cb += kLeaf) {
+#pragma unroll
+      for (int i = 0; i < kLeaf; ++i) {
+        float u[kLeaf];
+#pragma unroll
+        for (int c = 0; c < kLeaf; ++c) u[c] = sh.u12[i][cb + c];
+#pragma unroll
+        for (int k = 0; k < kLLRows; ++k) {
+          if (!act[k]) continue;
+          const float l = a[k][i];
+#pragma unroll
+          for (int c = 0; c < kLeaf; ++c) a[k][kLeaf + cb + c] = fmaf(-l, u[c], a[k][kLeaf + cb + c]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+#pragma unroll
+      for (int c = 0; c < kTrail; ++c) a[k][c] = a[k][c + kLeaf];
+#pragma unroll
+      for (int c = kTrail; c < kBaseW; ++c) a[k][c] = 0.f;
+    }
+    __syncthreads();
+  }
+}
+
+// Step 3: the rows of this CTA (original values) eliminated with U = sh.fin.
+// rk[k] packs register row k's final label (bits 0-16) and the column it is
+// the pivot of, plus 1 (bits 17-22; 0: none); -1: no row.  A pivot row stops
+// at its own column.  Each leaf's columns are written to A as they finish.
+constexpr int kRkBits = 17;
+static_assert(kTsluMaxCtas * kLLCap <= (1 << kRkBits), "tournament rows fit the packed label");
+__device__ __forceinline__ int rk_pcol(int rk) { return (rk >> kRkBits) - 1; }
+
+__device__ __forceinline__ void tslu_eliminate(float (&a)[kLLRows][kBaseW], const int (&rk)[kLLRows], int w,
+                                               const TsluShared& sh, float* __restrict__ A, int64_t lda) {
+#pragma unroll 1
+  for (int j0 = 0; j0 < w; j0 += kLeaf) {
+    const int lw = min(kLeaf, w - j0);
+#pragma unroll
+    for (int s = 0; s < kLeaf; ++s) {
+      if (s >= lw) break;
+      const int j = j0 + s;
+      const float* U = sh.fin[j];
+      const float pv = U[j];
+      if (pv == 0.f) continue;
+      const float inv = 1.f / pv;
+      float pc[kLeaf];
+#pragma unroll
+      for (int c = s + 1; c < kLeaf; ++c) pc[c] = U[j0 + c];
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) {
+        const int p = rk_pcol(rk[k]);
+        if (rk[k] < 0 || (p >= 0 && p <= j)) continue;
+        const float l = a[k][s] * inv;
+        a[k][s] = l;
+#pragma unroll
+        for (int c = s + 1; c < kLeaf; ++c) a[k][c] = fmaf(-l, pc[c], a[k][c]);
+      }
+    }
+    // trailing columns: multipliers of the leaf steps each row took part in
+    // (all kLeaf, up to its own column for this leaf's pivot rows, none for
+    // rows done in earlier leaves)
+#pragma unroll
+    for (int cb = 0; cb < kTrail; cb += kLeaf) {
+      if (j0 + kLeaf + cb >= kBaseW) break;
+#pragma unroll
+      for (int i = 0; i < kLeaf; ++i) {
+        if (i >= lw) break;
+        float u[kLeaf];
+        const float* U = sh.fin[j0 + i] + j0 + kLeaf + cb;
+#pragma unroll
+        for (int c = 0; c < kLeaf; ++c) u[c] = U[c];
+#pragma unroll
+        for (int k = 0; k < kLLRows; ++k) {
+          const int p = rk_pcol(rk[k]);
+          if (rk[k] < 0 || (p >= 0 && p <= j0 + i)) continue;
+          const float l = a[k][i];
+#pragma unroll
+          for (int c = 0; c < kLeaf; ++c) a[k][kLeaf + cb + c] = fmaf(-l, u[c], a[k][kLeaf + cb + c]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+      if (rk[k] >= 0) {
+        float* row = A + (int64_t)(rk[k] & ((1 << kRkBits) - 1)) + lda * j0;
+#pragma unroll
+        for (int c = 0; c < kLeaf; ++c)
+          if (c < lw) row[lda * c] = a[k][c];
+      }
+#pragma unroll
+      for (int c = 0; c < kTrail; ++c) a[k][c] = a[k][c + kLeaf];
+#pragma unroll
+      for (int c = kTrail; c < kBaseW; ++c) a[k][c] = 0.f;
+    }
+  }
+}
+
+// The pivots sh.sel[0..w) (labels) as LAPACK interchanges, by one warp:
+// piv[j] = place of row sel[j] after the interchanges of columns < j.  Lane
+// x < w tracks the row now at place x; lane j also keeps the one place >= w
+// that column j's interchange may create (far_pos, holding row far_row).  The
+// final label of every row of [r0, r0 + nrow) that moved goes to sh.pos.
+__device__ void tslu_interchanges(int w, int64_t r0, int nrow, int32_t* __restrict__ piv, int piv_add,
+                                  bool write_piv, TsluShared& sh) {
+  const int x = threadIdx.x & 31;
+  int row_at = x, far_pos = -1, far_row = -1;
+  for (int j = 0; j < w; ++j) {
+    const int p = sh.sel[j];
+    const unsigned near = __ballot_sync(0xffffffffu, x < w && row_at == p);
+    const unsigned far = __ballot_sync(0xffffffffu, far_pos >= 0 && far_row == p);
+    int cur;
+    if (near) cur = __ffs(near) - 1;
+    else if (far) cur = __shfl_sync(0xffffffffu, far_pos, __ffs(far) - 1);
+    else cur = p;
+    const int rj = __shfl_sync(0xffffffffu, row_at, j);
+    if (x == 0 && write_piv) piv[j] = cur + piv_add;
+    if (cur != j) {
+      if (x == j) row_at = p;
+      if (cur < w) {
+        if (x == cur) row_at = rj;
+      } else if (far) {
+        if (x == __ffs(far) - 1) far_row = rj;
+      } else if (x == j) {
+        far_pos = cur;
+        far_row = rj;
       }
     }
   }
-  __syncthreads();
-  const int nmv = s_nmv, ncol = left + right;
-  for (int i = tid; i < nmv * ncol; i += kLLThreads) {
-    const int q = i / ncol, cc = i - q * ncol;
-    const int64_t col = cc < left ? (int64_t)(cc - left) : (int64_t)(w + cc - left);
-    xtmp[(size_t)s_slot[q] * ncol + cc] = A[(int64_t)s_src[q] + lda * col];
+  if (x < w && row_at >= r0 && row_at < r0 + nrow) sh.pos[row_at - r0] = x;
+  if (far_pos >= 0 && far_row >= r0 && far_row < r0 + nrow) sh.pos[far_row - r0] = far_pos;
+}
+
+__global__ void __launch_bounds__(kLLThreads, 1) panel_tslu_kernel(
+    float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
+    uint64_t* __restrict__ slots, float* __restrict__ cand, int64_t* __restrict__ info, int64_t col_offset,
+    uint32_t tag0, int* __restrict__ err, int left, int right, float* __restrict__ xtmp, int piv_add) {
+  __shared__ TsluShared sh;
+  __shared__ MoveShared ms;
+  __shared__ int s_fail;
+  const int b = blockIdx.x, G = gridDim.x, tid = threadIdx.x;
+  const int64_t r0 = (int64_t)b * rpc;
+  const int nrow = (int)max((int64_t)0, min((int64_t)rpc, m - r0));
+  const int g0 = (int)r0 + tid;
+  const int nrow_left = nrow - tid;
+  uint64_t* bar = slots + (size_t)2 * kLLMaxCtas * kLLSlot;  // kLLMaxCtas words per barrier
+  int* cidx = reinterpret_cast<int*>(cand + (size_t)kTsluMaxCtas * kBaseW * kBaseW);
+  float a[kLLRows][kBaseW];
+  int lab[kLLRows];
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    lab[k] = k * kLLThreads < nrow_left ? g0 + k * kLLThreads : -1;
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c) a[k][c] = (lab[k] >= 0 && c < w) ? A[(int64_t)lab[k] + lda * c] : 0.f;
   }
-  // barrier: each CTA publishes one word with tag tag0 + 63 after its copies
-  // (release fence), every CTA waits for all (acquire fence after)
-  __syncthreads();
-  uint64_t* bar = slots + (size_t)2 * kLLMaxCtas * kLLSlot;
-  const uint32_t btag = tag0 + 63u;
-  if (tid == 0) {
-    __threadfence();
-    ll_store(bar + b, 0u, btag);
-  }
-  if (tid < G) {
-    const uint64_t t0 = global_ns();
-    while ((uint32_t)(ll_load(bar + tid) >> 32) != btag) {
-      if (global_ns() - t0 > kLLTimeoutNs) {
-        s_fail = 1;
-        break;
+  if (tid == 0) s_fail = 0;
+  const int rounds = G > 1 ? 2 : 1;
+#pragma unroll 1
+  for (int rd = 0; rd < rounds; ++rd) {
+    if (rd == 1) {
+      // candidates: original values of the rows chosen in round 0 at
+      // cand[(b kBaseW + i) kBaseW + c], their labels at cidx
+      for (int e = tid; e < kBaseW * kBaseW; e += kLLThreads) {
+        const int i = e / kBaseW, c = e - i * kBaseW;
+        const int r = i < w ? sh.sel[i] : -1;
+        cand[((size_t)b * kBaseW + i) * kBaseW + c] = (r >= 0 && c < w) ? A[(int64_t)r + lda * c] : 0.f;
+        if (c == 0) cidx[b * kBaseW + i] = r;
+      }
+      if (!ll_grid_barrier(bar + kLLMaxCtas, tag0 + 62u, s_fail)) {
+        if (tid == 0) atomicExch(err, 1);
+        return;
+      }
+      // list entry e = q kBaseW + i in register row e / kLLThreads of thread e % kLLThreads
+#pragma unroll
+      for (int k = 0; k < kLLRows; ++k) {
+        const int e = tid + k * kLLThreads;
+        lab[k] = e < G * kBaseW ? __ldcg(cidx + e) : -1;
+        const float4* src = reinterpret_cast<const float4*>(cand + (size_t)e * kBaseW);
+#pragma unroll
+        for (int c4 = 0; c4 < kBaseW / 4; ++c4) {
+          const float4 v = lab[k] >= 0 ? __ldcg(src + c4) : make_float4(0.f, 0.f, 0.f, 0.f);
+          a[k][4 * c4] = v.x;
+          a[k][4 * c4 + 1] = v.y;
+          a[k][4 * c4 + 2] = v.z;
+          a[k][4 * c4 + 3] = v.w;
+        }
       }
     }
-    __threadfence();
+    tslu_gepp(a, lab, w, rd == rounds - 1, sh);
+  }
+  if (b == 0 && tid == 0 && info && sh.zero < w && *info == 0) *info = col_offset + sh.zero + 1;
+  // own rows: pivot column, then final label
+  for (int i = tid; i < nrow; i += kLLThreads) sh.pos[i] = -1;
+  __syncthreads();
+  if (tid < w) {
+    const int r = sh.sel[tid];
+    if (r >= r0 && r < r0 + nrow) sh.pos[r - r0] = tid;
   }
   __syncthreads();
-  if (s_fail) {
+  int rk[kLLRows];  // pivot column + 1, then packed with the final label
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    lab[k] = k * kLLThreads < nrow_left ? g0 + k * kLLThreads : -1;
+    rk[k] = lab[k] >= 0 ? sh.pos[lab[k] - r0] + 1 : 0;
+  }
+  __syncthreads();
+  for (int i = tid; i < nrow; i += kLLThreads) sh.pos[i] = -1;
+  __syncthreads();
+  if (tid < 32) tslu_interchanges(w, r0, nrow, piv, piv_add, b == 0, sh);
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    const int moved = lab[k] >= 0 ? sh.pos[lab[k] - r0] : -1;
+    lab[k] = moved >= 0 ? moved : lab[k];  // final label from here on
+    rk[k] = lab[k] >= 0 ? lab[k] | (rk[k] << kRkBits) : -1;
+  }
+  // the block panel's other columns of moved rows to xtmp; then nobody reads
+  // this panel's rows any more, and every CTA writes its rows at their places
+  ll_moves_stash(ms, A, lda, w, lab, g0, left, 0, right, xtmp, s_fail);
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    const int r = k * kLLThreads < nrow_left ? g0 + k * kLLThreads : -1;
+#pragma unroll
+    for (int c = 0; c < kBaseW; ++c) a[k][c] = (r >= 0 && c < w) ? A[(int64_t)r + lda * c] : 0.f;
+  }
+  if (!ll_grid_barrier(bar, tag0 + 63u, s_fail)) {
     if (tid == 0) atomicExch(err, 1);
     return;
   }
   __threadfence();
-  for (int i = tid; i < nmv * ncol; i += kLLThreads) {
-    const int q = i / ncol, cc = i - q * ncol;
-    const int64_t col = cc < left ? (int64_t)(cc - left) : (int64_t)(w + cc - left);
-    A[(int64_t)s_dst[q] + lda * col] = xtmp[(size_t)s_slot[q] * ncol + cc];
-  }
+  tslu_eliminate(a, rk, w, sh, A, lda);
+  ll_moves_apply(ms, A, lda, w, left, 0, right, xtmp);
 }
 
 // -------------------------------------------------------------- row swaps
@@ -815,21 +1214,33 @@ struct LuWork {
   float* coef = nullptr;
   // moved rows of one base panel across the block panel: [2 kBaseW][nb]
   float* xtmp = nullptr;
+  // tournament candidates: [kTsluMaxCtas][kBaseW][kBaseW] rows, then labels
+  float* tslu = nullptr;
 };
 
-// HFPX_LU_PANEL=smem selects the shared-memory panel kernel for FP32 too.
-static bool ll_panel_enabled() {
-  static const bool on = [] {
+// FP32 base panels: partial pivoting in the register-resident kernel by
+// default; HFPX_LU_PANEL=smem takes the shared-memory kernel, =tslu the
+// tournament-pivoting kernel where its candidates fit.
+enum class PanelKind { Tournament, Register, Shared };
+static PanelKind panel_kind() {
+  static const PanelKind k = [] {
     const char* e = std::getenv("HFPX_LU_PANEL");
-    return !(e && std::string(e) == "smem");
+    const std::string s = e ? e : "";
+    return s == "smem" ? PanelKind::Shared : s == "tslu" ? PanelKind::Tournament : PanelKind::Register;
   }();
-  return on;
+  return k;
 }
+static bool ll_panel_enabled() { return panel_kind() != PanelKind::Shared; }
 
 // The register-resident panel takes m rows.
 template <class T>
 static bool ll_fits(const LuWork<T>& wk, int64_t m) {
-  return sizeof(T) == 4 && wk.ll_slots && (m + kLLCap - 1) / kLLCap <= kLLMaxCtas && ll_panel_enabled();
+  return sizeof(T) == 4 && wk.ll_slots && wk.xtmp && (m + kLLCap - 1) / kLLCap <= kLLMaxCtas && ll_panel_enabled();
+}
+// ... and with tournament pivoting.
+template <class T>
+static bool tslu_fits(const LuWork<T>& wk, int64_t m) {
+  return wk.tslu && ll_fits(wk, m) && (m + kLLCap - 1) / kLLCap <= kTsluMaxCtas;
 }
 
 struct PanelSpan {
@@ -915,9 +1326,17 @@ static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int
       int rpc = (int)((m + G - 1) / G);
       uint32_t tag0 = (++wk.ll_launches) << 6;
       int left = sp.eager ? sp.c0 : 0, right = sp.eager ? sp.bw - sp.c0 - w : 0, piv_add = sp.eager ? sp.c0 : 0;
+      ++g_launches;
+      if (tslu_fits(wk, m)) {
+        void* targs[] = {&A,          &lda, &m,         &w,    &rpc,   &piv,     &wk.ll_slots, &wk.tslu,
+                         &wk.d_info, &col_offset, &tag0, &wk.ll_err, &left, &right, &wk.xtmp,     &piv_add};
+        return check_cuda(c,
+                          cudaLaunchCooperativeKernel((void*)panel_tslu_kernel, dim3(G), dim3(kLLThreads), targs, 0,
+                                                      l.s),
+                          "panel_tslu_kernel launch");
+      }
       void* args[] = {&A,  &lda,       &m,           &w,    &rpc,  &piv,    &wk.ll_slots, &wk.d_info,
                       &col_offset, &tag0, &wk.ll_err, &left, &right, &wk.xtmp, &piv_add};
-      ++g_launches;
       return check_cuda(c, cudaLaunchCooperativeKernel((void*)panel_ll_kernel, dim3(G), dim3(kLLThreads), args, 0, l.s),
                         "panel_ll_kernel launch");
     }
@@ -1039,11 +1458,14 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   const int64_t n_blocks = (n + lu_block_size() - 1) / lu_block_size();
   wk.plan_panel = (int32_t*)alloc(kScrPlanPanel, sizeof(int32_t) * kSwapPlanInts);
   wk.plans = (int32_t*)alloc(kScrPlans, sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
-  // two column buffers of per-CTA words, then one barrier word per CTA
-  const size_t ll_bytes = sizeof(uint64_t) * (2 * kLLMaxCtas * kLLSlot + kLLMaxCtas);
+  // two column buffers of per-CTA words, then two barriers of one word per CTA
+  const size_t ll_bytes = sizeof(uint64_t) * (2 * kLLMaxCtas * kLLSlot + 2 * kLLMaxCtas);
   if (sizeof(T) == 4) {
     wk.ll_slots = (uint64_t*)alloc(kScrLLSlots, ll_bytes);
     wk.ll_err = (int*)alloc(kScrLLErr, sizeof(int));
+    // optional: without it the panels keep partial pivoting
+    if (panel_kind() == PanelKind::Tournament)
+      wk.tslu = (float*)alloc(kScrTslu, (sizeof(float) * kBaseW + sizeof(int)) * kTsluMaxCtas * kBaseW);
     // optional: without room for them the block row takes the triangular solve
     const size_t nb = (size_t)lu_block_size();
     wk.xtmp = (float*)alloc(kScrXtmp, sizeof(float) * 2 * kBaseW * nb);

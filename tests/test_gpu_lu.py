@@ -104,26 +104,46 @@ np.save(sys.argv[2], np.concatenate([x, [lu.last_info.iterations, lu.last_info.r
 '''
 
 
-@pytest.mark.parametrize('n_el', [300, 1200])
-def test_fp32_panel_kernels_agree_bitwise(tmp_path, n_el):
-    # the register-resident FP32 panel (L2 word exchange) and the shared-memory
-    # panel (grid barrier per column) take the same pivots and do the same
-    # arithmetic per element: the mixed solutions match bit for bit.  1200
-    # elements (21 600 rows) spread the first panels over 15 CTAs.
+def _panel_runs(tmp_path, n_el, kinds):
     import os
     import subprocess
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = {}
-    for kind in ('', 'smem'):
+    for kind in kinds:
         env = dict(os.environ, HFPX_LU_PANEL=kind, PYTHONPATH=root)
-        f = tmp_path / ('x_%s.npy' % (kind or 'll'))
+        f = tmp_path / ('x_%s.npy' % (kind or 'default'))
         r = subprocess.run([sys.executable, '-c', _PANEL_RUN, str(n_el), str(f)], env=env, cwd=root,
                            capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         out[kind] = np.load(f)
-    assert np.array_equal(out[''], out['smem'])
-    assert out[''][-1] <= 1e-12
+    return out
+
+
+@pytest.mark.parametrize('n_el', [300, 1200])
+def test_fp32_panel_kernels_agree_bitwise(tmp_path, n_el):
+    # the register-resident FP32 panel with partial pivoting (L2 word exchange
+    # per column) and the shared-memory panel (grid barrier per column) take
+    # the same pivots and do the same arithmetic per element: the mixed
+    # solutions match bit for bit.  1200 elements (21 600 rows) spread the
+    # first panels over 15 CTAs.
+    out = _panel_runs(tmp_path, n_el, ('ll', 'smem'))
+    assert np.array_equal(out['ll'], out['smem'])
+    assert out['ll'][-1] <= 1e-12
+
+
+@pytest.mark.parametrize('n_el', [300, 1200, 2500])
+def test_tournament_panel_reaches_the_same_solution(tmp_path, n_el):
+    # HFPX_LU_PANEL=tslu pivots the mixed factorisation by tournament (one
+    # exchange per 32 columns instead of one per column); its pivots differ
+    # from partial pivoting's, and the refinement against the FP64 matrix
+    # brings both to the same solution.  2500 elements (45 000 rows) spread
+    # the first panels over 30 CTAs, 960 tournament candidates.
+    out = _panel_runs(tmp_path, n_el, ('tslu', ''))
+    x0, x1 = out[''][:-2], out['tslu'][:-2]
+    assert out['tslu'][-1] <= 1e-12
+    assert out['tslu'][-2] <= out[''][-2] + 2     # refinement iterations
+    assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
 
 
 def test_mixed_singular_reports_column(ctx):
