@@ -33,17 +33,19 @@ namespace cg = cooperative_groups;
 namespace hfpx {
 
 constexpr int kBaseW = 32;
+constexpr int kLuNbMax = 1536;  // largest block (row-swap plans hold 2 nb rows)
 // Block size of the right-looking LU: each trailing update reads and writes
 // the remaining matrix once, so HBM traffic ~ N^3 / (3 nb) x 8 bytes (FP32);
-// larger blocks move work into the (overlapped) panel.  HFPX_LU_NB overrides
-// the default (multiple of 32 in [64, 1024]).
-static int lu_block_size() {
-  static const int nb = [] {
+// larger blocks move work into the (overlapped) panel.  Defaults measured at
+// N = 72 000: FP32 (mixed) 1536, FP64 768.  HFPX_LU_NB overrides both
+// (multiple of 32 in [64, kLuNbMax]).
+static int lu_block_size(bool fp32) {
+  static const int env = [] {
     const char* e = std::getenv("HFPX_LU_NB");
     const int v = e ? std::atoi(e) : 0;
-    return (v >= 64 && v <= 1024 && v % kBaseW == 0) ? v : 768;
+    return (v >= 64 && v <= kLuNbMax && v % kBaseW == 0) ? v : 0;
   }();
-  return nb;
+  return env ? env : fp32 ? kLuNbMax : 768;
 }
 constexpr int kPanelThreads = 256;
 
@@ -892,7 +894,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_tslu_kernel(
 // rows they touch (a "plan": new row dst[e] = old row src[e]), then applied
 // to every column as one gather: contiguous reads of the leading rows
 // instead of k dependent strided swaps per column.
-constexpr int kSwapMax = 1024;                  // interchanges per plan (block size cap)
+constexpr int kSwapMax = kLuNbMax;              // interchanges per plan (block size cap)
 constexpr int kSwapHash = 4096;                 // rows >= k touched, open addressing
 constexpr int kSwapPlanInts = 1 + 4 * kSwapMax; // count, src[2 kSwapMax], dst[2 kSwapMax]
 constexpr int kSwapThreads = 256;
@@ -1455,7 +1457,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   wk.sc.cidx = (int*)alloc(kScrPanelIdx, sizeof(int) * 2 * G);
   wk.sc.rowj = (T*)alloc(kScrPanelRowj, sizeof(T) * 2 * kBaseW);
   wk.d_info = (int64_t*)alloc(kScrInfo, sizeof(int64_t));
-  const int64_t n_blocks = (n + lu_block_size() - 1) / lu_block_size();
+  const int64_t n_blocks = (n + lu_block_size(sizeof(T) == 4) - 1) / lu_block_size(sizeof(T) == 4);
   wk.plan_panel = (int32_t*)alloc(kScrPlanPanel, sizeof(int32_t) * kSwapPlanInts);
   wk.plans = (int32_t*)alloc(kScrPlans, sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
   // two column buffers of per-CTA words, then two barriers of one word per CTA
@@ -1467,7 +1469,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     if (panel_kind() == PanelKind::Tournament)
       wk.tslu = (float*)alloc(kScrTslu, (sizeof(float) * kBaseW + sizeof(int)) * kTsluMaxCtas * kBaseW);
     // optional: without room for them the block row takes the triangular solve
-    const size_t nb = (size_t)lu_block_size();
+    const size_t nb = (size_t)lu_block_size(sizeof(T) == 4);
     wk.xtmp = (float*)alloc(kScrXtmp, sizeof(float) * 2 * kBaseW * nb);
     wk.linv = (T*)alloc(kScrLinv, sizeof(T) * nb * nb);
     wk.a12 = (T*)alloc(kScrA12, sizeof(T) * nb * (size_t)n);
@@ -1491,7 +1493,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   }
   const Lane M = main_lane(c), Pn = panel_lane(c);
   const cudaStream_t S = c->stream_left;
-  const int kNb = lu_block_size();
+  const int kNb = lu_block_size(sizeof(T) == 4);
   cudaEvent_t ev_panel = nullptr, ev_next = nullptr, ev_rest = nullptr, ev_left = nullptr, ev_start = nullptr;
   for (cudaEvent_t* e : {&ev_panel, &ev_next, &ev_rest, &ev_left, &ev_start})
     if (!rc) rc = check_cuda(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "LU events");
