@@ -1,6 +1,7 @@
 // The mixed-precision refinement's memory-bound pieces, one right-hand side:
 //   * triangular solves with the FP32 factors (forward with unit L, backward
-//     with U) as one persistent sweep over 128-row tiles;
+//     with U) as one persistent sweep over 128-row tiles, the factor blocks
+//     streamed through shared memory by bulk copies;
 //   * the FP64 residual r = b - A x and its largest magnitude.
 // Both replace cuBLAS calls of the refinement (dgetrs-style solve at
 // il/linear_algebra/dense/factorization/LU.h:106-120 applied to FP32 factors,
@@ -17,21 +18,29 @@ namespace hfpx {
 // Solve order s = 0 .. T-1 over the 128-row tiles (tile s forward, tile
 // T-1-s backward).  One CTA per SM, launched cooperatively; CTA g owns the
 // solves s = g, g + G, ... and keeps their right-hand sides in shared
-// memory.  For each s in turn, every CTA
+// memory.  For each s in turn, a CTA with work left
 //   * takes x_s: its owner computes x_s = D_s^-1 y_s with the inverse of the
 //     diagonal block (precomputed once per factorisation) and publishes it
 //     as 128 8-byte words (value + the solve's epoch); the others poll those
 //     words (one L2 round trip, no flag, no fence);
-//   * subtracts A(t', t_s) x_s from its owned tiles t' later in solve order,
-//     the next solve's tile first, with that tile and the next inverse
-//     loaded before the wait.
-// The critical path per tile: one word exchange and two 128 x 128 products.
-// Every wait gives up after kTrsvTimeoutNs and records the failure.
+//   * first the next solve's tile: its owner subtracts A(t_{s+1}, t_s) x_s
+//     (that block and the next inverse loaded before the wait), solves and
+//     publishes: the critical path per tile is one word exchange and two
+//     128 x 128 products;
+//   * then subtracts A(t', t_s) x_s from its other owned tiles t' later in
+//     solve order.  Those blocks are one stream per CTA, in the order they
+//     are used, fed into a two-block shared-memory ring by asynchronous
+//     16-byte copies (cp.async, one commit group per block), so the next
+//     blocks load while the CTA waits for x and works the critical path.
+// Every word wait gives up after kTrsvTimeoutNs, records the failure and
+// ends the kernel (after its copies in flight complete).
 constexpr int kTb = 128;
 constexpr int kSwThreads = 256;
 constexpr int kSwMaxOwn = 16;  // solves per CTA: n <= 16 * 148 * 128 rows
+constexpr int kSwRing = 2;
 constexpr unsigned long long kTrsvTimeoutNs = 200ull * 1000 * 1000;
-constexpr size_t kSwSmem = sizeof(float) * (2 * kTb * kTb + kSwMaxOwn * kTb + 6 * kTb);
+constexpr size_t kSwSmemFloats = (size_t)(kSwRing + 1) * kTb * kTb + kSwMaxOwn * kTb + 2 * kTb + 4 * kTb + 2 * kTb;
+constexpr size_t kSwSmem = sizeof(float) * kSwSmemFloats;
 
 __device__ __forceinline__ unsigned long long trsv_ns() {
   unsigned long long t;
@@ -47,19 +56,30 @@ __device__ __forceinline__ uint64_t xw_load(const uint64_t* p) {
   asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
   return w;
 }
+__device__ __forceinline__ uint32_t sw_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void sw_copy16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sw_smem(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void sw_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most `pending` of this thread's copy groups are in flight
+__device__ __forceinline__ void sw_wait_groups(int pending) {
+  if (pending <= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
+  else asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
 
 template <bool UPPER>
 __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* __restrict__ A, int64_t lda, int n,
                                                                    const float* __restrict__ dinv,
                                                                    float* __restrict__ x, uint64_t* __restrict__ xw,
                                                                    uint32_t epoch, int* __restrict__ err) {
-  extern __shared__ float sm[];
-  float* s_dinv = sm;                       // [2][kTb * kTb], column-major blocks
-  float* s_y = s_dinv + 2 * kTb * kTb;      // [kSwMaxOwn][kTb]
-  float* s_x = s_y + kSwMaxOwn * kTb;       // [kTb] x of the strip being applied
-  float* s_xo = s_x + kTb;                  // [kTb] x of this CTA's latest solve
-  float* s_red = s_xo + kTb;                // [2][kTb]
-  float* s_red2 = s_red + 2 * kTb;          // [2][kTb]
+  extern __shared__ __align__(16) float sm[];
+  float* s_ring = sm;                          // [kSwRing][kTb * kTb], column-major blocks
+  float* s_dinv = s_ring + kSwRing * kTb * kTb;  // [kTb * kTb] inverse for the next owned solve
+  float* s_y = s_dinv + kTb * kTb;             // [kSwMaxOwn][kTb]
+  float* s_x = s_y + kSwMaxOwn * kTb;          // [kTb] x of the strip being applied
+  float* s_xo = s_x + kTb;                     // [kTb] x of this CTA's latest solve
+  float* s_red = s_xo + kTb;                   // [2 parities][2 halves][kTb]
+  float* s_redc = s_red + 4 * kTb;             // [2 halves][kTb] (critical path)
   __shared__ int s_fail;
   const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x;
   const int T = (n + kTb - 1) / kTb;
@@ -67,34 +87,67 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
   constexpr int kHalf = kTb / 2;
   auto tile_of = [&](int s) { return UPPER ? T - 1 - s : s; };
   auto rows_of = [&](int t) { return min(kTb, n - t * kTb); };
-  auto load_dinv = [&](float* dst, int t) {
-    const float* src = dinv + (size_t)t * kTb * kTb;
-    for (int i = tid; i < kTb * kTb; i += kSwThreads) dst[i] = src[i];
-  };
   const int nown = g < T ? (T - 1 - g) / G + 1 : 0;
+  const int last_own = g + (nown - 1) * G;  // solve index of the last owned tile
+  // first owned index with solve index > s + 1
+  auto i_first = [&](int s) { return s + 1 - g >= 0 ? (s + 1 - g) / G + 1 : 0; };
   for (int i = 0; i < nown; ++i) {
     const int t = tile_of(g + i * G);
     if (tid < kTb) s_y[i * kTb + tid] = tid < rows_of(t) ? x[(int64_t)t * kTb + tid] : 0.f;
   }
+  // stale ring contents meet zero x entries only: start them finite
+  for (int i = tid; i < kSwRing * kTb * kTb; i += kSwThreads) s_ring[i] = 0.f;
   if (tid == 0) s_fail = 0;
-  if (nown > 0) load_dinv(s_dinv + (g & 1) * kTb * kTb, tile_of(g));
+  if (nown > 0) {
+    const float* src = dinv + (size_t)tile_of(g) * kTb * kTb;
+    for (int i = tid; i < kTb * kTb; i += kSwThreads) s_dinv[i] = src[i];
+  }
   __syncthreads();
+  // the block stream: (strip ps, owned index pi) in the order used
+  int ps = 0, pi = i_first(0);
+  while (ps < T && pi >= nown) {
+    ++ps;
+    if (ps < T) pi = i_first(ps);
+  }
+  int inflight = 0;   // blocks issued and not yet used (the same in every thread)
+  int slot_next = 0;  // slot of the next block to use
+  // every thread copies its 16-byte pieces of the next block of the stream
+  // into `slot` (piece q: column q / 32, rows 4 (q % 32) ..), one group, and
+  // the stream advances
+  auto issue = [&](int slot) {
+    if (ps >= T) return;
+    const int rt = tile_of(g + pi * G), ct = tile_of(ps);
+    const int rows = rows_of(rt), cols = rows_of(ct);
+    float* dst = s_ring + (size_t)slot * kTb * kTb;
+    const float* src = A + (int64_t)rt * kTb + lda * (int64_t)ct * kTb;
+    for (int q = tid; q < kTb * kTb / 4; q += kSwThreads) {
+      const int c = q >> 5, ro = (q & 31) * 4;
+      if (c < cols && ro < rows) sw_copy16(dst + c * kTb + ro, src + ro + lda * c);
+    }
+    sw_commit();
+    ++inflight;
+    ++pi;
+    while (ps < T && pi >= nown) {
+      ++ps;
+      if (ps < T) pi = i_first(ps);
+    }
+  };
+  for (int k = 0; k < kSwRing; ++k) issue(k);
   // y_s holds every update from earlier solves: x_s = D_s^-1 y_s into s_xo,
   // published at once (words + the caller's x)
   auto solve_own = [&](int s) {
     const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
-    const float* D = s_dinv + (s & 1) * kTb * kTb;
     const float* ys = s_y + (s / G) * kTb;
     float acc = 0.f;
 #pragma unroll 16
     for (int u = 0; u < kHalf; ++u) {
       const int c = half * kHalf + u;
-      acc = fmaf(D[r + kTb * c], ys[c], acc);
+      acc = fmaf(s_dinv[r + kTb * c], ys[c], acc);
     }
-    s_red[half * kTb + r] = acc;
+    s_redc[half * kTb + r] = acc;
     __syncthreads();
     if (tid < kTb) {
-      const float v = tid < cols ? s_red[tid] + s_red[kTb + tid] : 0.f;
+      const float v = tid < cols ? s_redc[tid] + s_redc[kTb + tid] : 0.f;
       s_xo[tid] = v;
       xw_store(xw + (size_t)s * kTb + tid, v, epoch);
       if (tid < cols) x[(int64_t)c0 + tid] = v;
@@ -102,11 +155,16 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
     __syncthreads();
   };
   if (g == 0) solve_own(0);
+  int nblk = 0;  // blocks used so far (selects the s_red parity)
   for (int s = 0; s < T; ++s) {
-    const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
     const bool mine = s % G == g;
     const bool mine_next = s + 1 < T && (s + 1) % G == g;
-    // the next owned solve: its tile of this strip and its inverse, early
+    if (!mine_next && last_own <= s + 1) {
+      if (nown == 0 || last_own <= s) break;  // nothing of this CTA is left
+      continue;
+    }
+    const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
+    // the next owned solve: its block of this strip and its inverse, early
     float pa[kHalf];
     if (mine_next) {
       const int tn = tile_of(s + 1), rn = rows_of(tn);
@@ -115,7 +173,8 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
         const int c = half * kHalf + u;
         pa[u] = (r < rn && c < cols) ? A[(int64_t)tn * kTb + r + lda * (c0 + c)] : 0.f;
       }
-      load_dinv(s_dinv + ((s + 1) & 1) * kTb * kTb, tn);
+      const float* src = dinv + (size_t)tn * kTb * kTb;
+      for (int i = tid; i < kTb * kTb; i += kSwThreads) s_dinv[i] = src[i];
     }
     if (mine) {
       if (tid < kTb) s_x[tid] = s_xo[tid];
@@ -133,49 +192,40 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
     }
     __syncthreads();
     if (s_fail) break;
-    // the critical path: the next solve's last update, its solve, publish
     if (mine_next) {
       float acc = 0.f;
 #pragma unroll
       for (int u = 0; u < kHalf; ++u) acc = fmaf(pa[u], s_x[half * kHalf + u], acc);
-      s_red[half * kTb + r] = acc;
+      s_redc[half * kTb + r] = acc;
       __syncthreads();
-      if (tid < kTb) s_y[((s + 1) / G) * kTb + tid] -= s_red[tid] + s_red[kTb + tid];
+      if (tid < kTb) s_y[((s + 1) / G) * kTb + tid] -= s_redc[tid] + s_redc[kTb + tid];
       __syncthreads();
       solve_own(s + 1);
     }
-    // the other owned tiles later in solve order, two at a time with all
-    // their loads in flight together
-    for (int i = 0; i < nown; i += 2) {
-      const int sa = g + i * G, sb = g + (i + 1) * G;
-      const bool ua = sa > s + 1, ub = i + 1 < nown && sb > s + 1;
-      if (!ua && !ub) continue;
-      const int ta = ua ? tile_of(sa) : 0, tb = ub ? tile_of(sb) : 0;
-      const int rna = ua ? rows_of(ta) : 0, rnb = ub ? rows_of(tb) : 0;
-      float va[kHalf], vb[kHalf];
-#pragma unroll
+    // this strip's blocks of the other owned tiles, from the ring
+    for (int i = i_first(s); i < nown; ++i) {
+      const int k = slot_next;
+      sw_wait_groups(inflight - 1);  // the block of slot k is the oldest group
+      __syncthreads();               // ... and every thread's pieces of it landed
+      --inflight;
+      const float* blk = s_ring + (size_t)k * kTb * kTb;
+      float acc = 0.f;
+#pragma unroll 16
       for (int u = 0; u < kHalf; ++u) {
         const int c = half * kHalf + u;
-        va[u] = (r < rna && c < cols) ? A[(int64_t)ta * kTb + r + lda * (c0 + c)] : 0.f;
-        vb[u] = (r < rnb && c < cols) ? A[(int64_t)tb * kTb + r + lda * (c0 + c)] : 0.f;
+        acc = fmaf(blk[r + kTb * c], s_x[c], acc);
       }
-      float acca = 0.f, accb = 0.f;
-#pragma unroll
-      for (int u = 0; u < kHalf; ++u) {
-        const float xv = s_x[half * kHalf + u];
-        acca = fmaf(va[u], xv, acca);
-        accb = fmaf(vb[u], xv, accb);
-      }
-      s_red[half * kTb + r] = acca;
-      s_red2[half * kTb + r] = accb;
-      __syncthreads();
-      if (tid < kTb) {
-        if (ua) s_y[i * kTb + tid] -= s_red[tid] + s_red[kTb + tid];
-        if (ub) s_y[(i + 1) * kTb + tid] -= s_red2[tid] + s_red2[kTb + tid];
-      }
-      __syncthreads();
+      float* red = s_red + (nblk & 1) * 2 * kTb;
+      red[half * kTb + r] = acc;
+      __syncthreads();  // every read of slot k and every partial sum done
+      if (tid < kTb) s_y[i * kTb + tid] -= red[tid] + red[kTb + tid];
+      issue(k);
+      slot_next = (k + 1) % kSwRing;
+      ++nblk;
     }
   }
+  // copies still in flight land before the CTA exits
+  sw_wait_groups(0);
   if (s_fail && tid == 0) atomicExch(err, 1);
 }
 
