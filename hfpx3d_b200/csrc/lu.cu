@@ -1794,6 +1794,7 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
       if (!rc) rc = read_max(&rmax);
       if (rc) break;
       worst = rmax / bnorm;
+      if (prof().on) std::fprintf(stderr, "[hfpx profile] refinement %d: residual %.3e\n", it, worst);
       if (worst <= tol) break;
     }
   }

@@ -1,7 +1,7 @@
 // The mixed-precision refinement's memory-bound pieces, one right-hand side:
 //   * triangular solves with the FP32 factors (forward with unit L, backward
 //     with U) as one persistent sweep over 128-row tiles, the factor blocks
-//     streamed through shared memory by bulk copies;
+//     streamed through shared memory by asynchronous copies;
 //   * the FP64 residual r = b - A x and its largest magnitude.
 // Both replace cuBLAS calls of the refinement (dgetrs-style solve at
 // il/linear_algebra/dense/factorization/LU.h:106-120 applied to FP32 factors,
@@ -28,7 +28,8 @@ namespace hfpx {
 //     publishes: the critical path per tile is one word exchange and two
 //     128 x 128 products;
 //   * then subtracts A(t', t_s) x_s from its other owned tiles t' later in
-//     solve order.  Those blocks are one stream per CTA, in the order they
+//     solve order (the owner of s + 2 takes its solve as soon as x_{s+1}
+//     arrives, between those blocks).  Those blocks are one stream per CTA, in the order they
 //     are used, fed into a two-block shared-memory ring by asynchronous
 //     16-byte copies (cp.async, one commit group per block), so the next
 //     blocks load while the CTA waits for x and works the critical path.
@@ -39,7 +40,7 @@ constexpr int kSwThreads = 256;
 constexpr int kSwMaxOwn = 16;  // solves per CTA: n <= 16 * 148 * 128 rows
 constexpr int kSwRing = 2;
 constexpr unsigned long long kTrsvTimeoutNs = 200ull * 1000 * 1000;
-constexpr size_t kSwSmemFloats = (size_t)(kSwRing + 1) * kTb * kTb + kSwMaxOwn * kTb + 2 * kTb + 4 * kTb + 2 * kTb;
+constexpr size_t kSwSmemFloats = (size_t)(kSwRing + 1) * kTb * kTb + kSwMaxOwn * kTb + 3 * kTb + 4 * kTb + 2 * kTb;
 constexpr size_t kSwSmem = sizeof(float) * kSwSmemFloats;
 
 __device__ __forceinline__ unsigned long long trsv_ns() {
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
   float* s_xo = s_x + kTb;                     // [kTb] x of this CTA's latest solve
   float* s_red = s_xo + kTb;                   // [2 parities][2 halves][kTb]
   float* s_redc = s_red + 4 * kTb;             // [2 halves][kTb] (critical path)
+  float* s_x2 = s_redc + 2 * kTb;              // [kTb] x_{s+1} taken early (see below)
   __shared__ int s_fail;
   const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x;
   const int T = (n + kTb - 1) / kTb;
@@ -155,18 +157,20 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
     __syncthreads();
   };
   if (g == 0) solve_own(0);
-  int nblk = 0;  // blocks used so far (selects the s_red parity)
+  int nblk = 0;    // blocks used so far (selects the s_red parity)
+  int early = -1;  // strip whose critical step (solve of strip + 1) was taken early
+  float pa[kHalf];
   for (int s = 0; s < T; ++s) {
     const bool mine = s % G == g;
     const bool mine_next = s + 1 < T && (s + 1) % G == g;
+    const bool crit = mine_next && early != s;
     if (!mine_next && last_own <= s + 1) {
       if (nown == 0 || last_own <= s) break;  // nothing of this CTA is left
       continue;
     }
     const int ts = tile_of(s), c0 = ts * kTb, cols = rows_of(ts);
     // the next owned solve: its block of this strip and its inverse, early
-    float pa[kHalf];
-    if (mine_next) {
+    if (crit) {
       const int tn = tile_of(s + 1), rn = rows_of(tn);
 #pragma unroll
       for (int u = 0; u < kHalf; ++u) {
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
     }
     __syncthreads();
     if (s_fail) break;
-    if (mine_next) {
+    if (crit) {
       float acc = 0.f;
 #pragma unroll
       for (int u = 0; u < kHalf; ++u) acc = fmaf(pa[u], s_x[half * kHalf + u], acc);
@@ -202,8 +206,25 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
       __syncthreads();
       solve_own(s + 1);
     }
+    // The solve of s + 2, if this CTA owns it, need not wait for this strip's
+    // other blocks: once its strip-s block (the first in the ring) is applied
+    // and x_{s+1} has arrived (probed between blocks, the probe's load in
+    // flight during a block), it is taken here and strip s + 1 skips it.
+    bool pending2 = s + 2 < T && (s + 2) % G == g;
+    if (pending2) {
+      const int tn = tile_of(s + 2), rn = rows_of(tn), t1 = tile_of(s + 1), cn = rows_of(t1);
+#pragma unroll
+      for (int u = 0; u < kHalf; ++u) {
+        const int c = half * kHalf + u;
+        pa[u] = (r < rn && c < cn) ? A[(int64_t)tn * kTb + r + lda * ((int64_t)t1 * kTb + c)] : 0.f;
+      }
+      const float* src = dinv + (size_t)tn * kTb * kTb;
+      for (int i = tid; i < kTb * kTb; i += kSwThreads) s_dinv[i] = src[i];
+    }
     // this strip's blocks of the other owned tiles, from the ring
     for (int i = i_first(s); i < nown; ++i) {
+      uint64_t w2 = 0;
+      if (pending2 && tid < kTb) w2 = xw_load(xw + (size_t)(s + 1) * kTb + tid);
       const int k = slot_next;
       sw_wait_groups(inflight - 1);  // the block of slot k is the oldest group
       __syncthreads();               // ... and every thread's pieces of it landed
@@ -222,6 +243,20 @@ __global__ void __launch_bounds__(kSwThreads, 1) trsv_sweep_kernel(const float* 
       issue(k);
       slot_next = (k + 1) % kSwRing;
       ++nblk;
+      if (pending2 && __syncthreads_and(tid >= kTb || (uint32_t)(w2 >> 32) == epoch)) {
+        if (tid < kTb) s_x2[tid] = __uint_as_float((uint32_t)w2);
+        __syncthreads();
+        float acc2 = 0.f;
+#pragma unroll
+        for (int u = 0; u < kHalf; ++u) acc2 = fmaf(pa[u], s_x2[half * kHalf + u], acc2);
+        s_redc[half * kTb + r] = acc2;
+        __syncthreads();
+        if (tid < kTb) s_y[((s + 2) / G) * kTb + tid] -= s_redc[tid] + s_redc[kTb + tid];
+        __syncthreads();
+        solve_own(s + 2);
+        early = s + 1;
+        pending2 = false;
+      }
     }
   }
   // copies still in flight land before the CTA exits
