@@ -9,8 +9,10 @@ internal pressure 1 (sigma_zz = 1).  Synthetic seeded mesh (the reference has
 no mesher).  One step = assemble the FP64 collocation matrix in HBM
 (41.5 GB) + LU factorisation + solve to a relative residual <= 1e-10.
 
-  --mode mixed (default): FP32 copy of the matrix factored with TF32
-        tensor-core trailing updates, FP64 iterative refinement;
+  --mode mixed (default): FP32 copy of the matrix factored with FP16/TF32
+        tensor-core updates, then flexible GMRES on the FP64 matrix
+        preconditioned by those factors (--solver gmres, the default) or FP64
+        iterative refinement (--solver refine);
   --mode fp64: the plain FP64 GPU path (in-place FP64 LU).
 The other mode is timed once after the timed loop for the speed-up and the
 opening error between the two (rel err target <= 1e-8).
@@ -157,8 +159,12 @@ def run_engine(args, rank, world, local_rank):
             ev[2].record(stream)
         d_x.copy_(d_rhs)
         torch.cuda.synchronize()
-        ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), 1, n, args.tol, 50,
-                                         ctypes.byref(info)))
+        if args.solver == 'gmres' and m == engine.HFPX_LU_MIXED:
+            ctx.check(L.hfpx_gmres_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), args.tol, 50, 200,
+                                          ctypes.byref(info)))
+        else:
+            ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), 1, n, args.tol, 50,
+                                             ctypes.byref(info)))
         if ev:
             ev[3].record(stream)
 
@@ -224,7 +230,7 @@ def run_engine(args, rank, world, local_rank):
                    'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
         'phases_ms': {'assembly': asm_ms, 'factor': statistics.mean(t_fac), 'solve': statistics.mean(t_sol)},
         'steps_ms': {'factor': [round(t, 2) for t in t_fac], 'solve': [round(t, 2) for t in t_sol]},
-        'refinement': {'iterations': iters_main, 'residual': res_main},
+        'refinement': {'solver': args.solver, 'iterations': iters_main, 'residual': res_main},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,
         # the factorisation is ~80 % of the step: 2/3 N^3 flop over its CUDA-event time on the
@@ -279,7 +285,10 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
         info_ = ctypes.c_int64()
         ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
         si = engine.SolveInfo()
-        ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
+        if args.solver == 'gmres' and mode == engine.HFPX_LU_MIXED:
+            ctx.check(L.hfpx_gmres(ctx.h, A.h, engine._dp(hr), args.tol, 50, 200, ctypes.byref(si)))
+        else:
+            ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
         e1.record(stream)
         torch.cuda.synchronize()
         L.hfpx_mesh_destroy(mh)
@@ -375,6 +384,9 @@ def main():
     ap.add_argument('--mode', default='mixed', choices=['mixed', 'fp64'])
     ap.add_argument('--n-el', type=int, default=4000)
     ap.add_argument('--tol', type=float, default=1e-10)
+    ap.add_argument('--solver', default='gmres', choices=['refine', 'gmres'],
+                    help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
+                         'FP32 factors')
     ap.add_argument('--no-compare', dest='compare', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--cpu-sample-el', type=int, default=600)

@@ -452,6 +452,37 @@ int hfpx_lu_solve_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t
   return refine_solve(c, m, d_b, nrhs, ld_b, tol > 0 ? tol : 1e-12, max_iter > 0 ? max_iter : 30, info);
 }
 
+int hfpx_gmres_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
+                      hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !d_b) return set_error(c, HFPX_ERR_ARG, "bad GMRES arguments");
+  if (m->factored != 2) return set_error(c, HFPX_ERR_STATE, "GMRES needs a mixed factorisation of the matrix");
+  if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
+  cudaSetDevice(c->device);
+  return gmres_solve(c, m, d_b, tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50, max_iter > 0 ? max_iter : 200,
+                     info);
+}
+
+int hfpx_gmres(hfpx_ctx* c, const hfpx_matrix* m, double* b, double tol, int restart, int max_iter,
+               hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !b) return set_error(c, HFPX_ERR_ARG, "bad GMRES arguments");
+  if (m->factored != 2) return set_error(c, HFPX_ERR_STATE, "GMRES needs a mixed factorisation of the matrix");
+  if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
+  cudaSetDevice(c->device);
+  DevBuf db;
+  int rc = check_cuda(c, db.alloc(sizeof(double) * m->n), "rhs alloc");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(db.p, b, sizeof(double) * m->n, cudaMemcpyHostToDevice, c->stream), "rhs");
+  if (!rc) rc = gmres_solve(c, m, db.as<double>(), tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50,
+                            max_iter > 0 ? max_iter : 200, info);
+  if (!rc || rc == HFPX_ERR_NOT_CONVERGED) {
+    int rc2 = check_cuda(c, cudaMemcpyAsync(b, db.p, sizeof(double) * m->n, cudaMemcpyDeviceToHost, c->stream), "x");
+    if (!rc2) rc2 = check_cuda(c, cudaStreamSynchronize(c->stream), "x");
+    if (rc2) rc = rc2;
+  }
+  return rc;
+}
+
 int64_t hfpx_ctx_launch_count(const hfpx_ctx* c) { return c ? (int64_t)g_launches.load() : -1; }
 
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,

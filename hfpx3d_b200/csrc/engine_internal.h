@@ -62,7 +62,7 @@ enum : int {
   kScrPanelCand, kScrPanelMax, kScrPanelIdx, kScrPanelRowj, kScrInfo, kScrPlanPanel, kScrPlans, kScrLLSlots,
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
-  kScrTrsvErr, kScrTslu, kScrCount
+  kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrCount
 };
 
 // assembly.cu
@@ -98,6 +98,8 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
                  double tol, int max_iter, hfpx_solve_info* info);
 int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
                             int64_t* info);
+int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
+                hfpx_solve_info* info);
 
 // solve.cu: one right-hand side of the refinement
 int trsv_tiles(int64_t n);

@@ -1717,7 +1717,7 @@ static bool own_solve_enabled() {
 }
 
 // The single right-hand side uses the engine's tile-sweep triangular solves
-// (solve.cu: 5.9-6.1 ms per triangle at N = 72 000, a little under cuBLAS);
+// (solve.cu: ~4 ms per triangle at N = 72 000, against ~6 for cuBLAS);
 // HFPX_TRSV=cublas selects cuBLAS instead.
 static bool own_trsv_enabled() {
   static const bool on = [] {
@@ -1725,6 +1725,44 @@ static bool own_trsv_enabled() {
     return !(e && std::string(e) == "cublas");
   }();
   return on;
+}
+
+// y = (P L U)^-1 v with the FP32 factors of a mixed factorisation, for one
+// FP64 vector v: v -> FP32 (rf), row interchanges (into y), then the two
+// triangular solves in place.  The diagonal-block inverses of the tile
+// solves are made once per factorisation.
+static int precond_f32(hfpx_ctx* c, const hfpx_matrix* m, const int32_t* d_perm, const double* v, float* rf,
+                       float* y) {
+  const int64_t n = m->n;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  ++g_launches;
+  d2f_kernel<<<nb, 256, 0, c->stream>>>(v, rf, n, 1, n, n);
+  ++g_launches;
+  permute_rows_kernel<float><<<nb, 256, 0, c->stream>>>(rf, y, d_perm, n, 1, n);
+  if (own_trsv_enabled()) {
+    const size_t blk = (size_t)trsv_tiles(n) * 128 * 128;
+    if (!m->dinv_valid) {
+      if (!m->d_dinv && cudaMalloc(&m->d_dinv, sizeof(float) * 2 * blk) != cudaSuccess) {
+        m->d_dinv = nullptr;
+        cudaGetLastError();
+        return set_error(c, HFPX_ERR_NOMEM, "diagonal block inverses");
+      }
+      int rc = tri_inverses(c, m->d_f, m->ld, n, m->d_dinv, m->d_dinv + blk);
+      if (rc) return rc;
+      m->dinv_valid = 1;
+    }
+    int rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv, y, false);
+    if (!rc) rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv + blk, y, true);
+    return rc;
+  }
+  // cuBLAS strsm with one column measured faster than strsv here
+  const float one = 1.f;
+  cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
+  cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)n, 1, &one, m->d_f,
+              (int)m->ld, y, (int)n);
+  cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
+              m->d_f, (int)m->ld, y, (int)n);
+  return check_cuda(c, cudaGetLastError(), "triangular solves");
 }
 
 // One right-hand side: the engine's residual (solve.cu; |r|_inf comes back
@@ -1758,34 +1796,7 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
     cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream);
     cudaMemcpyAsync(r, d_b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
     for (it = 1; it <= max_iter; ++it) {
-      ++g_launches;
-      d2f_kernel<<<nb, 256, 0, c->stream>>>(r, rf, n, 1, n, n);
-      ++g_launches;
-      permute_rows_kernel<float><<<nb, 256, 0, c->stream>>>(rf, y, d_perm, n, 1, n);
-      if (own_trsv_enabled()) {
-        const size_t blk = (size_t)trsv_tiles(n) * 128 * 128;
-        if (!m->dinv_valid) {
-          if (!m->d_dinv && cudaMalloc(&m->d_dinv, sizeof(float) * 2 * blk) != cudaSuccess) {
-            m->d_dinv = nullptr;
-            cudaGetLastError();
-            rc = set_error(c, HFPX_ERR_NOMEM, "diagonal block inverses");
-            break;
-          }
-          rc = tri_inverses(c, m->d_f, m->ld, n, m->d_dinv, m->d_dinv + blk);
-          if (rc) break;
-          m->dinv_valid = 1;
-        }
-        rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv, y, false);
-        if (!rc) rc = trsv_f32(c, m->d_f, m->ld, n, m->d_dinv + blk, y, true);
-      } else {
-        // cuBLAS strsm with one column measured faster than strsv here
-        const float one = 1.f;
-        cublasSetMathMode(H(c), CUBLAS_DEFAULT_MATH);
-        cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_UNIT, (int)n, 1, &one,
-                    m->d_f, (int)m->ld, y, (int)n);
-        cublasStrsm(H(c), CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)n, 1, &one,
-                    m->d_f, (int)m->ld, y, (int)n);
-      }
+      rc = precond_f32(c, m, d_perm, r, rf, y);
       if (rc) break;
       ++g_launches;
       axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(y, x, n, 1, n, n);
@@ -1813,6 +1824,173 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
 }
 
 // Iterative refinement: x += LU32^-1 r, r = b - A x in FP64.
+// GMRES(restart) on the FP64 matrix, right-preconditioned by the FP32
+// factors: A M^-1 u = b, x = M^-1 u, in the flexible form (the vectors
+// z_j = M^-1 v_j are kept, so x += Z y needs no further solve).  One step is
+// one preconditioner solve (precond_f32) and one FP64 product with A (the
+// residual kernel against a zero right-hand side gives -A z); the Arnoldi
+// vectors are orthogonalised by classical Gram-Schmidt applied twice (four
+// cuBLAS DGEMVs), the small Hessenberg least-squares problem is solved on the
+// host with Givens rotations.  A cycle stops when the rotated residual
+// |g_{j+1}| / |b|_2 is below tol / 4; then the residual r = b - A x decides,
+// in the max norm like the refinement: |r|_inf / |b|_inf <= tol, else the
+// next cycle starts from it.  The products A z_j are kept, so r = b - [A z] y
+// costs one small DGEMV instead of another pass over A (the same r as b - A x
+// up to rounding far below the tolerance).  d_b: right-hand side in, x out.
+constexpr int kGmresMax = 64;
+
+int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
+                hfpx_solve_info* info) {
+  const int64_t n = m->n;
+  const int k = std::max(1, std::min(restart, kGmresMax));
+  double* V = (double*)ctx_scratch(c, kScrGmresV, sizeof(double) * n * (k + 1));
+  double* Z = (double*)ctx_scratch(c, kScrGmresZ, sizeof(double) * n * 2 * k);  // Z, then A Z
+  double* dh = (double*)ctx_scratch(c, kScrGmresH, sizeof(double) * 2 * (kGmresMax + 1));
+  double* zero = (double*)ctx_scratch(c, kScrGmresZero, sizeof(double) * n);
+  double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * n);
+  double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * n);
+  float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * n);
+  float* y = (float*)ctx_scratch(c, kScrSolveTmp, sizeof(float) * n);
+  double* part = (double*)ctx_scratch(c, kScrResidPart, sizeof(double) * n * resid_chunks(n));
+  unsigned long long* dmax = (unsigned long long*)ctx_scratch(c, kScrResidMax, sizeof(unsigned long long));
+  if (!V || !Z || !dh || !zero || !x || !r || !rf || !y || !part || !dmax)
+    return set_error(c, HFPX_ERR_NOMEM, "GMRES buffers");
+  double* AZ = Z + (size_t)n * k;
+  int32_t* d_perm = nullptr;
+  int rc = build_perm(c, m, &d_perm);
+  if (rc) return rc;
+  cublasHandle_t h = H(c);
+  cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
+  cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  auto sync = [&](const char* what) { return check_cuda(c, cudaStreamSynchronize(c->stream), what); };
+  auto read_max = [&](double* v) {
+    unsigned long long bits = 0;
+    int e = check_cuda(c, cudaMemcpyAsync(&bits, dmax, sizeof(bits), cudaMemcpyDeviceToHost, c->stream), "max");
+    if (!e) e = sync("max");
+    std::memcpy(v, &bits, sizeof(double));
+    return e;
+  };
+  double bmax = 0.0, bnorm2 = 0.0, worst = INFINITY;
+  rc = absmax_f64(c, d_b, n, dmax);
+  if (!rc) rc = read_max(&bmax);
+  if (!rc) cublasDnrm2(h, (int)n, d_b, 1, &bnorm2);
+  if (!(bmax > 0.0)) bmax = 1.0;
+  if (!(bnorm2 > 0.0)) bnorm2 = 1.0;
+  cudaMemsetAsync(zero, 0, sizeof(double) * n, c->stream);
+  cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream);
+  cudaMemcpyAsync(r, d_b, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+  double Hm[kGmresMax + 1][kGmresMax];  // Hessenberg columns, rotated in place
+  double cs[kGmresMax], sn[kGmresMax], g[kGmresMax + 1], hv[kGmresMax + 1], h2[kGmresMax + 1];
+  int steps = 0;
+  double rnorm = bnorm2;  // |r|_2 of the cycle's start
+  while (!rc && steps < max_iter) {
+    // v_0 = r / |r|_2
+    if (steps > 0) {
+      cublasDnrm2(h, (int)n, r, 1, &rnorm);
+      rc = sync("GMRES restart");
+      if (rc || !(rnorm > 0.0)) break;
+    }
+    cudaMemcpyAsync(V, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+    const double inv0 = 1.0 / rnorm;
+    cublasDscal(h, (int)n, &inv0, V, 1);
+    for (int i = 0; i <= k; ++i) g[i] = 0.0;
+    g[0] = rnorm;
+    int j = 0;
+    for (; j < k && steps < max_iter; ++j, ++steps) {
+      double* vj = V + (size_t)n * j;
+      double* zj = Z + (size_t)n * j;
+      double* w = V + (size_t)n * (j + 1);
+      // z_j = M^-1 v_j (FP32 solve, widened), w = A z_j
+      rc = precond_f32(c, m, d_perm, vj, rf, y);
+      if (rc) break;
+      cudaMemsetAsync(zj, 0, sizeof(double) * n, c->stream);
+      ++g_launches;
+      axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(y, zj, n, 1, n, n);
+      rc = residual_f64(c, m->d_a, m->ld, n, zj, zero, w, part, dmax);  // w = -A z_j
+      if (rc) break;
+      const double mone = -1.0, one = 1.0, zero_s = 0.0;
+      cublasDscal(h, (int)n, &mone, w, 1);
+      cudaMemcpyAsync(AZ + (size_t)n * j, w, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+      // h = V^T w; w -= V h; twice
+      cublasDgemv(h, CUBLAS_OP_T, (int)n, j + 1, &one, V, (int)n, w, 1, &zero_s, dh, 1);
+      cublasDgemv(h, CUBLAS_OP_N, (int)n, j + 1, &mone, V, (int)n, dh, 1, &one, w, 1);
+      cublasDgemv(h, CUBLAS_OP_T, (int)n, j + 1, &one, V, (int)n, w, 1, &zero_s, dh + kGmresMax + 1, 1);
+      cublasDgemv(h, CUBLAS_OP_N, (int)n, j + 1, &mone, V, (int)n, dh + kGmresMax + 1, 1, &one, w, 1);
+      double beta = 0.0;
+      cublasDnrm2(h, (int)n, w, 1, &beta);  // synchronises (host pointer mode)
+      rc = check_cuda(c, cudaMemcpyAsync(hv, dh, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost, c->stream), "h");
+      if (!rc)
+        rc = check_cuda(c, cudaMemcpyAsync(h2, dh + kGmresMax + 1, sizeof(double) * (j + 1), cudaMemcpyDeviceToHost,
+                                           c->stream),
+                        "h");
+      if (!rc) rc = sync("GMRES step");
+      if (rc) break;
+      for (int i = 0; i <= j; ++i) Hm[i][j] = hv[i] + h2[i];
+      Hm[j + 1][j] = beta;
+      if (beta > 0.0) {
+        const double ib = 1.0 / beta;
+        cublasDscal(h, (int)n, &ib, w, 1);
+      }
+      // earlier rotations, then the one that zeroes H(j+1, j)
+      for (int i = 0; i < j; ++i) {
+        const double a = Hm[i][j], bb = Hm[i + 1][j];
+        Hm[i][j] = cs[i] * a + sn[i] * bb;
+        Hm[i + 1][j] = -sn[i] * a + cs[i] * bb;
+      }
+      const double a = Hm[j][j], bb = Hm[j + 1][j];
+      const double den = std::hypot(a, bb);
+      cs[j] = den > 0.0 ? a / den : 1.0;
+      sn[j] = den > 0.0 ? bb / den : 0.0;
+      Hm[j][j] = den;
+      Hm[j + 1][j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      if (prof().on)
+        std::fprintf(stderr, "[hfpx profile] GMRES step %d: |g| / |b|_2 %.3e\n", steps + 1, std::fabs(g[j + 1]) / bnorm2);
+      if (std::fabs(g[j + 1]) / bnorm2 <= 0.25 * tol || !(beta > 0.0)) {
+        ++j;
+        ++steps;
+        break;
+      }
+    }
+    if (rc || j == 0) break;
+    // y = R^-1 g (back substitution), x += Z y
+    double yv[kGmresMax];
+    for (int i = j - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int l = i + 1; l < j; ++l) t -= Hm[i][l] * yv[l];
+      yv[i] = Hm[i][i] != 0.0 ? t / Hm[i][i] : 0.0;
+    }
+    rc = check_cuda(c, cudaMemcpyAsync(dh, yv, sizeof(double) * j, cudaMemcpyHostToDevice, c->stream), "y");
+    if (rc) break;
+    const double one = 1.0, mone = -1.0;
+    cublasDgemv(h, CUBLAS_OP_N, (int)n, j, &one, Z, (int)n, dh, 1, &one, x, 1);
+    // r = r_0 - [A z] y (r holds the cycle's starting residual)
+    cublasDgemv(h, CUBLAS_OP_N, (int)n, j, &mone, AZ, (int)n, dh, 1, &one, r, 1);
+    rc = absmax_f64(c, r, n, dmax);
+    double rmax = 0.0;
+    if (!rc) rc = read_max(&rmax);
+    if (rc) break;
+    worst = rmax / bmax;
+    if (prof().on) std::fprintf(stderr, "[hfpx profile] GMRES cycle end: residual %.3e\n", worst);
+    if (worst <= tol) break;
+  }
+  if (!rc) rc = trsv_status(c);
+  if (!rc) rc = check_cuda(c, cudaGetLastError(), "GMRES");
+  if (!rc) {
+    cudaMemcpyAsync(d_b, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
+    rc = sync("GMRES");
+  }
+  if (info) {
+    info->iterations = steps;
+    info->residual = worst;
+    info->converged = worst <= tol;
+  }
+  if (!rc && !(worst <= tol)) rc = set_error(c, HFPX_ERR_NOT_CONVERGED, "GMRES did not reach the tolerance");
+  return rc;
+}
+
 int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, int64_t ldb, double tol, int max_iter,
                  hfpx_solve_info* info) {
   if (nrhs == 1 && own_solve_enabled()) return refine_one(c, m, d_b, tol, max_iter, info);

@@ -63,6 +63,8 @@ SIGNATURES = {
     'hfpx_lu_factor': (_int, [_V, _V, _int, _L]),
     'hfpx_lu_solve': (_int, [_V, _V, _D, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_lu_solve_device': (_int, [_V, _V, _V, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_gmres': (_int, [_V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_gmres_device': (_int, [_V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
     'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
@@ -301,6 +303,16 @@ class LU:
         self.last_info = info
         self.ctx.check(rc)
         return b[:, 0].copy() if one else b
+
+    def gmres(self, y, tol=0.0, restart=0, max_iter=0):
+        """One right-hand side by flexible GMRES on the FP64 matrix,
+        preconditioned by this (mixed) factorisation (hfpx_gmres)."""
+        b = np.array(y, dtype=np.float64, copy=True).reshape(-1)
+        info = SolveInfo()
+        rc = lib().hfpx_gmres(self.ctx.h, self.matrix.h, _dp(b), tol, restart, max_iter, ctypes.byref(info))
+        self.last_info = info
+        self.ctx.check(rc)
+        return b
 
 
 def make_3dbem_stress_f_s(ctx, dmesh: DeviceMesh, shear_m, poiss_r, dd, pts, s_inf, is_dd_local=False):

@@ -124,6 +124,21 @@ int hfpx_matrix_upload_lu(hfpx_ctx *ctx, const double *lu, int64_t n, int64_t ld
 int hfpx_lu_solve_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, int64_t nrhs,
                          int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
 
+/* ---- iterative solve: flexible GMRES(restart) on the FP64 matrix,
+ * right-preconditioned by the FP32 factors of its mixed factorisation
+ * (hfpx_lu_factor with HFPX_LU_MIXED), for one right-hand side b (host, n),
+ * overwritten with x.  The reference solves only directly (LU.h:106-120);
+ * this is the Krylov alternative to hfpx_lu_solve's refinement, with the same
+ * stopping rule |b - A x|_inf / |b|_inf <= tol (<= 0 selects 1e-12).
+ * restart <= 0 selects 50 (at most 64), max_iter <= 0 200 steps;
+ * info->iterations counts preconditioner solves.  HFPX_ERR_STATE without a
+ * mixed factorisation, HFPX_ERR_NOT_CONVERGED with x returned anyway. */
+int hfpx_gmres(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *b, double tol, int restart,
+               int max_iter, hfpx_solve_info *info);
+/* Same with b already in device memory. */
+int hfpx_gmres_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, double tol,
+                      int restart, int max_iter, hfpx_solve_info *info);
+
 /* Partial-pivoting LU of one tall panel already in device memory, in place,
  * without allocating anything: no counterpart in the reference.  For callers
  * that cannot call cudaMalloc (inside a stream capture, under a

@@ -176,3 +176,44 @@ def test_tile_sweep_triangular_solves(tmp_path):
     x0, x1 = out['cublas'][:-2], out[''][:-2]
     assert out[''][-1] <= 1e-12
     assert np.abs(x1 - x0).max() <= 1e-10 * np.abs(x0).max()
+
+
+def test_gmres_matches_the_reference_solution(ctx):
+    # flexible GMRES on the FP64 matrix, preconditioned by the mixed FP32
+    # factors (hfpx_gmres), against the reference's own LAPACK solution
+    from hfpx3d_b200 import engine
+    g = golden('ref_c1')
+    mesh = engine.MeshGeom(g['nods'], g['conn'])
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh)
+    A = engine.assemble(ctx, dm, dof, n, 1.0, 0.35)
+    lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+    x = lu.gmres(g['rhs'], tol=1e-12)
+    assert lu.last_info.converged and lu.last_info.residual <= 1e-12
+    assert 1 <= lu.last_info.iterations <= 10
+    assert np.abs(x - g['x']).max() / np.abs(g['x']).max() < 1e-9
+    # a second call on the same factors gives the same bits
+    x2 = lu.gmres(g['rhs'], tol=1e-12)
+    assert np.array_equal(x, x2)
+
+
+def test_gmres_against_refinement_and_states(ctx):
+    from hfpx3d_b200 import engine, meshgen
+    nods, conn = meshgen.penny(1200, seed=3)
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 1)
+    dm = engine.DeviceMesh(ctx, mesh)
+    rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, [0, 0, 1.0, 0, 0, 0])
+    A = engine.assemble(ctx, dm, dof, n, 1.0, 0.35)
+    lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+    xr = lu.solve(rhs, tol=1e-12)
+    it_refine = lu.last_info.iterations
+    xg = lu.gmres(rhs, tol=1e-12, restart=2)     # restarts: cycles of two steps
+    assert lu.last_info.converged and lu.last_info.iterations <= 2 * it_refine
+    assert np.abs(xg - xr).max() <= 1e-10 * np.abs(xr).max()
+    # GMRES needs the FP64 matrix beside FP32 factors: an FP64 factorisation is refused
+    A64 = engine.assemble(ctx, dm, dof, n, 1.0, 0.35)
+    lu64 = engine.LU(ctx, A64, engine.HFPX_LU_FP64)
+    with pytest.raises(engine.EngineError) as e:
+        lu64.gmres(rhs)
+    assert e.value.code == engine.HFPX_ERR_STATE
