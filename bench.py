@@ -390,7 +390,7 @@ def main():
     ap.add_argument('--no-compare', dest='compare', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--cpu-sample-el', type=int, default=600)
-    ap.add_argument('--e2e-steps', type=int, default=2)
+    ap.add_argument('--e2e-steps', type=int, default=3)
     ap.add_argument('--e2e-warmup', type=int, default=1)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -57,6 +57,20 @@ struct DevBuf {
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// A context scratch buffer with DevBuf's interface: grown on first use and
+// kept, so the host-buffer entry points allocate nothing in steady state.
+struct ScratchBuf {
+  hfpx_ctx* c;
+  int slot;
+  void* p = nullptr;
+  ScratchBuf(hfpx_ctx* ctx, int s) : c(ctx), slot(s) {}
+  cudaError_t alloc(size_t bytes) {
+    p = ctx_scratch(c, slot, bytes ? bytes : 16);
+    return p ? cudaSuccess : cudaErrorMemoryAllocation;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
 // dof_h (int64, n_el x 18) to int32 in the context's dof buffer.
 static int upload_dof(hfpx_ctx* c, const int64_t* dof_h, int64_t n_el, int64_t n_dof, int32_t** d) {
   std::vector<int32_t> tmp(18 * n_el);
@@ -201,7 +215,7 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(nods[k + ld_nods * n])) return set_error(c, HFPX_ERR_ARG, "non-finite node coordinate");
   cudaSetDevice(c->device);
-  DevBuf dn, dc;
+  ScratchBuf dn(c, kScrHostNods), dc(c, kScrHostConn);
   int rc = check_cuda(c, dn.alloc(sizeof(double) * ld_nods * n_nodes), "nods alloc");
   if (!rc) rc = check_cuda(c, dc.alloc(sizeof(int64_t) * ld_conn * n_el), "conn alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(dn.p, nods, sizeof(double) * ld_nods * n_nodes, cudaMemcpyHostToDevice, c->stream), "nods copy");
@@ -383,7 +397,7 @@ int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   if (!mesh || !dof_h || !s_inf || !rhs || n_rhs < 1 || ld_rhs < n_dof || n_dof < 1)
     return set_error(c, HFPX_ERR_ARG, "bad rhs arguments");
   cudaSetDevice(c->device);
-  DevBuf ds, dr;
+  ScratchBuf ds(c, kScrHostSinf), dr(c, kScrHostRhs);
   int32_t* dd = nullptr;
   int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, &dd);
   if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 6 * n_rhs), "s_inf alloc");
@@ -415,7 +429,7 @@ int hfpx_lu_solve(hfpx_ctx* c, const hfpx_matrix* m, double* b, int64_t nrhs, in
   if (m->factored == 0) return set_error(c, HFPX_ERR_STATE, "solve before factor");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
   cudaSetDevice(c->device);
-  DevBuf db;
+  ScratchBuf db(c, kScrHostRhs);
   int rc = check_cuda(c, db.alloc(sizeof(double) * m->ld * nrhs), "rhs alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpy2DAsync(db.p, m->ld * sizeof(double), b, ld_b * sizeof(double), m->n * sizeof(double),
                                                 nrhs, cudaMemcpyHostToDevice, c->stream),
@@ -470,7 +484,7 @@ int hfpx_gmres(hfpx_ctx* c, const hfpx_matrix* m, double* b, double tol, int res
   if (m->factored != 2) return set_error(c, HFPX_ERR_STATE, "GMRES needs a mixed factorisation of the matrix");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
   cudaSetDevice(c->device);
-  DevBuf db;
+  ScratchBuf db(c, kScrHostRhs);
   int rc = check_cuda(c, db.alloc(sizeof(double) * m->n), "rhs alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(db.p, b, sizeof(double) * m->n, cudaMemcpyHostToDevice, c->stream), "rhs");
   if (!rc) rc = gmres_solve(c, m, db.as<double>(), tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50,
