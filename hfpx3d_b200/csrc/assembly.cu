@@ -329,16 +329,21 @@ __device__ __forceinline__ void traction_3x3(const double* r, const double* nl, 
 constexpr int kTile = 128;
 constexpr int kStageRows = 3 * kTile;
 
+// The in-plane pass writes each matrix column segment straight from the
+// warp: the 96 rows of a warp (3 per collocation point) go through a
+// 768-byte per-warp buffer so that every lane stores 3 consecutive-row values
+// (coalesced), instead of staging the CTA's whole 18-column block (55 KB of
+// shared memory, 3 CTAs per SM) behind a CTA barrier.
 struct AsmSmem {
   ElemRec src;
   uint64_t bar;
   int32_t cols[18];
   int32_t rows[kStageRows];
-  double stage[18][kStageRows];
+  double wbuf[kTile / 32][96];
 };
 
 template <bool GENERAL>
-__global__ void __launch_bounds__(kTile) assemble_kernel(const ElemRec* __restrict__ elems,
+__global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const ElemRec* __restrict__ elems,
                                                          int64_t n_el,
                                                          const int32_t* __restrict__ dof,
                                                          double G, double nu, int is_dd_local,
@@ -371,33 +376,39 @@ __global__ void __launch_bounds__(kTile) assemble_kernel(const ElemRec* __restri
 
   if (!GENERAL) {
     const bool mine = valid && inplane;
+    const int lane = tid & 31, warp = tid >> 5;
     for (int k = 0; k < 3; ++k)
       sm.rows[3 * tid + k] = mine ? dof[t + n_el * (3 * nt + k)] : -1;
     const unsigned off = __ballot_sync(0xffffffffu, valid && !inplane);
-    if (off && (tid & 31) == 0) atomicAdd(status + 1, __popc(off));
-    if (mine) {
-      cplx P[6], Q[6];
-      inplane_moments(S, z, P, Q);
-      inplane_nodes(S, z, P, Q, nu, scale, [&](int a, const double Sx[6][3]) {
-        double B[3][3];
-        traction_3x3(S.r, nl, Sx, is_dd_local, B);
+    if (off && lane == 0) atomicAdd(status + 1, __popc(off));
+    __syncthreads();  // sm.cols and every lane's rows
+    // the rows this lane stores: warp rows lane, lane + 32, lane + 64
+    int32_t trow[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i)
+    for (int q = 0; q < 3; ++q) trow[q] = sm.rows[96 * warp + lane + 32 * q];
+    double* wb = sm.wbuf[warp];
+    // every lane runs the in-plane form (the warp stays converged for the
+    // per-warp transpose); rows of lanes that are not in-plane pairs are -1
+    cplx P[6], Q[6];
+    inplane_moments(S, z, P, Q);
+    inplane_nodes(S, z, P, Q, nu, scale, [&](int a, const double Sx[6][3]) {
+      double B[3][3];
+      traction_3x3(S.r, nl, Sx, is_dd_local, B);
 #pragma unroll
-          for (int j = 0; j < 3; ++j) sm.stage[3 * a + j][3 * tid + i] = B[i][j];
-      });
-    }
-    __syncthreads();
-    // coalesced column-segment stores: 18 columns x 384 rows
-    for (int c = 0; c < 18; ++c) {
-      const int32_t col = sm.cols[c];
-      if (col < 0) continue;
-      double* colp = A + (int64_t)col * ld;
-      for (int r = tid; r < kStageRows; r += kTile) {
-        const int32_t row = sm.rows[r];
-        if (row >= 0) colp[row] = sm.stage[c][r];
+      for (int j = 0; j < 3; ++j) {
+        const int32_t col = sm.cols[3 * a + j];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) wb[3 * lane + i] = B[i][j];
+        __syncwarp();
+        if (col >= 0) {
+          double* colp = A + (int64_t)col * ld;
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            if (trow[q] >= 0) colp[trow[q]] = wb[lane + 32 * q];
+        }
+        __syncwarp();
       }
-    }
+    });
   } else {
     __syncthreads();
     if (!(valid && !inplane)) return;
