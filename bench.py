@@ -54,9 +54,9 @@ def peaks():
 
 
 # DRAM bytes per matrix entry written by the in-plane assembly kernel, from
-# the ncu capture of profiles/assemble_kernel_penny1000.md (3.4297 GB for an
+# the ncu capture of profiles/assemble_kernel_penny1000.md (4.6305 GB for an
 # 18 000 x 18 000 fill; traffic grows with the entries, so it scales by N^2)
-ASM_DRAM_BYTES_PER_ENTRY = 3.429715e9 / 18000 ** 2
+ASM_DRAM_BYTES_PER_ENTRY = 4.630537e9 / 18000 ** 2
 
 
 class Clocks:
