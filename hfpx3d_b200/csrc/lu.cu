@@ -1255,39 +1255,57 @@ __global__ void identity_kernel(float* a, int n) {
   if (i < n) a[i + (int64_t)n * j] = i == j ? 1.f : 0.f;
 }
 
-// U12 = L11^-1 A12 for the trailing block row.  FP32: invert the unit lower
-// L11 (kb x kb triangular solve on the identity), then one TF32 GEMM over the
-// whole block row; the triangular solve over the block row (kb x rest) is
-// the slow path it replaces.  FP64: triangular solve.
+// U12 = L11^-1 A12 for columns [c0, c0 + nc) of the trailing block row (B:
+// its column 0).  FP32: with the inverse of the unit lower L11 (made by the
+// step's first call, with_inverse: a kb x kb triangular solve on the
+// identity), one TF32 GEMM; the triangular solve over the block row is the
+// slow path it replaces.  FP64: triangular solve.
 template <class T>
-static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L, int64_t lda, T* B) {
+static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t nc, const T* L, int64_t lda, T* B,
+                            bool with_inverse) {
+  if (nc <= 0) return;
+  B += lda * c0;
   if constexpr (sizeof(T) == 4) {
     if (wk.linv && wk.a12) {
-      ++g_launches;
-      identity_kernel<<<dim3((kb + 127) / 128, kb), 128, 0, l.s>>>(wk.linv, kb);
-      trsm_llu(l, kb, kb, L, lda, wk.linv, kb);
-      cudaMemcpy2DAsync(wk.a12, sizeof(T) * kb, B, sizeof(T) * lda, sizeof(T) * kb, rest, cudaMemcpyDeviceToDevice, l.s);
+      if (with_inverse) {
+        ++g_launches;
+        identity_kernel<<<dim3((kb + 127) / 128, kb), 128, 0, l.s>>>(wk.linv, kb);
+        trsm_llu(l, kb, kb, L, lda, wk.linv, kb);
+      }
+      cudaMemcpy2DAsync(wk.a12, sizeof(T) * kb, B, sizeof(T) * lda, sizeof(T) * kb, nc, cudaMemcpyDeviceToDevice, l.s);
       const float one = 1.f, zero = 0.f;
-      cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, kb, (int)rest, kb, &one, wk.linv, kb, wk.a12, kb, &zero, B, (int)lda);
+      cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, kb, (int)nc, kb, &one, wk.linv, kb, wk.a12, kb, &zero, B, (int)lda);
       return;
     }
   }
-  trsm_llu(l, kb, rest, L, lda, B, lda);
+  trsm_llu(l, kb, nc, L, lda, B, lda);
 }
 
-// Trailing update of step k: FP16 copies of L21 and U12 (FP32 with the FP16
-// update), then C -= L21 U12[:, c0:c0+nc] for one range of columns.
+// Trailing update of step k (FP32 with the FP16 update): the FP16 copy of
+// L21 (rest x kb), once per step ...
 template <class T>
-static void update_prepare(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L21, const T* U12, int64_t lda) {
+static void prepare_l21(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L21, int64_t lda) {
   if constexpr (sizeof(T) == 4) {
     if (wk.l16) {
       ++g_launches;
       to_half_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(L21, lda, rest, kb, wk.l16, rest, nullptr, nullptr);
+    }
+  }
+}
+// ... and of U12's columns [c0, c0 + nc), scaled by their own largest
+// magnitude into the GEMM's alpha (wk.amax and wk.coef are reused by the next
+// range: same stream, so the GEMM of this range has read them first)
+template <class T>
+static void prepare_u12(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t nc, const T* U12, int64_t lda) {
+  if constexpr (sizeof(T) == 4) {
+    if (wk.l16 && nc > 0) {
+      U12 += lda * c0;
       cudaMemsetAsync(wk.amax, 0, sizeof(unsigned), l.s);
       ++g_launches;
-      amax_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(U12, lda, kb, rest, wk.amax);
+      amax_kernel<<<grid_for(nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.amax);
       ++g_launches;
-      to_half_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(U12, lda, kb, rest, wk.u16, kb, wk.amax, wk.coef);
+      to_half_kernel<<<grid_for(nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.u16 + (size_t)kb * c0, kb, wk.amax,
+                                                         wk.coef);
     }
   }
 }
@@ -1441,9 +1459,9 @@ __global__ void globalise_piv_kernel(int32_t* piv, int64_t n, int nb) {
 }
 
 // Right-looking blocked LU with depth-1 look-ahead.  Step k on the main
-// stream: swaps of panel k on the columns to its right, U12 = L11^-1 A12, the
-// update of the next block column only, then (while the panel stream
-// factors that next block column) the update of everything right of it.
+// stream: for the next block column only, the swaps of panel k, its part of
+// U12 = L11^-1 A12 and its update; then (while the panel stream factors that
+// next block column) the same for everything right of it.
 // Swaps on the columns left of each panel wait for the step that last read
 // those columns and run on a third stream.
 template <class T>
@@ -1526,15 +1544,18 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     if (k > 0) cudaStreamWaitEvent(S, ev_rest, 0);
     const int32_t* plan_k = wk.plans + (size_t)(k / kNb) * kSwapPlanInts;
     swap_apply(Lane{S, nullptr}, A + k, lda, k, plan_k);
-    P.begin(M.s);
-    swap_apply(M, A + k + lda * (k + kb), lda, n - k - kb, plan_k);
-    P.end(1);
     if (k + kb < n) {
       const int64_t rest = n - k - kb;
       const int kn = (int)std::min<int64_t>(kNb, rest);
-      block_row_solve(M, wk, kb, rest, Akk, lda, Akk + lda * kb);
+      // first everything the next panel needs: the next block column's
+      // interchanges, U12 and update; the rest of the block row after
+      P.begin(M.s);
+      swap_apply(M, A + k + lda * (k + kb), lda, kn, plan_k);
+      P.end(1);
+      block_row_solve(M, wk, kb, 0, kn, Akk, lda, Akk + lda * kb, true);
       P.end(2);
-      update_prepare(M, wk, kb, rest, Akk + kb, Akk + lda * kb, lda);
+      prepare_l21(M, wk, kb, rest, Akk + kb, lda);
+      prepare_u12(M, wk, kb, 0, kn, Akk + lda * kb, lda);
       update_gemm(M, wk, kb, rest, 0, kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * kb, lda);
       P.end(3);
       cudaEventRecord(ev_next, M.s);
@@ -1547,6 +1568,11 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       cudaEventRecord(ev_panel, Pn.s);
       if (rc) break;
       P.begin(M.s);
+      swap_apply(M, A + k + lda * (k + kb + kn), lda, rest - kn, plan_k);
+      P.end(1);
+      block_row_solve(M, wk, kb, kn, rest - kn, Akk, lda, Akk + lda * kb, false);
+      P.end(2);
+      prepare_u12(M, wk, kb, kn, rest - kn, Akk + lda * kb, lda);
       update_gemm(M, wk, kb, rest, kn, rest - kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * (kb + kn), lda);
       P.end(3);
       cudaEventRecord(ev_rest, M.s);
