@@ -732,17 +732,34 @@ void launch_local_block(double G, double nu, double h, double zr, double zi, con
 
 // ------------------------------------------------------- FP64 -> FP32 copy
 // Whole columns (ld entries each, padding rows included) as a flat range.
-__global__ void convert_f32_kernel(const double* __restrict__ a, int64_t ld, int64_t n,
-                                   float* __restrict__ f) {
-  const int64_t total = ld * n;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
-    f[i] = (float)a[i];
+// FP64 -> FP32 copy, one fixed 2048-element chunk per CTA (16-byte loads and
+// stores; the ragged tail element by element).  Short-lived CTAs let a
+// higher-priority stream's kernels take SMs as they free up while a large
+// conversion runs beside them.
+constexpr int kConvThreads = 256;
+constexpr int kConvPer = 8;  // elements per thread
+__global__ void __launch_bounds__(kConvThreads) convert_f32_kernel(const double* __restrict__ a, int64_t total,
+                                                                    float* __restrict__ f) {
+  const int64_t i0 = ((int64_t)blockIdx.x * kConvThreads + threadIdx.x) * kConvPer;
+  if (i0 + kConvPer <= total) {
+    const double2* src = reinterpret_cast<const double2*>(a + i0);
+    const double2 v0 = src[0], v1 = src[1], v2 = src[2], v3 = src[3];
+    float4* dst = reinterpret_cast<float4*>(f + i0);
+    dst[0] = make_float4((float)v0.x, (float)v0.y, (float)v1.x, (float)v1.y);
+    dst[1] = make_float4((float)v2.x, (float)v2.y, (float)v3.x, (float)v3.y);
+  } else {
+    for (int64_t i = i0; i < total; ++i) f[i] = (float)a[i];
+  }
 }
 
+// ld x n elements; both pointers 16-byte aligned (column offsets of a
+// cudaMalloc'd matrix whose ld is a multiple of 32).
 void launch_convert_f32(const double* d_a, int64_t ld, int64_t n, float* d_f, cudaStream_t s) {
-  const dim3 grid(148 * 16);
+  const int64_t total = ld * n;
+  const int64_t per_cta = (int64_t)kConvThreads * kConvPer;
+  if (total <= 0) return;
   ++g_launches;
-  convert_f32_kernel<<<grid, 256, 0, s>>>(d_a, ld, n, d_f);
+  convert_f32_kernel<<<(unsigned)((total + per_cta - 1) / per_cta), kConvThreads, 0, s>>>(d_a, total, d_f);
 }
 
 }  // namespace hfpx

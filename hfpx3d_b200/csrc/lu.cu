@@ -1465,7 +1465,10 @@ __global__ void globalise_piv_kernel(int32_t* piv, int64_t n, int nb) {
 // Swaps on the columns left of each panel wait for the step that last read
 // those columns and run on a third stream.
 template <class T>
-static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, int64_t* info_out) {
+// src64 (FP32 only): A is first filled from this FP64 matrix (same ld), the
+// first block column before the first panel, the rest beside it.
+static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, int64_t* info_out,
+                     const double* src64 = nullptr) {
   LuWork<T> wk;
   const int G = c->num_sms;
   // work buffers live in the context and are reused by later factorisations
@@ -1518,14 +1521,18 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   PhaseProfile& P = prof();
   if (!rc) {
     cudaMemsetAsync(wk.d_info, 0, sizeof(int64_t), c->stream);
+    const int kb0 = (int)std::min<int64_t>(kNb, n);
+    if constexpr (sizeof(T) == 4)
+      if (src64) launch_convert_f32(src64, lda, kb0, A, M.s);
     // the panel and swap streams start after everything queued on the main stream
     cudaEventRecord(ev_start, M.s);
     cudaStreamWaitEvent(Pn.s, ev_start, 0);
     cudaStreamWaitEvent(S, ev_start, 0);
-    const int kb0 = (int)std::min<int64_t>(kNb, n);
     rc = block_panel(c, Pn, wk, A, lda, n, kb0, piv, 0);
     if (!rc) swap_plan(Pn, piv, kb0, 0, wk.plans);
     cudaEventRecord(ev_panel, Pn.s);
+    if constexpr (sizeof(T) == 4)
+      if (src64 && n > kb0) launch_convert_f32(src64 + lda * kb0, lda, n - kb0, A + lda * kb0, M.s);
   }
   for (int64_t k = 0; k < n && !rc; k += kNb) {
     const int kb = (int)std::min<int64_t>(kNb, n - k);
@@ -1629,7 +1636,6 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
       return set_error(c, HFPX_ERR_NOMEM, "FP32 working copy");
     }
   }
-  launch_convert_f32(m->d_a, m->ld, m->n, m->d_f, c->stream);
   set_math(c, CUBLAS_TF32_TENSOR_OP_MATH);
   // The main stream's cuBLAS kernels fill all SMs but 48 during the
   // factorisation, so that a panel (<= 47 CTAs, one per SM) never waits for
@@ -1641,7 +1647,7 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
   }();
   const int main_sms = main_sms_env >= 0 ? main_sms_env : std::max(0, c->num_sms - kPanelCtas);
   if (main_sms) cublasSetSmCountTarget(H(c), main_sms);
-  int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info);
+  int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info, m->d_a);
   if (main_sms) cublasSetSmCountTarget(H(c), 0);
   set_math(c, CUBLAS_DEFAULT_MATH);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
