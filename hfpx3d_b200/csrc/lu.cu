@@ -1220,6 +1220,19 @@ struct LuWork {
   float* tslu = nullptr;
 };
 
+// Remaining size below which the main stream leaves SMs to the panel stream
+// (HFPX_LU_CAP_REST; 0: never, a large value: always).  Measured on a B200 at
+// N = 72 000 (bench, nb 1536): below ~62 000 remaining rows a panel outlasts
+// the trailing update; factor 501 ms with this threshold, 505 ms capped at
+// every step, 521 ms never capped.
+static int64_t lu_cap_rest() {
+  static const int64_t v = [] {
+    const char* e = std::getenv("HFPX_LU_CAP_REST");
+    return e ? std::max<int64_t>(0, std::atoll(e)) : (int64_t)62000;
+  }();
+  return v;
+}
+
 // FP32 base panels: partial pivoting in the register-resident kernel by
 // default; HFPX_LU_PANEL=smem takes the shared-memory kernel, =tslu the
 // tournament-pivoting kernel where its candidates fit.
@@ -1553,6 +1566,14 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     swap_apply(Lane{S, nullptr}, A + k, lda, k, plan_k);
     if (k + kb < n) {
       const int64_t rest = n - k - kb;
+      if constexpr (sizeof(T) == 4) {
+        // While the trailing update outlasts the panel, the main stream's
+        // cuBLAS kernels take every SM; once the panel chain is the longer
+        // one (rest below lu_cap_rest()), they leave 48 SMs to it so that a
+        // panel (<= 47 CTAs, one per SM) never waits for SMs.
+        const int target = rest < lu_cap_rest() ? std::max(1, c->num_sms - kPanelCtas) : 0;
+        cublasSetSmCountTarget(M.h, target);
+      }
       const int kn = (int)std::min<int64_t>(kNb, rest);
       // first everything the next panel needs: the next block column's
       // interchanges, U12 and update; the rest of the block row after
@@ -1637,18 +1658,8 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
     }
   }
   set_math(c, CUBLAS_TF32_TENSOR_OP_MATH);
-  // The main stream's cuBLAS kernels fill all SMs but 48 during the
-  // factorisation, so that a panel (<= 47 CTAs, one per SM) never waits for
-  // SMs held by the trailing update (measured at N = 72 000: 0.662 s against
-  // 0.675 s with all SMs).  HFPX_LU_MAIN_SMS sets the count (0: all SMs).
-  static const int main_sms_env = [] {
-    const char* e = std::getenv("HFPX_LU_MAIN_SMS");
-    return e ? std::max(0, std::atoi(e)) : -1;
-  }();
-  const int main_sms = main_sms_env >= 0 ? main_sms_env : std::max(0, c->num_sms - kPanelCtas);
-  if (main_sms) cublasSetSmCountTarget(H(c), main_sms);
   int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info, m->d_a);
-  if (main_sms) cublasSetSmCountTarget(H(c), 0);
+  cublasSetSmCountTarget(H(c), 0);
   set_math(c, CUBLAS_DEFAULT_MATH);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
   m->dinv_valid = 0;
