@@ -33,19 +33,21 @@ namespace cg = cooperative_groups;
 namespace hfpx {
 
 constexpr int kBaseW = 32;
-constexpr int kLuNbMax = 1536;  // largest block (row-swap plans hold 2 nb rows)
+constexpr int kLuNbMax = 2048;    // largest FP32 block (row-swap plans hold 2 nb rows)
+constexpr int kLuNbMax64 = 1024;  // largest FP64 block (the gather's register budget)
 // Block size of the right-looking LU: each trailing update reads and writes
 // the remaining matrix once, so HBM traffic ~ N^3 / (3 nb) x 8 bytes (FP32);
 // larger blocks move work into the (overlapped) panel.  Defaults measured at
-// N = 72 000: FP32 (mixed) 1536, FP64 768.  HFPX_LU_NB overrides both
-// (multiple of 32 in [64, kLuNbMax]).
+// N = 72 000: FP32 (mixed) 2048, FP64 768.  HFPX_LU_NB overrides both
+// (multiple of 32 in [64, kLuNbMax]; FP64 at most kLuNbMax64).
 static int lu_block_size(bool fp32) {
   static const int env = [] {
     const char* e = std::getenv("HFPX_LU_NB");
     const int v = e ? std::atoi(e) : 0;
     return (v >= 64 && v <= kLuNbMax && v % kBaseW == 0) ? v : 0;
   }();
-  return env ? env : fp32 ? kLuNbMax : 768;
+  if (env) return fp32 ? env : std::min(env, kLuNbMax64);
+  return fp32 ? kLuNbMax : 768;
 }
 constexpr int kPanelThreads = 256;
 
@@ -895,17 +897,25 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_tslu_kernel(
 // to every column as one gather: contiguous reads of the leading rows
 // instead of k dependent strided swaps per column.
 constexpr int kSwapMax = kLuNbMax;              // interchanges per plan (block size cap)
-constexpr int kSwapHash = 4096;                 // rows >= k touched, open addressing
+constexpr int kSwapHash = 8192;                 // rows >= k touched, open addressing (<= 25 % full)
+constexpr int kSwapHashShift = 32 - 13;         // multiplicative hash to 13 bits
 constexpr int kSwapPlanInts = 1 + 4 * kSwapMax; // count, src[2 kSwapMax], dst[2 kSwapMax]
 constexpr int kSwapThreads = 256;
-constexpr int kSwapPer = 2 * kSwapMax / kSwapThreads;
+// plan entries each thread gathers: all 2 kSwapMax for FP32, 2 kLuNbMax64 for FP64
+template <class T>
+constexpr int swap_per() { return 2 * (sizeof(T) == 8 ? kLuNbMax64 : kSwapMax) / kSwapThreads; }
 constexpr int kSwapCols = 4;                    // columns per gather pass
+constexpr size_t kSwapPlanSmem = sizeof(int32_t) * (2 * kSwapMax + 2 * kSwapHash);
 
 // add != 0: piv[i] += add afterwards (pivots of a sub-panel made relative to
 // the enclosing panel).
 __global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __restrict__ piv, int k, int base,
                                                                   int32_t* __restrict__ plan, int add) {
-  __shared__ int32_t content[kSwapMax], spiv[kSwapMax], hkey[kSwapHash], hval[kSwapHash];
+  extern __shared__ int32_t swsm[];  // kSwapPlanSmem bytes
+  int32_t* content = swsm;
+  int32_t* spiv = content + kSwapMax;
+  int32_t* hkey = spiv + kSwapMax;
+  int32_t* hval = hkey + kSwapHash;
   __shared__ int moved;
   const int tid = threadIdx.x;
   for (int i = tid; i < k; i += kSwapThreads) {
@@ -925,7 +935,7 @@ __global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __rest
       if (p < k) {
         slot = &content[p];
       } else {
-        unsigned h = ((unsigned)p * 2654435761u) >> 20;
+        unsigned h = ((unsigned)p * 2654435761u) >> kSwapHashShift;
         while (hkey[h] != -1 && hkey[h] != p) h = (h + 1) & (kSwapHash - 1);
         if (hkey[h] == -1) { hkey[h] = p; hval[h] = p; }
         slot = &hval[h];
@@ -957,6 +967,7 @@ __global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __rest
 template <class T>
 __global__ void __launch_bounds__(kSwapThreads) swap_apply_kernel(T* __restrict__ A, int64_t lda, int64_t ncols,
                                                                    const int32_t* __restrict__ plan) {
+  constexpr int kSwapPer = swap_per<T>();
   const int cnt = plan[0];
   const int tid = threadIdx.x;
   int s[kSwapPer], d[kSwapPer];
@@ -1394,7 +1405,12 @@ static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int
 static void swap_plan(Lane l, int32_t* piv, int k, int base, int32_t* plan, int add = 0) {
   if (k <= 0) return;
   ++g_launches;
-  swap_plan_kernel<<<1, kSwapThreads, 0, l.s>>>(piv, k, base, plan, add);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(swap_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapPlanSmem);
+    attr = true;
+  }
+  swap_plan_kernel<<<1, kSwapThreads, kSwapPlanSmem, l.s>>>(piv, k, base, plan, add);
 }
 
 template <class T>
