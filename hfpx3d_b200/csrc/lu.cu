@@ -2,7 +2,8 @@
 // il/linear_algebra/dense/factorization/LU.h:79-120) and the mixed-precision
 // solve.
 //
-// Blocked right-looking LU, block nb = 768 (HFPX_LU_NB), depth-1 look-ahead:
+// Blocked right-looking LU, block nb = 2048 FP32 / 768 FP64 (HFPX_LU_NB),
+// depth-1 look-ahead:
 //   panel  (n-k) x nb : recursive halving (dgetrf2 order); the <=32-column
 //          base case is one cooperative kernel: for FP32 the rows sit in
 //          registers and the pivot search is exchanged through L2 words
@@ -325,17 +326,81 @@ __device__ void ll_finish(MoveShared& ms, float* __restrict__ A, int64_t lda, in
   ll_moves_apply(ms, A, lda, w, left, w, right, xtmp);
 }
 
+// CTA arg-max of |a(i, jj)| (register column 0) over the rows labelled >= jj,
+// lowest label on ties, in every thread.  Arg-max keys are |a| bits + 1
+// (non-negative floats order as their bits), 0 for "no row".  Holds one CTA
+// barrier between the two reductions.
+__device__ __forceinline__ void ll_cta_argmax(const float (&a)[kLLRows][kBaseW], const int (&lab)[kLLRows], int jj,
+                                              unsigned* s_wk, unsigned* s_wi, unsigned& bkey, unsigned& bidx) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bkey = 0u;
+  bidx = 0xFFFFFFFFu;
+#pragma unroll
+  for (int k = 0; k < kLLRows; ++k) {
+    const unsigned kk = lab[k] >= jj ? __float_as_uint(fabsf(a[k][0])) + 1u : 0u;
+    if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) { bkey = kk; bidx = (unsigned)lab[k]; }
+  }
+  {
+    const unsigned wm = __reduce_max_sync(0xffffffffu, bkey);
+    const unsigned wi = __reduce_min_sync(0xffffffffu, bkey == wm ? bidx : 0xFFFFFFFFu);
+    if (lane == 0) { s_wk[warp] = wm; s_wi[warp] = wi; }
+  }
+  __syncthreads();
+  const unsigned k2 = lane < kLLThreads / 32 ? s_wk[lane] : 0u;
+  const unsigned i2 = lane < kLLThreads / 32 ? s_wi[lane] : 0xFFFFFFFFu;
+  bkey = __reduce_max_sync(0xffffffffu, k2);
+  bidx = __reduce_min_sync(0xffffffffu, k2 == bkey ? i2 : 0xFFFFFFFFu);
+}
+
+// Register row k of this thread after step j's rank-1 update, to shared
+// memory, while only its register column 0 holds the updated value (the
+// update of the other columns comes later; the same fmaf, so the same bits).
+template <int K = 0>
+__device__ __forceinline__ void ll_next_row_to_smem(const float (&a)[kLLRows][kBaseW], const float (&lz)[kLLRows],
+                                                    const uint32_t* prow, int k, float* dst) {
+  if (k == K) {
+    dst[0] = a[K][0];
+#pragma unroll
+    for (int c = 1; c + 1 < kBaseW; ++c) dst[c] = fmaf(-lz[K], __uint_as_float(prow[c + 1]), a[K][c + 1]);
+    dst[kBaseW - 1] = 0.f;
+  } else if constexpr (K + 1 < kLLRows) {
+    ll_next_row_to_smem<K + 1>(a, lz, prow, k, dst);
+  }
+}
+
+// Publishes this CTA's candidate for one column in its words `mine` (tag):
+// thread 0 the key and row, the warp holding the candidate row the row, one
+// word per lane (stage: that warp's staging row, filled by the caller); a CTA
+// without candidates publishes zeros.  `hit`: this warp holds the row.
+__device__ __forceinline__ void ll_publish(uint64_t* mine, unsigned bkey, unsigned bidx, uint32_t tag, int w,
+                                           bool hit, const float* stage) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) {
+    ll_store(mine, bkey, tag);
+    ll_store(mine + 1, bidx, tag);
+  }
+  if (hit) {
+    if (lane < w) ll_store(mine + 2 + lane, __float_as_uint(stage[lane]), tag);
+  } else if (bkey == 0u && tid < 32 && lane < w) {
+    ll_store(mine + 2 + lane, 0u, tag);
+  }
+}
+
 // piv[j] = pivot row + piv_add; left/right: columns of the enclosing block
 // panel on either side that take the interchanges too (ll_finish).
+// Step j, once the pivot p and its row are known: the labels swap, every row
+// takes the update of its register column 0 only (column j + 1 of the panel),
+// the CTA's candidate for column j + 1 is found and published, and only then
+// do the other 30 register columns take their update and column j go to A, so
+// that work overlaps the exchange of column j + 1.
 __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     float* __restrict__ A, int64_t lda, int64_t m, int w, int rpc, int32_t* __restrict__ piv,
     uint64_t* __restrict__ slots, int64_t* __restrict__ info, int64_t col_offset, uint32_t tag0,
     int* __restrict__ err, int left, int right, float* __restrict__ xtmp, int piv_add) {
-  // arg-max candidates travel as keys: |a| bits + 1 (non-negative floats
-  // order as their bits), 0 for "no row"; ties go to the lower row
-  __shared__ float s_cand[2][kLLMaxCtas][kBaseW];
-  __shared__ unsigned s_key[2][kLLMaxCtas];
-  __shared__ unsigned s_idx[2][kLLMaxCtas];
+  // the polled words of columns j (buffer j & 1), laid out as in `slots`:
+  // per CTA (key, row, candidate row); words never written stay zero, so
+  // candidate columns past w read as zeros
+  __shared__ __align__(16) uint32_t s_w[2][kLLMaxCtas * kLLSlot];
   __shared__ unsigned s_wk[kLLThreads / 32];
   __shared__ unsigned s_wi[kLLThreads / 32];
   __shared__ float s_stage[kLLThreads / 32][kBaseW];
@@ -354,8 +419,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     for (int c = 0; c < kBaseW; ++c)
       a[k][c] = (lab[k] >= 0 && c < w) ? A[(int64_t)lab[k] + lda * c] : 0.f;
   }
-  // candidate rows past column w stay zero
-  for (int i = tid; i < 2 * kLLMaxCtas * kBaseW; i += kLLThreads) (&s_cand[0][0][0])[i] = 0.f;
+  for (int i = tid; i < 2 * kLLMaxCtas * kLLSlot; i += kLLThreads) (&s_w[0][0])[i] = 0u;
   if (tid == 0) s_fail = 0;
   // words this thread polls: CTA q's (key, row, candidate row)
   const int per = 2 + w, units = G * per;
@@ -365,52 +429,24 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const int x = tid + u * kLLThreads;
     off[u] = x < units ? (x / per) * kLLSlot + x % per : -1;
   }
+  // column 0's candidate, the rows as loaded
+  {
+    unsigned bkey, bidx;
+    ll_cta_argmax(a, lab, 0, s_wk, s_wi, bkey, bidx);
+    int kc = -1;
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) kc = ((unsigned)lab[k] == bidx && bkey != 0u) ? k : kc;
+    const bool hit = __ballot_sync(0xffffffffu, kc >= 0) != 0u;
+    if (kc >= 0) ll_row_to_smem(a, kc, s_stage[warp]);
+    __syncwarp();
+    ll_publish(slots + (size_t)b * kLLSlot, bkey, bidx, tag0 + 1u, w, hit, s_stage[warp]);
+  }
   for (int j = 0; j < w; ++j) {
     const int buf = j & 1;
     const uint32_t tag = tag0 + (uint32_t)j + 1u;
-    // CTA arg-max of |a(i, j)| (register column 0) over rows labelled >= j,
-    // lowest label on ties
-    unsigned bkey = 0u, bidx = 0xFFFFFFFFu;
-#pragma unroll
-    for (int k = 0; k < kLLRows; ++k) {
-      const unsigned kk = lab[k] >= j ? __float_as_uint(fabsf(a[k][0])) + 1u : 0u;
-      if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) { bkey = kk; bidx = (unsigned)lab[k]; }
-    }
-    {
-      const unsigned wm = __reduce_max_sync(0xffffffffu, bkey);
-      const unsigned wi = __reduce_min_sync(0xffffffffu, bkey == wm ? bidx : 0xFFFFFFFFu);
-      if (lane == 0) { s_wk[warp] = wm; s_wi[warp] = wi; }
-    }
-    __syncthreads();
-    {
-      const unsigned k2 = lane < kLLThreads / 32 ? s_wk[lane] : 0u;
-      const unsigned i2 = lane < kLLThreads / 32 ? s_wi[lane] : 0xFFFFFFFFu;
-      bkey = __reduce_max_sync(0xffffffffu, k2);
-      bidx = __reduce_min_sync(0xffffffffu, k2 == bkey ? i2 : 0xFFFFFFFFu);
-    }
-    // publish: thread 0 the key and row; the warp holding the candidate row
-    // (staged through shared memory by its lane) that row, one word per
-    // lane; a CTA without candidates publishes zeros
-    uint64_t* mine = slots + ((size_t)buf * G + b) * kLLSlot;
-    if (tid == 0) {
-      ll_store(mine, bkey, tag);
-      ll_store(mine + 1, bidx, tag);
-    }
-    {
-      int kc = -1;
-#pragma unroll
-      for (int k = 0; k < kLLRows; ++k) kc = ((unsigned)lab[k] == bidx && bkey != 0u) ? k : kc;
-      const unsigned hit = __ballot_sync(0xffffffffu, kc >= 0);
-      if (hit) {
-        if (kc >= 0) ll_row_to_smem(a, kc, s_stage[warp]);
-        __syncwarp();
-        if (lane < w) ll_store(mine + 2 + lane, __float_as_uint(s_stage[warp][lane]), tag);
-      } else if (bkey == 0u && warp == 0 && lane < w) {
-        ll_store(mine + 2 + lane, 0u, tag);
-      }
-    }
     // poll every CTA's words for this column
     const uint64_t* xb = slots + (size_t)buf * G * kLLSlot;
+    uint32_t* sw = s_w[buf];
     bool need[kLLUnits];
 #pragma unroll
     for (int u = 0; u < kLLUnits; ++u) need[u] = off[u] >= 0;
@@ -426,11 +462,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
         if (!need[u]) continue;
         if ((uint32_t)(v[u] >> 32) != tag) { pending = true; continue; }
         need[u] = false;
-        const uint32_t d = (uint32_t)v[u];
-        const int q = off[u] / kLLSlot, o = off[u] - q * kLLSlot;
-        if (o == 0) s_key[buf][q] = d;
-        else if (o == 1) s_idx[buf][q] = d;
-        else s_cand[buf][q][o - 2] = __uint_as_float(d);
+        sw[off[u]] = (uint32_t)v[u];
       }
       if (!pending) break;
       const uint64_t now = global_ns();
@@ -446,13 +478,13 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     // global pivot, identical in every warp of every CTA
     unsigned gk = 0u, gi = 0xFFFFFFFFu, gq = 0u;
     for (int q = lane; q < G; q += 32) {
-      const unsigned kq = s_key[buf][q], iq = s_idx[buf][q];
+      const unsigned kq = sw[q * kLLSlot], iq = sw[q * kLLSlot + 1];
       if (kq > gk || (kq == gk && iq < gi)) { gk = kq; gi = iq; gq = (unsigned)q; }
     }
     const unsigned gmax = __reduce_max_sync(0xffffffffu, gk);
     const unsigned pu = __reduce_min_sync(0xffffffffu, gk == gmax ? gi : 0xFFFFFFFFu);
     const int p = (int)pu;
-    const float* prow = s_cand[buf][__reduce_max_sync(0xffffffffu, (gk == gmax && gi == pu) ? gq : 0u)];
+    const uint32_t* prow = sw + __reduce_max_sync(0xffffffffu, (gk == gmax && gi == pu) ? gq : 0u) * kLLSlot + 2;
     if (b == 0 && tid == 0) {
       piv[j] = p + piv_add;
       if (gmax == 1u && info && *info == 0) *info = col_offset + j + 1;  // |pivot| == 0
@@ -462,21 +494,39 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
 #pragma unroll
       for (int k = 0; k < kLLRows; ++k) lab[k] = lab[k] == j ? p : (lab[k] == p ? j : lab[k]);
     }
-    const float pv = prow[0];
+    const float pv = __uint_as_float(prow[0]);
     const bool nz = pv != 0.f;
     const float inv = nz ? 1.f / pv : 0.f;
     // Column j of every row is final after this step (the multiplier of a
-    // row below, U of the pivot and of earlier pivots): it goes to the row's
-    // slot in A, and the registers shift left by one as the rows below take
-    // the rank-1 update (multiplier 0 for the others: a plain shift).
+    // row below, U of the pivot and of earlier pivots); the registers shift
+    // left by one as the rows below take the rank-1 update (multiplier 0 for
+    // the others: a plain shift).  Register column 0 first.
+    float l[kLLRows], lz[kLLRows];
+    const float p1 = __uint_as_float(prow[1]);
 #pragma unroll
     for (int k = 0; k < kLLRows; ++k) {
       const bool below = nz && lab[k] > j;
-      const float l = below ? a[k][0] * inv : a[k][0];
-      const float lz = below ? l : 0.f;
-      if (lab[k] >= 0) A[(int64_t)(g0 + k * kLLThreads) + lda * j] = l;
+      l[k] = below ? a[k][0] * inv : a[k][0];
+      lz[k] = below ? l[k] : 0.f;
+      a[k][0] = fmaf(-lz[k], p1, a[k][1]);
+    }
+    if (j + 1 < w) {
+      unsigned bkey, bidx;
+      ll_cta_argmax(a, lab, j + 1, s_wk, s_wi, bkey, bidx);
+      int kc = -1;
 #pragma unroll
-      for (int c = 0; c + 1 < kBaseW; ++c) a[k][c] = fmaf(-lz, prow[c + 1], a[k][c + 1]);
+      for (int k = 0; k < kLLRows; ++k) kc = ((unsigned)lab[k] == bidx && bkey != 0u) ? k : kc;
+      const bool hit = __ballot_sync(0xffffffffu, kc >= 0) != 0u;
+      if (kc >= 0) ll_next_row_to_smem(a, lz, prow, kc, s_stage[warp]);
+      __syncwarp();
+      ll_publish(slots + ((size_t)(buf ^ 1) * G + b) * kLLSlot, bkey, bidx, tag + 1u, w, hit, s_stage[warp]);
+    }
+    // the rest of the update and column j, behind the exchange of column j + 1
+#pragma unroll
+    for (int k = 0; k < kLLRows; ++k) {
+      if (lab[k] >= 0) A[(int64_t)(g0 + k * kLLThreads) + lda * j] = l[k];
+#pragma unroll
+      for (int c = 1; c + 1 < kBaseW; ++c) a[k][c] = fmaf(-lz[k], __uint_as_float(prow[c + 1]), a[k][c + 1]);
       a[k][kBaseW - 1] = 0.f;
     }
   }
