@@ -1279,6 +1279,8 @@ struct LuWork {
   float* xtmp = nullptr;
   // tournament candidates: [kTsluMaxCtas][kBaseW][kBaseW] rows, then labels
   float* tslu = nullptr;
+  // panel_update32_kernel's ticket counter (zero between launches)
+  unsigned* pu32_ticket = nullptr;
 };
 
 // Remaining size below which the main stream leaves SMs to the panel stream
@@ -1480,6 +1482,76 @@ static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, int32_t* piv, int k,
   swap_apply(l, A, lda, ncols, plan);
 }
 
+// Lowest level of the FP32 panel recursion, a 32-column left half: dgetrf2's
+// U12 = L11^-1 A12 (unit lower L11) and A22 -= L21 U12 in one launch, where
+// cuBLAS spends a TRSM launch of ~20 us on the 32 x 32 triangle alone.
+// Every CTA solves U12 (w2 <= 32 columns) in shared memory, the same
+// arithmetic in each, and CTA 0 stores it; then each thread takes one row of
+// A22 through the 32-term update in FP32 (U12 broadcast from shared memory,
+// L21 and A22 read once, coalesced down the columns).  U12 overwrites A12
+// in place, so it is stored by the last CTA to have read A12: each CTA takes
+// a ticket once its copy is in shared memory, and the CTA holding the last
+// ticket stores U12 and puts the counter back to 0 for the next launch (the
+// launches of one factorisation are ordered on one stream).  No CTA waits for
+// another.
+constexpr int kPu32Threads = 256;
+__global__ void __launch_bounds__(kPu32Threads) panel_update32_kernel(float* __restrict__ A, int64_t lda, int64_t m,
+                                                                      int w2, unsigned* __restrict__ ticket) {
+  __shared__ float s_l[kBaseW][kBaseW + 1];  // L11(i, t)
+  __shared__ __align__(16) float s_u[kBaseW][kBaseW];  // A12 -> U12 (t, c)
+  __shared__ bool s_last;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kBaseW * kBaseW; e += kPu32Threads) {
+    const int i = e % kBaseW, t = e / kBaseW;  // column-major: neighbouring threads, neighbouring rows
+    s_l[i][t] = A[i + lda * t];
+    s_u[i][t] = t < w2 ? A[i + lda * (kBaseW + t)] : 0.f;
+  }
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1u;
+  if (tid < kBaseW) {
+    // forward substitution down column c of U12 (row i takes rows t < i)
+    const int c = tid;
+    float u[kBaseW];
+#pragma unroll
+    for (int i = 0; i < kBaseW; ++i) u[i] = s_u[i][c];
+#pragma unroll
+    for (int t = 0; t < kBaseW; ++t)
+#pragma unroll
+      for (int i = t + 1; i < kBaseW; ++i) u[i] = fmaf(-s_l[i][t], u[t], u[i]);
+#pragma unroll
+    for (int i = 0; i < kBaseW; ++i) s_u[i][c] = u[i];
+  }
+  __syncthreads();
+  if (s_last) {
+    for (int e = tid; e < kBaseW * w2; e += kPu32Threads) {
+      const int i = e % kBaseW, t = e / kBaseW;
+      A[i + lda * (kBaseW + t)] = s_u[i][t];
+    }
+    if (tid == 0) *ticket = 0u;
+  }
+  const int64_t r = kBaseW + (int64_t)blockIdx.x * kPu32Threads + tid;
+  if (r >= m) return;
+  float acc[kBaseW];
+#pragma unroll
+  for (int c = 0; c < kBaseW; ++c) acc[c] = c < w2 ? A[r + lda * (kBaseW + c)] : 0.f;
+#pragma unroll 4
+  for (int t = 0; t < kBaseW; ++t) {
+    const float l = A[r + lda * t];
+    const float4* ut = reinterpret_cast<const float4*>(s_u[t]);
+#pragma unroll
+    for (int q = 0; q < kBaseW / 4; ++q) {
+      const float4 v = ut[q];
+      acc[4 * q] = fmaf(-l, v.x, acc[4 * q]);
+      acc[4 * q + 1] = fmaf(-l, v.y, acc[4 * q + 1]);
+      acc[4 * q + 2] = fmaf(-l, v.z, acc[4 * q + 2]);
+      acc[4 * q + 3] = fmaf(-l, v.w, acc[4 * q + 3]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kBaseW; ++c)
+    if (c < w2) A[r + lda * (kBaseW + c)] = acc[c];
+}
+
 // dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
 // sp.c0: column (and row) offset of this sub-panel inside its block panel of
 // sp.bw columns.  sp.eager: every base panel applies its own interchanges to
@@ -1502,10 +1574,22 @@ static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int6
   P.begin(l.s);
   if (!sp.eager) laswp(l, A + lda * w1, lda, w2, piv, w1, 0, wk.plan_panel);
   P.end(1);
-  trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
-  P.end(2);
-  gemm_sub(l, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
-  P.end(3);
+  bool fused = false;
+  if constexpr (sizeof(T) == 4) {
+    if (w1 == kBaseW && w2 <= kBaseW && m > w1 && wk.pu32_ticket) {
+      ++g_launches;
+      panel_update32_kernel<<<(unsigned)((m - w1 + kPu32Threads - 1) / kPu32Threads), kPu32Threads, 0, l.s>>>(
+          A, lda, m, w2, wk.pu32_ticket);
+      P.end(3);
+      fused = true;
+    }
+  }
+  if (!fused) {
+    trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
+    P.end(2);
+    gemm_sub(l, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
+    P.end(3);
+  }
   PanelSpan sr = sp;
   sr.c0 += w1;
   rc = panel_rec(c, l, wk, A + w1 + lda * w1, lda, m - w1, w2, piv + w1, col_offset + w1, sr);
@@ -1560,10 +1644,12 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   const int64_t n_blocks = (n + lu_block_size(sizeof(T) == 4) - 1) / lu_block_size(sizeof(T) == 4);
   wk.plan_panel = (int32_t*)alloc(kScrPlanPanel, sizeof(int32_t) * kSwapPlanInts);
   wk.plans = (int32_t*)alloc(kScrPlans, sizeof(int32_t) * kSwapPlanInts * (size_t)n_blocks);
-  // two column buffers of per-CTA words, then two barriers of one word per CTA
-  const size_t ll_bytes = sizeof(uint64_t) * (2 * kLLMaxCtas * kLLSlot + 2 * kLLMaxCtas);
+  // two column buffers of per-CTA words, two barriers of one word per CTA,
+  // then panel_update32_kernel's ticket
+  const size_t ll_bytes = sizeof(uint64_t) * (2 * kLLMaxCtas * kLLSlot + 2 * kLLMaxCtas + 1);
   if (sizeof(T) == 4) {
     wk.ll_slots = (uint64_t*)alloc(kScrLLSlots, ll_bytes);
+    if (wk.ll_slots) wk.pu32_ticket = reinterpret_cast<unsigned*>(wk.ll_slots + 2 * kLLMaxCtas * kLLSlot + 2 * kLLMaxCtas);
     wk.ll_err = (int*)alloc(kScrLLErr, sizeof(int));
     // optional: without it the panels keep partial pivoting
     if (panel_kind() == PanelKind::Tournament)
