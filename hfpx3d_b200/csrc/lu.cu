@@ -352,35 +352,34 @@ __device__ __forceinline__ void ll_cta_argmax(const float (&a)[kLLRows][kBaseW],
   bidx = __reduce_min_sync(0xffffffffu, k2 == bkey ? i2 : 0xFFFFFFFFu);
 }
 
-// Register row k of this thread after step j's rank-1 update, to shared
-// memory, while only its register column 0 holds the updated value (the
-// update of the other columns comes later; the same fmaf, so the same bits).
+// Register row k of this thread and its multiplier lz[k] to shared memory
+// (dst[0..kBaseW), then dst[kBaseW]) as they stand: during step j's update
+// register column 0 already holds the updated value, the others not yet.
 template <int K = 0>
-__device__ __forceinline__ void ll_next_row_to_smem(const float (&a)[kLLRows][kBaseW], const float (&lz)[kLLRows],
-                                                    const uint32_t* prow, int k, float* dst) {
+__device__ __forceinline__ void ll_row_lz_to_smem(const float (&a)[kLLRows][kBaseW], const float (&lz)[kLLRows], int k,
+                                                  float* dst) {
   if (k == K) {
-    dst[0] = a[K][0];
 #pragma unroll
-    for (int c = 1; c + 1 < kBaseW; ++c) dst[c] = fmaf(-lz[K], __uint_as_float(prow[c + 1]), a[K][c + 1]);
-    dst[kBaseW - 1] = 0.f;
+    for (int c = 0; c < kBaseW; ++c) dst[c] = a[K][c];
+    dst[kBaseW] = lz[K];
   } else if constexpr (K + 1 < kLLRows) {
-    ll_next_row_to_smem<K + 1>(a, lz, prow, k, dst);
+    ll_row_lz_to_smem<K + 1>(a, lz, k, dst);
   }
 }
 
 // Publishes this CTA's candidate for one column in its words `mine` (tag):
 // thread 0 the key and row, the warp holding the candidate row the row, one
-// word per lane (stage: that warp's staging row, filled by the caller); a CTA
-// without candidates publishes zeros.  `hit`: this warp holds the row.
+// word per lane (v: this lane's column of it); a CTA without candidates
+// publishes zeros.  `hit`: this warp holds the row.
 __device__ __forceinline__ void ll_publish(uint64_t* mine, unsigned bkey, unsigned bidx, uint32_t tag, int w,
-                                           bool hit, const float* stage) {
+                                           bool hit, float v) {
   const int tid = threadIdx.x, lane = tid & 31;
   if (tid == 0) {
     ll_store(mine, bkey, tag);
     ll_store(mine + 1, bidx, tag);
   }
   if (hit) {
-    if (lane < w) ll_store(mine + 2 + lane, __float_as_uint(stage[lane]), tag);
+    if (lane < w) ll_store(mine + 2 + lane, __float_as_uint(v), tag);
   } else if (bkey == 0u && tid < 32 && lane < w) {
     ll_store(mine + 2 + lane, 0u, tag);
   }
@@ -403,7 +402,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
   __shared__ __align__(16) uint32_t s_w[2][kLLMaxCtas * kLLSlot];
   __shared__ unsigned s_wk[kLLThreads / 32];
   __shared__ unsigned s_wi[kLLThreads / 32];
-  __shared__ float s_stage[kLLThreads / 32][kBaseW];
+  __shared__ float s_stage[kLLThreads / 32][kBaseW + 1];  // a warp's candidate row (+ its multiplier)
   __shared__ int s_fail;
   const int b = blockIdx.x, G = gridDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t r0 = (int64_t)b * rpc;
@@ -420,6 +419,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
       a[k][c] = (lab[k] >= 0 && c < w) ? A[(int64_t)lab[k] + lda * c] : 0.f;
   }
   for (int i = tid; i < 2 * kLLMaxCtas * kLLSlot; i += kLLThreads) (&s_w[0][0])[i] = 0u;
+  const float* st = s_stage[warp];
   if (tid == 0) s_fail = 0;
   // words this thread polls: CTA q's (key, row, candidate row)
   const int per = 2 + w, units = G * per;
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const bool hit = __ballot_sync(0xffffffffu, kc >= 0) != 0u;
     if (kc >= 0) ll_row_to_smem(a, kc, s_stage[warp]);
     __syncwarp();
-    ll_publish(slots + (size_t)b * kLLSlot, bkey, bidx, tag0 + 1u, w, hit, s_stage[warp]);
+    ll_publish(slots + (size_t)b * kLLSlot, bkey, bidx, tag0 + 1u, w, hit, st[lane]);
   }
   for (int j = 0; j < w; ++j) {
     const int buf = j & 1;
@@ -517,9 +517,16 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
 #pragma unroll
       for (int k = 0; k < kLLRows; ++k) kc = ((unsigned)lab[k] == bidx && bkey != 0u) ? k : kc;
       const bool hit = __ballot_sync(0xffffffffu, kc >= 0) != 0u;
-      if (kc >= 0) ll_next_row_to_smem(a, lz, prow, kc, s_stage[warp]);
+      // the candidate row after step j, one column per lane: the owner's
+      // registers as they stand, then the same fmaf as the update below
+      if (kc >= 0) ll_row_lz_to_smem(a, lz, kc, s_stage[warp]);
       __syncwarp();
-      ll_publish(slots + ((size_t)(buf ^ 1) * G + b) * kLLSlot, bkey, bidx, tag + 1u, w, hit, s_stage[warp]);
+      float v = 0.f;
+      if (hit) {
+        v = lane == 0 ? st[0]
+                      : (lane + 1 < kBaseW ? fmaf(-st[kBaseW], __uint_as_float(prow[lane + 1]), st[lane + 1]) : 0.f);
+      }
+      ll_publish(slots + ((size_t)(buf ^ 1) * G + b) * kLLSlot, bkey, bidx, tag + 1u, w, hit, v);
     }
     // the rest of the update and column j, behind the exchange of column j + 1
 #pragma unroll
