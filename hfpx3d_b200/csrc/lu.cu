@@ -333,13 +333,28 @@ __device__ void ll_finish(MoveShared& ms, float* __restrict__ A, int64_t lda, in
 __device__ __forceinline__ void ll_cta_argmax(const float (&a)[kLLRows][kBaseW], const int (&lab)[kLLRows], int jj,
                                               unsigned* s_wk, unsigned* s_wi, unsigned& bkey, unsigned& bidx) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  bkey = 0u;
-  bidx = 0xFFFFFFFFu;
+  // the thread's rows pairwise (a tree, not a chain); a row without a key
+  // carries label 0xFFFFFFFF, so equal keys keep the lower label
+  static_assert(kLLRows == 6, "the tree below pairs 6 rows");
+  unsigned kk[kLLRows], ii[kLLRows];
 #pragma unroll
   for (int k = 0; k < kLLRows; ++k) {
-    const unsigned kk = lab[k] >= jj ? __float_as_uint(fabsf(a[k][0])) + 1u : 0u;
-    if (kk > bkey || (kk == bkey && kk != 0u && (unsigned)lab[k] < bidx)) { bkey = kk; bidx = (unsigned)lab[k]; }
+    const bool on = lab[k] >= jj;
+    kk[k] = on ? __float_as_uint(fabsf(a[k][0])) + 1u : 0u;
+    ii[k] = on ? (unsigned)lab[k] : 0xFFFFFFFFu;
   }
+  auto pick = [](unsigned& k1, unsigned& i1, unsigned k2, unsigned i2) {
+    const bool two = k2 > k1 || (k2 == k1 && i2 < i1);
+    k1 = two ? k2 : k1;
+    i1 = two ? i2 : i1;
+  };
+  pick(kk[0], ii[0], kk[1], ii[1]);
+  pick(kk[2], ii[2], kk[3], ii[3]);
+  pick(kk[4], ii[4], kk[5], ii[5]);
+  pick(kk[0], ii[0], kk[2], ii[2]);
+  pick(kk[0], ii[0], kk[4], ii[4]);
+  bkey = kk[0];
+  bidx = ii[0];
   {
     const unsigned wm = __reduce_max_sync(0xffffffffu, bkey);
     const unsigned wi = __reduce_min_sync(0xffffffffu, bkey == wm ? bidx : 0xFFFFFFFFu);
@@ -484,7 +499,10 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const unsigned gmax = __reduce_max_sync(0xffffffffu, gk);
     const unsigned pu = __reduce_min_sync(0xffffffffu, gk == gmax ? gi : 0xFFFFFFFFu);
     const int p = (int)pu;
-    const uint32_t* prow = sw + __reduce_max_sync(0xffffffffu, (gk == gmax && gi == pu) ? gq : 0u) * kLLSlot + 2;
+    // the lane holding the winner (labels are unique; with no row left
+    // anywhere every lane holds key 0 and label 0xFFFFFFFF: lane 0, CTA 0)
+    const unsigned wl = __ffs(__ballot_sync(0xffffffffu, gk == gmax && gi == pu)) - 1;
+    const uint32_t* prow = sw + __shfl_sync(0xffffffffu, gq, wl) * kLLSlot + 2;
     if (b == 0 && tid == 0) {
       piv[j] = p + piv_add;
       if (gmax == 1u && info && *info == 0) *info = col_offset + j + 1;  // |pivot| == 0
