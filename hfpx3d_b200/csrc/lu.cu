@@ -444,6 +444,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     const int x = tid + u * kLLThreads;
     off[u] = x < units ? (x / per) * kLLSlot + x % per : -1;
   }
+  bool swapped = false;  // an interchange happened (the same in every CTA)
   // column 0's candidate, the rows as loaded
   {
     unsigned bkey, bidx;
@@ -509,6 +510,7 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
     }
     // interchange rows j and p: swap the labels
     if (p != j) {
+      swapped = true;
 #pragma unroll
       for (int k = 0; k < kLLRows; ++k) lab[k] = lab[k] == j ? p : (lab[k] == p ? j : lab[k]);
     }
@@ -555,9 +557,11 @@ __global__ void __launch_bounds__(kLLThreads, 1) panel_ll_kernel(
       a[k][kBaseW - 1] = 0.f;
     }
   }
+  // without interchanges every row is in its slot: no moves, no barrier
   __shared__ MoveShared ms;
-  ll_finish(ms, A, lda, w, lab, g0, left, right, xtmp, slots + (size_t)2 * kLLMaxCtas * kLLSlot, tag0 + 63u, err,
-            s_fail);
+  if (swapped)
+    ll_finish(ms, A, lda, w, lab, g0, left, right, xtmp, slots + (size_t)2 * kLLMaxCtas * kLLSlot, tag0 + 63u, err,
+              s_fail);
 }
 
 // ------------------------------------------ tournament-pivoting FP32 panel
@@ -1021,22 +1025,42 @@ __global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __rest
     }
   }
   __syncthreads();
-  // all k leading rows in order (contiguous writes, near-contiguous reads),
-  // then the rows below k that changed, in any order
+  // the leading rows that changed, in order (neighbouring rows stay
+  // neighbours in a warp's gather), then the rows below k that changed, in
+  // any order; no interchange at all leaves an empty plan
   int32_t* src = plan + 1;
   int32_t* dst = plan + 1 + 2 * kSwapMax;
-  for (int i = tid; i < k; i += kSwapThreads) {
-    src[i] = content[i];
-    dst[i] = i;
+  __shared__ int wcount[kSwapThreads / 32];
+  const int lane = tid & 31, warp = tid >> 5;
+  int nlead = 0;
+  for (int i0 = 0; i0 < k; i0 += kSwapThreads) {
+    const int i = i0 + tid;
+    const bool f = i < k && content[i] != i;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcount[warp] = __popc(bal);
+    __syncthreads();
+    int off = nlead, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kSwapThreads / 32; ++w) {
+      off += w < warp ? wcount[w] : 0;
+      tot += wcount[w];
+    }
+    if (f) {
+      const int e = off + __popc(bal & ((1u << lane) - 1u));
+      src[e] = content[i];
+      dst[e] = i;
+    }
+    __syncthreads();
+    nlead += tot;
   }
   for (int h = tid; h < kSwapHash; h += kSwapThreads)
     if (hkey[h] >= 0 && hval[h] != hkey[h]) {
-      const int e = k + atomicAdd(&moved, 1);
+      const int e = nlead + atomicAdd(&moved, 1);
       src[e] = hval[h];
       dst[e] = hkey[h];
     }
   __syncthreads();
-  if (tid == 0) plan[0] = k + moved;
+  if (tid == 0) plan[0] = nlead + moved;
 }
 
 template <class T>
@@ -1044,6 +1068,7 @@ __global__ void __launch_bounds__(kSwapThreads) swap_apply_kernel(T* __restrict_
                                                                    const int32_t* __restrict__ plan) {
   constexpr int kSwapPer = swap_per<T>();
   const int cnt = plan[0];
+  if (cnt == 0) return;  // no interchange (the same in every thread)
   const int tid = threadIdx.x;
   int s[kSwapPer], d[kSwapPer];
 #pragma unroll

@@ -104,7 +104,32 @@ np.save(sys.argv[2], np.concatenate([x, [lu.last_info.iterations, lu.last_info.r
 '''
 
 
-def _panel_runs(tmp_path, n_el, kinds):
+# a strongly diagonal matrix with its rows shuffled: partial pivoting
+# interchanges rows at nearly every column (it undoes the shuffle), in every
+# base panel and across block panels, and the system stays well conditioned
+def _shuffled_system(n):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)) + 3.0 * n ** 0.5 * np.eye(n)
+    return A[rng.permutation(n)], rng.standard_normal(n)
+
+
+_RANDOM_RUN = r'''
+import sys
+import numpy as np
+from hfpx3d_b200 import engine
+ctx = engine.Context(0)
+n = int(sys.argv[1])
+rng = np.random.default_rng(n)
+A = rng.standard_normal((n, n)) + 3.0 * n ** 0.5 * np.eye(n)
+A = A[rng.permutation(n)]
+b = rng.standard_normal(n)
+lu = engine.LU(ctx, engine.DeviceMatrix.upload(ctx, A), engine.HFPX_LU_MIXED)
+x = lu.solve(b, tol=1e-12, max_iter=60)
+np.save(sys.argv[2], np.concatenate([x, [lu.last_info.iterations, lu.last_info.residual]]))
+'''
+
+
+def _panel_runs(tmp_path, n_el, kinds, script=_PANEL_RUN):
     import os
     import subprocess
     import sys
@@ -113,7 +138,7 @@ def _panel_runs(tmp_path, n_el, kinds):
     for kind in kinds:
         env = dict(os.environ, HFPX_LU_PANEL=kind, PYTHONPATH=root)
         f = tmp_path / ('x_%s.npy' % (kind or 'default'))
-        r = subprocess.run([sys.executable, '-c', _PANEL_RUN, str(n_el), str(f)], env=env, cwd=root,
+        r = subprocess.run([sys.executable, '-c', script, str(n_el), str(f)], env=env, cwd=root,
                            capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         out[kind] = np.load(f)
@@ -130,6 +155,22 @@ def test_fp32_panel_kernels_agree_bitwise(tmp_path, n_el):
     out = _panel_runs(tmp_path, n_el, ('ll', 'smem'))
     assert np.array_equal(out['ll'], out['smem'])
     assert out['ll'][-1] <= 1e-12
+
+
+def test_fp32_panel_kernels_agree_bitwise_with_interchanges(tmp_path):
+    # 4500 rows: three block panels, rows interchanged at nearly every column,
+    # so the register panel's row moves (and the compacted row-swap plans of
+    # the block steps) carry the factorisation; the shared-memory panel swaps
+    # by plans inside the recursion.  Same pivots, same bits, and the solution
+    # meets the Gaussian system.
+    n = 4500
+    out = _panel_runs(tmp_path, n, ('ll', 'smem'), script=_RANDOM_RUN)
+    assert np.array_equal(out['ll'], out['smem'])
+    A, b = _shuffled_system(n)
+    x = out['ll'][:n]
+    assert out['ll'][-1] <= 1e-12
+    assert np.abs(A @ x - b).max() <= 1e-10 * np.abs(A).max() * np.abs(x).max()
+    assert np.abs(x - np.linalg.solve(A, b)).max() <= 1e-10 * np.abs(x).max()
 
 
 @pytest.mark.parametrize('n_el', [300, 1200, 2500])
