@@ -1381,11 +1381,59 @@ __global__ void identity_kernel(float* a, int n) {
   if (i < n) a[i + (int64_t)n * j] = i == j ? 1.f : 0.f;
 }
 
+// Inverses of the 32 x 32 diagonal blocks of the unit lower L (lda) into X
+// (ld ldx; its strictly upper part and diagonal already hold the identity's):
+// one CTA per block, thread c forward-substitutes column c of the inverse.
+__global__ void __launch_bounds__(kBaseW) unit_lower_diag_inv_kernel(const float* __restrict__ L, int64_t lda,
+                                                                     float* __restrict__ X, int64_t ldx) {
+  __shared__ float s[kBaseW][kBaseW + 1];
+  const int c = threadIdx.x;
+  const int64_t o = (int64_t)blockIdx.x * kBaseW;
+  for (int t = 0; t < kBaseW; ++t) s[c][t] = L[o + c + lda * (o + t)];
+  __syncwarp();
+  float x[kBaseW];
+#pragma unroll
+  for (int i = 0; i < kBaseW; ++i) {
+    float acc = i == c ? 1.f : 0.f;  // rows above c stay 0: every x_t with t < c is 0
+#pragma unroll
+    for (int t = 0; t < i; ++t) acc = fmaf(-s[i][t], x[t], acc);
+    x[i] = acc;
+  }
+#pragma unroll
+  for (int i = 1; i < kBaseW; ++i)
+    if (i > c) X[o + i + ldx * (o + c)] = x[i];
+}
+
+// inv(L11) for a kb x kb unit lower L11 with kb = 32 * 2^k, level by level:
+// the 32 x 32 diagonal blocks, then for b = 32, 64, .. kb / 2 every 2b x 2b
+// diagonal block [L1 0; L2 L3] from its halves' inverses,
+// inv = [inv(L1) 0; -inv(L3) L2 inv(L1) inv(L3)], as two strided-batched
+// GEMMs (the pairs sit at a fixed stride down the diagonal).  Replaces the
+// kb x kb triangular solve on the identity (13 launches at kb = 2048).
+// X holds the identity on entry; T: scratch of kb * kb / 4 floats.
+static bool unit_lower_inverse(Lane l, int kb, const float* L, int64_t lda, float* X, float* T) {
+  const int blocks = kb / kBaseW;
+  if (kb < 2 * kBaseW || kb % kBaseW || (blocks & (blocks - 1))) return false;
+  ++g_launches;
+  unit_lower_diag_inv_kernel<<<blocks, kBaseW, 0, l.s>>>(L, lda, X, kb);
+  const float one = 1.f, zero = 0.f, mone = -1.f;
+  for (int b = kBaseW; b < kb; b *= 2) {
+    const int nbatch = kb / (2 * b);
+    const long long sL = 2LL * b * (lda + 1), sX = 2LL * b * (kb + 1), sT = (long long)b * b;
+    // T = L2 inv(L1), then X21 = -inv(L3) T
+    cublasSgemmStridedBatched(l.h, CUBLAS_OP_N, CUBLAS_OP_N, b, b, b, &one, L + b, (int)lda, sL, X, kb, sX, &zero, T,
+                              b, sT, nbatch);
+    cublasSgemmStridedBatched(l.h, CUBLAS_OP_N, CUBLAS_OP_N, b, b, b, &mone, X + b + (int64_t)b * kb, kb, sX, T, b,
+                              sT, &zero, X + b, kb, sX, nbatch);
+  }
+  return true;
+}
+
 // U12 = L11^-1 A12 for columns [c0, c0 + nc) of the trailing block row (B:
 // its column 0).  FP32: with the inverse of the unit lower L11 (made by the
-// step's first call, with_inverse: a kb x kb triangular solve on the
-// identity), one TF32 GEMM; the triangular solve over the block row is the
-// slow path it replaces.  FP64: triangular solve.
+// step's first call, with_inverse: unit_lower_inverse, or a kb x kb
+// triangular solve on the identity), one TF32 GEMM; the triangular solve over
+// the block row is the slow path it replaces.  FP64: triangular solve.
 template <class T>
 static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t nc, const T* L, int64_t lda, T* B,
                             bool with_inverse) {
@@ -1396,7 +1444,7 @@ static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t n
       if (with_inverse) {
         ++g_launches;
         identity_kernel<<<dim3((kb + 127) / 128, kb), 128, 0, l.s>>>(wk.linv, kb);
-        trsm_llu(l, kb, kb, L, lda, wk.linv, kb);
+        if (!unit_lower_inverse(l, kb, L, lda, wk.linv, wk.a12)) trsm_llu(l, kb, kb, L, lda, wk.linv, kb);
       }
       cudaMemcpy2DAsync(wk.a12, sizeof(T) * kb, B, sizeof(T) * lda, sizeof(T) * kb, nc, cudaMemcpyDeviceToDevice, l.s);
       const float one = 1.f, zero = 0.f;
