@@ -63,7 +63,7 @@ enum : int {
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
-  kScrHostSinf, kScrHostRhs, kScrCount
+  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrCount
 };
 
 // assembly.cu

@@ -997,10 +997,18 @@ __global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int32_t* __rest
   int32_t* hval = hkey + kSwapHash;
   __shared__ int moved;
   const int tid = threadIdx.x;
+  int any = 0;
   for (int i = tid; i < k; i += kSwapThreads) {
     content[i] = i;
     spiv[i] = piv[i] - base;
+    any |= spiv[i] != i;
     if (add) piv[i] += add;
+  }
+  // no interchange at all (the same answer in every thread): an empty plan
+  // without the serial walk below
+  if (!__syncthreads_or(any)) {
+    if (tid == 0) plan[0] = 0;
+    return;
   }
   for (int i = tid; i < kSwapHash; i += kSwapThreads) hkey[i] = -1;
   if (tid == 0) moved = 0;
@@ -1331,6 +1339,9 @@ struct LuWork {
   float* tslu = nullptr;
   // panel_update32_kernel's ticket counter (zero between launches)
   unsigned* pu32_ticket = nullptr;
+  // panel stream's U12 by inverse (panel_u12_by_inverse): inv(L11), the
+  // inverse's scratch and a copy of A12, for a left half of up to nb / 2
+  float* pinv = nullptr;
 };
 
 // Remaining size below which the main stream leaves SMs to the panel stream
@@ -1650,6 +1661,29 @@ __global__ void __launch_bounds__(kPu32Threads) panel_update32_kernel(float* __r
     if (c < w2) A[r + lda * (kBaseW + c)] = acc[c];
 }
 
+// U12 = L11^-1 A12 of a recursion node whose left half is w1 >= 512 wide
+// (FP32, panel stream): inv(L11) by unit_lower_inverse into the panel's own
+// buffer, A12 copied beside it, one TF32 GEMM back into A12.  A cuBLAS
+// triangular solve of that shape is launch- and latency-bound (~140 us at
+// w1 = 1024 on a B200); this is 13 launches of small GEMMs.  Smaller halves
+// keep the triangular solve.  False: not taken.
+constexpr int kPanelInvMin = 512;
+static bool panel_u12_by_inverse(Lane l, LuWork<float>& wk, int w1, int w2, float* A, int64_t lda) {
+  const int blocks = w1 / kBaseW;
+  if (!wk.pinv || w1 < kPanelInvMin || w1 % kBaseW || (blocks & (blocks - 1)) || w2 > w1) return false;
+  float* X = wk.pinv;
+  float* T = X + (size_t)w1 * w1;
+  float* C = T + (size_t)w1 * w1;  // the inverse's scratch needs w1 * w1 / 4
+  ++g_launches;
+  identity_kernel<<<dim3((w1 + 127) / 128, w1), 128, 0, l.s>>>(X, w1);
+  unit_lower_inverse(l, w1, A, lda, X, T);
+  cudaMemcpy2DAsync(C, sizeof(float) * w1, A + lda * w1, sizeof(float) * lda, sizeof(float) * w1, w2,
+                    cudaMemcpyDeviceToDevice, l.s);
+  const float one = 1.f, zero = 0.f;
+  cublasSgemm(l.h, CUBLAS_OP_N, CUBLAS_OP_N, w1, w2, w1, &one, X, w1, C, w1, &zero, A + lda * w1, (int)lda);
+  return true;
+}
+
 // dgetrf2-style recursion on an m x w panel (pivots relative to A's top row).
 // sp.c0: column (and row) offset of this sub-panel inside its block panel of
 // sp.bw columns.  sp.eager: every base panel applies its own interchanges to
@@ -1683,7 +1717,9 @@ static int panel_rec(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int6
     }
   }
   if (!fused) {
-    trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
+    bool solved = false;
+    if constexpr (sizeof(T) == 4) solved = panel_u12_by_inverse(l, wk, w1, w2, A, lda);
+    if (!solved) trsm_llu(l, w1, w2, A, lda, A + lda * w1, lda);
     P.end(2);
     gemm_sub(l, m - w1, w2, w1, A + w1, lda, A + lda * w1, lda, A + w1 + lda * w1, lda);
     P.end(3);
@@ -1758,6 +1794,9 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     wk.linv = (T*)alloc(kScrLinv, sizeof(T) * nb * nb);
     wk.a12 = (T*)alloc(kScrA12, sizeof(T) * nb * (size_t)n);
     if (!wk.linv || !wk.a12) wk.linv = wk.a12 = nullptr;
+    // optional: without it the recursion's wide halves keep the triangular solve
+    const size_t w1max = (nb / 2 + kBaseW - 1) / kBaseW * kBaseW;  // widest left half of a block panel
+    if (wk.linv) wk.pinv = (float*)alloc(kScrPanelInv, sizeof(float) * w1max * w1max * 3);
     // optional too: without them the update stays on TF32
     if (fp16_update_enabled()) {
       wk.l16 = (__half*)alloc(kScrL16, sizeof(__half) * nb * (size_t)n);
