@@ -194,7 +194,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_base_kernel(
 //    p swaps the two labels; the pivot row's data stays where it is and, now
 //    labelled j, takes no further updates.  At the end the rows whose label
 //    is not their slot (<= 2 w of them) move to it with all of the block
-//    panel's columns (ll_finish).
+//    panel's columns (ll_finish; skipped when no column interchanged rows);
+//  * the exchange of column j + 1 overlaps the rest of step j's update (see
+//    panel_ll_kernel).
 // Words of column j sit in buffer j & 1: a CTA can only write column j + 2
 // after all CTAs published column j + 1, i.e. after all finished reading j.
 // Tags are unique within one factorisation and the buffers are zeroed before
@@ -1595,9 +1597,9 @@ static void laswp(Lane l, T* A, int64_t lda, int64_t ncols, int32_t* piv, int k,
 // U12 = L11^-1 A12 (unit lower L11) and A22 -= L21 U12 in one launch, where
 // cuBLAS spends a TRSM launch of ~20 us on the 32 x 32 triangle alone.
 // Every CTA solves U12 (w2 <= 32 columns) in shared memory, the same
-// arithmetic in each, and CTA 0 stores it; then each thread takes one row of
-// A22 through the 32-term update in FP32 (U12 broadcast from shared memory,
-// L21 and A22 read once, coalesced down the columns).  U12 overwrites A12
+// arithmetic in each, and one CTA stores it (below); then each thread takes
+// one row of A22 through the 32-term update in FP32 (U12 broadcast from
+// shared memory, L21 and A22 read once, coalesced down the columns).  U12 overwrites A12
 // in place, so it is stored by the last CTA to have read A12: each CTA takes
 // a ticket once its copy is in shared memory, and the CTA holding the last
 // ticket stores U12 and puts the counter back to 0 for the next launch (the
