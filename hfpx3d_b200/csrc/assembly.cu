@@ -22,10 +22,10 @@
 namespace hfpx {
 
 __constant__ GL12 c_gl;
-static bool g_gl_ready = false;
+static PerDeviceOnce g_gl_ready;
 
 static void gl_host_init(cudaStream_t s) {
-  if (g_gl_ready) return;
+  if (!g_gl_ready.pending()) return;
   GL12 g;
   const int n = 12;
   for (int i = 0; i < n; ++i) {
@@ -45,8 +45,7 @@ static void gl_host_init(cudaStream_t s) {
     g.x[i] = x;
     g.w[i] = 2.0 / ((1.0 - x * x) * dp * dp);
   }
-  cudaMemcpyToSymbolAsync(c_gl, &g, sizeof(g), 0, cudaMemcpyHostToDevice, s);
-  g_gl_ready = true;
+  if (cudaMemcpyToSymbolAsync(c_gl, &g, sizeof(g), 0, cudaMemcpyHostToDevice, s) == cudaSuccess) g_gl_ready.mark();
 }
 
 // ------------------------------------------------------------- bulk copy
@@ -445,12 +444,9 @@ void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, dou
                      int is_dd_local, double* d_a, int64_t ld, int* d_status, cudaStream_t s) {
   gl_host_init(s);
   const size_t smem = sizeof(AsmSmem);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(assemble_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(assemble_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static PerDeviceOnce attr0, attr1;
+  smem_attr_once(attr0, assemble_kernel<false>, (int)smem);
+  smem_attr_once(attr1, assemble_kernel<true>, (int)smem);
   cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
   const dim3 grid((unsigned)((6 * n_el + kTile - 1) / kTile), (unsigned)n_el);
   const ElemRec* e = static_cast<const ElemRec*>(d_elem);

@@ -502,7 +502,7 @@ int64_t hfpx_ctx_launch_count(const hfpx_ctx* c) { return c ? (int64_t)g_launche
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,
                                  int64_t* info) {
   if (!c) return HFPX_ERR_ARG;
-  cudaSetDevice(c->device);
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
   return lu_panel_factor_noalloc(c, d_a, lda, m, w, d_piv, info);
 }
 

@@ -51,6 +51,32 @@ struct hfpx_matrix {
 namespace hfpx {
 // launches of this engine's own kernels in this process (library kernels excluded)
 extern std::atomic<long long> g_launches;
+
+// Per-device set-up flags.  Kernel attributes and __constant__ data belong to
+// one device's context, so "done" is one bit per device, set only after the
+// set-up succeeded on the current device.
+struct PerDeviceOnce {
+  std::atomic<unsigned long long> done{0};
+  // true when the current device still needs the set-up (devices >= 64 always do)
+  bool pending(int* dev_out = nullptr) const {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return true;
+    if (dev_out) *dev_out = dev;
+    return dev >= 64 || !(done.load() & (1ull << dev));
+  }
+  void mark() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev < 64) done.fetch_or(1ull << dev);
+  }
+};
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per device
+template <class F>
+inline cudaError_t smem_attr_once(PerDeviceOnce& once, F* func, int bytes) {
+  if (!once.pending()) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) once.mark();
+  return e;
+}
 int set_error(hfpx_ctx* c, int code, const std::string& msg);
 int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what);
 // Work buffer `slot` of the context with at least `bytes` bytes (null when

@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 #include "engine_internal.h"
 
@@ -1110,9 +1111,12 @@ static inline cublasHandle_t H(hfpx_ctx* c) { return static_cast<cublasHandle_t>
 struct Lane {
   cudaStream_t s;
   cublasHandle_t h;
+  int sms;  // the device's SM count (grid caps)
 };
-static Lane main_lane(hfpx_ctx* c) { return {c->stream, H(c)}; }
-static Lane panel_lane(hfpx_ctx* c) { return {c->stream_panel, static_cast<cublasHandle_t>(c->cublas_panel)}; }
+static Lane main_lane(hfpx_ctx* c) { return {c->stream, H(c), c->num_sms}; }
+static Lane panel_lane(hfpx_ctx* c) {
+  return {c->stream_panel, static_cast<cublasHandle_t>(c->cublas_panel), c->num_sms};
+}
 
 static void trsm_llu(Lane l, int64_t m, int64_t n, const double* L, int64_t ldl, double* B, int64_t ldb) {
   if (m <= 0 || n <= 0) return;
@@ -1189,8 +1193,10 @@ __global__ void to_half_kernel(const float* __restrict__ a, int64_t lda, int64_t
   }
 }
 
-static unsigned grid_for(int64_t tot) {
-  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, 148 * 16));
+// grid of 256-thread CTAs for a grid-stride loop over tot elements: at most
+// 16 resident CTAs per SM
+static unsigned grid_for(const Lane& l, int64_t tot) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, (int64_t)std::max(1, l.sms) * 16));
 }
 
 // C = coef[0] A B + coef[1] C, FP16 A and B, FP32 C, FP32 accumulation.
@@ -1475,7 +1481,7 @@ static void prepare_l21(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L2
   if constexpr (sizeof(T) == 4) {
     if (wk.l16) {
       ++g_launches;
-      to_half_kernel<<<grid_for(rest * kb), 256, 0, l.s>>>(L21, lda, rest, kb, wk.l16, rest, nullptr, nullptr);
+      to_half_kernel<<<grid_for(l, rest * kb), 256, 0, l.s>>>(L21, lda, rest, kb, wk.l16, rest, nullptr, nullptr);
     }
   }
 }
@@ -1489,9 +1495,9 @@ static void prepare_u12(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t nc, c
       U12 += lda * c0;
       cudaMemsetAsync(wk.amax, 0, sizeof(unsigned), l.s);
       ++g_launches;
-      amax_kernel<<<grid_for(nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.amax);
+      amax_kernel<<<grid_for(l, nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.amax);
       ++g_launches;
-      to_half_kernel<<<grid_for(nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.u16 + (size_t)kb * c0, kb, wk.amax,
+      to_half_kernel<<<grid_for(l, nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.u16 + (size_t)kb * c0, kb, wk.amax,
                                                          wk.coef);
     }
   }
@@ -1552,12 +1558,8 @@ static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int
   int rpc = (int)((m + G - 1) / G);
   size_t smem = (size_t)w * rpc * sizeof(T) + kBaseW * sizeof(T);
   if (smem > kPanelSmemCap) return set_error(c, HFPX_ERR_ARG, "panel too tall for shared memory");
-  static bool attr_d = false, attr_f = false;
-  bool& attr = sizeof(T) == 8 ? attr_d : attr_f;
-  if (!attr) {
-    cudaFuncSetAttribute(panel_base_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemCap);
-    attr = true;
-  }
+  static PerDeviceOnce attr;  // one per instantiation of T
+  smem_attr_once(attr, panel_base_kernel<T>, (int)kPanelSmemCap);
   void* args[] = {&A, &lda, &m, &w, &rpc, &piv, &wk.sc, &wk.d_info, &col_offset};
   ++g_launches;
   cudaError_t e =
@@ -1568,18 +1570,15 @@ static int panel_base(hfpx_ctx* c, Lane l, LuWork<T>& wk, T* A, int64_t lda, int
 static void swap_plan(Lane l, int32_t* piv, int k, int base, int32_t* plan, int add = 0) {
   if (k <= 0) return;
   ++g_launches;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(swap_plan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwapPlanSmem);
-    attr = true;
-  }
+  static PerDeviceOnce attr;
+  smem_attr_once(attr, swap_plan_kernel, (int)kSwapPlanSmem);
   swap_plan_kernel<<<1, kSwapThreads, kSwapPlanSmem, l.s>>>(piv, k, base, plan, add);
 }
 
 template <class T>
 static void swap_apply(Lane l, T* A, int64_t lda, int64_t ncols, const int32_t* plan) {
   if (ncols <= 0) return;
-  const int64_t blocks = std::min<int64_t>((ncols + kSwapCols - 1) / kSwapCols, 148 * 8);
+  const int64_t blocks = std::min<int64_t>((ncols + kSwapCols - 1) / kSwapCols, (int64_t)std::max(1, l.sms) * 8);
   ++g_launches;
   swap_apply_kernel<T><<<(unsigned)blocks, kSwapThreads, 0, l.s>>>(A, lda, ncols, plan);
 }
@@ -1854,7 +1853,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     cudaStreamWaitEvent(S, ev_panel, 0);
     if (k > 0) cudaStreamWaitEvent(S, ev_rest, 0);
     const int32_t* plan_k = wk.plans + (size_t)(k / kNb) * kSwapPlanInts;
-    swap_apply(Lane{S, nullptr}, A + k, lda, k, plan_k);
+    swap_apply(Lane{S, nullptr, c->num_sms}, A + k, lda, k, plan_k);
     if (k + kb < n) {
       const int64_t rest = n - k - kb;
       if constexpr (sizeof(T) == 4) {
@@ -2389,15 +2388,15 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
 }
 
 // ------------------------------------------------- allocation-free panel LU
-// For callers that cannot allocate device memory: code running while a CUDA
-// stream is being captured into a graph (cudaMalloc is illegal there), hosts
-// whose device memory belongs to an arena or pool they manage themselves, and
-// embedded or real-time callers that forbid allocation after start-up.  The
-// pivot search scratch of the panel kernel lives in this file-scope array
-// instead of in cudaMalloc'd buffers.  Every GPU that loads the library holds
-// it until the process exits; all calls share it, so calls that overlap on the
-// GPU (other streams, other host threads) race and must be serialised by the
-// caller.
+// For callers that cannot allocate device memory: hosts that hand all of the
+// device's memory to an arena or pool of their own at start-up (a cudaMalloc
+// then fails, or takes memory the arena counts on), and real-time or embedded
+// loops that forbid allocation after start-up (cudaMalloc and cudaFree can
+// synchronise the device and take unbounded time).  The pivot-search scratch
+// of the panel kernel lives in this file-scope array instead of in
+// cudaMalloc'd buffers.  Every GPU that loads the library holds it until the
+// process exits; all calls share it, so calls that overlap on the GPU (other
+// streams, other host threads) race and must be serialised by the caller.
 constexpr int kNoAllocMaxCtas = 256;
 constexpr size_t kNoAllocCand = sizeof(double) * 2 * kNoAllocMaxCtas * kBaseW;
 constexpr size_t kNoAllocCmax = sizeof(double) * 2 * kNoAllocMaxCtas;
@@ -2406,21 +2405,26 @@ constexpr size_t kNoAllocRowj = sizeof(double) * 2 * kBaseW;
 constexpr size_t kNoAllocBytes = kNoAllocCand + kNoAllocCmax + kNoAllocCidx + kNoAllocRowj + sizeof(int64_t);
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of the array, looked up once per device with that device
-// current.  In host code the symbol's name is a host-side stand-in, not a
-// device address, so only the looked-up pointer is passed to kernels.
+// Device address of the array, looked up by the first call on each device
+// with that device current (the caller has made it current).  In host code the
+// symbol's name is a host-side stand-in, not a device address, so only the
+// looked-up pointer is passed to kernels.  The lookup runs under a lock, so
+// first calls from several host threads do not race on the cache.
 static unsigned char* noalloc_scratch(hfpx_ctx* c) {
-  static unsigned char* addr[64] = {nullptr};
-  if (c->device < 0 || c->device >= 64) return nullptr;
-  if (!addr[c->device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
-    if (cudaFuncSetAttribute(panel_base_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
-        cudaSuccess)
-      return nullptr;
-    addr[c->device] = static_cast<unsigned char*>(p);
-  }
-  return addr[c->device];
+  constexpr int kMaxDevices = 64;
+  static std::atomic<unsigned char*> addr[kMaxDevices];
+  static std::mutex lock;
+  if (c->device < 0 || c->device >= kMaxDevices) return nullptr;
+  if (unsigned char* p = addr[c->device].load(std::memory_order_acquire)) return p;
+  std::lock_guard<std::mutex> g(lock);
+  if (unsigned char* p = addr[c->device].load(std::memory_order_relaxed)) return p;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+  if (cudaFuncSetAttribute(panel_base_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+      cudaSuccess)
+    return nullptr;
+  addr[c->device].store(static_cast<unsigned char*>(p), std::memory_order_release);
+  return static_cast<unsigned char*>(p);
 }
 
 int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,

@@ -298,13 +298,10 @@ __global__ void __launch_bounds__(kTb) tri_inverse_kernel(const float* __restric
 int trsv_tiles(int64_t n) { return (int)((n + kTb - 1) / kTb); }
 
 int tri_inverses(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, float* dinv_lower, float* dinv_upper) {
-  static bool attr = false;
+  static PerDeviceOnce attr0, attr1;
   const size_t smem = sizeof(float) * 2 * kTb * (kTb + 1);
-  if (!attr) {
-    cudaFuncSetAttribute(tri_inverse_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(tri_inverse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  smem_attr_once(attr0, tri_inverse_kernel<false>, (int)smem);
+  smem_attr_once(attr1, tri_inverse_kernel<true>, (int)smem);
   const unsigned T = (unsigned)trsv_tiles(n);
   ++g_launches;
   tri_inverse_kernel<false><<<T, kTb, smem, c->stream>>>(A, lda, (int)n, dinv_lower);
@@ -332,12 +329,9 @@ int trsv_f32(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const float* d
     c->trsv_epoch = 0;
   }
   if (++c->trsv_epoch <= 0) c->trsv_epoch = 1;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(trsv_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwSmem);
-    cudaFuncSetAttribute(trsv_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSwSmem);
-    attr = true;
-  }
+  static PerDeviceOnce attr0, attr1;
+  smem_attr_once(attr0, trsv_sweep_kernel<false>, (int)kSwSmem);
+  smem_attr_once(attr1, trsv_sweep_kernel<true>, (int)kSwSmem);
   int nn = (int)n;
   uint32_t ep = (uint32_t)c->trsv_epoch;
   void* args[] = {&A, &lda, &nn, &dinv, &x, &xw, &ep, &err};
@@ -459,7 +453,8 @@ int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const dou
 int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max) {
   cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
   ++g_launches;
-  absmax_kernel<<<(unsigned)std::min<int64_t>(148 * 4, (n + 255) / 256), 256, 0, c->stream>>>(v, (int)n, d_max);
+  absmax_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)c->num_sms * 4, (n + 255) / 256)), 256, 0,
+                  c->stream>>>(v, (int)n, d_max);
   return check_cuda(c, cudaGetLastError(), "absmax launch");
 }
 

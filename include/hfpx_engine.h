@@ -141,8 +141,10 @@ int hfpx_gmres_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, dou
 
 /* Partial-pivoting LU of one tall panel already in device memory, in place,
  * without allocating anything: no counterpart in the reference.  For callers
- * that cannot call cudaMalloc (inside a stream capture, under a
- * caller-managed memory arena, or in allocation-free real-time code).
+ * that cannot call cudaMalloc: hosts whose device memory all belongs to an
+ * arena of their own (an allocation would fail or take memory the arena
+ * counts on), and real-time loops that forbid allocation after start-up
+ * (cudaMalloc can synchronise the device and take unbounded time).
  * d_a: m x w column-major (lda >= m, 1 <= w <= 32, m >= w), overwritten with
  * L (unit lower, below the diagonal) and U; d_piv: w int32 pivot rows
  * (0-based, relative to the panel's first row, applied in order as LAPACK
@@ -151,8 +153,8 @@ int hfpx_gmres_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, dou
  * can hold (about 118000 rows at w = 32 on a B200) are rejected with
  * HFPX_ERR_ARG.  Its pivot-search scratch is one static device array of
  * about 138 KB shared by every call: the first call on a device looks up its
- * address (make that call before any stream capture), and calls that overlap
- * on the GPU race. */
+ * address (make that first call before any stream capture), and calls that
+ * overlap on the GPU race. */
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx *ctx, double *d_a, int64_t lda, int64_t m, int w,
                                  int32_t *d_piv, int64_t *info);
 

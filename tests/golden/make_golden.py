@@ -31,7 +31,9 @@ sys.path.insert(0, os.path.dirname(HERE))
 from oracle_lib import dp, lp, ref  # noqa: E402
 from hfpx3d_b200 import meshgen  # noqa: E402
 
-REF = os.environ.get('HFPX_REFERENCE', '/root/reference')
+REF = os.environ.get('HFPX_REFERENCE', '')
+if not os.path.isdir(REF):
+    sys.exit('set HFPX_REFERENCE to the reference tree')
 G, NU, BETA = 1.0, 0.35, 0.125
 
 

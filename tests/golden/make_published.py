@@ -19,10 +19,13 @@ arrays exactly as shipped (dtype, shape and Fortran order), the solution and the
 stresses; and the observation points (n x 3, as in the csv).
 """
 import os
+import sys
 
 import numpy as np
 
-REF = os.environ.get('HFPX_REFERENCE', '/root/reference')
+REF = os.environ.get('HFPX_REFERENCE', '')
+if not os.path.isdir(REF):
+    sys.exit('set HFPX_REFERENCE to the reference tree')
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 CASES = {'psc_24': 'pennymesh24el', 'psc_121': 'pennymesh121el', 'psc_1025': 'pennymesh1025el',

@@ -1,12 +1,14 @@
 """The allocation-free panel LU (hfpx_lu_panel_factor_noalloc) through the C-ABI.
 
-It is for callers that cannot allocate device memory: code running while a
-stream is captured into a CUDA graph, hosts that hand all device memory to
-their own arena, allocation-free real-time loops.  The caller passes device
-buffers (made here with torch); the entry point itself allocates nothing and
-keeps its pivot-search scratch in one static device array.  Its results are
-checked against the existing entry point (hfpx_lu_factor), within the
-tolerance the other LU tests use, on two calls in a row."""
+It is for callers that cannot allocate device memory: hosts whose device
+memory all belongs to an arena of their own, and real-time loops that forbid
+allocation after start-up (cudaMalloc can synchronise the device and take
+unbounded time).  The caller passes device buffers (made here with torch); the
+entry point itself allocates nothing and keeps its pivot-search scratch in one
+static device array.  Its results are checked against the existing entry
+point (hfpx_lu_factor), within the tolerance the other LU tests use, on two
+calls in a row, and the device's free memory is checked to stay the same
+across warmed-up calls."""
 import ctypes
 
 import numpy as np
@@ -100,3 +102,29 @@ def test_zero_pivot_reported(ctx):
     assert rc == engine.HFPX_ERR_SINGULAR and info == 8
     rc, F, piv, info = factor_noalloc(ctx, np.eye(40, 20))   # scratch reused: info cleared again
     assert rc == engine.HFPX_OK and info == 0
+
+
+def test_allocates_nothing(ctx):
+    import torch
+    from hfpx3d_b200 import engine
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((20000, 32))
+    d = torch.from_numpy(np.ascontiguousarray(A.T)).to('cuda:0')
+    piv = torch.zeros(32, dtype=torch.int32, device='cuda:0')
+    info = ctypes.c_int64(-1)
+    L = engine.lib()
+
+    def call():
+        d.copy_(torch.from_numpy(np.ascontiguousarray(A.T)))
+        torch.cuda.synchronize()
+        rc = L.hfpx_lu_panel_factor_noalloc(ctx.h, ctypes.c_void_p(d.data_ptr()), 20000, 20000, 32,
+                                            ctypes.c_void_p(piv.data_ptr()), ctypes.byref(info))
+        torch.cuda.synchronize()
+        assert rc == engine.HFPX_OK and info.value == 0
+
+    call()                                   # first call on the device: address look-up
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        call()
+    # any cudaMalloc inside the call would take at least one 2 MiB page
+    assert torch.cuda.mem_get_info(0)[0] == free0
