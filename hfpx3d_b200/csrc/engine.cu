@@ -381,6 +381,21 @@ int hfpx_matrix_download(hfpx_ctx* c, const hfpx_matrix* m, double* a, int64_t l
   return rc;
 }
 
+int hfpx_matrix_download_block(hfpx_ctx* c, const hfpx_matrix* m, int64_t i0, int64_t j0, int64_t rows, int64_t cols,
+                               double* a, int64_t ld_host) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !a || rows < 0 || cols < 0 || i0 < 0 || j0 < 0 || i0 + rows > m->n || j0 + cols > m->n ||
+      ld_host < rows)
+    return set_error(c, HFPX_ERR_ARG, "bad block download arguments");
+  if (rows == 0 || cols == 0) return HFPX_OK;
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  int rc = check_cuda(c, cudaMemcpy2DAsync(a, ld_host * sizeof(double), m->d_a + i0 + m->ld * j0, m->ld * sizeof(double),
+                                           rows * sizeof(double), cols, cudaMemcpyDeviceToHost, c->stream),
+                      "block download");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "block download");
+  return rc;
+}
+
 int hfpx_matrix_destroy(hfpx_matrix* m) {
   if (!m) return HFPX_OK;
   if (m->d_a) cudaFree(m->d_a);

@@ -58,6 +58,7 @@ SIGNATURES = {
     'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
     'hfpx_matrix_dims': (_int, [_V, _L, _L]),
     'hfpx_matrix_download': (_int, [_V, _V, _D, _i64]),
+    'hfpx_matrix_download_block': (_int, [_V, _V, _i64, _i64, _i64, _i64, _D, _i64]),
     'hfpx_matrix_destroy': (_int, [_V]),
     'hfpx_rhs_sinf': (_int, [_V, _V, _L, _i64, _D, _i64, _D, _i64]),
     'hfpx_lu_factor': (_int, [_V, _V, _int, _L]),
@@ -216,6 +217,13 @@ class DeviceMatrix:
     def download(self):
         out = np.empty((self.n, self.n), order='F')
         self.ctx.check(lib().hfpx_matrix_download(self.ctx.h, self.h, _dp(out), self.n))
+        return out
+
+    def block(self, i0, j0, rows, cols):
+        """Rows [i0, i0 + rows) x columns [j0, j0 + cols) (column-major numpy)."""
+        out = np.empty((rows, cols), order='F')
+        self.ctx.check(lib().hfpx_matrix_download_block(self.ctx.h, self.h, i0, j0, rows, cols, _dp(out),
+                                                        max(rows, 1)))
         return out
 
     def close(self):

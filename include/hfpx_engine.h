@@ -91,6 +91,12 @@ int hfpx_matrix_upload(hfpx_ctx *ctx, const double *a, int64_t n, int64_t ld_hos
 int hfpx_matrix_dims(const hfpx_matrix *matrix, int64_t *n, int64_t *ld);
 /* Copy the FP64 matrix (or, after an FP64 factorisation, its LU factors) to host. */
 int hfpx_matrix_download(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *a, int64_t ld_host);
+/* Rows [i0, i0 + rows) x columns [j0, j0 + cols) of the same, into a host
+ * block (ld_host >= rows): the reference's do_save_matrix output
+ * (main.cpp:130-145) one block at a time, for matrices larger than host
+ * memory. */
+int hfpx_matrix_download_block(hfpx_ctx *ctx, const hfpx_matrix *matrix, int64_t i0, int64_t j0,
+                               int64_t rows, int64_t cols, double *a, int64_t ld_host);
 int hfpx_matrix_destroy(hfpx_matrix *matrix);
 
 /* ---- right-hand side: add_s_inf_to_3dbem_rhs, system_assembly.cpp:222-274.

@@ -143,7 +143,7 @@ class Oracle:
         lo, hi = rows[0], rows[-1] + 1
         buf = np.zeros((hi - lo, n_dof), order='F')
         # ora_assemble_rows writes at absolute row indices; shift the base pointer
-        base = buf.ctypes.data - lo * 8
+        base = buf.ctypes.data - int(lo) * 8
         self.L.ora_assemble_rows(dp(nods), nods.shape[0], nods.shape[1], lp(conn), conn.shape[0], conn.shape[1],
                                  lp(dof), n_dof, G, nu, beta, int(is_dd_local), t0, t1,
                                  ctypes.cast(base, _D), hi - lo)

@@ -1,0 +1,156 @@
+"""Parity at the two large configurations, against the reference itself
+(fixtures from oracle/_ref by tests/golden/make_configs.py):
+
+* the volume-control 2:1 ellipse of 1025 triangles (18 450 DoF + the pressure
+  unknown; make_3dbem_matrix_vc, src/Solvers/system_assembly.cpp:458-557):
+  the device matrix against the reference's through weighted row and column
+  sums, its volume row and column, diagonal and entry samples; the engine's
+  right-hand side (add_s_inf_to_3dbem_rhs, :222-274, with V = 1) exactly; the
+  FP64 and mixed solutions against the LAPACK solution of the reference's own
+  matrix (the dgesv il::LU calls, il/linear_algebra/dense/factorization/LU.h:87);
+* the 4000-triangle penny of the headline step (72 000 DoF,
+  make_3dbem_matrix_s, :30-219): 198 rows and 198 columns of the device FP64
+  matrix against the reference's, the full blocks of each sampled element
+  with its nearest neighbours, entry samples; the mixed solution's opening
+  against the FP64 GPU solution (<= 1e-8), and both against Sneddon's closed
+  form for r < 0.9 (test_radial_crack_static.cpp:316-337).
+
+Tolerances.  In far pairs whose collocation point lies near the line of one
+of the source element's edges the in-plane closed form cancels, and the
+reference and this engine (which follows its own derivation) both miss the
+exact value there, in different directions: at C2 the reference and the CPU
+oracle (which the engine matches to 1e-11) differ by up to 8.9e-10 of the
+matrix scale in 20 such entries (3.2e-6 of the entry), at C3 by 1.3e-11.
+Hence 2e-9 (C2) and 1e-10 (C3) of the matrix scale for entries and weighted
+sums.  The solutions are insensitive to it: the oracle's matrix and the
+reference's give C2 solutions 4.7e-12 apart."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+G, NU, BETA = 1.0, 0.35, 0.125
+
+
+def mesh_digest(nods, conn):
+    h = hashlib.sha256()
+    h.update(np.ascontiguousarray(nods, dtype=np.float64).tobytes())
+    h.update(np.ascontiguousarray(conn, dtype=np.int64).tobytes())
+    return h.hexdigest()
+
+
+def weights(seed, n, k):
+    return np.random.default_rng(int(seed)).uniform(-1.0, 1.0, (n, k))
+
+
+def rel(a, b, scale):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / scale)
+
+
+def test_c2_vc_ellipse_1025(ctx):
+    from hfpx3d_b200 import engine, meshgen
+    z = golden('ref_c2')
+    nods, conn = meshgen.ellipse(1025, seed=1025)
+    assert mesh_digest(nods, conn) == str(z['mesh_digest']), 'mesh generator changed'
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    assert n == int(z['n_dof']) == 18450
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    rhs = np.concatenate([engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, z['s_inf']), [1.0]])
+    assert np.array_equal(rhs, z['rhs'])
+    A = engine.assemble(ctx, dm, dof, n, G, NU, vc=True)
+    Ah = A.download()
+    scale = np.abs(Ah).max()
+    w = weights(z['w_seed'], n + 1, 1)[:, 0]
+    errs = dict(Aw=rel(Ah @ w, z['Aw'], z['abs_Aw'].max()),
+                wA=rel(w @ Ah, z['wA'], (np.abs(w) @ np.abs(Ah)).max()),
+                samples=rel(Ah[z['sample_i'], z['sample_j']], z['sample_v'], scale),
+                diag=rel(np.diag(Ah), z['diag'], scale),
+                vc_row=rel(Ah[n], z['vc_row'], np.abs(z['vc_row']).max()))
+    print('C2 matrix vs reference:', {k: f'{v:.1e}' for k, v in errs.items()})
+    assert errs['Aw'] <= 2e-9 and errs['wA'] <= 2e-9 and errs['samples'] <= 2e-9
+    assert errs['diag'] <= 1e-13 and errs['vc_row'] <= 1e-13
+    assert np.array_equal(Ah[:, n], z['vc_col'])
+    assert Ah[n, n] == 0.0
+    del Ah
+    x_ref = z['x']
+    xs = {}
+    for mode, tol in ((engine.HFPX_LU_MIXED, 1e-9), (engine.HFPX_LU_FP64, 1e-10)):
+        lu = engine.LU(ctx, A, mode)
+        xs[mode] = lu.solve(rhs, tol=1e-13)
+        e = rel(xs[mode], x_ref, np.abs(x_ref).max())
+        print(f'C2 solution mode {mode} vs LAPACK on the reference matrix: {e:.1e}')
+        assert e <= tol
+    # the volume row holds the injected volume
+    assert abs(z['vc_row'][:n] @ xs[engine.HFPX_LU_FP64][:n] - 1.0) < 1e-10
+
+
+@pytest.fixture(scope='module')
+def c3(ctx):
+    from hfpx3d_b200 import engine, meshgen
+    z = golden('ref_c3')
+    nods, conn = meshgen.penny(4000, seed=2026)
+    assert mesh_digest(nods, conn) == str(z['mesh_digest']), 'mesh generator changed'
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    assert n == int(z['n_dof']) == 72000
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    A = engine.assemble(ctx, dm, dof, n, G, NU)
+    yield dict(z=z, nods=nods, conn=conn, mesh=mesh, dof=dof, n=n, dm=dm, A=A)
+    A.close()
+    dm.close()
+
+
+def test_c3_matrix_rows_and_columns(c3):
+    z, A, n = c3['z'], c3['A'], c3['n']
+    W = weights(z['w_seed'], n, 3)
+    T = z['elems']
+    rows = np.concatenate([A.block(18 * int(t), 0, 18, n) for t in T])          # 198 x n
+    cols = np.concatenate([A.block(0, 18 * int(t), n, 18) for t in T], axis=1)  # n x 198
+    scale = max(np.abs(rows).max(), np.abs(cols).max())
+    errs = dict(rows=float((np.abs(rows @ W - z['row_w']) / z['row_abs']).max()),
+                cols=float((np.abs(W.T @ cols - z['col_w']) / z['col_abs']).max()),
+                row_samples=rel(rows[z['row_si'], z['row_sj']], z['row_sv'], scale),
+                col_samples=rel(cols[z['col_si'], z['col_sj']], z['col_sv'], scale))
+    near = np.stack([np.stack([rows[18 * i:18 * i + 18, 18 * s:18 * s + 18] for s in z['near'][i]])
+                     for i in range(len(T))])
+    errs['near_blocks'] = rel(near, z['near_blocks'], np.abs(z['near_blocks']).max())
+    print('C3 matrix vs reference:', {k: f'{v:.1e}' for k, v in errs.items()})
+    assert errs['rows'] <= 1e-10 and errs['cols'] <= 1e-10
+    assert errs['row_samples'] <= 1e-10 and errs['col_samples'] <= 1e-10
+    assert errs['near_blocks'] <= 1e-11
+
+
+def test_c3_mixed_vs_fp64_and_sneddon(c3, ora):
+    from hfpx3d_b200 import engine
+    A, n, dof, dm, nods, conn = c3['A'], c3['n'], c3['dof'], c3['dm'], c3['nods'], c3['conn']
+    ne = conn.shape[1]
+    rhs = engine.add_s_inf_to_3dbem_rhs(ctx_of(A), dm, dof, n, [0, 0, 1.0, 0, 0, 0])
+    x_mixed = engine.LU(ctx_of(A), A, engine.HFPX_LU_MIXED).gmres(rhs, tol=1e-12)
+    x_fp64 = engine.LU(ctx_of(A), A, engine.HFPX_LU_FP64).solve(rhs)       # factors A in place: last
+    dd_m = engine.write_dd_vector_to_md(x_mixed, dof, ne)
+    dd_f = engine.write_dd_vector_to_md(x_fp64, dof, ne)
+    open_err = rel(dd_m[:, 2], dd_f[:, 2], np.abs(dd_f[:, 2]).max())
+    # Sneddon's opening at every node with r < 0.9 (pressure 1, unit radius)
+    xs, ws_m, ws_f = [], [], []
+    for e in range(ne):
+        v = nods[:3, conn[:3, e]]
+        nodes = list(v.T) + [0.5 * (v[:, (a + 1) % 3] + v[:, (a + 2) % 3]) for a in range(3)]
+        for k, x in enumerate(nodes):
+            if np.hypot(x[0], x[1]) < 0.9:
+                xs.append(ora.sneddon_dd(G, NU, 1.0, 1.0, x)[2])
+                ws_m.append(dd_m[6 * e + k, 2])
+                ws_f.append(dd_f[6 * e + k, 2])
+    xs = np.array(xs)
+    sn_m = rel(ws_m, xs, np.abs(xs).max())
+    sn_f = rel(ws_f, xs, np.abs(xs).max())
+    print(f'C3 opening: mixed vs FP64 {open_err:.1e}; vs Sneddon (r < 0.9) mixed {sn_m:.1e}, FP64 {sn_f:.1e}')
+    assert open_err <= 1e-8
+    assert sn_m <= 1e-2 and sn_f <= 1e-2
+
+
+def ctx_of(matrix):
+    return matrix.ctx
