@@ -2,6 +2,7 @@
 // host<->device copies around the kernels of assembly.cu and lu.cu.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -509,6 +510,25 @@ int hfpx_gmres(hfpx_ctx* c, const hfpx_matrix* m, double* b, double tol, int res
     if (!rc2) rc2 = check_cuda(c, cudaStreamSynchronize(c->stream), "x");
     if (rc2) rc = rc2;
   }
+  return rc;
+}
+
+int hfpx_gemm_f16_update(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const void* d_a, int64_t lda_k, const void* d_b,
+                         int64_t ldb_k, float* d_c, int64_t ldc, const float* d_alpha) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!d_a || !d_b || !d_c || !d_alpha || m < 0 || n < 0 || k < 0 || lda_k < k || ldb_k < k || ldc < std::max<int64_t>(m, 1))
+    return set_error(c, HFPX_ERR_ARG, "bad update arguments");
+  if (!tc_update_supported(lda_k, ldb_k, d_a, d_b))
+    return set_error(c, HFPX_ERR_ARG, "update operands need 16-byte aligned bases and row strides (multiples of 8)");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
+  if (!err) return set_error(c, HFPX_ERR_NOMEM, "update status word");
+  int rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "update status");
+  if (!rc) rc = tc_update_f16(c, c->stream, m, n, k, d_a, lda_k, d_b, ldb_k, d_c, ldc, d_alpha, err, 0);
+  int h_err = 0;
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "update status");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "tensor-core update");
+  if (!rc && h_err) rc = set_error(c, HFPX_ERR_CUDA, "tensor-core update: a pipeline wait timed out");
   return rc;
 }
 

@@ -89,7 +89,7 @@ enum : int {
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
-  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrCount
+  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrCount
 };
 
 // assembly.cu
@@ -127,6 +127,14 @@ int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, in
                             int64_t* info);
 int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
                 hfpx_solve_info* info);
+
+// gemm_tc.cu: C (m x n FP32, column-major, ldc) += alpha A B^T on tcgen05
+// tensor cores, A (m x k) and B (n x k) FP16 K-major with row strides lda_k,
+// ldb_k (multiples of 8), alpha = *d_alpha; d_err a zeroed failure word
+// (set when a pipeline wait times out); at most max_ctas CTAs (<= 0: all SMs).
+bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void* B);
+int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
+                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, int* d_err, int max_ctas);
 
 // solve.cu: one right-hand side of the refinement
 int trsv_tiles(int64_t n);

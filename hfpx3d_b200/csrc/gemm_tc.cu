@@ -1,0 +1,389 @@
+// Trailing update of the mixed LU on the 5th-generation tensor cores:
+//
+//     C (m x n, FP32, column-major, ldc)  +=  alpha * A B^T
+//     A: m x k FP16, K-major (row i at A + i * lda_k),
+//     B: n x k FP16, K-major (column j of the k x n factor at B + j * ldb_k),
+//     alpha read from device memory (the power-of-two scale of the FP16 copy
+//     of U12, with its sign).
+//
+// This is the O(N^3) contraction of the factorisation: LAPACK dgetrf's
+// trailing update A22 -= L21 U12, the step il::LU reaches through
+// LAPACKE_dgetrf (il/linear_algebra/dense/factorization/LU.h:87).
+//
+// Design (one CTA per SM, persistent over 128 x 256 output tiles):
+//   * warp 0, one lane: TMA producer.  Each k-block of 64 brings a 128 x 64
+//     tile of A and a 256 x 64 tile of B into shared memory with
+//     cp.async.bulk.tensor (128-byte swizzle, plain loads of this GPU's own
+//     memory), four stages on full/empty mbarriers;
+//   * warp 1: allocates 512 TMEM columns (two 128 x 256 FP32 accumulators);
+//     one lane issues tcgen05.mma kind::f16 (M 128, N 256, K 16; four per
+//     k-block) and tcgen05.commit to release stages and publish finished
+//     accumulators;
+//   * warps 2..9: epilogue.  Warp w reads TMEM lanes 32 (w % 4) .. + 31 (one
+//     output row per thread) and half of the 256 columns with tcgen05.ld, and
+//     applies C += alpha acc with coalesced 128-byte column segments.  The
+//     second accumulator lets the next tile's MMAs run during the epilogue.
+// Every wait is bounded (%globaltimer); a wait that runs out sets the
+// failure word and an abort flag, every role leaves its loop, outstanding
+// copies and MMAs are waited for (bounded), TMEM is freed and the kernel
+// returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+#include "engine_internal.h"
+
+namespace hfpx {
+namespace {
+
+constexpr int kBM = 128, kBN = 256, kBK = 64, kStages = 4;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr uint32_t kStageA = kBM * kBK * 2;   // 16 KB
+constexpr uint32_t kStageB = kBN * kBK * 2;   // 32 KB
+constexpr uint32_t kTmemCols = 2 * kBN;       // two accumulators
+constexpr int kGroupM = 16;                   // tile raster: 16 row blocks per group
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
+
+struct alignas(1024) TcSmem {
+  uint8_t a[kStages][kStageA];
+  uint8_t b[kStages][kStageB];
+  uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], drain;
+  uint32_t tmem_base;
+  int abort;
+};
+constexpr size_t kSmemBytes = sizeof(TcSmem) + 1024;  // + alignment slack of the dynamic base
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of `parity` to complete, at most kWaitNs; on time-out
+// (or when another role has aborted) set the abort flag and the failure
+// word and return false.
+__device__ __forceinline__ bool wait_phase(uint64_t* b, uint32_t parity, volatile int* abort, int* err, int code) {
+  if (mbar_try_wait(b, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait(b, parity)) return true;
+    if ((it & 63) == 0) {
+      if (*abort) return false;
+      if (now_ns() - t0 > kWaitNs) {
+        *abort = 1;
+        atomicExch(err, code);
+        return false;
+      }
+    }
+  }
+}
+// after an abort: wait for a phase that an operation already in flight (a
+// copy or an MMA) will complete, bounded, without looking at the flag
+__device__ __forceinline__ void drain_phase(uint64_t* b, uint32_t parity) {
+  const unsigned long long t0 = now_ns();
+  while (!mbar_try_wait(b, parity))
+    if (now_ns() - t0 > kWaitNs) return;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major operand tile in shared memory with the 128-byte swizzle: rows of
+// 64 FP16 (128 bytes), 8-row atoms of 1024 bytes one after another (stride
+// byte offset 1024), leading byte offset unused for swizzled K-major (1),
+// descriptor version 1, layout 2 = 128-byte swizzle.  Advancing K by 16
+// elements inside the atom adds 32 bytes to the start address.
+__device__ __forceinline__ uint64_t smem_desc(const void* tile, int k16) {
+  const uint32_t addr = smem_u32(tile) + 32u * (uint32_t)k16;
+  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;                 // leading byte offset (16 B units)
+  d |= (uint64_t)(1024u >> 4) << 32;       // stride byte offset
+  d |= (uint64_t)1u << 46;                 // version (sm_100)
+  d |= (uint64_t)2u << 61;                 // 128-byte swizzle
+  return d;
+}
+// kind::f16 instruction descriptor: D FP32 (bits 4-5 = 1), A and B FP16
+// (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
+// M >> 4 at bit 24.
+constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+struct TileMap {
+  int64_t tiles_m, tiles_n;
+  __device__ void coords(int64_t t, int64_t& mb, int64_t& nb) const {
+    const int64_t per_group = (int64_t)kGroupM * tiles_n;
+    const int64_t g = t / per_group, r = t - g * per_group;
+    const int64_t gm = min((int64_t)kGroupM, tiles_m - g * kGroupM);
+    mb = g * kGroupM + r % gm;
+    nb = r / gm;
+  }
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+    update_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     float* __restrict__ C, int64_t ldc, int64_t m, int64_t n, int k, const float* __restrict__ d_alpha,
+                     int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const TileMap tm{(m + kBM - 1) / kBM, (n + kBN - 1) / kBN};
+  const int64_t tiles = tm.tiles_m * tm.tiles_n;
+  const int nk = (k + kBK - 1) / kBK;
+  volatile int* abort = &s.abort;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&s.full[i], 1);
+      mbar_init(&s.empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&s.tfull[i], 1);
+      mbar_init(&s.tempty[i], kEpiWarps);
+    }
+    mbar_init(&s.drain, 1);
+    s.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem_base;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t armed = 0, armed_par = 0;  // stages with a copy in flight, and its phase
+      for (int64_t t = blockIdx.x; t < tiles && !*abort; t += gridDim.x) {
+        int64_t mb, nb;
+        tm.coords(t, mb, nb);
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.empty[stage], phase ^ 1u, abort, err, 0x101)) break;
+          armed &= ~(1u << stage);
+          mbar_expect_tx(&s.full[stage], kStageA + kStageB);
+          tma_load_2d(s.a[stage], &map_a, &s.full[stage], kb * kBK, (int)(mb * kBM));
+          tma_load_2d(s.b[stage], &map_b, &s.full[stage], kb * kBK, (int)(nb * kBN));
+          armed |= 1u << stage;
+          armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (*abort)  // copies still in flight must land before the CTA exits
+        for (int i = 0; i < kStages; ++i)
+          if (armed & (1u << i)) drain_phase(&s.full[i], (armed_par >> i) & 1u);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ----------------------------------------------------------------- MMA
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      bool issued = false;
+      for (int64_t t = blockIdx.x; t < tiles && !*abort; t += gridDim.x, ++it) {
+        const int acc = it & 1;
+        const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+        if (!wait_phase(&s.tempty[acc], acc_phase ^ 1u, abort, err, 0x102)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * kBN);
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.full[stage], phase, abort, err, 0x103)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int k16 = 0; k16 < kBK / 16; ++k16)
+            mma_f16(d, smem_desc(s.a[stage], k16), smem_desc(s.b[stage], k16), (kb | k16) != 0);
+          issued = true;
+          mma_commit(&s.empty[stage]);
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&s.tfull[acc]);
+      }
+      if (*abort && issued) {  // MMAs still in flight must finish before TMEM is freed
+        mma_commit(&s.drain);
+        drain_phase(&s.drain, 0);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;                 // TMEM lane quarter this warp may read
+    const int half = (warp - 2) >> 2;       // columns [128 half, 128 half + 128)
+    const float alpha = *d_alpha;
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int acc = it & 1;
+      const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+      bool ok = wait_phase(&s.tfull[acc], acc_phase, abort, err, 0x104);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      int64_t mb, nb;
+      tm.coords(t, mb, nb);
+      const int64_t row = mb * kBM + q * 32 + lane;
+      const bool row_ok = row < m;
+      const int64_t col0 = nb * kBN + half * 128;
+#pragma unroll 1
+      for (int ch = 0; ch < 4; ++ch) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
+        const int64_t cb = col0 + ch * 32;
+        // columns of this chunk inside the matrix (0 for rows below it)
+        const int ncol = row_ok ? (int)min((int64_t)32, max((int64_t)0, n - cb)) : 0;
+        float* p = C + row + ldc * cb;
+        // two groups of 16 column segments in flight
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float c[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(p + ldc * (16 * h + j)) : 0.f;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (16 * h + j < ncol) __stcg(p + ldc * (16 * h + j), fmaf(alpha, v[16 * h + j], c[j]));
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s.tempty[acc]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// rows x k FP16, K-major with ld elements between rows; box = box_rows x 64
+bool make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t k, int64_t ld, uint32_t box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void* B) {
+  // TMA: 16-byte aligned bases and row strides
+  return lda_k % 8 == 0 && ldb_k % 8 == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 &&
+         (reinterpret_cast<uintptr_t>(B) & 15) == 0 && encode_fn() != nullptr;
+}
+
+int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
+                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, int* d_err, int max_ctas) {
+  if (m <= 0 || n <= 0 || k <= 0) return HFPX_OK;
+  if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || !tc_update_supported(lda_k, ldb_k, A, B))
+    return set_error(c, HFPX_ERR_ARG, "tensor-core update: unsupported operand layout");
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, A, m, k, lda_k, kBM) || !make_map(&mb, B, n, k, ldb_k, kBN))
+    return set_error(c, HFPX_ERR_CUDA, "tensor-core update: tensor map encoding failed");
+  static PerDeviceOnce attr;
+  if (int rc = check_cuda(c, smem_attr_once(attr, update_tc_kernel, (int)kSmemBytes), "tensor-core update attribute"))
+    return rc;
+  const int64_t tiles = ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+  const int cap = max_ctas > 0 ? std::min(max_ctas, c->num_sms) : c->num_sms;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
+  ++g_launches;
+  update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, C, ldc, m, n, (int)k, d_alpha, d_err);
+  return check_cuda(c, cudaGetLastError(), "tensor-core update launch");
+}
+
+}  // namespace hfpx

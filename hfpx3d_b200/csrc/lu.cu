@@ -1199,14 +1199,52 @@ static unsigned grid_for(const Lane& l, int64_t tot) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, (int64_t)std::max(1, l.sms) * 16));
 }
 
-// C = coef[0] A B + coef[1] C, FP16 A and B, FP32 C, FP32 accumulation.
-static void gemm16(Lane l, int64_t m, int64_t n, int64_t k, const __half* A, int64_t lda, const __half* B,
-                   int64_t ldb, float* C, int64_t ldc, const float* d_coef) {
+// C = coef[0] A B^T + coef[1] C with A (m x k) and B (n x k) FP16, both
+// K-major (ld elements between rows), FP32 C, FP32 accumulation: the cuBLAS
+// comparison arm of the engine's own tensor-core update (gemm_tc.cu).
+static void gemm16_cublas(Lane l, int64_t m, int64_t n, int64_t k, const __half* A, int64_t lda, const __half* B,
+                          int64_t ldb, float* C, int64_t ldc, const float* d_coef) {
   if (m <= 0 || n <= 0 || k <= 0) return;
   cublasSetPointerMode(l.h, CUBLAS_POINTER_MODE_DEVICE);
-  cublasGemmEx(l.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)m, (int)n, (int)k, d_coef, A, CUDA_R_16F, (int)lda, B, CUDA_R_16F,
+  cublasGemmEx(l.h, CUBLAS_OP_T, CUBLAS_OP_N, (int)m, (int)n, (int)k, d_coef, A, CUDA_R_16F, (int)lda, B, CUDA_R_16F,
                (int)ldb, d_coef + 1, C, CUDA_R_32F, (int)ldc, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
   cublasSetPointerMode(l.h, CUBLAS_POINTER_MODE_HOST);
+}
+
+// HFPX_LU_GEMM=cublas runs the FP16 trailing update through cuBLAS instead of
+// the engine's tcgen05 kernel (for comparison).
+static bool own_update_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_LU_GEMM");
+    return !(e && std::string(e) == "cublas");
+  }();
+  return on;
+}
+
+// K stride of the FP16 operands: kb rounded up to 8 elements (16 bytes, the
+// row-stride granule of the tensor copies)
+static inline int64_t ld16(int kb) { return ((int64_t)kb + 7) / 8 * 8; }
+
+// l16 (rows x ldk, K-major FP16) = L21 (rows x cols, column-major FP32, lda),
+// transposed through a 32 x 33 shared tile so that the reads (down the
+// columns) and the writes (along the rows) are both coalesced.
+__global__ void __launch_bounds__(256) to_half_rows_kernel(const float* __restrict__ a, int64_t lda, int64_t rows,
+                                                           int cols, __half* __restrict__ h, int64_t ldk) {
+  __shared__ float t[32][33];
+  const int64_t r0 = (int64_t)blockIdx.x * 32;
+  const int c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t r = r0 + tx;
+    const int cc = c0 + i;
+    t[i][tx] = (r < rows && cc < cols) ? a[r + lda * cc] : 0.f;
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t r = r0 + i;
+    const int cc = c0 + tx;
+    if (r < rows && cc < cols) h[r * ldk + cc] = __float2half_rn(t[tx][i]);
+  }
 }
 
 // HFPX_LU_UPDATE=tf32 keeps the trailing update on TF32 tensor cores.
@@ -1337,10 +1375,15 @@ struct LuWork {
   int32_t* plans = nullptr;
   // FP32 with the FP16 trailing update: L21 (rest x nb) and scaled U12
   // (nb x rest) in FP16, U12's largest magnitude and the update's alpha/beta
+  // (layouts: l16 rest x ld16(kb) K-major, u16 ld16(kb) x n column-major)
   __half* l16 = nullptr;
   __half* u16 = nullptr;
   unsigned* amax = nullptr;
   float* coef = nullptr;
+  // the tensor-core update's failure word, and its CTA cap (the SMs the
+  // main stream may take at this step)
+  int* tc_err = nullptr;
+  int gemm_ctas = 0;
   // moved rows of one base panel across the block panel: [2 kBaseW][nb]
   float* xtmp = nullptr;
   // tournament candidates: [kTsluMaxCtas][kBaseW][kBaseW] rows, then labels
@@ -1475,13 +1518,14 @@ static void block_row_solve(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t n
 }
 
 // Trailing update of step k (FP32 with the FP16 update): the FP16 copy of
-// L21 (rest x kb), once per step ...
+// L21 (rest x kb, K-major), once per step ...
 template <class T>
 static void prepare_l21(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L21, int64_t lda) {
   if constexpr (sizeof(T) == 4) {
-    if (wk.l16) {
+    if (wk.l16 && rest > 0) {
       ++g_launches;
-      to_half_kernel<<<grid_for(l, rest * kb), 256, 0, l.s>>>(L21, lda, rest, kb, wk.l16, rest, nullptr, nullptr);
+      to_half_rows_kernel<<<dim3((unsigned)((rest + 31) / 32), (unsigned)((kb + 31) / 32)), 256, 0, l.s>>>(
+          L21, lda, rest, kb, wk.l16, ld16(kb));
     }
   }
 }
@@ -1497,22 +1541,27 @@ static void prepare_u12(Lane l, LuWork<T>& wk, int kb, int64_t c0, int64_t nc, c
       ++g_launches;
       amax_kernel<<<grid_for(l, nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.amax);
       ++g_launches;
-      to_half_kernel<<<grid_for(l, nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.u16 + (size_t)kb * c0, kb, wk.amax,
-                                                         wk.coef);
+      to_half_kernel<<<grid_for(l, nc * kb), 256, 0, l.s>>>(U12, lda, kb, nc, wk.u16 + (size_t)ld16(kb) * c0, ld16(kb),
+                                                            wk.amax, wk.coef);
     }
   }
 }
 
 template <class T>
-static void update_gemm(Lane l, LuWork<T>& wk, int kb, int64_t rest, int64_t c0, int64_t nc, const T* L21,
-                        const T* U12, T* C, int64_t lda) {
+static int update_gemm(hfpx_ctx* c, Lane l, LuWork<T>& wk, int kb, int64_t rest, int64_t c0, int64_t nc, const T* L21,
+                       const T* U12, T* C, int64_t lda) {
   if constexpr (sizeof(T) == 4) {
     if (wk.l16) {
-      gemm16(l, rest, nc, kb, wk.l16, rest, wk.u16 + (size_t)kb * c0, kb, C, lda, wk.coef);
-      return;
+      const int64_t k16 = ld16(kb);
+      const __half* B = wk.u16 + (size_t)k16 * c0;
+      if (own_update_enabled() && wk.tc_err)
+        return tc_update_f16(c, l.s, rest, nc, kb, wk.l16, k16, B, k16, C, lda, wk.coef, wk.tc_err, wk.gemm_ctas);
+      gemm16_cublas(l, rest, nc, kb, wk.l16, k16, B, k16, C, lda, wk.coef);
+      return 0;
     }
   }
   gemm_sub(l, rest, nc, kb, L21, lda, U12 + lda * c0, lda, C, lda);
+  return 0;
 }
 
 // CTAs for a panel of m rows: enough for the panel to fit in shared memory,
@@ -1804,6 +1853,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       wk.u16 = (__half*)alloc(kScrU16, sizeof(__half) * nb * (size_t)n);
       wk.amax = (unsigned*)alloc(kScrAmax, sizeof(unsigned));
       wk.coef = (float*)alloc(kScrCoef, 2 * sizeof(float));
+      wk.tc_err = (int*)alloc(kScrTcErr, sizeof(int));
       if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) wk.l16 = wk.u16 = nullptr;
     }
   }
@@ -1815,6 +1865,8 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
     cudaMemsetAsync(wk.ll_slots, 0, ll_bytes, c->stream);
     cudaMemsetAsync(wk.ll_err, 0, sizeof(int), c->stream);
   }
+  if (!rc && wk.tc_err) cudaMemsetAsync(wk.tc_err, 0, sizeof(int), c->stream);
+  wk.gemm_ctas = c->num_sms;
   const Lane M = main_lane(c), Pn = panel_lane(c);
   const cudaStream_t S = c->stream_left;
   const int kNb = lu_block_size(sizeof(T) == 4);
@@ -1863,6 +1915,7 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
         // panel (<= 47 CTAs, one per SM) never waits for SMs.
         const int target = rest < lu_cap_rest() ? std::max(1, c->num_sms - kPanelCtas) : 0;
         cublasSetSmCountTarget(M.h, target);
+        wk.gemm_ctas = target ? target : c->num_sms;
       }
       const int kn = (int)std::min<int64_t>(kNb, rest);
       // first everything the next panel needs: the next block column's
@@ -1874,7 +1927,8 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       P.end(2);
       prepare_l21(M, wk, kb, rest, Akk + kb, lda);
       prepare_u12(M, wk, kb, 0, kn, Akk + lda * kb, lda);
-      update_gemm(M, wk, kb, rest, 0, kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * kb, lda);
+      rc = update_gemm(c, M, wk, kb, rest, 0, kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * kb, lda);
+      if (rc) break;
       P.end(3);
       cudaEventRecord(ev_next, M.s);
       if (ts) cudaEventRecord(ts->p_idle, Pn.s);
@@ -1891,7 +1945,8 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       block_row_solve(M, wk, kb, kn, rest - kn, Akk, lda, Akk + lda * kb, false);
       P.end(2);
       prepare_u12(M, wk, kb, kn, rest - kn, Akk + lda * kb, lda);
-      update_gemm(M, wk, kb, rest, kn, rest - kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * (kb + kn), lda);
+      rc = update_gemm(c, M, wk, kb, rest, kn, rest - kn, Akk + kb, Akk + lda * kb, Akk + kb + lda * (kb + kn), lda);
+      if (rc) break;
       P.end(3);
       cudaEventRecord(ev_rest, M.s);
       if (ts) cudaEventRecord(ts->m_done, M.s);
@@ -1910,17 +1965,21 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
   }
   P.report(sizeof(T) == 8 ? "LU fp64" : "LU fp32");
   int64_t info = 0;
-  int ll_err = 0;
+  int ll_err = 0, tc_err = 0;
   if (!rc) {
     rc = check_cuda(c, cudaMemcpyAsync(&info, wk.d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, M.s), "info");
     if (!rc && wk.ll_err)
       rc = check_cuda(c, cudaMemcpyAsync(&ll_err, wk.ll_err, sizeof(int), cudaMemcpyDeviceToHost, M.s), "panel status");
+    if (!rc && wk.tc_err)
+      rc = check_cuda(c, cudaMemcpyAsync(&tc_err, wk.tc_err, sizeof(int), cudaMemcpyDeviceToHost, M.s), "update status");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(M.s), "LU factorisation");
   }
   cudaStreamSynchronize(Pn.s);
   cudaStreamSynchronize(S);
   timeline().report();
   if (!rc && ll_err) rc = set_error(c, HFPX_ERR_CUDA, "panel pivot exchange timed out");
+  if (!rc && tc_err)
+    rc = set_error(c, HFPX_ERR_CUDA, "tensor-core update: a pipeline wait timed out (code " + std::to_string(tc_err) + ")");
   for (cudaEvent_t e : {ev_panel, ev_next, ev_rest, ev_left, ev_start})
     if (e) cudaEventDestroy(e);
   *info_out = info;

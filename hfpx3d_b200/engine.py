@@ -67,6 +67,7 @@ SIGNATURES = {
     'hfpx_gmres': (_int, [_V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres_device': (_int, [_V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
+    'hfpx_gemm_f16_update': (_int, [_V, _i64, _i64, _i64, _V, _i64, _V, _i64, _V, _i64, _V]),
     'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
     'hfpx_stress_batch': (_int, [_V, _V, _f64, _f64, _int, _D, _i64, _D, _i64, _D, _D]),

@@ -164,6 +164,17 @@ int hfpx_gmres_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, dou
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx *ctx, double *d_a, int64_t lda, int64_t m, int w,
                                  int32_t *d_piv, int64_t *info);
 
+/* The trailing-update contraction of hfpx_lu_factor's mixed mode on device
+ * buffers: C += alpha A B^T, the GEMM inside LAPACK dgetrf's blocked loop
+ * (A22 -= L21 U12) that il::LU reaches at
+ * il/linear_algebra/dense/factorization/LU.h:87.  Runs on the engine's own
+ * tcgen05 tensor-core kernel: A (m x k) and B (n x k) FP16, each K-major
+ * (lda_k, ldb_k >= k elements between rows, multiples of 8, 16-byte aligned
+ * bases), C (m x n) FP32 column-major (ldc >= m), FP32 accumulation, alpha
+ * read from device memory (d_alpha).  Synchronises the context's stream. */
+int hfpx_gemm_f16_update(hfpx_ctx *ctx, int64_t m, int64_t n, int64_t k, const void *d_a, int64_t lda_k,
+                         const void *d_b, int64_t ldb_k, float *d_c, int64_t ldc, const float *d_alpha);
+
 /* Number of this engine's own kernels launched on the context so far
  * (library kernels such as cuBLAS are not counted). */
 int64_t hfpx_ctx_launch_count(const hfpx_ctx *ctx);
