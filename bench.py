@@ -213,6 +213,9 @@ def run_engine(args, rank, world, local_rank):
         opening = lambda x: x[2::3]   # global z components of the nodal DD (tip free: 18 per element)
         rel_err = float(np.abs(opening(xm) - opening(x64)).max() / np.abs(opening(x64)).max())
 
+    # the 1025-element volume-control ellipse, measured on the engine as well
+    c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
+
     if rank != 0:
         return None
     hbm, tensor_peak, peak_src = peaks()
@@ -256,8 +259,57 @@ def run_engine(args, rank, world, local_rank):
         line['speedup_vs_plain_fp64'] = (other_s / (ms / 1e3)) if mode == engine.HFPX_LU_MIXED else None
         line['opening_rel_err_mixed_vs_fp64'] = rel_err
     if args.cpu_baseline:
-        line['cpu_baseline'] = cpu_baseline(args)
+        cb = cpu_baseline(args)
+        x_ref = cb.pop('_c2_x', None)
+        line['cpu_baseline'] = cb
+        if c2 is not None and cb['measured_c2']:
+            c2['reference_cpu_s'] = cb['measured_c2']['value']
+            c2['speedup_mixed_vs_reference_cpu'] = c2['reference_cpu_s'] / c2['engine_mixed_s']
+            if x_ref is not None:
+                for k in ('mixed', 'fp64'):
+                    x = c2.pop('_x_' + k)
+                    c2[f'rel_err_{k}_vs_reference'] = float(np.abs(x - x_ref).max() / np.abs(x_ref).max())
+    if c2 is not None:
+        for k in ('mixed', 'fp64'):
+            c2.pop('_x_' + k, None)
+        line['c2'] = c2
     return line
+
+
+def run_c2(args, ctx, engine, L, torch, stream, local_rank, reps=3):
+    """Assembly + LU + solve of the 1025-element VC ellipse on the engine,
+    best of `reps`, in both precisions (CUDA events on the engine's stream)."""
+    nods, conn, s_inf, vol = c2_case()
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    rhs = np.concatenate([engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, s_inf), [vol]])
+    A = engine.assemble(ctx, dm, dof, n, G, NU, vc=True)
+    d_rhs = torch.from_numpy(rhs).to(f'cuda:{local_rank}')
+    d_x = torch.empty_like(d_rhs)
+    info = engine.SolveInfo()
+    out = {'workload': f'VC 2:1 ellipse {C2_NEL} el, N={n}+1, Haar in-situ stress, V=1'}
+    for name, mode in (('mixed', engine.HFPX_LU_MIXED), ('fp64', engine.HFPX_LU_FP64)):
+        best = float('inf')
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            engine.assemble_into(ctx, dm, dof, n, G, NU, A, vc=True)
+            info_ = ctypes.c_int64()
+            ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
+            d_x.copy_(d_rhs)
+            torch.cuda.synchronize()
+            ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), 1, n + 1, 1e-12, 50,
+                                             ctypes.byref(info)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out[f'engine_{name}_s'] = best
+        out['_x_' + name] = d_x.cpu().numpy()
+    A.close()
+    dm.close()
+    return out
 
 
 def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
@@ -301,78 +353,153 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
 
 
 # ------------------------------------------------------------- CPU reference
-def ref_sample(n_el_sample, threads):
-    """The reference's own assembly (make_3dbem_matrix_s, OpenMP build) and
-    LAPACK dgesv on a smaller penny of the same family; returns
-    (t_assembly, t_solve, n_dof_sample, kind)."""
-    sys.path.insert(0, os.path.join(ROOT, 'tests'))
-    import oracle_lib
+# The reference's own CPU path (oracle/_ref/libhfpx_ref_cpu.so: its sources
+# compiled with OpenMP, il::LU on multithreaded OpenBLAS; run and timed as
+# its main.cpp does, "Assembly" and "Solution"), or, where that library was
+# not built, the CPU oracle port with numpy's LAPACK.  Measured on penny
+# meshes of the same family at FIT_SIZES elements, and at the 1025-element
+# volume-control ellipse for real; the 4000-element value is fitted from the
+# measured sizes (t_asm = a Ne^p, t_lu = b N^q by least squares in log-log)
+# and labelled extrapolated.
+FIT_SIZES = (600, 900, 1200)
+C2_NEL, C2_SEED = 1025, 1025
+
+
+def c2_case():
+    """The 1025-element 2:1 volume-control ellipse: mesh, Haar in-situ stress, V = 1."""
     from hfpx3d_b200 import meshgen
-    os.environ.setdefault('OMP_NUM_THREADS', str(threads))
-    nods, conn = meshgen.penny(n_el_sample, seed=7)
-    nods, conn = np.asfortranarray(nods), np.asfortranarray(conn, dtype=np.int64)
-    ne = conn.shape[1]
-    omp = os.path.join(ROOT, 'oracle', '_ref', 'libhfpx_ref_omp.so')
-    n = 18 * ne
-    A = np.zeros((n, n), order='F')
-    if os.path.exists(omp):
-        lib = oracle_lib._bind(omp, oracle_lib._REF_SIG)
-        dof = np.zeros((ne, 18), dtype=np.int64, order='F')
-        nd = ctypes.c_int64()
+    nods, conn = meshgen.ellipse(C2_NEL, seed=C2_SEED)
+    rng = np.random.default_rng(C2_SEED)
+    q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+    q = q * np.sign(np.diag(r))
+    st = q @ np.diag(rng.uniform(-1.0, 0.0, 3)) @ q.T
+    s_inf = np.array([st[0, 0], st[1, 1], st[2, 2], st[0, 1], st[0, 2], st[1, 2]])
+    return np.asfortranarray(nods), np.asfortranarray(conn, dtype=np.int64), s_inf, 1.0
+
+
+class RefCPU:
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, 'tests'))
+        import oracle_lib
+        self.ol = oracle_lib
+        path = os.path.join(ROOT, 'oracle', '_ref', 'libhfpx_ref_cpu.so')
+        self.lib = None
+        if os.path.exists(path):
+            D, L = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)
+            lib = ctypes.CDLL(path)
+            lib.ref_cpu_path.restype = ctypes.c_int
+            lib.ref_cpu_path.argtypes = [D, ctypes.c_int64, ctypes.c_int64, L, ctypes.c_int64, ctypes.c_int64,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, D,
+                                         ctypes.c_double, D, D, D, L]
+            self.lib = lib
+        self.kind = 'reference' if self.lib else 'port'
+
+    def run(self, nods, conn, s_inf, vc=False, volume=0.0):
+        """(t_assembly, t_solution, x) of one assembly + solve."""
+        ol = self.ol
+        ne = conn.shape[1]
+        s = np.ascontiguousarray(s_inf, dtype=np.float64)
+        if self.lib:
+            x = np.zeros(18 * ne + 1)
+            ta, ts, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+            rc = self.lib.ref_cpu_path(ol.dp(nods), nods.shape[0], nods.shape[1], ol.lp(conn), conn.shape[0], ne,
+                                       G, NU, BETA, int(vc), ol.dp(s), volume, ctypes.byref(ta), ctypes.byref(ts),
+                                       ol.dp(x), ctypes.byref(n))
+            if rc != 0:
+                raise RuntimeError(f'reference LU reports a singular matrix (rc {rc})')
+            return ta.value, ts.value, x[:n.value]
+        o = ol.Oracle()
         t0 = time.perf_counter()
-        lib.ref_assemble(oracle_lib.dp(nods), nods.shape[0], nods.shape[1], oracle_lib.lp(conn), conn.shape[0], ne,
-                         G, NU, BETA, 0, 0, 0, oracle_lib.dp(A), oracle_lib.lp(dof), ctypes.byref(nd))
-        t_asm = time.perf_counter() - t0
-        kind = 'reference'
-    else:
-        o = oracle_lib.Oracle()
         dof, n = o.dof_handle(nods, conn, 0)
-        t0 = time.perf_counter()
-        A = o.assemble(nods, conn, dof, n)
+        A = o.assemble(nods, conn, dof, n, vc=int(vc))
+        b = o.rhs(nods, conn, dof, n, s)
+        if vc:
+            b = np.concatenate([b, [volume]])
         t_asm = time.perf_counter() - t0
-        kind = 'port'
-    b = np.ones(n)
-    t0 = time.perf_counter()
-    np.linalg.solve(A, b)
-    t_sol = time.perf_counter() - t0
-    return t_asm, t_sol, n, kind
+        t0 = time.perf_counter()
+        x = np.linalg.solve(A, b)
+        return t_asm, time.perf_counter() - t0, x
+
+
+def fit_power(sizes, times):
+    """Least-squares t = c size^p in log-log: (c, p, max relative residual)."""
+    ls, lt = np.log(np.asarray(sizes, float)), np.log(np.asarray(times, float))
+    p, lc = np.polyfit(ls, lt, 1)
+    resid = float(np.max(np.abs(np.exp(lc + p * ls) / np.exp(lt) - 1.0)))
+    return float(np.exp(lc)), float(p), resid
+
+
+def cpu_measurement(passes, warmup, n_el_target, sizes=FIT_SIZES, with_c2=True):
+    """Best-of-`passes` times of the CPU path at `sizes` (penny elements) and
+    at the C2 ellipse, and the fitted value at n_el_target elements."""
+    from hfpx3d_b200 import meshgen
+    R = RefCPU()
+    sizes = tuple(sorted(sizes))
+    meshes = {ne: tuple(np.asfortranarray(a) for a in meshgen.penny(ne, seed=7)) for ne in sizes}
+    meshes = {ne: (m[0], m[1].astype(np.int64)) for ne, m in meshes.items()}
+    for _ in range(warmup):                      # warm-up: the smallest sample
+        R.run(*meshes[sizes[0]], S_ZZ)
+    best = {ne: [np.inf, np.inf] for ne in sizes}
+    c2_best = [np.inf, np.inf]
+    c2_x = None
+    if with_c2:
+        c2_nods, c2_conn, c2_s, c2_v = c2_case()
+    for _ in range(passes):
+        for ne in sizes:
+            ta, ts, _ = R.run(*meshes[ne], S_ZZ)
+            best[ne] = [min(best[ne][0], ta), min(best[ne][1], ts)]
+        if with_c2:
+            ta, ts, c2_x = R.run(c2_nods, c2_conn, c2_s, vc=True, volume=c2_v)
+            c2_best = [min(c2_best[0], ta), min(c2_best[1], ts)]
+    ca, pa, ra = fit_power(sizes, [best[ne][0] for ne in sizes])
+    cl, pl, rl = fit_power([18 * ne for ne in sizes], [best[ne][1] for ne in sizes])
+    FIT = sizes
+    t_asm = ca * n_el_target ** pa
+    t_lu = cl * (18 * n_el_target) ** pl
+    threads = len(os.sched_getaffinity(0))
+    return {
+        'value': t_asm + t_lu, 'unit': UNIT, 'cores': threads, 'kind': R.kind, 'extrapolated': True,
+        'sample': (f'{"the reference (OpenMP assembly, il::LU on OpenBLAS)" if R.kind == "reference" else "the CPU oracle port + numpy LAPACK"} '
+                   f'on {threads} host threads, best of {passes}, measured on seeded pennies of '
+                   f'{"/".join(str(s) for s in FIT)} elements; {n_el_target} elements fitted as '
+                   f'a Ne^{pa:.2f} (assembly) + b N^{pl:.2f} (LU), fit residuals {ra:.1%} / {rl:.1%}'),
+        'assembly_s': t_asm, 'solve_s': t_lu,
+        'fit': {'sizes_el': list(FIT), 'assembly_s': [round(best[ne][0], 4) for ne in FIT],
+                'solution_s': [round(best[ne][1], 4) for ne in FIT], 'assembly_exponent': pa,
+                'lu_exponent': pl, 'assembly_residual': ra, 'lu_residual': rl},
+        'measured_c2': ({'workload': f'VC 2:1 ellipse {C2_NEL} el, N={18 * C2_NEL}+1, Haar in-situ stress, V=1',
+                         'assembly_s': c2_best[0], 'solution_s': c2_best[1], 'value': c2_best[0] + c2_best[1]}
+                        if with_c2 else None),
+        '_c2_x': c2_x,
+    }
+
+
+def fit_sizes(args):
+    return tuple(int(x) for x in args.fit_sizes.split(','))
 
 
 def cpu_baseline(args):
-    threads = len(os.sched_getaffinity(0))
-    t_asm, t_sol, n_s, kind = ref_sample(args.cpu_sample_el, threads)
-    N = 18 * args.n_el
-    scale_asm = (args.n_el / args.cpu_sample_el) ** 2   # pair evaluations
-    scale_lu = (N / n_s) ** 3                              # 2/3 n^3
-    v = t_asm * scale_asm + t_sol * scale_lu
-    return {'value': v, 'unit': UNIT, 'cores': threads, 'kind': kind,
-            'sample': (f'reference assembly (OpenMP, {threads} threads) + LAPACK dgesv on a '
-                       f'{args.cpu_sample_el}-element penny ({n_s} DoF): {t_asm:.2f} s + {t_sol:.2f} s, '
-                       f'extrapolated to {args.n_el} elements by pair count (x{scale_asm:.1f}) and n^3 '
-                       f'(x{scale_lu:.0f})'),
-            'assembly_s': t_asm * scale_asm, 'solve_s': t_sol * scale_lu}
+    return cpu_measurement(passes=3, warmup=0, n_el_target=args.n_el, sizes=fit_sizes(args),
+                           with_c2=args.c2_ref)
 
 
 def run_reference(args, rank):
     if rank != 0:
         return None
-    threads = len(os.sched_getaffinity(0))
-    vals = []
-    for k in range(args.warmup + args.steps):
-        t_asm, t_sol, n_s, kind = ref_sample(args.cpu_sample_el, threads)
-        N = 18 * args.n_el
-        v = t_asm * (args.n_el / args.cpu_sample_el) ** 2 + t_sol * (N / n_s) ** 3
-        if k >= args.warmup:
-            vals.append(v)
-    v = statistics.mean(vals)
-    sample = (f'reference assembly (OpenMP) + LAPACK dgesv on a {args.cpu_sample_el}-element penny per step, '
-              f'extrapolated to {args.n_el} elements (pair count, n^3)')
+    # each step is one pass over the measured sizes and the C2 ellipse; the
+    # warm-up steps run the smallest sample only
+    m = cpu_measurement(passes=max(1, args.steps), warmup=args.warmup, n_el_target=args.n_el,
+                        sizes=fit_sizes(args), with_c2=args.c2_ref)
+    m.pop('_c2_x', None)
+    v = m['value']
     return {'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': v * 1e3, 'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
-            'dtype': 'f64', 'data': 'synthetic (seeded penny meshes)', 'impl': 'reference',
+            'dtype': 'f64', 'data': 'synthetic (seeded penny and ellipse meshes)', 'impl': 'reference',
+            'extrapolated': True,
             'config': {'workload': f'penny crack {args.n_el} el, N={18 * args.n_el} DoF, assembly + LU solve',
-                       'n_el': args.n_el},
-            'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': threads, 'kind': kind, 'sample': sample},
+                       'n_el': args.n_el, 'mode': 'fp64'},
+            'measured_c2': m['measured_c2'], 'fit': m['fit'],
+            'cpu_baseline': {k: m[k] for k in ('value', 'unit', 'cores', 'kind', 'sample', 'extrapolated')},
             'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
 
 
@@ -390,7 +517,10 @@ def main():
                          'FP32 factors')
     ap.add_argument('--no-compare', dest='compare', action='store_false')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
-    ap.add_argument('--cpu-sample-el', type=int, default=600)
+    ap.add_argument('--fit-sizes', default=','.join(str(x) for x in FIT_SIZES),
+                    help='penny sizes (elements) the CPU reference is measured at and fitted from')
+    ap.add_argument('--no-c2-ref', dest='c2_ref', action='store_false',
+                    help='skip the CPU reference run of the 1025-element VC ellipse')
     ap.add_argument('--e2e-steps', type=int, default=3)
     ap.add_argument('--e2e-warmup', type=int, default=1)
     args = ap.parse_args()

@@ -32,7 +32,8 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdint>
-#include <mutex>
+#include <cstdlib>
+#include <cstring>
 #include "engine_internal.h"
 
 namespace hfpx {
@@ -44,7 +45,7 @@ constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kStageA = kBM * kBK * 2;   // 16 KB
 constexpr uint32_t kStageB = kBN * kBK * 2;   // 32 KB
 constexpr uint32_t kTmemCols = 2 * kBN;       // two accumulators
-constexpr int kGroupM = 16;                   // tile raster: 16 row blocks per group
+constexpr int kGroupM = 16;                   // tile raster: row blocks per group (default)
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
 
 struct alignas(1024) TcSmem {
@@ -117,6 +118,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// the tile's block of C into L2 ahead of its epilogue (no shared memory, no
+// completion to wait for)
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y)
+               : "memory");
+}
+
 // K-major operand tile in shared memory with the 128-byte swizzle: rows of
 // 64 FP16 (128 bytes), 8-row atoms of 1024 bytes one after another (stride
 // byte offset 1024), leading byte offset unused for swizzled K-major (1),
@@ -167,25 +176,30 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// Output tiles in groups of `group` row blocks: inside a group the row block
+// changes fastest, so the CTAs working at one time share B tiles (and A tiles
+// across neighbouring groups) in L2.
 struct TileMap {
   int64_t tiles_m, tiles_n;
+  int group;
   __device__ void coords(int64_t t, int64_t& mb, int64_t& nb) const {
-    const int64_t per_group = (int64_t)kGroupM * tiles_n;
+    const int64_t per_group = (int64_t)group * tiles_n;
     const int64_t g = t / per_group, r = t - g * per_group;
-    const int64_t gm = min((int64_t)kGroupM, tiles_m - g * kGroupM);
-    mb = g * kGroupM + r % gm;
+    const int64_t gm = min((int64_t)group, tiles_m - g * group);
+    mb = g * group + r % gm;
     nb = r / gm;
   }
 };
 
 __global__ void __launch_bounds__(kThreads, 1)
     update_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
-                     float* __restrict__ C, int64_t ldc, int64_t m, int64_t n, int k, const float* __restrict__ d_alpha,
+                     const __grid_constant__ CUtensorMap map_c, int prefetch_c, float* __restrict__ C, int64_t ldc,
+                     int64_t m, int64_t n, int k, int group, const float* __restrict__ d_alpha,
                      int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const TileMap tm{(m + kBM - 1) / kBM, (n + kBN - 1) / kBN};
+  const TileMap tm{(m + kBM - 1) / kBM, (n + kBN - 1) / kBN, group};
   const int64_t tiles = tm.tiles_m * tm.tiles_n;
   const int nk = (k + kBK - 1) / kBK;
   volatile int* abort = &s.abort;
@@ -204,6 +218,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+    if (prefetch_c) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_c)) : "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
@@ -225,6 +240,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int64_t t = blockIdx.x; t < tiles && !*abort; t += gridDim.x) {
         int64_t mb, nb;
         tm.coords(t, mb, nb);
+        if (prefetch_c) tma_prefetch_2d(&map_c, (int)(mb * kBM), (int)(nb * kBN));
         for (int kb = 0; kb < nk; ++kb) {
           if (!wait_phase(&s.empty[stage], phase ^ 1u, abort, err, 0x101)) break;
           armed &= ~(1u << stage);
@@ -359,6 +375,30 @@ bool make_map(CUtensorMap* map, const void* base, int64_t rows, int64_t k, int64
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// C (m x n FP32, column-major, ldc) for the L2 prefetch: boxes of 128 rows x
+// 256 columns, the output tile
+bool make_map_c(CUtensorMap* map, const float* C, int64_t m, int64_t n, int64_t ldc) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
+  const cuuint32_t box[2] = {(cuuint32_t)kBM, (cuuint32_t)kBN};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(C), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// HFPX_TC_GROUP (1..64) overrides the raster group, for tuning sweeps
+int raster_group() {
+  static const int g = [] {
+    const char* e = std::getenv("HFPX_TC_GROUP");
+    const int v = e ? std::atoi(e) : 0;
+    return v >= 1 && v <= 64 ? v : kGroupM;
+  }();
+  return g;
+}
+
 }  // namespace
 
 bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void* B) {
@@ -372,9 +412,13 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k,
   if (m <= 0 || n <= 0 || k <= 0) return HFPX_OK;
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || !tc_update_supported(lda_k, ldb_k, A, B))
     return set_error(c, HFPX_ERR_ARG, "tensor-core update: unsupported operand layout");
-  CUtensorMap ma, mb;
+  CUtensorMap ma, mb, mc;
   if (!make_map(&ma, A, m, k, lda_k, kBM) || !make_map(&mb, B, n, k, ldb_k, kBN))
     return set_error(c, HFPX_ERR_CUDA, "tensor-core update: tensor map encoding failed");
+  // C's prefetch needs a 16-byte aligned base and row stride (it only warms
+  // L2: without it the epilogue reads C from HBM)
+  int prefetch_c = (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ldc % 4 == 0 && make_map_c(&mc, C, m, n, ldc);
+  if (!prefetch_c) std::memset(&mc, 0, sizeof(mc));
   static PerDeviceOnce attr;
   if (int rc = check_cuda(c, smem_attr_once(attr, update_tc_kernel, (int)kSmemBytes), "tensor-core update attribute"))
     return rc;
@@ -382,7 +426,8 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k,
   const int cap = max_ctas > 0 ? std::min(max_ctas, c->num_sms) : c->num_sms;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
   ++g_launches;
-  update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, C, ldc, m, n, (int)k, d_alpha, d_err);
+  update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, mc, prefetch_c, C, ldc, m, n, (int)k, raster_group(),
+                                                       d_alpha, d_err);
   return check_cuda(c, cudaGetLastError(), "tensor-core update launch");
 }
 

@@ -51,7 +51,8 @@ def test_reference_arm_under_torchrun():
     port = free_port()
     cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1', '--nproc-per-node', '2',
            '--master-addr', '127.0.0.1', '--master-port', str(port), 'bench.py', '--impl', 'reference',
-           '--gpus', '2', '--steps', '1', '--warmup', '0', '--n-el', '24', '--cpu-sample-el', '24']
+           '--gpus', '2', '--steps', '1', '--warmup', '0', '--n-el', '96', '--fit-sizes', '24,36,48',
+           '--no-c2-ref']
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith('{')]
@@ -60,3 +61,4 @@ def test_reference_arm_under_torchrun():
     assert d['impl'] == 'reference' and d['unit'] == 's' and d['higher_is_better'] is False
     assert d['cpu_baseline']['kind'] in ('reference', 'port')
     assert d['e2e']['h2d_bytes_per_step'] == 0
+    assert d['extrapolated'] is True and d['fit']['sizes_el'] == [24, 36, 48]
