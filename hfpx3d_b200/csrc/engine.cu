@@ -224,6 +224,14 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
   hfpx_mesh* m = new (std::nothrow) hfpx_mesh;
   if (!m) return HFPX_ERR_NOMEM;
   m->n_el = n_el;
+  m->h_vid.resize(3 * n_el);
+  m->h_vert.resize(9 * n_el);
+  for (int64_t e = 0; e < n_el; ++e)
+    for (int j = 0; j < 3; ++j) {
+      const int64_t v = conn[j + ld_conn * e];
+      m->h_vid[3 * e + j] = v;
+      for (int k = 0; k < 3; ++k) m->h_vert[9 * e + 3 * j + k] = nods[k + ld_nods * v];
+    }
   if (!rc) rc = check_cuda(c, cudaMalloc(&m->d_elem, elem_record_bytes() * n_el), "element records");
   if (!rc) launch_element_precompute(dn.as<double>(), ld_nods, dc.as<int64_t>(), ld_conn, n_el, beta, m->d_elem, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "element precompute");

@@ -2,6 +2,7 @@
 #pragma once
 #include <atomic>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -33,6 +34,37 @@ struct hfpx_ctx {
 struct hfpx_mesh {
   int64_t n_el = 0;
   void* d_elem = nullptr;          // ElemRec[n_el]
+  // host copies for the near-field pattern and the learned preconditioner's
+  // geometry features: vertex ids (3 per element) and vertex coordinates
+  // (9 per element, vertex j's x, y, z at 3 j)
+  std::vector<int64_t> h_vid;
+  std::vector<double> h_vert;
+};
+
+// Near-field pattern of a mesh: the elements sharing a vertex with element j
+// are its neighbours N(j); the pattern of block column j is P(j) = {j} + N(j).
+// Blocks of a near-field operator are stored column by column: column j's
+// self block at j + ptr[j], its neighbour blocks after it in idx order, so
+// edge e (src idx[e] -> column dst[e]) is block dst[e] + 1 + e.
+struct NearPattern {
+  int64_t n_el = 0, n_edges = 0;
+  int maxdeg = 0;
+  std::vector<int32_t> ptr, idx, dst, rev;   // rev[e]: the edge (dst[e] -> idx[e])
+  // row view for products: row i's blocks rblk[k] with column rcol[k], k in [rptr[i], rptr[i+1])
+  std::vector<int32_t> rptr, rblk, rcol;
+  int32_t *d_ptr = nullptr, *d_idx = nullptr, *d_dst = nullptr, *d_rev = nullptr;
+  int32_t *d_rptr = nullptr, *d_rblk = nullptr, *d_rcol = nullptr;
+  int64_t blocks() const { return n_el + n_edges; }
+};
+
+struct hfpx_gnn;
+
+struct hfpx_precond {
+  int kind = 0;
+  int64_t n_el = 0, n = 0;
+  NearPattern pat;
+  double* d_blocks = nullptr;      // blocks() x 18 x 18, each column-major
+  double* d_dinv = nullptr;        // inverses of the diagonal blocks, n_el x 18 x 18
 };
 
 struct hfpx_matrix {
@@ -135,6 +167,23 @@ int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int 
 bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void* B);
 int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
                   const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, int* d_err, int max_ctas);
+
+// precond.cu: near-field preconditioners on the FP64 matrix (block-Jacobi,
+// first-order Neumann, exact local inverse, learned) and their product
+int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p);
+void free_pattern(NearPattern* p);
+int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z);
+int gather_diag_inverse(hfpx_ctx* c, const double* A, int64_t lda, int64_t n_el, double* dinv, int* d_err);
+int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, const double* dinv, double* blocks,
+                   bool offdiag);
+// gnn.cu: the learned corrections added to the Neumann blocks of pc
+int gnn_correct_blocks(hfpx_ctx* c, const hfpx_gnn* net, const hfpx_mesh* mesh, const hfpx_matrix* m,
+                       hfpx_precond* pc, double shear_m);
+int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks);
+// lu.cu: flexible GMRES on the FP64 matrix with a right preconditioner
+// apply(v, z): z = M v (FP64, device), for one right-hand side
+int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
+               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply);
 
 // solve.cu: one right-hand side of the refinement
 int trsv_tiles(int64_t n);

@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <vector>
 #include "engine_internal.h"
@@ -2215,15 +2216,14 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
   return rc;
 }
 
-// Iterative refinement: x += LU32^-1 r, r = b - A x in FP64.
-// GMRES(restart) on the FP64 matrix, right-preconditioned by the FP32
-// factors: A M^-1 u = b, x = M^-1 u, in the flexible form (the vectors
-// z_j = M^-1 v_j are kept, so x += Z y needs no further solve).  One step is
-// one preconditioner solve (precond_f32) and one FP64 product with A (the
-// residual kernel against a zero right-hand side gives -A z); the Arnoldi
-// vectors are orthogonalised by classical Gram-Schmidt applied twice (four
-// cuBLAS DGEMVs), the small Hessenberg least-squares problem is solved on the
-// host with Givens rotations.  A cycle stops when the rotated residual
+// GMRES(restart) on the FP64 matrix with a right preconditioner M:
+// A M u = b, x = M u, in the flexible form (the vectors z_j = M v_j are
+// kept, so x += Z y needs no further application of M).  One step is one
+// application of M (apply) and one FP64 product with A (the residual kernel
+// against a zero right-hand side gives -A z); the Arnoldi vectors are
+// orthogonalised by classical Gram-Schmidt applied twice (four cuBLAS
+// DGEMVs), the small Hessenberg least-squares problem is solved on the host
+// with Givens rotations.  A cycle stops when the rotated residual
 // |g_{j+1}| / |b|_2 is below tol / 4; then the residual r = b - A x decides,
 // in the max norm like the refinement: |r|_inf / |b|_inf <= tol, else the
 // next cycle starts from it.  The products A z_j are kept, so r = b - [A z] y
@@ -2231,9 +2231,8 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
 // up to rounding far below the tolerance).  d_b: right-hand side in, x out.
 constexpr int kGmresMax = 64;
 
-int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
-                hfpx_solve_info* info) {
-  const int64_t n = m->n;
+int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
+               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply) {
   const int k = std::max(1, std::min(restart, kGmresMax));
   double* V = (double*)ctx_scratch(c, kScrGmresV, sizeof(double) * n * (k + 1));
   double* Z = (double*)ctx_scratch(c, kScrGmresZ, sizeof(double) * n * 2 * k);  // Z, then A Z
@@ -2241,20 +2240,14 @@ int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int 
   double* zero = (double*)ctx_scratch(c, kScrGmresZero, sizeof(double) * n);
   double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * n);
   double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * n);
-  float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * n);
-  float* y = (float*)ctx_scratch(c, kScrSolveTmp, sizeof(float) * n);
   double* part = (double*)ctx_scratch(c, kScrResidPart, sizeof(double) * n * resid_chunks(n));
   unsigned long long* dmax = (unsigned long long*)ctx_scratch(c, kScrResidMax, sizeof(unsigned long long));
-  if (!V || !Z || !dh || !zero || !x || !r || !rf || !y || !part || !dmax)
-    return set_error(c, HFPX_ERR_NOMEM, "GMRES buffers");
+  if (!V || !Z || !dh || !zero || !x || !r || !part || !dmax) return set_error(c, HFPX_ERR_NOMEM, "GMRES buffers");
   double* AZ = Z + (size_t)n * k;
-  int32_t* d_perm = nullptr;
-  int rc = build_perm(c, m, &d_perm);
-  if (rc) return rc;
+  int rc = 0;
   cublasHandle_t h = H(c);
   cublasSetPointerMode(h, CUBLAS_POINTER_MODE_HOST);
   cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
-  const unsigned nb = (unsigned)((n + 255) / 256);
   auto sync = [&](const char* what) { return check_cuda(c, cudaStreamSynchronize(c->stream), what); };
   auto read_max = [&](double* v) {
     unsigned long long bits = 0;
@@ -2293,13 +2286,10 @@ int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int 
       double* vj = V + (size_t)n * j;
       double* zj = Z + (size_t)n * j;
       double* w = V + (size_t)n * (j + 1);
-      // z_j = M^-1 v_j (FP32 solve, widened), w = A z_j
-      rc = precond_f32(c, m, d_perm, vj, rf, y);
+      // z_j = M v_j (the preconditioner), w = A z_j
+      rc = apply(vj, zj);
       if (rc) break;
-      cudaMemsetAsync(zj, 0, sizeof(double) * n, c->stream);
-      ++g_launches;
-      axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(y, zj, n, 1, n, n);
-      rc = residual_f64(c, m->d_a, m->ld, n, zj, zero, w, part, dmax);  // w = -A z_j
+      rc = residual_f64(c, A, lda, n, zj, zero, w, part, dmax);  // w = -A z_j
       if (rc) break;
       const double mone = -1.0, one = 1.0, zero_s = 0.0;
       cublasDscal(h, (int)n, &mone, w, 1);
@@ -2368,7 +2358,6 @@ int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int 
     if (prof().on) std::fprintf(stderr, "[hfpx profile] GMRES cycle end: residual %.3e\n", worst);
     if (worst <= tol) break;
   }
-  if (!rc) rc = trsv_status(c);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "GMRES");
   if (!rc) {
     cudaMemcpyAsync(d_b, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream);
@@ -2380,6 +2369,32 @@ int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int 
     info->converged = worst <= tol;
   }
   if (!rc && !(worst <= tol)) rc = set_error(c, HFPX_ERR_NOT_CONVERGED, "GMRES did not reach the tolerance");
+  return rc;
+}
+
+
+// The mixed-LU preconditioned form: M = (P L U)^-1 of the FP32 factors,
+// applied in FP32 and widened to FP64.
+int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
+                hfpx_solve_info* info) {
+  const int64_t n = m->n;
+  float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * n);
+  float* y = (float*)ctx_scratch(c, kScrSolveTmp, sizeof(float) * n);
+  if (!rf || !y) return set_error(c, HFPX_ERR_NOMEM, "GMRES buffers");
+  int32_t* d_perm = nullptr;
+  int rc = build_perm(c, m, &d_perm);
+  if (rc) return rc;
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  auto apply = [&](const double* v, double* z) {
+    int e = precond_f32(c, m, d_perm, v, rf, y);
+    if (e) return e;
+    cudaMemsetAsync(z, 0, sizeof(double) * n, c->stream);
+    ++g_launches;
+    axpy_f2d_kernel<<<nb, 256, 0, c->stream>>>(y, z, n, 1, n, n);
+    return 0;
+  };
+  rc = gmres_core(c, m->d_a, m->ld, n, d_b, tol, restart, max_iter, info, apply);
+  if (!rc) rc = trsv_status(c);
   return rc;
 }
 

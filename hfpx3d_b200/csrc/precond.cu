@@ -1,0 +1,461 @@
+// Near-field preconditioners for flexible GMRES on the dense FP64 operator
+// (the matrix make_3dbem_matrix_s fills, src/Solvers/system_assembly.cpp:30-219;
+// the reference itself only solves directly, il::LU at
+// il/linear_algebra/dense/factorization/LU.h:79-120).
+//
+// All of them are block-sparse right preconditioners M ~ A^-1 on the
+// near-field pattern: block column j holds blocks for the rows of the
+// elements P(j) = {j} + N(j) (N(j): the elements sharing a vertex with j),
+// 18 x 18 each (6 nodes x 3 DD components).  For a mesh without fixed DoF
+// the element's DoF are 18 e .. 18 e + 17, so block (i, j) is rows 18 i..,
+// columns 18 j.. of A.
+//   block-Jacobi:    M_jj = A_jj^-1;
+//   Neumann:         M_jj = D_j^-1, M_ij = -D_i^-1 A_ij D_j^-1 (D = the diagonal
+//                    blocks): the first-order term of (D + A_near)^-1;
+//   local inverse:   column j of M = L_j^-1 e_j on its pattern, L_j the square
+//                    block system A[P(j), P(j)] (the square-pattern sparse
+//                    approximate inverse), by batched dense LU;
+//   learned:         the Neumann blocks plus corrections predicted by a graph
+//                    network (gnn.cu).
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <set>
+#include <vector>
+#include "engine_internal.h"
+
+namespace hfpx {
+namespace {
+
+constexpr int kB = 18;          // block size
+constexpr int kBB = kB * kB;
+
+// Gauss-Jordan inverse of each 18 x 18 diagonal block, partial pivoting, in
+// shared memory (one CTA per element).  A zero pivot sets *err.
+__global__ void __launch_bounds__(128) diag_inverse_kernel(const double* __restrict__ A, int64_t lda, int64_t n_el,
+                                                           double* __restrict__ dinv, int* __restrict__ err) {
+  __shared__ double a[kB][2 * kB + 1];
+  __shared__ double f[kB];
+  __shared__ int piv;
+  const int64_t e = blockIdx.x;
+  const double* Ae = A + kB * e + lda * kB * e;
+  for (int t = threadIdx.x; t < kB * 2 * kB; t += blockDim.x) {
+    const int r = t % kB, c = t / kB;
+    a[r][c] = c < kB ? Ae[r + lda * c] : (c - kB == r ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  for (int c = 0; c < kB; ++c) {
+    if (threadIdx.x == 0) {
+      int p = c;
+      double best = fabs(a[c][c]);
+      for (int r = c + 1; r < kB; ++r)
+        if (fabs(a[r][c]) > best) {
+          best = fabs(a[r][c]);
+          p = r;
+        }
+      piv = p;
+      if (best == 0.0) atomicExch(err, 1);
+    }
+    __syncthreads();
+    const int p = piv;
+    if (p != c)
+      for (int t = threadIdx.x; t < 2 * kB; t += blockDim.x) {
+        const double x = a[c][t];
+        a[c][t] = a[p][t];
+        a[p][t] = x;
+      }
+    __syncthreads();
+    const double d = a[c][c];
+    const double inv = d != 0.0 ? 1.0 / d : 0.0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * kB; t += blockDim.x) a[c][t] *= inv;
+    if (threadIdx.x < kB) f[threadIdx.x] = a[threadIdx.x][c];   // row c is read after the barrier
+    __syncthreads();
+    if (threadIdx.x == c) f[c] = 0.0;                          // the pivot row stays
+    __syncthreads();
+    for (int t = threadIdx.x; t < kB * 2 * kB; t += blockDim.x) {
+      const int r = t / (2 * kB), q = t % (2 * kB);
+      if (r != c) a[r][q] -= f[r] * a[c][q];
+    }
+    __syncthreads();
+  }
+  double* out = dinv + (size_t)kBB * e;
+  for (int t = threadIdx.x; t < kBB; t += blockDim.x) {
+    const int r = t % kB, c = t / kB;
+    out[t] = a[r][kB + c];
+  }
+}
+
+// C = alpha X Y for 18 x 18 column-major blocks in shared memory, one thread
+// per output entry (324 threads)
+__device__ __forceinline__ void mul18(const double* X, const double* Y, double* C, double alpha) {
+  const int t = threadIdx.x;
+  if (t < kBB) {
+    const int r = t % kB, c = t / kB;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kB; ++k) s = fma(X[r + kB * k], Y[k + kB * c], s);
+    C[t] = alpha * s;
+  }
+}
+
+// Neumann blocks: M_jj = D_j^-1, M_ij = -D_i^-1 A_ij D_j^-1 (one CTA per block)
+__global__ void __launch_bounds__(352) neumann_kernel(const double* __restrict__ A, int64_t lda, int64_t n_el,
+                                                      const int32_t* __restrict__ ptr,
+                                                      const int32_t* __restrict__ idx,
+                                                      const int32_t* __restrict__ dst,
+                                                      const double* __restrict__ dinv, double* __restrict__ blocks,
+                                                      int offdiag) {
+  __shared__ double s_a[kBB], s_t[kBB], s_di[kBB], s_dj[kBB];
+  const int64_t b = blockIdx.x;  // blocks: first the n_el self blocks, then the edges
+  const int t = threadIdx.x;
+  if (b < n_el) {
+    const int64_t j = b;
+    if (t < kBB) blocks[(size_t)kBB * (j + ptr[j]) + t] = dinv[(size_t)kBB * j + t];
+    return;
+  }
+  if (!offdiag) return;  // block-Jacobi: the neighbour blocks stay zero
+  const int64_t e = b - n_el;
+  const int64_t i = idx[e], j = dst[e];
+  if (t < kBB) {
+    const int r = t % kB, c = t / kB;
+    s_a[t] = A[(kB * i + r) + lda * (kB * j + c)];
+    s_di[t] = dinv[(size_t)kBB * i + t];
+    s_dj[t] = dinv[(size_t)kBB * j + t];
+  }
+  __syncthreads();
+  mul18(s_a, s_dj, s_t, 1.0);
+  __syncthreads();
+  mul18(s_di, s_t, s_a, -1.0);
+  __syncthreads();
+  if (t < kBB) blocks[(size_t)kBB * (j + 1 + e) + t] = s_a[t];
+}
+
+// Local systems of the exact local inverse: L_j (Q x Q, column-major) =
+// A[P(j), P(j)] padded with the identity to Q = 18 (1 + maxdeg) rows, and
+// its right-hand side E_j = the first 18 columns of the identity.  One CTA
+// per (column j, pattern block a, pattern block b).
+__global__ void local_system_kernel(const double* __restrict__ A, int64_t lda, const int32_t* __restrict__ ptr,
+                                    const int32_t* __restrict__ idx, int slots, double* __restrict__ L,
+                                    double* __restrict__ E) {
+  const int64_t j = blockIdx.x;
+  const int a = blockIdx.y, bsl = blockIdx.z;
+  const int Q = kB * slots;
+  const int deg = ptr[j + 1] - ptr[j];
+  double* Lj = L + (size_t)Q * Q * j;
+  const int t = threadIdx.x;
+  if (t >= kBB) return;
+  const int r = t % kB, c = t / kB;
+  double v;
+  if (a <= deg && bsl <= deg) {
+    const int64_t pa = a == 0 ? j : idx[ptr[j] + a - 1];
+    const int64_t pb = bsl == 0 ? j : idx[ptr[j] + bsl - 1];
+    v = A[(kB * pa + r) + lda * (kB * pb + c)];
+  } else {
+    v = (a == bsl && r == c) ? 1.0 : 0.0;
+  }
+  Lj[(kB * a + r) + (size_t)Q * (kB * bsl + c)] = v;
+  if (bsl == 0) E[(size_t)Q * kB * j + (kB * a + r) + (size_t)Q * c] = (a == 0 && r == c) ? 1.0 : 0.0;
+}
+
+__global__ void local_scatter_kernel(const double* __restrict__ E, const int32_t* __restrict__ ptr, int slots,
+                                     double* __restrict__ blocks) {
+  const int64_t j = blockIdx.x;
+  const int s = blockIdx.y;
+  const int deg = ptr[j + 1] - ptr[j];
+  if (s > deg) return;
+  const int Q = kB * slots;
+  const int t = threadIdx.x;
+  if (t >= kBB) return;
+  const int r = t % kB, c = t / kB;
+  const int64_t blk = s == 0 ? j + ptr[j] : j + 1 + ptr[j] + (s - 1);
+  blocks[(size_t)kBB * blk + t] = E[(size_t)Q * kB * j + (kB * s + r) + (size_t)Q * c];
+}
+
+__global__ void ptr_array_kernel(double* base, int64_t stride, int64_t count, double** out) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k < count) out[k] = base + stride * k;
+}
+
+// z = M v by rows: one warp per block row, lanes 0..17 own its 18 rows
+__global__ void __launch_bounds__(256) block_spmv_kernel(const double* __restrict__ blocks,
+                                                         const int32_t* __restrict__ rptr,
+                                                         const int32_t* __restrict__ rblk,
+                                                         const int32_t* __restrict__ rcol, int64_t n_el,
+                                                         const double* __restrict__ v, double* __restrict__ z) {
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n_el) return;
+  double acc = 0.0;
+  for (int k = rptr[i]; k < rptr[i + 1]; ++k) {
+    const double* M = blocks + (size_t)kBB * rblk[k];
+    const double* vj = v + (size_t)kB * rcol[k];
+    const double vl = lane < kB ? vj[lane] : 0.0;
+#pragma unroll
+    for (int c = 0; c < kB; ++c) {
+      const double vc = __shfl_sync(0xffffffffu, vl, c);
+      if (lane < kB) acc = fma(M[lane + kB * c], vc, acc);
+    }
+  }
+  if (lane < kB) z[(size_t)kB * i + lane] = acc;
+}
+
+template <class T>
+T* dev_copy(hfpx_ctx* c, const std::vector<T>& h, int* rc) {
+  if (*rc) return nullptr;
+  T* d = nullptr;
+  *rc = check_cuda(c, cudaMalloc(&d, sizeof(T) * std::max<size_t>(1, h.size())), "pattern alloc");
+  if (!*rc && !h.empty())
+    *rc = check_cuda(c, cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream),
+                     "pattern copy");
+  return d;
+}
+
+}  // namespace
+
+int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
+  const int64_t ne = mesh->n_el;
+  if ((int64_t)mesh->h_vid.size() != 3 * ne) return set_error(c, HFPX_ERR_STATE, "mesh has no host connectivity");
+  std::map<int64_t, std::vector<int32_t>> v2e;
+  for (int64_t e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) v2e[mesh->h_vid[3 * e + k]].push_back((int32_t)e);
+  p->n_el = ne;
+  p->ptr.assign(ne + 1, 0);
+  p->idx.clear();
+  p->dst.clear();
+  p->maxdeg = 0;
+  for (int64_t j = 0; j < ne; ++j) {
+    std::set<int32_t> nb;
+    for (int k = 0; k < 3; ++k)
+      for (int32_t i : v2e[mesh->h_vid[3 * j + k]])
+        if (i != j) nb.insert(i);
+    for (int32_t i : nb) {
+      p->idx.push_back(i);
+      p->dst.push_back((int32_t)j);
+    }
+    p->ptr[j + 1] = (int32_t)p->idx.size();
+    p->maxdeg = std::max(p->maxdeg, (int)nb.size());
+  }
+  p->n_edges = (int64_t)p->idx.size();
+  // reverse edges and the row view (the pattern is symmetric)
+  p->rev.assign(p->n_edges, -1);
+  for (int64_t j = 0; j < ne; ++j)
+    for (int32_t e = p->ptr[j]; e < p->ptr[j + 1]; ++e) {
+      const int32_t i = p->idx[e];
+      const auto b = p->idx.begin() + p->ptr[i], en = p->idx.begin() + p->ptr[i + 1];
+      const auto it = std::lower_bound(b, en, (int32_t)j);
+      if (it == en || *it != (int32_t)j) return set_error(c, HFPX_ERR_STATE, "near-field pattern is not symmetric");
+      p->rev[e] = (int32_t)(it - p->idx.begin());
+    }
+  p->rptr.assign(ne + 1, 0);
+  p->rblk.clear();
+  p->rcol.clear();
+  for (int64_t i = 0; i < ne; ++i) {
+    p->rblk.push_back((int32_t)(i + p->ptr[i]));  // self
+    p->rcol.push_back((int32_t)i);
+    for (int32_t e = p->ptr[i]; e < p->ptr[i + 1]; ++e) {
+      const int32_t j = p->idx[e];           // column j holds block (i, j) as its edge rev[e]
+      p->rblk.push_back(j + 1 + p->rev[e]);
+      p->rcol.push_back(j);
+    }
+    p->rptr[i + 1] = (int32_t)p->rblk.size();
+  }
+  int rc = 0;
+  p->d_ptr = dev_copy(c, p->ptr, &rc);
+  p->d_idx = dev_copy(c, p->idx, &rc);
+  p->d_dst = dev_copy(c, p->dst, &rc);
+  p->d_rev = dev_copy(c, p->rev, &rc);
+  p->d_rptr = dev_copy(c, p->rptr, &rc);
+  p->d_rblk = dev_copy(c, p->rblk, &rc);
+  p->d_rcol = dev_copy(c, p->rcol, &rc);
+  return rc;
+}
+
+void free_pattern(NearPattern* p) {
+  for (int32_t* d : {p->d_ptr, p->d_idx, p->d_dst, p->d_rev, p->d_rptr, p->d_rblk, p->d_rcol})
+    if (d) cudaFree(d);
+  p->d_ptr = p->d_idx = p->d_dst = p->d_rev = p->d_rptr = p->d_rblk = p->d_rcol = nullptr;
+}
+
+int gather_diag_inverse(hfpx_ctx* c, const double* A, int64_t lda, int64_t n_el, double* dinv, int* d_err) {
+  ++g_launches;
+  diag_inverse_kernel<<<(unsigned)n_el, 128, 0, c->stream>>>(A, lda, n_el, dinv, d_err);
+  return check_cuda(c, cudaGetLastError(), "diagonal block inverses");
+}
+
+int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, const double* dinv,
+                   double* blocks, bool offdiag) {
+  ++g_launches;
+  neumann_kernel<<<(unsigned)(offdiag ? p.blocks() : p.n_el), 352, 0, c->stream>>>(
+      A, lda, p.n_el, p.d_ptr, p.d_idx, p.d_dst, dinv, blocks, offdiag ? 1 : 0);
+  return check_cuda(c, cudaGetLastError(), "Neumann blocks");
+}
+
+int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks) {
+  const int slots = 1 + p.maxdeg;
+  const int Q = kB * slots;
+  const int64_t ne = p.n_el;
+  double *L = nullptr, *E = nullptr, **Lp = nullptr, **Ep = nullptr;
+  int *piv = nullptr, *info = nullptr;
+  int rc = check_cuda(c, cudaMalloc(&L, sizeof(double) * Q * Q * ne), "local systems");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&E, sizeof(double) * Q * kB * ne), "local right-hand sides");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&Lp, sizeof(double*) * ne), "local pointers");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&Ep, sizeof(double*) * ne), "local pointers");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&piv, sizeof(int) * Q * ne), "local pivots");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&info, sizeof(int) * ne), "local info");
+  if (!rc) {
+    g_launches += 4;
+    local_system_kernel<<<dim3((unsigned)ne, slots, slots), 352, 0, c->stream>>>(A, lda, p.d_ptr, p.d_idx, slots,
+                                                                                  L, E);
+    ptr_array_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, c->stream>>>(L, (int64_t)Q * Q, ne, Lp);
+    ptr_array_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, c->stream>>>(E, (int64_t)Q * kB, ne, Ep);
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
+    cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+    int hinfo = 0;
+    if (cublasDgetrfBatched(h, Q, Lp, Q, piv, info, (int)ne) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgetrsBatched(h, CUBLAS_OP_N, Q, kB, (const double* const*)Lp, Q, piv, Ep, Q, &hinfo, (int)ne) !=
+            CUBLAS_STATUS_SUCCESS)
+      rc = set_error(c, HFPX_ERR_CUDA, "batched local solves");
+    if (!rc) local_scatter_kernel<<<dim3((unsigned)ne, slots), 352, 0, c->stream>>>(E, p.d_ptr, slots, blocks);
+    if (!rc) rc = check_cuda(c, cudaGetLastError(), "local inverse");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "local inverse");
+  }
+  for (void* q : {(void*)L, (void*)E, (void*)Lp, (void*)Ep, (void*)piv, (void*)info})
+    if (q) cudaFree(q);
+  return rc;
+}
+
+int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z) {
+  const int64_t ne = pc->n_el;
+  ++g_launches;
+  block_spmv_kernel<<<(unsigned)((ne * 32 + 255) / 256), 256, 0, c->stream>>>(
+      pc->d_blocks, pc->pat.d_rptr, pc->pat.d_rblk, pc->pat.d_rcol, ne, v, z);
+  return check_cuda(c, cudaGetLastError(), "preconditioner product");
+}
+
+}  // namespace hfpx
+
+// ------------------------------------------------------------------ C-ABI
+using namespace hfpx;
+
+extern "C" {
+
+int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, int kind, const hfpx_gnn* net,
+                        double shear_m, hfpx_precond** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  if (!mesh || !m) return set_error(c, HFPX_ERR_ARG, "null mesh or matrix");
+  if (kind < HFPX_PC_BLOCK_JACOBI || kind > HFPX_PC_LEARNED) return set_error(c, HFPX_ERR_ARG, "unknown preconditioner");
+  if (kind == HFPX_PC_LEARNED && !net) return set_error(c, HFPX_ERR_ARG, "the learned preconditioner needs a network");
+  if (m->n != 18 * mesh->n_el)
+    return set_error(c, HFPX_ERR_ARG, "near-field preconditioners need a matrix of 18 DoF per element (no fixed DoF, "
+                                      "no volume-control border)");
+  if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "the matrix holds FP64 LU factors, not the operator");
+  if (!(shear_m > 0)) return set_error(c, HFPX_ERR_ARG, "bad shear modulus");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  hfpx_precond* pc = new (std::nothrow) hfpx_precond;
+  if (!pc) return set_error(c, HFPX_ERR_NOMEM, "preconditioner");
+  pc->kind = kind;
+  pc->n_el = mesh->n_el;
+  pc->n = m->n;
+  int rc = build_pattern(c, mesh, &pc->pat);
+  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
+  if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_blocks, sizeof(double) * 324 * pc->pat.blocks()), "blocks");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * pc->pat.blocks(), c->stream),
+                           "blocks");
+  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_dinv, sizeof(double) * 324 * pc->n_el), "block inverses");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
+  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, pc->n_el, pc->d_dinv, err);
+  if (!rc) {
+    if (kind == HFPX_PC_LOCAL_INVERSE)
+      rc = local_inverse_blocks(c, m->d_a, m->ld, pc->pat, pc->d_blocks);
+    else
+      rc = neumann_blocks(c, m->d_a, m->ld, pc->pat, pc->d_dinv, pc->d_blocks, kind != HFPX_PC_BLOCK_JACOBI);
+  }
+  if (!rc && kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
+  int herr = 0;
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "preconditioner");
+  if (!rc && herr) rc = set_error(c, HFPX_ERR_SINGULAR, "a diagonal block of the matrix is singular");
+  if (rc) {
+    hfpx_precond_destroy(pc);
+    return rc;
+  }
+  *out = pc;
+  return HFPX_OK;
+}
+
+int hfpx_precond_destroy(hfpx_precond* pc) {
+  if (!pc) return HFPX_OK;
+  free_pattern(&pc->pat);
+  if (pc->d_blocks) cudaFree(pc->d_blocks);
+  if (pc->d_dinv) cudaFree(pc->d_dinv);
+  delete pc;
+  return HFPX_OK;
+}
+
+int hfpx_precond_blocks(hfpx_ctx* c, const hfpx_precond* pc, int64_t* n_blocks, int32_t* block_row,
+                        int32_t* block_col, double* blocks) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!pc || !n_blocks) return set_error(c, HFPX_ERR_ARG, "null preconditioner");
+  *n_blocks = pc->pat.blocks();
+  if (!block_row && !block_col && !blocks) return HFPX_OK;
+  if (block_row || block_col) {
+    for (int64_t j = 0; j < pc->n_el; ++j) {
+      const int64_t base = j + pc->pat.ptr[j];
+      if (block_row) block_row[base] = (int32_t)j;
+      if (block_col) block_col[base] = (int32_t)j;
+      for (int32_t e = pc->pat.ptr[j]; e < pc->pat.ptr[j + 1]; ++e) {
+        if (block_row) block_row[j + 1 + e] = pc->pat.idx[e];
+        if (block_col) block_col[j + 1 + e] = (int32_t)j;
+      }
+    }
+  }
+  if (blocks) {
+    if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+    int rc = check_cuda(c, cudaMemcpyAsync(blocks, pc->d_blocks, sizeof(double) * 324 * pc->pat.blocks(),
+                                           cudaMemcpyDeviceToHost, c->stream),
+                        "blocks");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "blocks");
+    return rc;
+  }
+  return HFPX_OK;
+}
+
+int hfpx_gmres_precond_device(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_precond* pc, double* d_b, double tol,
+                              int restart, int max_iter, hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !d_b) return set_error(c, HFPX_ERR_ARG, "null argument");
+  if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "the matrix holds FP64 LU factors, not the operator");
+  if (pc && pc->n != m->n) return set_error(c, HFPX_ERR_ARG, "preconditioner and matrix differ in size");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  const int64_t n = m->n;
+  auto apply = [&](const double* v, double* z) -> int {
+    if (pc) return precond_apply(c, pc, v, z);
+    return check_cuda(c, cudaMemcpyAsync(z, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream), "identity");
+  };
+  return gmres_core(c, m->d_a, m->ld, n, d_b, tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50,
+                    max_iter > 0 ? max_iter : 1000, info, apply);
+}
+
+int hfpx_gmres_precond(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_precond* pc, double* b, double tol, int restart,
+                       int max_iter, hfpx_solve_info* info) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !b) return set_error(c, HFPX_ERR_ARG, "null argument");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  double* d = (double*)ctx_scratch(c, kScrHostRhs, sizeof(double) * m->n);
+  if (!d) return set_error(c, HFPX_ERR_NOMEM, "right-hand side");
+  int rc = check_cuda(c, cudaMemcpyAsync(d, b, sizeof(double) * m->n, cudaMemcpyHostToDevice, c->stream), "b");
+  if (!rc) rc = hfpx_gmres_precond_device(c, m, pc, d, tol, restart, max_iter, info);
+  if (!rc || rc == HFPX_ERR_NOT_CONVERGED) {
+    int rc2 = check_cuda(c, cudaMemcpyAsync(b, d, sizeof(double) * m->n, cudaMemcpyDeviceToHost, c->stream), "x");
+    if (!rc2) rc2 = check_cuda(c, cudaStreamSynchronize(c->stream), "x");
+    if (rc2) rc = rc2;
+  }
+  return rc;
+}
+
+}  // extern "C"

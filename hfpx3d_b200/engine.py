@@ -68,6 +68,27 @@ SIGNATURES = {
     'hfpx_gmres_device': (_int, [_V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
     'hfpx_gemm_f16_update': (_int, [_V, _i64, _i64, _i64, _V, _i64, _V, _i64, _V, _i64, _V]),
+    'hfpx_precond_create': (_int, [_V, _V, _V, _int, _V, _f64, ctypes.POINTER(_V)]),
+    'hfpx_precond_destroy': (_int, [_V]),
+    'hfpx_precond_blocks': (_int, [_V, _V, _L, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), _D]),
+    'hfpx_gmres_precond': (_int, [_V, _V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_gmres_precond_device': (_int, [_V, _V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_gnn_create': (_int, [_V, ctypes.c_uint64, ctypes.POINTER(_V)]),
+    'hfpx_gnn_destroy': (_int, [_V]),
+    'hfpx_gnn_param_count': (_i64, [_V]),
+    'hfpx_gnn_get_params': (_int, [_V, _V, ctypes.POINTER(ctypes.c_float)]),
+    'hfpx_gnn_set_params': (_int, [_V, _V, ctypes.POINTER(ctypes.c_float)]),
+    'hfpx_gnn_save': (_int, [_V, _V, ctypes.c_char_p]),
+    'hfpx_gnn_load': (_int, [_V, ctypes.c_char_p, ctypes.POINTER(_V)]),
+    'hfpx_gnn_graph_create': (_int, [_V, _V, _V, _f64, _int, ctypes.POINTER(_V)]),
+    'hfpx_gnn_graph_destroy': (_int, [_V]),
+    'hfpx_gnn_graph_dims': (_int, [_V, _L, _L]),
+    'hfpx_gnn_graph_data': (_int, [_V, _V, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                   ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    'hfpx_gnn_forward': (_int, [_V, _V, _V, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    'hfpx_gnn_gradients': (_int, [_V, _V, _V, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)]),
+    'hfpx_gnn_train': (_int, [_V, _V, _V, _int, _f64, ctypes.POINTER(ctypes.c_double)]),
     'hfpx_lu_panel_factor_noalloc': (_int, [_V, _V, _i64, _i64, _int, _V, _L]),
     'hfpx_stress': (_int, [_V, _V, _f64, _f64, _int, _D, _D, _i64, _D, _D]),
     'hfpx_stress_batch': (_int, [_V, _V, _f64, _f64, _int, _D, _i64, _D, _i64, _D, _D]),
@@ -386,3 +407,155 @@ def write_dd_vector_to_md(sol, dof_h, n_el):
         ok = g >= 0
         dd[rows[ok], j % 3] = sol[g[ok]]
     return dd
+
+
+# ------------------------------------------------- near-field preconditioners
+HFPX_PC_BLOCK_JACOBI, HFPX_PC_NEUMANN, HFPX_PC_LOCAL_INVERSE, HFPX_PC_LEARNED = 0, 1, 2, 3
+# the trained network shipped with the engine (HFPX_PC_WEIGHTS overrides the path)
+WEIGHTS_PATH = os.environ.get('HFPX_PC_WEIGHTS') or os.path.join(_HERE, 'data', 'pc_gnn.bin')
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+class Precond:
+    """A near-field right preconditioner of the FP64 matrix (hfpx_precond)."""
+
+    def __init__(self, ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, kind, net=None, shear_m=1.0):
+        self.ctx = ctx
+        self.h = _V()
+        ctx.check(lib().hfpx_precond_create(ctx.h, dmesh.h, matrix.h, kind, net.h if net is not None else None,
+                                            shear_m, ctypes.byref(self.h)))
+
+    def blocks(self):
+        """(block_row, block_col, blocks[nb, 18, 18]) with blocks[k][r, c] = M[18 row + r, 18 col + c]."""
+        nb = _i64()
+        self.ctx.check(lib().hfpx_precond_blocks(self.ctx.h, self.h, ctypes.byref(nb), None, None, None))
+        r = np.empty(nb.value, dtype=np.int32)
+        c = np.empty(nb.value, dtype=np.int32)
+        b = np.empty(nb.value * 324)
+        self.ctx.check(lib().hfpx_precond_blocks(self.ctx.h, self.h, ctypes.byref(nb), _ip(r), _ip(c), _dp(b)))
+        return r, c, b.reshape(nb.value, 18, 18).transpose(0, 2, 1)
+
+    def close(self):
+        if self.h:
+            lib().hfpx_precond_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gmres(ctx, matrix: DeviceMatrix, b, precond: Precond = None, tol=1e-10, restart=50, max_iter=1000):
+    """Flexible GMRES on the FP64 matrix with a near-field preconditioner
+    (hfpx_gmres_precond); returns (x, SolveInfo)."""
+    x = np.array(b, dtype=np.float64, copy=True).reshape(-1)
+    info = SolveInfo()
+    rc = lib().hfpx_gmres_precond(ctx.h, matrix.h, precond.h if precond is not None else None, _dp(x), tol, restart,
+                                  max_iter, ctypes.byref(info))
+    if rc not in (HFPX_OK, HFPX_ERR_NOT_CONVERGED):
+        ctx.check(rc)
+    return x, info
+
+
+class Gnn:
+    """The learned preconditioner's graph network (hfpx_gnn)."""
+
+    def __init__(self, ctx, seed=0, path=None):
+        self.ctx = ctx
+        self.h = _V()
+        if path is not None:
+            ctx.check(lib().hfpx_gnn_load(ctx.h, os.fsencode(path), ctypes.byref(self.h)))
+        else:
+            ctx.check(lib().hfpx_gnn_create(ctx.h, seed, ctypes.byref(self.h)))
+
+    @property
+    def n_params(self):
+        return int(lib().hfpx_gnn_param_count(self.h))
+
+    def params(self):
+        p = np.empty(self.n_params, dtype=np.float32)
+        self.ctx.check(lib().hfpx_gnn_get_params(self.ctx.h, self.h, _fp(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self.ctx.check(lib().hfpx_gnn_set_params(self.ctx.h, self.h, _fp(p)))
+
+    def save(self, path):
+        self.ctx.check(lib().hfpx_gnn_save(self.ctx.h, self.h, os.fsencode(path)))
+
+    def gradients(self, graph):
+        loss = ctypes.c_double()
+        g = np.empty(self.n_params, dtype=np.float32)
+        self.ctx.check(lib().hfpx_gnn_gradients(self.ctx.h, self.h, graph.h, ctypes.byref(loss), _fp(g)))
+        return loss.value, g
+
+    def forward(self, graph):
+        on = np.empty((graph.n_nodes, 324), dtype=np.float32)
+        oe = np.empty((graph.n_edges, 324), dtype=np.float32)
+        self.ctx.check(lib().hfpx_gnn_forward(self.ctx.h, self.h, graph.h, _fp(on), _fp(oe)))
+        return on, oe
+
+    def train(self, graph, steps, lr):
+        losses = np.empty(steps)
+        self.ctx.check(lib().hfpx_gnn_train(self.ctx.h, self.h, graph.h, steps, lr,
+                                            losses.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return losses
+
+    def close(self):
+        if self.h:
+            lib().hfpx_gnn_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GnnGraph:
+    """The network's graph of a mesh and its assembled matrix (hfpx_gnn_graph)."""
+
+    def __init__(self, ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, shear_m=1.0, targets=True):
+        self.ctx = ctx
+        self.h = _V()
+        ctx.check(lib().hfpx_gnn_graph_create(ctx.h, dmesh.h, matrix.h, shear_m, int(targets), ctypes.byref(self.h)))
+        n, e = _i64(), _i64()
+        lib().hfpx_gnn_graph_dims(self.h, ctypes.byref(n), ctypes.byref(e))
+        self.n_nodes, self.n_edges = n.value, e.value
+        self.targets = targets
+
+    def data(self):
+        """dict of xn, xe (inputs as the network reads them), src, dst and, with targets, tn, te."""
+        n, E = self.n_nodes, self.n_edges
+        d = dict(xn=np.empty((n, 336), dtype=np.float32), xe=np.empty((E, 336), dtype=np.float32),
+                 src=np.empty(E, dtype=np.int32), dst=np.empty(E, dtype=np.int32))
+        tn = np.empty((n, 324), dtype=np.float32) if self.targets else None
+        te = np.empty((E, 324), dtype=np.float32) if self.targets else None
+        self.ctx.check(lib().hfpx_gnn_graph_data(self.ctx.h, self.h, _fp(d['xn']), _fp(d['xe']), _ip(d['src']),
+                                                 _ip(d['dst']), _fp(tn) if tn is not None else None,
+                                                 _fp(te) if te is not None else None))
+        if tn is not None:
+            d.update(tn=tn, te=te)
+        return d
+
+    def close(self):
+        if self.h:
+            lib().hfpx_gnn_graph_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -179,6 +179,86 @@ int hfpx_gemm_f16_update(hfpx_ctx *ctx, int64_t m, int64_t n, int64_t k, const v
  * (library kernels such as cuBLAS are not counted). */
 int64_t hfpx_ctx_launch_count(const hfpx_ctx *ctx);
 
+/* ---- near-field preconditioners for GMRES on the FP64 operator: no
+ * counterpart in the reference, which solves directly (il::LU,
+ * il/linear_algebra/dense/factorization/LU.h:79-120).  Block-sparse right
+ * preconditioners M ~ A^-1 on the pattern of element adjacency (elements
+ * sharing a vertex), built from the assembled FP64 matrix of a mesh without
+ * fixed DoF (n = 18 n_el, no volume-control border):
+ *   HFPX_PC_BLOCK_JACOBI   the inverses of the 18 x 18 diagonal blocks;
+ *   HFPX_PC_NEUMANN        those plus -D_i^-1 A_ij D_j^-1 for neighbours;
+ *   HFPX_PC_LOCAL_INVERSE  column j = (A[P(j), P(j)])^-1 e_j on the pattern
+ *                          P(j) of element j (the square-pattern sparse
+ *                          approximate inverse), by batched dense LU;
+ *   HFPX_PC_LEARNED        the Neumann blocks plus corrections predicted by
+ *                          the graph network `net` (hfpx_gnn_*).
+ * The matrix must hold the operator (not FP64 LU factors); shear_m scales
+ * the learned corrections. */
+typedef struct hfpx_precond hfpx_precond;
+typedef struct hfpx_gnn hfpx_gnn;
+typedef enum {
+  HFPX_PC_BLOCK_JACOBI = 0,
+  HFPX_PC_NEUMANN = 1,
+  HFPX_PC_LOCAL_INVERSE = 2,
+  HFPX_PC_LEARNED = 3
+} hfpx_pc_kind;
+int hfpx_precond_create(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix, int kind,
+                        const hfpx_gnn *net, double shear_m, hfpx_precond **precond);
+int hfpx_precond_destroy(hfpx_precond *precond);
+/* The blocks (18 x 18 column-major each) and their block row and column:
+ * call with null arrays to get n_blocks first. */
+int hfpx_precond_blocks(hfpx_ctx *ctx, const hfpx_precond *precond, int64_t *n_blocks, int32_t *block_row,
+                        int32_t *block_col, double *blocks);
+/* Flexible GMRES(restart) on the FP64 matrix (not factored), right-
+ * preconditioned by precond (null: none), for one right-hand side b (host,
+ * n; overwritten with x); stopping rule |b - A x|_inf / |b|_inf <= tol (<= 0
+ * selects 1e-12); restart <= 0 selects 50 (at most 64), max_iter <= 0 1000
+ * steps.  HFPX_ERR_NOT_CONVERGED with x returned anyway. */
+int hfpx_gmres_precond(hfpx_ctx *ctx, const hfpx_matrix *matrix, const hfpx_precond *precond, double *b,
+                       double tol, int restart, int max_iter, hfpx_solve_info *info);
+/* Same with b already in device memory. */
+int hfpx_gmres_precond_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, const hfpx_precond *precond,
+                              double *d_b, double tol, int restart, int max_iter, hfpx_solve_info *info);
+
+/* ---- the graph network of HFPX_PC_LEARNED: no counterpart in the
+ * reference.  One node per element, one directed edge per pair of elements
+ * sharing a vertex; 4 message-passing layers 64 wide, BF16 weights and
+ * activations with FP32 accumulation, trained on the GPU by the engine's own
+ * forward and backward kernels with Adam.  It predicts, for every block of
+ * the near-field pattern, the correction that takes the Neumann block to the
+ * exact local inverse's (in the frame and scale of the block's column
+ * element); training regresses on that correction (mean squared error). */
+typedef struct hfpx_gnn_graph hfpx_gnn_graph;
+/* A new network (seeded He initialisation; output heads zero, so it starts
+ * as the Neumann preconditioner). */
+int hfpx_gnn_create(hfpx_ctx *ctx, uint64_t seed, hfpx_gnn **net);
+int hfpx_gnn_destroy(hfpx_gnn *net);
+int64_t hfpx_gnn_param_count(const hfpx_gnn *net);
+/* FP32 master parameters, tensor by tensor (each weight row-major, in x
+ * out, then its bias): Wn, We, (Wm, Wu) per layer, Woe, Won. */
+int hfpx_gnn_get_params(hfpx_ctx *ctx, const hfpx_gnn *net, float *params);
+int hfpx_gnn_set_params(hfpx_ctx *ctx, hfpx_gnn *net, const float *params);
+int hfpx_gnn_save(hfpx_ctx *ctx, const hfpx_gnn *net, const char *path);
+int hfpx_gnn_load(hfpx_ctx *ctx, const char *path, hfpx_gnn **net);
+/* The graph of a mesh and its assembled FP64 matrix (n = 18 n_el): inputs,
+ * and with with_targets the training targets (exact local inverse). */
+int hfpx_gnn_graph_create(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix, double shear_m,
+                          int with_targets, hfpx_gnn_graph **graph);
+int hfpx_gnn_graph_destroy(hfpx_gnn_graph *graph);
+int hfpx_gnn_graph_dims(const hfpx_gnn_graph *graph, int64_t *n_nodes, int64_t *n_edges);
+/* Inputs (n_nodes x 336, n_edges x 336, as the network reads them), edge
+ * endpoints (src = neighbour i, dst = column element j) and targets
+ * (n_nodes x 324, n_edges x 324); any pointer may be null. */
+int hfpx_gnn_graph_data(hfpx_ctx *ctx, const hfpx_gnn_graph *graph, float *xn, float *xe, int32_t *src,
+                        int32_t *dst, float *tn, float *te);
+/* Outputs of one forward pass (n_nodes x 324, n_edges x 324). */
+int hfpx_gnn_forward(hfpx_ctx *ctx, const hfpx_gnn *net, hfpx_gnn_graph *graph, float *out_nodes,
+                     float *out_edges);
+/* Loss and the gradient of every parameter (layout of get_params), no update. */
+int hfpx_gnn_gradients(hfpx_ctx *ctx, hfpx_gnn *net, hfpx_gnn_graph *graph, double *loss, float *grads);
+/* `steps` Adam steps (learning rate lr) on one graph; losses (steps) may be null. */
+int hfpx_gnn_train(hfpx_ctx *ctx, hfpx_gnn *net, hfpx_gnn_graph *graph, int steps, double lr, double *losses);
+
 /* ---- stress: make_3dbem_stress_f_s, system_assembly.cpp:279-455.
  * dd is (6 n_el) x 3 nodal DD (row 6 e + node), pts 3 x n_pts, out n_pts x 6
  * [Sxx,Syy,Szz,Sxy,Sxz,Syz]; s_inf (6) is added.  Deterministic (no atomics). */
