@@ -201,7 +201,7 @@ def run_engine(args, rank, world, local_rank):
         e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A)
 
     # the other precision, once, for the speed-up and the opening error
-    other_s, rel_err = None, None
+    other_s, rel_err, x64 = None, None, None
     if args.compare and rank == 0:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         step(other, ev)
@@ -212,6 +212,17 @@ def run_engine(args, rank, world, local_rank):
         xm = x_main if other == engine.HFPX_LU_FP64 else x_other
         opening = lambda x: x[2::3]   # global z components of the nodal DD (tip free: 18 per element)
         rel_err = float(np.abs(opening(xm) - opening(x64)).max() / np.abs(opening(x64)).max())
+
+    # the learned form: assembly + the learned near-field preconditioner +
+    # GMRES(50) on the FP64 operator, timed after the main loop
+    learned = None
+    if rank == 0 and args.learned:
+        learned = run_learned(args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x)
+        if x64 is not None:
+            opening = lambda x: x[2::3]
+            learned['opening_rel_err_vs_fp64'] = float(np.abs(opening(learned.pop('_x')) - opening(x64)).max()
+                                                       / np.abs(opening(x64)).max())
+        learned.pop('_x', None)
 
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
@@ -273,7 +284,47 @@ def run_engine(args, rank, world, local_rank):
         for k in ('mixed', 'fp64'):
             c2.pop('_x_' + k, None)
         line['c2'] = c2
+    if learned is not None:
+        line['learned'] = learned
+        if other_s is not None and mode == engine.HFPX_LU_MIXED:
+            line['learned']['speedup_vs_plain_fp64'] = other_s / learned['value']
     return line
+
+
+def run_learned(args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x, reps=3):
+    """One step of the learned form: FP64 assembly into A, the learned
+    preconditioner (pattern, network inputs, BF16 forward pass, blocks), then
+    flexible GMRES(50) on the FP64 matrix to args.tol; best of `reps` after
+    one warm-up, CUDA events on the engine's stream."""
+    net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
+    info = engine.SolveInfo()
+    best = None
+    for r in range(reps + 1):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        engine.assemble_into(ctx, dm, dof, n, G, NU, A)
+        ev[1].record(stream)
+        pc = engine.Precond(ctx, dm, A, engine.HFPX_PC_LEARNED, net=net, shear_m=G)
+        ev[2].record(stream)
+        d_x.copy_(d_rhs)
+        torch.cuda.synchronize()
+        rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, ctypes.c_void_p(d_x.data_ptr()), args.tol, 50, 2000,
+                                         ctypes.byref(info))
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        pc.close()
+        if rc not in (engine.HFPX_OK, engine.HFPX_ERR_NOT_CONVERGED):
+            ctx.check(rc)
+        t = [ev[0].elapsed_time(ev[k]) for k in (1, 2, 3)]
+        if r > 0 and (best is None or t[2] < best[2]):
+            best = t
+    net.close()
+    return {'value': best[2] / 1e3, 'unit': UNIT, 'workload': 'FP64 assembly + learned preconditioner + GMRES(50) '
+                                                               f'on the FP64 operator to rel residual {args.tol:g}',
+            'phases_ms': {'assembly': best[0], 'preconditioner': best[1] - best[0], 'gmres': best[2] - best[1]},
+            'iterations': info.iterations, 'residual': info.residual, 'converged': bool(info.converged),
+            '_x': d_x.cpu().numpy()}
 
 
 def run_c2(args, ctx, engine, L, torch, stream, local_rank, reps=3):
@@ -516,6 +567,8 @@ def main():
                     help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
                          'FP32 factors')
     ap.add_argument('--no-compare', dest='compare', action='store_false')
+    ap.add_argument('--no-learned', dest='learned', action='store_false',
+                    help='skip the learned-preconditioner form (assembly + learned preconditioner + GMRES)')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--fit-sizes', default=','.join(str(x) for x in FIT_SIZES),
                     help='penny sizes (elements) the CPU reference is measured at and fitted from')

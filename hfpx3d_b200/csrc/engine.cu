@@ -532,7 +532,7 @@ int hfpx_gemm_f16_update(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const voi
   int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
   if (!err) return set_error(c, HFPX_ERR_NOMEM, "update status word");
   int rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "update status");
-  if (!rc) rc = tc_update_f16(c, c->stream, m, n, k, d_a, lda_k, d_b, ldb_k, d_c, ldc, d_alpha, err, 0);
+  if (!rc) rc = tc_update_f16(c, c->stream, m, n, k, d_a, lda_k, d_b, ldb_k, d_c, ldc, d_alpha, nullptr, err, 0);
   int h_err = 0;
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "update status");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "tensor-core update");

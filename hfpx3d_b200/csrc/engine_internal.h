@@ -121,7 +121,7 @@ enum : int {
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
-  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrCount
+  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrCount
 };
 
 // assembly.cu
@@ -160,13 +160,15 @@ int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, in
 int gmres_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol, int restart, int max_iter,
                 hfpx_solve_info* info);
 
-// gemm_tc.cu: C (m x n FP32, column-major, ldc) += alpha A B^T on tcgen05
-// tensor cores, A (m x k) and B (n x k) FP16 K-major with row strides lda_k,
-// ldb_k (multiples of 8), alpha = *d_alpha; d_err a zeroed failure word
-// (set when a pipeline wait times out); at most max_ctas CTAs (<= 0: all SMs).
+// gemm_tc.cu: C (m x n FP32, column-major, ldc) += alpha s_i (A B^T)_ij on
+// tcgen05 tensor cores, A (m x k) and B (n x k) FP16 K-major with row strides
+// lda_k, ldb_k (multiples of 8), alpha = *d_alpha, s_i = d_row_scale[i]
+// (null: 1); d_err a zeroed failure word (set when a pipeline wait times
+// out); at most max_ctas CTAs (<= 0: all SMs).
 bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void* B);
 int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
-                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, int* d_err, int max_ctas);
+                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, const float* d_row_scale,
+                  int* d_err, int max_ctas);
 
 // precond.cu: near-field preconditioners on the FP64 matrix (block-Jacobi,
 // first-order Neumann, exact local inverse, learned) and their product

@@ -21,8 +21,10 @@
 //     accumulators;
 //   * warps 2..9: epilogue.  Warp w reads TMEM lanes 32 (w % 4) .. + 31 (one
 //     output row per thread) and half of the 256 columns with tcgen05.ld, and
-//     applies C += alpha acc with coalesced 128-byte column segments.  The
-//     second accumulator lets the next tile's MMAs run during the epilogue.
+//     applies C += alpha s_i acc with coalesced 128-byte column segments (s_i
+//     an optional per-row scale: the LU keeps each row of L21 scaled into the
+//     normal FP16 range and undoes it here).  The second accumulator lets the
+//     next tile's MMAs run during the epilogue.
 // Every wait is bounded (%globaltimer); a wait that runs out sets the
 // failure word and an abort flag, every role leaves its loop, outstanding
 // copies and MMAs are waited for (bounded), TMEM is freed and the kernel
@@ -195,7 +197,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     update_tc_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      const __grid_constant__ CUtensorMap map_c, int prefetch_c, float* __restrict__ C, int64_t ldc,
                      int64_t m, int64_t n, int k, int group, const float* __restrict__ d_alpha,
-                     int* __restrict__ err) {
+                     const float* __restrict__ row_scale, int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       tm.coords(t, mb, nb);
       const int64_t row = mb * kBM + q * 32 + lane;
       const bool row_ok = row < m;
+      const float ra = row_ok && row_scale ? alpha * row_scale[row] : alpha;
       const int64_t col0 = nb * kBN + half * 128;
 #pragma unroll 1
       for (int ch = 0; ch < 4; ++ch) {
@@ -333,7 +336,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(p + ldc * (16 * h + j)) : 0.f;
 #pragma unroll
           for (int j = 0; j < 16; ++j)
-            if (16 * h + j < ncol) __stcg(p + ldc * (16 * h + j), fmaf(alpha, v[16 * h + j], c[j]));
+            if (16 * h + j < ncol) __stcg(p + ldc * (16 * h + j), fmaf(ra, v[16 * h + j], c[j]));
         }
       }
       tc_fence_before();
@@ -408,7 +411,8 @@ bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void
 }
 
 int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
-                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, int* d_err, int max_ctas) {
+                  const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, const float* d_row_scale,
+                  int* d_err, int max_ctas) {
   if (m <= 0 || n <= 0 || k <= 0) return HFPX_OK;
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || !tc_update_supported(lda_k, ldb_k, A, B))
     return set_error(c, HFPX_ERR_ARG, "tensor-core update: unsupported operand layout");
@@ -427,7 +431,7 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k,
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
   ++g_launches;
   update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, mc, prefetch_c, C, ldc, m, n, (int)k, raster_group(),
-                                                       d_alpha, d_err);
+                                                       d_alpha, d_row_scale, d_err);
   return check_cuda(c, cudaGetLastError(), "tensor-core update launch");
 }
 

@@ -313,7 +313,8 @@ def add_s_inf_to_3dbem_rhs(ctx, dmesh: DeviceMesh, dof_h, n_dof, s_inf, rhs=None
 class LU:
     """il::LU<il::Array2D<double>> (LU.h:46-120) on the device: factor on
     construction (dgetrf), solve(y) (dgetrs).  mode HFPX_LU_MIXED factors an
-    FP32 copy on TF32 tensor cores and refines in FP64."""
+    FP32 copy (FP16 tensor-core trailing updates with FP32 accumulation) and
+    refines in FP64."""
 
     def __init__(self, ctx, matrix: DeviceMatrix, mode=HFPX_LU_FP64):
         self.ctx, self.matrix, self.mode = ctx, matrix, mode

@@ -38,8 +38,11 @@ typedef enum {
 
 typedef enum {
   HFPX_LU_FP64 = 0,   /* FP64 LU in place, FP64 triangular solves */
-  HFPX_LU_MIXED = 1   /* FP32 LU of a copy (TF32 tensor-core trailing updates),
-                         FP64 iterative refinement against the FP64 matrix */
+  HFPX_LU_MIXED = 1   /* FP32 LU of a copy (trailing updates in FP16 with FP32
+                         accumulation on the engine's tcgen05 kernel, each row
+                         of L21 and U12 as a whole scaled by a power of two;
+                         TF32 in-panel products), FP64 iterative refinement
+                         against the FP64 matrix */
 } hfpx_lu_mode;
 
 typedef struct {

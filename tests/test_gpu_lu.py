@@ -1,5 +1,7 @@
 """Dense LU (il::LU / LAPACK dgetrf+dgetrs semantics) on the GPU: FP64 and mixed
-(TF32 tensor-core factorisation + FP64 refinement), against LAPACK (numpy)."""
+(FP32 factorisation whose trailing updates run in FP16 with FP32 accumulation
+on the engine's own tcgen05 kernel, L21 and U12 scaled by powers of two, plus
+FP64 refinement), against LAPACK (numpy)."""
 import numpy as np
 import pytest
 
