@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark: assembly + dense solve of the 72k-DoF penny crack on one B200.
+"""Benchmark: assembly + solve of the 72k-DoF penny crack on one B200.
 
 Workload (the configuration the headline metric is quoted on): unit-disk
 crack in z = 0, 4000 quadratic 6-node triangles (concentric rings, seeded
@@ -7,15 +7,17 @@ in-plane jitter <= 5 % of the ring spacing), N = 18 x 4000 = 72000 DoF,
 G = 1, nu = 0.35, collocation offset 0.125, no fixed tip DoF, uniform
 internal pressure 1 (sigma_zz = 1).  Synthetic seeded mesh (the reference has
 no mesher).  One step = assemble the FP64 collocation matrix in HBM
-(41.5 GB) + LU factorisation + solve to a relative residual <= 1e-10.
+(41.5 GB) + solve to a relative residual <= 1e-10 in one of three forms:
 
-  --mode mixed (default): FP32 copy of the matrix factored with FP16/TF32
-        tensor-core updates, then flexible GMRES on the FP64 matrix
-        preconditioned by those factors (--solver gmres, the default) or FP64
-        iterative refinement (--solver refine);
+  --mode learned (default): the learned near-field preconditioner (a graph
+        network over element adjacency, hfpx3d_b200/data/pc_gnn.bin) and
+        flexible GMRES(50) on the FP64 operator;
+  --mode mixed: the FP32 LU of a copy with FP16 tcgen05 trailing updates and
+        flexible GMRES on the FP64 operator preconditioned by it (--solver
+        gmres, the default) or FP64 iterative refinement (--solver refine);
   --mode fp64: the plain FP64 GPU path (in-place FP64 LU).
-The other mode is timed once after the timed loop for the speed-up and the
-opening error between the two (rel err target <= 1e-8).
+After the timed loop the plain FP64 path is timed once (speed-up, opening
+error against it; target rel err <= 1e-8), and the other fast form once.
 
 Multi-GPU: the path has no exchange step; --gpus N runs N independent
 replicas (one process per GPU, weak scaling); value = seconds per
@@ -57,6 +59,10 @@ def peaks():
 # the ncu capture of profiles/assemble_kernel_penny1000.md (4.6305 GB for an
 # 18 000 x 18 000 fill; traffic grows with the entries, so it scales by N^2)
 ASM_DRAM_BYTES_PER_ENTRY = 4.630537e9 / 18000 ** 2
+# DRAM bytes per matrix entry of one FP64 operator product (resid_partial_kernel
+# + resid_finish_kernel), from an ncu capture of the product alone; None until
+# measured
+RESID_DRAM_BYTES_PER_ENTRY = None
 
 
 class Clocks:
@@ -123,6 +129,83 @@ def replica_max(x, world, local_rank):
 
 
 # ---------------------------------------------------------------- engine arm
+class Forms:
+    """The three forms of one step on the device matrix A: FP64 assembly into
+    A, then
+      learned: the learned near-field preconditioner (hfpx_precond_create with
+               the trained network) and flexible GMRES(50) on the FP64
+               operator (hfpx_gmres_precond_device);
+      mixed:   the mixed LU (FP32 copy, FP16 tcgen05 updates) and flexible
+               GMRES on the FP64 matrix preconditioned by it (hfpx_gmres_device);
+      fp64:    the plain FP64 LU and its triangular solves.
+    Four CUDA events per step on the engine's stream: before the assembly,
+    after it, after the factorisation / preconditioner, after the solve."""
+
+    def __init__(self, args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x):
+        self.args, self.ctx, self.engine, self.L, self.torch, self.stream = args, ctx, engine, L, torch, stream
+        self.dm, self.dof, self.n, self.A, self.d_rhs, self.d_x = dm, dof, n, A, d_rhs, d_x
+        self.info = engine.SolveInfo()
+        self.net = None
+
+    def step(self, form, ev=None):
+        engine, L, ctx, A, torch = self.engine, self.L, self.ctx, self.A, self.torch
+        rec = (lambda k: ev[k].record(self.stream)) if ev else (lambda k: None)
+        rec(0)
+        engine.assemble_into(ctx, self.dm, self.dof, self.n, G, NU, A)
+        rec(1)
+        x = ctypes.c_void_p(self.d_x.data_ptr())
+        if form == 'learned':
+            if self.net is None:
+                self.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
+            pc = engine.Precond(ctx, self.dm, A, engine.HFPX_PC_LEARNED, net=self.net, shear_m=G)
+            rec(2)
+            with torch.cuda.stream(self.stream):
+                self.d_x.copy_(self.d_rhs)
+            rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, x, self.args.tol, 50, 2000, ctypes.byref(self.info))
+            rec(3)
+            pc.close()
+            ctx.check(rc)
+            return
+        mode = engine.HFPX_LU_MIXED if form == 'mixed' else engine.HFPX_LU_FP64
+        info_ = ctypes.c_int64()
+        ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
+        rec(2)
+        with torch.cuda.stream(self.stream):
+            self.d_x.copy_(self.d_rhs)
+        if form == 'mixed' and self.args.solver == 'gmres':
+            ctx.check(L.hfpx_gmres_device(ctx.h, A.h, x, self.args.tol, 50, 200, ctypes.byref(self.info)))
+        else:
+            ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, x, 1, self.n, self.args.tol, 50, ctypes.byref(self.info)))
+        rec(3)
+
+    def timed(self, form, reps):
+        """Best of `reps` steps after one warm-up: (phases ms, iterations, residual, x)."""
+        torch = self.torch
+        best = None
+        for r in range(reps + 1):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            torch.cuda.synchronize()
+            self.step(form, ev)
+            torch.cuda.synchronize()
+            t = [ev[0].elapsed_time(ev[k]) for k in (1, 2, 3)]
+            if r > 0 and (best is None or t[2] < best[2]):
+                best = t
+        return best, self.info.iterations, self.info.residual, self.d_x.cpu().numpy()
+
+    def close(self):
+        if self.net is not None:
+            self.net.close()
+
+
+def opening(x):
+    """Global z components of the nodal DD (no fixed DoF: 18 per element)."""
+    return x[2::3]
+
+
+def rel_opening_err(x, x64):
+    return float(np.abs(opening(x) - opening(x64)).max() / np.abs(opening(x64)).max())
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     from hfpx3d_b200 import build, engine
@@ -142,34 +225,11 @@ def run_engine(args, rank, world, local_rank):
     d_x = torch.empty_like(d_rhs)
     d_rhs.copy_(torch.from_numpy(rhs))
     A = engine.assemble(ctx, dm, dof, n, G, NU)
-    mode = engine.HFPX_LU_MIXED if args.mode == 'mixed' else engine.HFPX_LU_FP64
-    other = engine.HFPX_LU_FP64 if mode == engine.HFPX_LU_MIXED else engine.HFPX_LU_MIXED
-    info = engine.SolveInfo()
     L = engine.lib()
-
-    def step(m, ev=None):
-        if ev:
-            ev[0].record(stream)
-        engine.assemble_into(ctx, dm, dof, n, G, NU, A)
-        if ev:
-            ev[1].record(stream)
-        info_ = ctypes.c_int64()
-        ctx.check(L.hfpx_lu_factor(ctx.h, A.h, m, ctypes.byref(info_)))
-        if ev:
-            ev[2].record(stream)
-        d_x.copy_(d_rhs)
-        torch.cuda.synchronize()
-        if args.solver == 'gmres' and m == engine.HFPX_LU_MIXED:
-            ctx.check(L.hfpx_gmres_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), args.tol, 50, 200,
-                                          ctypes.byref(info)))
-        else:
-            ctx.check(L.hfpx_lu_solve_device(ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), 1, n, args.tol, 50,
-                                             ctypes.byref(info)))
-        if ev:
-            ev[3].record(stream)
+    F = Forms(args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x)
 
     for _ in range(args.warmup):
-        step(mode)
+        F.step(args.mode)
     torch.cuda.synchronize()
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     launches0 = L.hfpx_ctx_launch_count(ctx.h)
@@ -181,7 +241,7 @@ def run_engine(args, rank, world, local_rank):
         end = torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for k in range(args.steps):
-            step(mode, evs[k])
+            F.step(args.mode, evs[k])
         end.record(stream)
         torch.cuda.synchronize()
     launches = L.hfpx_ctx_launch_count(ctx.h) - launches0
@@ -191,41 +251,57 @@ def run_engine(args, rank, world, local_rank):
     t_sol = [e[2].elapsed_time(e[3]) for e in evs]
     ms = total_ms / args.steps
     x_main = d_x.cpu().numpy()
-    res_main, iters_main = info.residual, info.iterations
+    res_main, iters_main = F.info.residual, F.info.iterations
     ms = replica_max(ms, world, local_rank)
 
     # end to end through the C-ABI with host buffers (pinned), before the
     # seconds-long FP64 comparison heats the GPU
     e2e = None
     if rank == 0 and args.e2e_steps > 0:
-        e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A)
+        e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, args.mode, stream, torch, A, F)
 
-    # the other precision, once, for the speed-up and the opening error
+    # the plain FP64 GPU path, once, for the speed-up and the opening error
     other_s, rel_err, x64 = None, None, None
-    if args.compare and rank == 0:
+    if args.compare and rank == 0 and args.mode != 'fp64':
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        step(other, ev)
+        torch.cuda.synchronize()
+        F.step('fp64', ev)
         torch.cuda.synchronize()
         other_s = ev[0].elapsed_time(ev[3]) / 1e3
-        x_other = d_x.cpu().numpy()
-        x64 = x_other if other == engine.HFPX_LU_FP64 else x_main
-        xm = x_main if other == engine.HFPX_LU_FP64 else x_other
-        opening = lambda x: x[2::3]   # global z components of the nodal DD (tip free: 18 per element)
-        rel_err = float(np.abs(opening(xm) - opening(x64)).max() / np.abs(opening(x64)).max())
+        x64 = d_x.cpu().numpy()
+        rel_err = rel_opening_err(x_main, x64)
 
-    # the learned form: assembly + the learned near-field preconditioner +
-    # GMRES(50) on the FP64 operator, timed after the main loop
-    learned = None
-    if rank == 0 and args.learned:
-        learned = run_learned(args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x)
+    # the other fast form (mixed LU or learned), best of 2 after a warm-up
+    second = None
+    second_form = {'learned': 'mixed', 'mixed': 'learned'}.get(args.mode)
+    if rank == 0 and args.second and second_form:
+        t, it, res, xs = F.timed(second_form, 2)
+        second = {'value': t[2] / 1e3, 'unit': UNIT,
+                  'phases_ms': {'assembly': t[0], 'factor' if second_form == 'mixed' else 'preconditioner': t[1] - t[0],
+                                'solve': t[2] - t[1]},
+                  'iterations': it, 'residual': res}
         if x64 is not None:
-            opening = lambda x: x[2::3]
-            learned['opening_rel_err_vs_fp64'] = float(np.abs(opening(learned.pop('_x')) - opening(x64)).max()
-                                                       / np.abs(opening(x64)).max())
-        learned.pop('_x', None)
+            second['opening_rel_err_vs_fp64'] = rel_opening_err(xs, x64)
+            second['speedup_vs_plain_fp64'] = other_s / second['value']
+        if second_form == 'mixed':
+            flops_lu = 2.0 / 3.0 * float(n) ** 3
+            fac_s = (t[1] - t[0]) / 1e3
+            _, tensor_peak, peak_src = peaks()
+            second['roofline'] = {'kernel': 'LU factorisation (panel_ll_kernel chain + tcgen05 FP16 updates)',
+                                  'bound': 'tensor', 'achieved': flops_lu / fac_s / 1e12, 'peak': tensor_peak,
+                                  'unit': 'TFLOP/s', 'frac': flops_lu / fac_s / 1e12 / tensor_peak, 'traffic': None,
+                                  'peak_source': f'{peak_src} bf16_tflops_sustained'}
+
+    # the dominant kernel of the learned form: the FP64 operator product
+    # (resid_partial_kernel + resid_finish_kernel, one per GMRES step), timed
+    # alone on the engine's stream: N^2 8 bytes of matrix per launch
+    resid = None
+    if rank == 0:
+        resid = time_residual(ctx, engine, L, torch, stream, A, d_rhs, d_x, n)
 
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
+    F.close()
 
     if rank != 0:
         return None
@@ -234,28 +310,23 @@ def run_engine(args, rank, world, local_rank):
     fac_ms = statistics.mean(t_fac)
     bytes_asm = float(n) * n * 8
     flops_lu = 2.0 / 3.0 * float(n) ** 3
+    dtype = {'learned': 'f64 operator + bf16 network', 'mixed': 'f64+f32+f16', 'fp64': 'f64'}[args.mode]
     line = {
         'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
-        'vs_baseline': None, 'dtype': 'f64+f32+f16' if mode == engine.HFPX_LU_MIXED else 'f64',
+        'vs_baseline': None, 'dtype': dtype,
         'data': 'synthetic (seeded 4000-triangle penny mesh, pressure 1)',
-        'config': {'workload': f'penny crack {args.n_el} el, N={n} DoF, assembly + LU + solve to rel residual '
-                               f'{args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'mode': args.mode,
+        'config': {'workload': f'penny crack {args.n_el} el, N={n} DoF, assembly + {FORM_TEXT[args.mode]} to rel '
+                               f'residual {args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'form': args.mode,
                    'parallelism': f'replicas x{world}',
                    'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
-        'phases_ms': {'assembly': asm_ms, 'factor': statistics.mean(t_fac), 'solve': statistics.mean(t_sol)},
-        'steps_ms': {'factor': [round(t, 2) for t in t_fac], 'solve': [round(t, 2) for t in t_sol]},
-        'refinement': {'solver': args.solver, 'iterations': iters_main, 'residual': res_main},
+        'phases_ms': {'assembly': asm_ms, 'preconditioner' if args.mode == 'learned' else 'factor': fac_ms,
+                      'solve': statistics.mean(t_sol)},
+        'steps_ms': {'total': [round(a + b + c, 2) for a, b, c in zip(t_asm, t_fac, t_sol)],
+                     'solve': [round(t, 2) for t in t_sol]},
+        'solver': {'form': args.mode, 'iterations': iters_main, 'residual': res_main},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,
-        # the factorisation is ~80 % of the step: 2/3 N^3 flop over its CUDA-event time on the
-        # engine's stream, against the sustained dense tensor peak (the FP16 update and the
-        # BF16 GEMM of the peak run on the same pipe); the panel chain keeps it latency-bound
-        'roofline': {'kernel': 'LU factorisation (panel_ll_kernel chain + FP16/TF32 tensor-core updates)',
-                     'bound': 'tensor', 'achieved': flops_lu / (fac_ms / 1e3) / 1e12, 'peak': tensor_peak,
-                     'unit': 'TFLOP/s', 'frac': flops_lu / (fac_ms / 1e3) / 1e12 / tensor_peak,
-                     'traffic': None, 'peak_source': f'{peak_src} bf16_tflops_sustained',
-                     'algorithmic_flops': flops_lu},
         'roofline_assembly': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
                               'achieved': bytes_asm / (asm_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
                               'frac': bytes_asm / (asm_ms / 1e3) / 1e9 / hbm,
@@ -265,10 +336,26 @@ def run_engine(args, rank, world, local_rank):
         'clocks': clk.summary(),
         'e2e': e2e,
     }
+    if args.mode == 'learned' and resid is not None:
+        line['roofline'] = {'kernel': 'resid_partial_kernel + resid_finish_kernel (FP64 operator product, one per '
+                                      'GMRES step)', 'bound': 'hbm', 'achieved': resid['gbs'], 'peak': hbm,
+                            'unit': 'GB/s', 'frac': resid['gbs'] / hbm,
+                            'traffic': (RESID_DRAM_BYTES_PER_ENTRY * float(n) * n
+                                        if RESID_DRAM_BYTES_PER_ENTRY else None),
+                            'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm,
+                            'launch_ms': resid['ms']}
+    else:
+        line['roofline'] = {'kernel': 'LU factorisation (panel_ll_kernel chain + tcgen05 FP16 updates)',
+                            'bound': 'tensor', 'achieved': flops_lu / (fac_ms / 1e3) / 1e12, 'peak': tensor_peak,
+                            'unit': 'TFLOP/s', 'frac': flops_lu / (fac_ms / 1e3) / 1e12 / tensor_peak,
+                            'traffic': None, 'peak_source': f'{peak_src} bf16_tflops_sustained',
+                            'algorithmic_flops': flops_lu}
     if other_s is not None:
-        line['other_mode_s'] = other_s
-        line['speedup_vs_plain_fp64'] = (other_s / (ms / 1e3)) if mode == engine.HFPX_LU_MIXED else None
-        line['opening_rel_err_mixed_vs_fp64'] = rel_err
+        line['plain_fp64_s'] = other_s
+        line['speedup_vs_plain_fp64'] = other_s / (ms / 1e3)
+        line['opening_rel_err_vs_fp64'] = rel_err
+    if second is not None:
+        line[second_form] = second
     if args.cpu_baseline:
         cb = cpu_baseline(args)
         x_ref = cb.pop('_c2_x', None)
@@ -284,47 +371,31 @@ def run_engine(args, rank, world, local_rank):
         for k in ('mixed', 'fp64'):
             c2.pop('_x_' + k, None)
         line['c2'] = c2
-    if learned is not None:
-        line['learned'] = learned
-        if other_s is not None and mode == engine.HFPX_LU_MIXED:
-            line['learned']['speedup_vs_plain_fp64'] = other_s / learned['value']
     return line
 
 
-def run_learned(args, ctx, engine, L, torch, stream, dm, dof, n, A, d_rhs, d_x, reps=3):
-    """One step of the learned form: FP64 assembly into A, the learned
-    preconditioner (pattern, network inputs, BF16 forward pass, blocks), then
-    flexible GMRES(50) on the FP64 matrix to args.tol; best of `reps` after
-    one warm-up, CUDA events on the engine's stream."""
-    net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
-    info = engine.SolveInfo()
-    best = None
-    for r in range(reps + 1):
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        torch.cuda.synchronize()
-        ev[0].record(stream)
-        engine.assemble_into(ctx, dm, dof, n, G, NU, A)
-        ev[1].record(stream)
-        pc = engine.Precond(ctx, dm, A, engine.HFPX_PC_LEARNED, net=net, shear_m=G)
-        ev[2].record(stream)
-        d_x.copy_(d_rhs)
-        torch.cuda.synchronize()
-        rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, ctypes.c_void_p(d_x.data_ptr()), args.tol, 50, 2000,
-                                         ctypes.byref(info))
-        ev[3].record(stream)
-        torch.cuda.synchronize()
-        pc.close()
-        if rc not in (engine.HFPX_OK, engine.HFPX_ERR_NOT_CONVERGED):
-            ctx.check(rc)
-        t = [ev[0].elapsed_time(ev[k]) for k in (1, 2, 3)]
-        if r > 0 and (best is None or t[2] < best[2]):
-            best = t
-    net.close()
-    return {'value': best[2] / 1e3, 'unit': UNIT, 'workload': 'FP64 assembly + learned preconditioner + GMRES(50) '
-                                                               f'on the FP64 operator to rel residual {args.tol:g}',
-            'phases_ms': {'assembly': best[0], 'preconditioner': best[1] - best[0], 'gmres': best[2] - best[1]},
-            'iterations': info.iterations, 'residual': info.residual, 'converged': bool(info.converged),
-            '_x': d_x.cpu().numpy()}
+FORM_TEXT = {'learned': 'learned near-field preconditioner + GMRES(50) on the FP64 operator',
+             'mixed': 'mixed LU (FP16 tcgen05 updates) + GMRES on the FP64 operator',
+             'fp64': 'FP64 LU + triangular solves'}
+
+
+def time_residual(ctx, engine, L, torch, stream, A, d_b, d_x, n, reps=5):
+    """CUDA-event time of one FP64 operator product r = b - A x (the GMRES
+    step's pass over A), average of `reps` launches after one warm-up; the
+    41.5 GB matrix is larger than L2, so every launch reads it from HBM."""
+    d_r = torch.empty_like(d_x)
+    args = (ctx.h, A.h, ctypes.c_void_p(d_x.data_ptr()), ctypes.c_void_p(d_b.data_ptr()),
+            ctypes.c_void_p(d_r.data_ptr()))
+    ctx.check(L.hfpx_residual_device(*args))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.check(L.hfpx_residual_device(*args))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return {'ms': ms, 'gbs': float(n) * n * 8 / (ms / 1e3) / 1e9}
 
 
 def run_c2(args, ctx, engine, L, torch, stream, local_rank, reps=3):
@@ -363,10 +434,12 @@ def run_c2(args, ctx, engine, L, torch, stream, local_rank, reps=3):
     return out
 
 
-def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
-    """hfpx_mesh_create -> hfpx_assemble_into -> hfpx_rhs_sinf -> hfpx_lu_factor ->
-    hfpx_lu_solve from pinned host buffers, the solution read back each step
-    (the device matrix storage of the main loop is reused)."""
+def run_e2e(args, ctx, engine, L, nods, conn, dof, n, form, stream, torch, A, F):
+    """The same step through the C-ABI from pinned host buffers, the solution
+    read back each step: hfpx_mesh_create -> hfpx_assemble_into ->
+    hfpx_rhs_sinf -> (learned) hfpx_precond_create + hfpx_gmres_precond, or
+    (mixed / fp64) hfpx_lu_factor + hfpx_gmres / hfpx_lu_solve.  The device
+    matrix storage of the main loop and the loaded network are reused."""
     def pinned(a):
         t = torch.from_numpy(np.ascontiguousarray(a.reshape(-1, order='F'))).pin_memory()
         return t, t.numpy()
@@ -375,6 +448,8 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
     td, hd = pinned(dof)
     tr, hr = pinned(np.zeros(n))
     s = np.ascontiguousarray(S_ZZ)
+    if form == 'learned' and F.net is None:
+        F.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
     times = []
     for k in range(args.e2e_warmup + args.e2e_steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -386,13 +461,21 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, mode, stream, torch, A):
         ctx.check(L.hfpx_assemble_into(ctx.h, mh, engine._lp(hd), n, G, NU, 0, 0, A.h))
         hr[:] = 0.0
         ctx.check(L.hfpx_rhs_sinf(ctx.h, mh, engine._lp(hd), n, engine._dp(s), 1, engine._dp(hr), n))
-        info_ = ctypes.c_int64()
-        ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
         si = engine.SolveInfo()
-        if args.solver == 'gmres' and mode == engine.HFPX_LU_MIXED:
-            ctx.check(L.hfpx_gmres(ctx.h, A.h, engine._dp(hr), args.tol, 50, 200, ctypes.byref(si)))
+        if form == 'learned':
+            pc = ctypes.c_void_p()
+            ctx.check(L.hfpx_precond_create(ctx.h, mh, A.h, engine.HFPX_PC_LEARNED, F.net.h, G, ctypes.byref(pc)))
+            rc = L.hfpx_gmres_precond(ctx.h, A.h, pc, engine._dp(hr), args.tol, 50, 2000, ctypes.byref(si))
+            L.hfpx_precond_destroy(pc)
+            ctx.check(rc)
         else:
-            ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
+            info_ = ctypes.c_int64()
+            mode = engine.HFPX_LU_MIXED if form == 'mixed' else engine.HFPX_LU_FP64
+            ctx.check(L.hfpx_lu_factor(ctx.h, A.h, mode, ctypes.byref(info_)))
+            if args.solver == 'gmres' and form == 'mixed':
+                ctx.check(L.hfpx_gmres(ctx.h, A.h, engine._dp(hr), args.tol, 50, 200, ctypes.byref(si)))
+            else:
+                ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
         e1.record(stream)
         torch.cuda.synchronize()
         L.hfpx_mesh_destroy(mh)
@@ -560,15 +643,16 @@ def main():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='engine', choices=['engine', 'reference'])
-    ap.add_argument('--mode', default='mixed', choices=['mixed', 'fp64'])
+    ap.add_argument('--mode', default='learned', choices=['learned', 'mixed', 'fp64'],
+                    help='the form of the timed step (the other fast form is timed once beside it)')
     ap.add_argument('--n-el', type=int, default=4000)
     ap.add_argument('--tol', type=float, default=1e-10)
     ap.add_argument('--solver', default='gmres', choices=['refine', 'gmres'],
                     help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
                          'FP32 factors')
     ap.add_argument('--no-compare', dest='compare', action='store_false')
-    ap.add_argument('--no-learned', dest='learned', action='store_false',
-                    help='skip the learned-preconditioner form (assembly + learned preconditioner + GMRES)')
+    ap.add_argument('--no-second', dest='second', action='store_false',
+                    help='skip the timing of the other fast form (mixed beside learned, or learned beside mixed)')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--fit-sizes', default=','.join(str(x) for x in FIT_SIZES),
                     help='penny sizes (elements) the CPU reference is measured at and fitted from')

@@ -540,6 +540,23 @@ int hfpx_gemm_f16_update(hfpx_ctx* c, int64_t m, int64_t n, int64_t k, const voi
   return rc;
 }
 
+int hfpx_residual_device(hfpx_ctx* c, const hfpx_matrix* m, const double* d_x, const double* d_b, double* d_r) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!m || !d_x || !d_r) return set_error(c, HFPX_ERR_ARG, "null argument");
+  if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "the matrix holds FP64 LU factors, not the operator");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  const int64_t n = m->n;
+  double* part = (double*)ctx_scratch(c, kScrResidPart, sizeof(double) * n * resid_chunks(n));
+  unsigned long long* dmax = (unsigned long long*)ctx_scratch(c, kScrResidMax, sizeof(unsigned long long));
+  double* zero = nullptr;
+  if (!d_b) {
+    zero = (double*)ctx_scratch(c, kScrGmresZero, sizeof(double) * n);
+    if (zero) cudaMemsetAsync(zero, 0, sizeof(double) * n, c->stream);
+  }
+  if (!part || !dmax || (!d_b && !zero)) return set_error(c, HFPX_ERR_NOMEM, "residual buffers");
+  return residual_f64(c, m->d_a, m->ld, n, d_x, d_b ? d_b : zero, d_r, part, dmax);
+}
+
 int64_t hfpx_ctx_launch_count(const hfpx_ctx* c) { return c ? (int64_t)g_launches.load() : -1; }
 
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, int w, int32_t* d_piv,

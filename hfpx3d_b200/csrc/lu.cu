@@ -1229,27 +1229,36 @@ static inline int64_t ld16(int kb) { return ((int64_t)kb + 7) / 8 * 8; }
 // Per-row power-of-two scales of L21: row i's largest magnitude f 2^e
 // (f in [0.5, 1)) goes to [2^14, 2^15) in FP16, so small multipliers keep
 // their 11 bits instead of falling into FP16's subnormal range (below 6.1e-5)
-// or to zero (below 6e-8).  rs[i] = 2^(e - 15) undoes it in the update's
-// epilogue; rows of zeros keep scale 1.  One thread per row: a warp reads 32
-// consecutive rows of a column at a time (coalesced).
-__global__ void row_scale_kernel(const float* __restrict__ a, int64_t lda, int64_t rows, int cols,
-                                 float* __restrict__ rs) {
+// or to zero (below 6e-8); 2^(e - 15) undoes it in the update's epilogue.
+// The row maxima come from a 2-D grid (256 rows x 64 columns per CTA, one
+// row per thread: a warp reads 32 consecutive rows of a column at a time),
+// combined by atomicMax on the non-negative floats' bits.
+constexpr int kRowScaleCols = 64;
+__global__ void row_amax_kernel(const float* __restrict__ a, int64_t lda, int64_t rows, int cols,
+                                unsigned* __restrict__ amax) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows) return;
+  const int c0 = blockIdx.y * kRowScaleCols, c1 = min(cols, c0 + kRowScaleCols);
   float m = 0.f;
-  for (int c = 0; c < cols; ++c) m = fmaxf(m, fabsf(a[r + lda * c]));
+  for (int c = c0; c < c1; ++c) m = fmaxf(m, fabsf(a[r + lda * c]));
+  atomicMax(amax + r, __float_as_uint(m));
+}
+__device__ __forceinline__ float row_unscale(unsigned amax_bits) {
+  const float m = __uint_as_float(amax_bits);
   int e = 15;
   if (m > 0.f) frexpf(m, &e);
-  rs[r] = ldexpf(1.f, e - 15);
+  return ldexpf(1.f, e - 15);
 }
 
 // l16 (rows x ldk, K-major FP16) = L21 (rows x cols, column-major FP32, lda)
-// divided by its row scale rs (null: unscaled), transposed through a 32 x 33
-// shared tile so that the reads (down the columns) and the writes (along the
-// rows) are both coalesced.
+// divided by its row scale (from the row maxima amax; null: unscaled; the
+// CTAs of the first column tile store the scales in rs for the epilogue),
+// transposed through a 32 x 33 shared tile so that the reads (down the
+// columns) and the writes (along the rows) are both coalesced.
 __global__ void __launch_bounds__(256) to_half_rows_kernel(const float* __restrict__ a, int64_t lda, int64_t rows,
-                                                           int cols, const float* __restrict__ rs,
-                                                           __half* __restrict__ h, int64_t ldk) {
+                                                           int cols, const unsigned* __restrict__ amax,
+                                                           float* __restrict__ rs, __half* __restrict__ h,
+                                                           int64_t ldk) {
   __shared__ float t[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int c0 = blockIdx.y * 32;
@@ -1263,7 +1272,11 @@ __global__ void __launch_bounds__(256) to_half_rows_kernel(const float* __restri
   for (int i = ty; i < 32; i += 8) {
     const int64_t r = r0 + i;
     const int cc = c0 + tx;
-    if (r < rows && cc < cols) h[r * ldk + cc] = __float2half_rn(rs ? t[tx][i] / rs[r] : t[tx][i]);
+    if (r < rows && cc < cols) {
+      const float sc = amax ? row_unscale(amax[r]) : 1.f;
+      if (amax && c0 == 0 && tx == 0) rs[r] = sc;
+      h[r * ldk + cc] = __float2half_rn(t[tx][i] / sc);
+    }
   }
 }
 
@@ -1404,7 +1417,9 @@ struct LuWork {
   // main stream may take at this step)
   int* tc_err = nullptr;
   int gemm_ctas = 0;
-  // per-row scales of the FP16 L21 (own update only; cuBLAS takes it unscaled)
+  // per-row maxima and scales of the FP16 L21 (own update only; cuBLAS takes
+  // it unscaled)
+  unsigned* row_amax = nullptr;
   float* row_scale = nullptr;
   // moved rows of one base panel across the block panel: [2 kBaseW][nb]
   float* xtmp = nullptr;
@@ -1545,14 +1560,16 @@ template <class T>
 static void prepare_l21(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L21, int64_t lda) {
   if constexpr (sizeof(T) == 4) {
     if (wk.l16 && rest > 0) {
-      const bool scaled = wk.row_scale && own_update_enabled();
+      const bool scaled = wk.row_scale && wk.row_amax && own_update_enabled();
       if (scaled) {
+        cudaMemsetAsync(wk.row_amax, 0, sizeof(unsigned) * rest, l.s);
         ++g_launches;
-        row_scale_kernel<<<(unsigned)((rest + 255) / 256), 256, 0, l.s>>>(L21, lda, rest, kb, wk.row_scale);
+        row_amax_kernel<<<dim3((unsigned)((rest + 255) / 256), (unsigned)((kb + kRowScaleCols - 1) / kRowScaleCols)),
+                          256, 0, l.s>>>(L21, lda, rest, kb, wk.row_amax);
       }
       ++g_launches;
       to_half_rows_kernel<<<dim3((unsigned)((rest + 31) / 32), (unsigned)((kb + 31) / 32)), 256, 0, l.s>>>(
-          L21, lda, rest, kb, scaled ? wk.row_scale : nullptr, wk.l16, ld16(kb));
+          L21, lda, rest, kb, scaled ? wk.row_amax : nullptr, wk.row_scale, wk.l16, ld16(kb));
     }
   }
 }
@@ -1582,8 +1599,8 @@ static int update_gemm(hfpx_ctx* c, Lane l, LuWork<T>& wk, int kb, int64_t rest,
       const int64_t k16 = ld16(kb);
       const __half* B = wk.u16 + (size_t)k16 * c0;
       if (own_update_enabled() && wk.tc_err)
-        return tc_update_f16(c, l.s, rest, nc, kb, wk.l16, k16, B, k16, C, lda, wk.coef, wk.row_scale, wk.tc_err,
-                             wk.gemm_ctas);
+        return tc_update_f16(c, l.s, rest, nc, kb, wk.l16, k16, B, k16, C, lda, wk.coef,
+                             wk.row_amax ? wk.row_scale : nullptr, wk.tc_err, wk.gemm_ctas);
       gemm16_cublas(l, rest, nc, kb, wk.l16, k16, B, k16, C, lda, wk.coef);
       return 0;
     }
@@ -1882,7 +1899,8 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       wk.amax = (unsigned*)alloc(kScrAmax, sizeof(unsigned));
       wk.coef = (float*)alloc(kScrCoef, 2 * sizeof(float));
       wk.tc_err = (int*)alloc(kScrTcErr, sizeof(int));
-      wk.row_scale = (float*)alloc(kScrRowScale, sizeof(float) * (size_t)n);
+      wk.row_scale = (float*)alloc(kScrRowScale, sizeof(float) * 2 * (size_t)n);
+      if (wk.row_scale) wk.row_amax = reinterpret_cast<unsigned*>(wk.row_scale + n);
       if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) wk.l16 = wk.u16 = nullptr;
     }
   }

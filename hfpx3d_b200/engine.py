@@ -67,6 +67,7 @@ SIGNATURES = {
     'hfpx_gmres': (_int, [_V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres_device': (_int, [_V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
+    'hfpx_residual_device': (_int, [_V, _V, _V, _V, _V]),
     'hfpx_gemm_f16_update': (_int, [_V, _i64, _i64, _i64, _V, _i64, _V, _i64, _V, _i64, _V]),
     'hfpx_precond_create': (_int, [_V, _V, _V, _int, _V, _f64, ctypes.POINTER(_V)]),
     'hfpx_precond_destroy': (_int, [_V]),

@@ -178,6 +178,13 @@ int hfpx_lu_panel_factor_noalloc(hfpx_ctx *ctx, double *d_a, int64_t lda, int64_
 int hfpx_gemm_f16_update(hfpx_ctx *ctx, int64_t m, int64_t n, int64_t k, const void *d_a, int64_t lda_k,
                          const void *d_b, int64_t ldb_k, float *d_c, int64_t ldc, const float *d_alpha);
 
+/* r = b - A x with the FP64 matrix (device vectors of n; b null: r = -A x),
+ * the product of the refinement and of GMRES: no counterpart in the
+ * reference, which solves directly (LU.h:106-120).  Deterministic (fixed
+ * chunk sums, no atomics); queued on the context's stream, not synchronised. */
+int hfpx_residual_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, const double *d_x, const double *d_b,
+                         double *d_r);
+
 /* Number of this engine's own kernels launched on the context so far
  * (library kernels such as cuBLAS are not counted). */
 int64_t hfpx_ctx_launch_count(const hfpx_ctx *ctx);
