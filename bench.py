@@ -301,6 +301,8 @@ def run_engine(args, rank, world, local_rank):
 
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
+    # stresses at observation points (make_3dbem_stress_f_s) on the C1 penny
+    stress = run_stress(ctx, engine) if rank == 0 and args.stress else None
     F.close()
 
     if rank != 0:
@@ -371,7 +373,56 @@ def run_engine(args, rank, world, local_rank):
         for k in ('mixed', 'fp64'):
             c2.pop('_x_' + k, None)
         line['c2'] = c2
+    if stress is not None:
+        line['stress'] = stress
     return line
+
+
+def run_stress(ctx, engine, reps=5):
+    """Stress at observation points through the C-ABI with host buffers
+    (hfpx_stress, make_3dbem_stress_f_s system_assembly.cpp:279-455; and
+    hfpx_stress_batch for many load cases at once), on the seeded
+    121-element penny: 100 seeded points in [-1.5, 1.5]^3 (the C1 set-up),
+    one load case, and 64 load cases (pressures U[0.5, 2] and random in-situ
+    stresses).  Best of `reps` host wall times of the call."""
+    from hfpx3d_b200 import meshgen
+    nods, conn = meshgen.penny(121, seed=4)
+    ne = conn.shape[1]
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 0)
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    A = engine.assemble(ctx, dm, dof, n, G, NU)
+    rng = np.random.default_rng(64)
+    S = np.zeros((6, 64))
+    for kcase in range(64):
+        if kcase % 2 == 0:
+            S[2, kcase] = rng.uniform(0.5, 2.0)
+        else:
+            q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+            q = q * np.sign(np.diag(r))
+            st = q @ np.diag(rng.uniform(-1.0, 0.0, 3)) @ q.T
+            S[:, kcase] = [st[0, 0], st[1, 1], st[2, 2], st[0, 1], st[0, 2], st[1, 2]]
+    rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, S)
+    X = engine.LU(ctx, A, engine.HFPX_LU_FP64).solve(rhs)
+    dds = np.stack([engine.write_dd_vector_to_md(X[:, kcase], dof, ne) for kcase in range(64)])
+    pts = meshgen.observation_points(100, seed=5, nods=nods, conn=conn)
+
+    def best(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return min(ts)
+    t1 = best(lambda: engine.make_3dbem_stress_f_s(ctx, dm, G, NU, dds[0], pts, S[:, 0]))
+    t64 = best(lambda: engine.make_3dbem_stress_f_s_batch(ctx, dm, G, NU, dds, pts, S))
+    A.close()
+    dm.close()
+    npts = pts.shape[1]
+    return {'workload': f'penny {ne} el, {npts} seeded points in [-1.5, 1.5]^3; host buffers through the C-ABI',
+            'one_case_s': t1, 'points_per_s': npts / t1, 'pair_evaluations_per_s': npts * ne / t1,
+            'cases_64_s': t64, 'point_cases_per_s': 64 * npts / t64}
 
 
 FORM_TEXT = {'learned': 'learned near-field preconditioner + GMRES(50) on the FP64 operator',
@@ -651,6 +702,8 @@ def main():
                     help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
                          'FP32 factors')
     ap.add_argument('--no-compare', dest='compare', action='store_false')
+    ap.add_argument('--no-stress', dest='stress', action='store_false',
+                    help='skip the stress-at-points timing (121-element penny, 100 points, 1 and 64 load cases)')
     ap.add_argument('--no-second', dest='second', action='store_false',
                     help='skip the timing of the other fast form (mixed beside learned, or learned beside mixed)')
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')

@@ -36,6 +36,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include "engine_internal.h"
 
 namespace hfpx {
@@ -353,6 +354,256 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ------------------------------------------------------- 2-SM variant
+// A cluster of two CTAs on two SMs computes one 256 x 256 output tile with
+// tcgen05.mma.cta_group::2 (M 256, N 256, K 16).  CTA r of the pair (r =
+// %cluster_ctarank) holds rows [128 r, 128 r + 128) of the tile's A rows and
+// of its B rows (output columns) in its own shared memory at the same
+// offsets; the leader (r = 0) issues the MMAs, and each CTA's TMEM receives
+// its 128 output rows x all 256 columns.  Per k-block each SM loads 32 KB
+// instead of the 1-SM kernel's 48 KB for the same 128 x 256 x 64 of MMA
+// work: the operand traffic from L2 into shared memory, which bounds the
+// 1-SM kernel, drops by a third.
+//   * both CTAs' producers wait on their own `empty` barrier and load their
+//     halves with plain (non-multicast) TMA loads that complete on the
+//     leader's `full` barrier; the leader arms it for both halves;
+//   * the leader's MMA thread commits each stage to both CTAs' `empty`
+//     barriers and each finished accumulator to both CTAs' `tfull`;
+//   * both CTAs' epilogue warps arrive on the leader's `tempty` (the peer's
+//     remotely), so the leader reuses an accumulator only when both halves
+//     are read;
+//   * a cluster barrier after the set-up (barriers initialised, TMEM
+//     allocated in both CTAs) and before the teardown.
+constexpr int kStages2 = 6;
+constexpr uint32_t kHalf = 128 * kBK * 2;  // 16 KB: 128 rows x 64 FP16
+struct alignas(1024) TcSmem2 {
+  uint8_t a[kStages2][kHalf];
+  uint8_t b[kStages2][kHalf];
+  uint64_t full[kStages2], empty[kStages2], tfull[2], tempty[2], drain;
+  uint32_t tmem_base;
+  int abort;
+};
+constexpr size_t kSmemBytes2 = sizeof(TcSmem2) + 1024;
+// kind::f16, D FP32, A and B FP16 K-major, N 256, M 256 (the pair)
+constexpr uint32_t kIdesc2 = (1u << 4) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// TMA load into this CTA's shared memory completing on a barrier of the pair
+// (the leader's), given as a shared::cluster address
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void mma_f16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc2), "r"(accumulate)
+      : "memory");
+}
+// arrive on the barrier at this offset in both CTAs of the pair when the
+// MMAs issued so far have completed
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit_pair_local(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    update_tc2_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                      const __grid_constant__ CUtensorMap map_c, int prefetch_c, float* __restrict__ C, int64_t ldc,
+                      int64_t m, int64_t n, int k, int group, const float* __restrict__ d_alpha,
+                      const float* __restrict__ row_scale, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  TcSmem2& s = *reinterpret_cast<TcSmem2*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int64_t pair = blockIdx.x >> 1, pairs = gridDim.x >> 1;
+  const TileMap tm{(m + 255) / 256, (n + 255) / 256, group};
+  const int64_t tiles = tm.tiles_m * tm.tiles_n;
+  const int nk = (k + kBK - 1) / kBK;
+  volatile int* abort = &s.abort;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages2; ++i) {
+      mbar_init(&s.full[i], 1);
+      mbar_init(&s.empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&s.tfull[i], 1);
+      mbar_init(&s.tempty[i], 2 * kEpiWarps);
+    }
+    mbar_init(&s.drain, 1);
+    s.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+    if (prefetch_c) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_c)) : "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem_base;
+
+  if (warp == 0) {
+    // ------------------------------------------------------ producers (both)
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t armed = 0, armed_par = 0;  // leader: stages armed for both halves, and their phase
+      for (int64_t t = pair; t < tiles && !*abort; t += pairs) {
+        int64_t mb, nb;
+        tm.coords(t, mb, nb);
+        const int row0 = (int)(mb * 256 + 128 * rank), col0 = (int)(nb * 256 + 128 * rank);
+        if (prefetch_c) tma_prefetch_2d(&map_c, row0, (int)(nb * 256));
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.empty[stage], phase ^ 1u, abort, err, 0x201)) break;
+          if (leader) {
+            armed &= ~(1u << stage);
+            mbar_expect_tx(&s.full[stage], 4 * kHalf);  // A and B halves of both CTAs
+            armed |= 1u << stage;
+            armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
+          }
+          const uint32_t fb = cluster_addr(&s.full[stage], 0);
+          tma_load_2d_pair(s.a[stage], &map_a, fb, kb * kBK, row0);
+          tma_load_2d_pair(s.b[stage], &map_b, fb, kb * kBK, col0);
+          if (++stage == kStages2) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (*abort && leader)  // copies of both halves land on the leader's barriers
+        for (int i = 0; i < kStages2; ++i)
+          if (armed & (1u << i)) drain_phase(&s.full[i], (armed_par >> i) & 1u);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------- MMA (leader only)
+    if (lane == 0 && leader) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      bool issued = false;
+      for (int64_t t = pair; t < tiles && !*abort; t += pairs, ++it) {
+        const int acc = it & 1;
+        const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+        if (!wait_phase(&s.tempty[acc], acc_phase ^ 1u, abort, err, 0x202)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * kBN);
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.full[stage], phase, abort, err, 0x203)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int k16 = 0; k16 < kBK / 16; ++k16)
+            mma_f16_pair(d, smem_desc(s.a[stage], k16), smem_desc(s.b[stage], k16), (kb | k16) != 0);
+          issued = true;
+          mma_commit_pair(&s.empty[stage]);
+          if (++stage == kStages2) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit_pair(&s.tfull[acc]);
+      }
+      if (*abort && issued) {
+        mma_commit_pair_local(&s.drain);
+        drain_phase(&s.drain, 0);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------ epilogue (both)
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const float alpha = *d_alpha;
+    const uint32_t tempty_leader0 = cluster_addr(&s.tempty[0], 0), tempty_leader1 = cluster_addr(&s.tempty[1], 0);
+    int it = 0;
+    for (int64_t t = pair; t < tiles; t += pairs, ++it) {
+      const int acc = it & 1;
+      const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+      bool ok = wait_phase(&s.tfull[acc], acc_phase, abort, err, 0x204);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      int64_t mb, nb;
+      tm.coords(t, mb, nb);
+      const int64_t row = mb * 256 + 128 * rank + q * 32 + lane;
+      const bool row_ok = row < m;
+      const float ra = row_ok && row_scale ? alpha * row_scale[row] : alpha;
+      const int64_t col0 = nb * 256 + half * 128;
+#pragma unroll 1
+      for (int ch = 0; ch < 4; ++ch) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
+        const int64_t cb = col0 + ch * 32;
+        const int ncol = row_ok ? (int)min((int64_t)32, max((int64_t)0, n - cb)) : 0;
+        float* p = C + row + ldc * cb;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float c[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(p + ldc * (16 * h + j)) : 0.f;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (16 * h + j < ncol) __stcg(p + ldc * (16 * h + j), fmaf(ra, v[16 * h + j], c[j]));
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(acc ? tempty_leader1 : tempty_leader0);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  // the peer's copies and remote arrivals target the leader's barriers, and
+  // both CTAs read their TMEM: neither leaves before the other is done
+  cluster_sync_all();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
@@ -416,22 +667,36 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k,
   if (m <= 0 || n <= 0 || k <= 0) return HFPX_OK;
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX || !tc_update_supported(lda_k, ldb_k, A, B))
     return set_error(c, HFPX_ERR_ARG, "tensor-core update: unsupported operand layout");
+  // the 2-SM kernel unless HFPX_TC_2SM=0 (or a single SM may be used)
+  const int cap = max_ctas > 0 ? std::min(max_ctas, c->num_sms) : c->num_sms;
+  const char* env2 = std::getenv("HFPX_TC_2SM");
+  const bool two_sm = cap >= 2 && !(env2 && std::string(env2) == "0");
   CUtensorMap ma, mb, mc;
-  if (!make_map(&ma, A, m, k, lda_k, kBM) || !make_map(&mb, B, n, k, ldb_k, kBN))
+  if (!make_map(&ma, A, m, k, lda_k, kBM) || !make_map(&mb, B, n, k, ldb_k, two_sm ? 128 : kBN))
     return set_error(c, HFPX_ERR_CUDA, "tensor-core update: tensor map encoding failed");
   // C's prefetch needs a 16-byte aligned base and row stride (it only warms
   // L2: without it the epilogue reads C from HBM)
   int prefetch_c = (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ldc % 4 == 0 && make_map_c(&mc, C, m, n, ldc);
   if (!prefetch_c) std::memset(&mc, 0, sizeof(mc));
-  static PerDeviceOnce attr;
-  if (int rc = check_cuda(c, smem_attr_once(attr, update_tc_kernel, (int)kSmemBytes), "tensor-core update attribute"))
-    return rc;
-  const int64_t tiles = ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
-  const int cap = max_ctas > 0 ? std::min(max_ctas, c->num_sms) : c->num_sms;
-  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
   ++g_launches;
-  update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, mc, prefetch_c, C, ldc, m, n, (int)k, raster_group(),
-                                                       d_alpha, d_row_scale, d_err);
+  if (two_sm) {
+    static PerDeviceOnce attr2;
+    if (int rc = check_cuda(c, smem_attr_once(attr2, update_tc2_kernel, (int)kSmemBytes2),
+                            "tensor-core update attribute"))
+      return rc;
+    const int64_t tiles = ((m + 255) / 256) * ((n + 255) / 256);
+    const int64_t pairs = std::max<int64_t>(1, std::min<int64_t>(tiles, cap / 2));
+    update_tc2_kernel<<<(unsigned)(2 * pairs), kThreads, kSmemBytes2, st>>>(
+        ma, mb, mc, prefetch_c, C, ldc, m, n, (int)k, raster_group(), d_alpha, d_row_scale, d_err);
+  } else {
+    static PerDeviceOnce attr;
+    if (int rc = check_cuda(c, smem_attr_once(attr, update_tc_kernel, (int)kSmemBytes), "tensor-core update attribute"))
+      return rc;
+    const int64_t tiles = ((m + kBM - 1) / kBM) * ((n + kBN - 1) / kBN);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, cap));
+    update_tc_kernel<<<grid, kThreads, kSmemBytes, st>>>(ma, mb, mc, prefetch_c, C, ldc, m, n, (int)k, raster_group(),
+                                                         d_alpha, d_row_scale, d_err);
+  }
   return check_cuda(c, cudaGetLastError(), "tensor-core update launch");
 }
 

@@ -1243,22 +1243,26 @@ __global__ void row_amax_kernel(const float* __restrict__ a, int64_t lda, int64_
   for (int c = c0; c < c1; ++c) m = fmaxf(m, fabsf(a[r + lda * c]));
   atomicMax(amax + r, __float_as_uint(m));
 }
-__device__ __forceinline__ float row_unscale(unsigned amax_bits) {
-  const float m = __uint_as_float(amax_bits);
+// per row: rs = 2^(e - 15) (the epilogue's factor) and its exact inverse
+// (the conversion's), from the row maxima
+__global__ void row_scale_kernel(const unsigned* __restrict__ amax, int64_t rows, float* __restrict__ rs,
+                                 float* __restrict__ inv) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const float m = __uint_as_float(amax[r]);
   int e = 15;
   if (m > 0.f) frexpf(m, &e);
-  return ldexpf(1.f, e - 15);
+  rs[r] = ldexpf(1.f, e - 15);
+  inv[r] = ldexpf(1.f, 15 - e);
 }
 
 // l16 (rows x ldk, K-major FP16) = L21 (rows x cols, column-major FP32, lda)
-// divided by its row scale (from the row maxima amax; null: unscaled; the
-// CTAs of the first column tile store the scales in rs for the epilogue),
+// times the inverse row scale inv (a power of two, exact; null: unscaled),
 // transposed through a 32 x 33 shared tile so that the reads (down the
 // columns) and the writes (along the rows) are both coalesced.
 __global__ void __launch_bounds__(256) to_half_rows_kernel(const float* __restrict__ a, int64_t lda, int64_t rows,
-                                                           int cols, const unsigned* __restrict__ amax,
-                                                           float* __restrict__ rs, __half* __restrict__ h,
-                                                           int64_t ldk) {
+                                                           int cols, const float* __restrict__ inv,
+                                                           __half* __restrict__ h, int64_t ldk) {
   __shared__ float t[32][33];
   const int64_t r0 = (int64_t)blockIdx.x * 32;
   const int c0 = blockIdx.y * 32;
@@ -1272,11 +1276,7 @@ __global__ void __launch_bounds__(256) to_half_rows_kernel(const float* __restri
   for (int i = ty; i < 32; i += 8) {
     const int64_t r = r0 + i;
     const int cc = c0 + tx;
-    if (r < rows && cc < cols) {
-      const float sc = amax ? row_unscale(amax[r]) : 1.f;
-      if (amax && c0 == 0 && tx == 0) rs[r] = sc;
-      h[r * ldk + cc] = __float2half_rn(t[tx][i] / sc);
-    }
+    if (r < rows && cc < cols) h[r * ldk + cc] = __float2half_rn(inv ? t[tx][i] * inv[r] : t[tx][i]);
   }
 }
 
@@ -1420,7 +1420,8 @@ struct LuWork {
   // per-row maxima and scales of the FP16 L21 (own update only; cuBLAS takes
   // it unscaled)
   unsigned* row_amax = nullptr;
-  float* row_scale = nullptr;
+  float* row_scale = nullptr;   // n_rows scales, then n_rows inverse scales
+  int64_t n_rows = 0;
   // moved rows of one base panel across the block panel: [2 kBaseW][nb]
   float* xtmp = nullptr;
   // tournament candidates: [kTsluMaxCtas][kBaseW][kBaseW] rows, then labels
@@ -1567,9 +1568,14 @@ static void prepare_l21(Lane l, LuWork<T>& wk, int kb, int64_t rest, const T* L2
         row_amax_kernel<<<dim3((unsigned)((rest + 255) / 256), (unsigned)((kb + kRowScaleCols - 1) / kRowScaleCols)),
                           256, 0, l.s>>>(L21, lda, rest, kb, wk.row_amax);
       }
+      float* inv = scaled ? wk.row_scale + (size_t)wk.n_rows : nullptr;
+      if (scaled) {
+        ++g_launches;
+        row_scale_kernel<<<(unsigned)((rest + 255) / 256), 256, 0, l.s>>>(wk.row_amax, rest, wk.row_scale, inv);
+      }
       ++g_launches;
       to_half_rows_kernel<<<dim3((unsigned)((rest + 31) / 32), (unsigned)((kb + 31) / 32)), 256, 0, l.s>>>(
-          L21, lda, rest, kb, scaled ? wk.row_amax : nullptr, wk.row_scale, wk.l16, ld16(kb));
+          L21, lda, rest, kb, scaled ? inv : nullptr, wk.l16, ld16(kb));
     }
   }
 }
@@ -1899,8 +1905,9 @@ static int lu_factor(hfpx_ctx* c, T* A, int64_t lda, int64_t n, int32_t* piv, in
       wk.amax = (unsigned*)alloc(kScrAmax, sizeof(unsigned));
       wk.coef = (float*)alloc(kScrCoef, 2 * sizeof(float));
       wk.tc_err = (int*)alloc(kScrTcErr, sizeof(int));
-      wk.row_scale = (float*)alloc(kScrRowScale, sizeof(float) * 2 * (size_t)n);
-      if (wk.row_scale) wk.row_amax = reinterpret_cast<unsigned*>(wk.row_scale + n);
+      wk.row_scale = (float*)alloc(kScrRowScale, sizeof(float) * 3 * (size_t)n);
+      wk.n_rows = n;
+      if (wk.row_scale) wk.row_amax = reinterpret_cast<unsigned*>(wk.row_scale + 2 * n);
       if (!wk.l16 || !wk.u16 || !wk.amax || !wk.coef) wk.l16 = wk.u16 = nullptr;
     }
   }

@@ -1,5 +1,5 @@
-"""The engine's own tcgen05 tensor-core kernel for the mixed LU's trailing
-update (hfpx_gemm_f16_update; the GEMM of LAPACK dgetrf's blocked loop,
+"""The engine's own tcgen05 tensor-core kernels (the 2-SM pair and the 1-SM
+kernel) for the mixed LU's trailing update (hfpx_gemm_f16_update; the GEMM of LAPACK dgetrf's blocked loop,
 A22 -= L21 U12, that il::LU reaches at
 il/linear_algebra/dense/factorization/LU.h:87), against a plain PyTorch FP32
 reference of the same operation on the same FP16 operands.
@@ -14,6 +14,14 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=['2sm', '1sm'])
+def variant(request, monkeypatch):
+    """Both kernels: the 2-SM pair (cta_group::2, the default) and the 1-SM
+    kernel (HFPX_TC_2SM=0), chosen per call from the environment."""
+    monkeypatch.setenv('HFPX_TC_2SM', '1' if request.param == '2sm' else '0')
+    return request.param
 
 
 def run_update(ctx, m, n, k, lda_k=None, ldb_k=None, ldc=None, alpha=-0.75, seed=0, lu_like=False):
@@ -63,19 +71,19 @@ def run_update(ctx, m, n, k, lda_k=None, ldb_k=None, ldc=None, alpha=-0.75, seed
 
 @pytest.mark.parametrize('m,n,k', [(128, 256, 64), (1, 1, 8), (1000, 700, 2048), (5000, 300, 320),
                                    (333, 1027, 136), (129, 257, 72)])
-def test_update_matches_fp32_reference(ctx, m, n, k):
+def test_update_matches_fp32_reference(ctx, variant, m, n, k):
     err, untouched = run_update(ctx, m, n, k)
     assert err <= 1.0 and untouched, err
 
 
-def test_padded_strides_and_ldc(ctx):
+def test_padded_strides_and_ldc(ctx, variant):
     # K strides beyond k (padding filled with NaN) and C with ldc > m
     err, untouched = run_update(ctx, 700, 513, 200, lda_k=208, ldb_k=256, ldc=800)
     assert err <= 1.0 and untouched, err
 
 
 @pytest.mark.parametrize('m,n', [(20000, 2048), (8000, 8000)])
-def test_lu_shaped_update(ctx, m, n):
+def test_lu_shaped_update(ctx, variant, m, n):
     # tall-skinny L21 (m x 2048) times scaled U12 (2048 x n), as one LU step
     err, untouched = run_update(ctx, m, n, 2048, lu_like=True, seed=m)
     assert err <= 1.0 and untouched, err
