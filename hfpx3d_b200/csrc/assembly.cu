@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
                                                          const int32_t* __restrict__ dof,
                                                          double G, double nu, int is_dd_local,
                                                          double* __restrict__ A, int64_t ld,
+                                                         float* __restrict__ Af,
                                                          int* __restrict__ status) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
@@ -404,6 +405,12 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
 #pragma unroll
           for (int q = 0; q < 3; ++q)
             if (trow[q] >= 0) colp[trow[q]] = wb[lane + 32 * q];
+          if (Af) {
+            float* colf = Af + (int64_t)col * ld;
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+              if (trow[q] >= 0) colf[trow[q]] = (float)wb[lane + 32 * q];
+          }
         }
         __syncwarp();
       }
@@ -422,7 +429,10 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
         const int32_t col = sm.cols[3 * a + j];
         if (col < 0) continue;
         for (int i = 0; i < 3; ++i)
-          if (rows[i] >= 0) A[(int64_t)col * ld + rows[i]] = B[i][j];
+          if (rows[i] >= 0) {
+            A[(int64_t)col * ld + rows[i]] = B[i][j];
+            if (Af) Af[(int64_t)col * ld + rows[i]] = (float)B[i][j];
+          }
       }
     });
   }
@@ -441,7 +451,7 @@ void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int6
 }
 
 void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
-                     int is_dd_local, double* d_a, int64_t ld, int* d_status, cudaStream_t s) {
+                     int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s) {
   gl_host_init(s);
   const size_t smem = sizeof(AsmSmem);
   static PerDeviceOnce attr0, attr1;
@@ -451,9 +461,9 @@ void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, dou
   const dim3 grid((unsigned)((6 * n_el + kTile - 1) / kTile), (unsigned)n_el);
   const ElemRec* e = static_cast<const ElemRec*>(d_elem);
   ++g_launches;
-  assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_status);
+  assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status);
   ++g_launches;
-  assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_status);
+  assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status);
 }
 
 // ----------------------------------------------------------- VC border

@@ -246,6 +246,8 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
 
 int hfpx_mesh_destroy(hfpx_mesh* m) {
   if (!m) return HFPX_OK;
+  if (m->gnn_graph) gnn_graph_release(m->gnn_graph);
+  m->pattern.reset();
   if (m->d_elem) cudaFree(m->d_elem);
   delete m;
   return HFPX_OK;
@@ -283,7 +285,11 @@ static int assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_
   if (rc) return rc;
   m->factored = 0;
   m->info = 0;
-  launch_assemble(mesh->d_elem, mesh->n_el, dd, G, nu, is_dd_local, m->d_a, m->ld, c->d_flags, c->stream);
+  // a matrix that has an FP32 working copy gets it written in the same pass
+  // (not with the volume-control border, which only the FP64 matrix takes)
+  float* f = vc_border ? nullptr : m->d_f;
+  launch_assemble(mesh->d_elem, mesh->n_el, dd, G, nu, is_dd_local, m->d_a, m->ld, f, c->d_flags, c->stream);
+  m->f32_current = f != nullptr;
   if (vc_border) launch_vc_border(mesh->d_elem, mesh->n_el, dd, n_dof, is_dd_local, m->d_a, m->ld, c->stream);
   rc = check_cuda(c, cudaGetLastError(), "assembly launch");
   int flags[2] = {0, 0};

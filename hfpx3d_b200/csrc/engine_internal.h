@@ -3,6 +3,7 @@
 #include <atomic>
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -31,16 +32,6 @@ struct hfpx_ctx {
   unsigned long long trsv_base = 0;
 };
 
-struct hfpx_mesh {
-  int64_t n_el = 0;
-  void* d_elem = nullptr;          // ElemRec[n_el]
-  // host copies for the near-field pattern and the learned preconditioner's
-  // geometry features: vertex ids (3 per element) and vertex coordinates
-  // (9 per element, vertex j's x, y, z at 3 j)
-  std::vector<int64_t> h_vid;
-  std::vector<double> h_vert;
-};
-
 // Near-field pattern of a mesh: the elements sharing a vertex with element j
 // are its neighbours N(j); the pattern of block column j is P(j) = {j} + N(j).
 // Blocks of a near-field operator are stored column by column: column j's
@@ -57,12 +48,28 @@ struct NearPattern {
   int64_t blocks() const { return n_el + n_edges; }
 };
 
+struct hfpx_gnn_graph;
+
+struct hfpx_mesh {
+  int64_t n_el = 0;
+  void* d_elem = nullptr;          // ElemRec[n_el]
+  // host copies for the near-field pattern and the learned preconditioner's
+  // geometry features: vertex ids (3 per element) and vertex coordinates
+  // (9 per element, vertex j's x, y, z at 3 j)
+  std::vector<int64_t> h_vid;
+  std::vector<double> h_vert;
+  // built on first use and kept with the mesh: the near-field pattern and the
+  // learned preconditioner's graph (geometry inputs and buffers)
+  std::shared_ptr<NearPattern> pattern;
+  hfpx_gnn_graph* gnn_graph = nullptr;
+};
+
 struct hfpx_gnn;
 
 struct hfpx_precond {
   int kind = 0;
   int64_t n_el = 0, n = 0;
-  NearPattern pat;
+  std::shared_ptr<NearPattern> pat;   // the mesh's
   double* d_blocks = nullptr;      // blocks() x 18 x 18, each column-major
   double* d_dinv = nullptr;        // inverses of the diagonal blocks, n_el x 18 x 18
 };
@@ -71,6 +78,7 @@ struct hfpx_matrix {
   int64_t n = 0, ld = 0;
   double* d_a = nullptr;           // FP64 n x n column-major (ld)
   float* d_f = nullptr;            // FP32 working copy (mixed mode), ld
+  int f32_current = 0;             // d_f holds the operator (written by the assembly), not factors
   int32_t* d_piv = nullptr;        // pivots (0-based global rows), n
   int factored = 0;                // 0 none, 1 fp64 in place, 2 fp32 copy
   int64_t info = 0;
@@ -129,8 +137,9 @@ size_t elem_record_bytes();
 void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int64_t* d_conn,
                                int64_t ld_conn, int64_t n_el, double beta, void* d_elem,
                                cudaStream_t s);
+// d_f (optional): an FP32 copy of the matrix written in the same pass
 void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
-                     int is_dd_local, double* d_a, int64_t ld, int* d_general_count,
+                     int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_general_count,
                      cudaStream_t s);
 void launch_vc_border(const void* d_elem, int64_t n_el, const int32_t* d_dof, int64_t n_dof,
                       int is_dd_local, double* d_a, int64_t ld, cudaStream_t s);
@@ -174,6 +183,9 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, 
 // first-order Neumann, exact local inverse, learned) and their product
 int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p);
 void free_pattern(NearPattern* p);
+// the mesh's pattern, built on first use (null on failure)
+std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh);
+void gnn_graph_release(hfpx_gnn_graph* g);
 int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z);
 int gather_diag_inverse(hfpx_ctx* c, const double* A, int64_t lda, int64_t n_el, double* dinv, int* d_err);
 int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, const double* dinv, double* blocks,
@@ -184,8 +196,12 @@ int gnn_correct_blocks(hfpx_ctx* c, const hfpx_gnn* net, const hfpx_mesh* mesh, 
 int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks);
 // lu.cu: flexible GMRES on the FP64 matrix with a right preconditioner
 // apply(v, z): z = M v (FP64, device), for one right-hand side
+// Af (optional): the FP32 copy of A; products use it once the rotated
+// residual is below relax_below (relative), with an FP64 residual at the end
+// of such a cycle
 int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
-               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply);
+               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply,
+               const float* Af = nullptr, double relax_below = 0.0);
 
 // solve.cu: one right-hand side of the refinement
 int trsv_tiles(int64_t n);
@@ -195,5 +211,8 @@ int trsv_status(hfpx_ctx* c);
 int resid_chunks(int64_t n);
 int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
                  double* part, unsigned long long* d_max);
+// the same with the FP32 copy of the matrix (products and sums in FP64)
+int residual_f32m(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
+                  double* part, unsigned long long* d_max);
 int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max);
 }  // namespace hfpx

@@ -85,7 +85,7 @@ struct hfpx_gnn {
 // A graph of one mesh: structure, inputs, optional targets, activations.
 struct hfpx_gnn_graph {
   int64_t n_nodes = 0, n_edges = 0;
-  NearPattern pat;
+  std::shared_ptr<NearPattern> pat;   // the mesh's
   float* d_size = nullptr;        // s_j
   float* d_rot = nullptr;         // R_j (9, row-major: rows e1, e2, e3)
   double* d_dinv = nullptr;       // D_j^-1
@@ -609,15 +609,15 @@ int forward(hfpx_ctx* c, const hfpx_gnn* net, hfpx_gnn_graph* g) {
   lin(c, E, kH, kFE, g->xe, true, kFE, w(1), b(1), g->z, true, kH, true, false);
   for (int l = 0; l < kLayers; ++l) {
     g_launches += 3;
-    gather3_kernel<<<blocks_for(E * 3 * kH), 256, 0, c->stream>>>(E, g->pat.d_idx, g->pat.d_dst, g->h[l], g->z,
+    gather3_kernel<<<blocks_for(E * 3 * kH), 256, 0, c->stream>>>(E, g->pat->d_idx, g->pat->d_dst, g->h[l], g->z,
                                                                    g->cm[l]);
     lin(c, E, kH, 3 * kH, g->cm[l], true, 3 * kH, w(2 + 2 * l), b(2 + 2 * l), g->m[l], true, kH, true, false);
-    mean_concat_kernel<<<blocks_for(n * kH), 256, 0, c->stream>>>(n, g->pat.d_ptr, g->h[l], g->m[l], g->cu[l]);
+    mean_concat_kernel<<<blocks_for(n * kH), 256, 0, c->stream>>>(n, g->pat->d_ptr, g->h[l], g->m[l], g->cu[l]);
     lin(c, n, kH, 2 * kH, g->cu[l], true, 2 * kH, w(3 + 2 * l), b(3 + 2 * l), g->u[l], true, kH, true, false);
     residual_kernel<<<blocks_for(n * kH), 256, 0, c->stream>>>(n * kH, g->h[l], g->u[l], g->h[l + 1]);
   }
   ++g_launches;
-  gather3_kernel<<<blocks_for(E * 3 * kH), 256, 0, c->stream>>>(E, g->pat.d_idx, g->pat.d_dst, g->h[kLayers], g->z,
+  gather3_kernel<<<blocks_for(E * 3 * kH), 256, 0, c->stream>>>(E, g->pat->d_idx, g->pat->d_dst, g->h[kLayers], g->z,
                                                                  g->ce);
   const int te = 2 + 2 * kLayers, tn = te + 1;
   lin(c, E, kOut, 3 * kH, g->ce, true, 3 * kH, w(te), b(te), g->oe, false, kOut, false, false);
@@ -648,7 +648,7 @@ int backward(hfpx_ctx* c, hfpx_gnn* net, hfpx_gnn_graph* g) {
   lin_dw(c, g, n, kOut, kH, g->h[kLayers], kH, g->don, kOut, gw(tn), gb(tn));
   lin_dx(c, n, kOut, kH, g->don, kOut, w(tn), g->dh, kH, false);
   ++g_launches;
-  scatter3_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat.d_ptr, g->pat.d_rev, g->dce,
+  scatter3_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat->d_ptr, g->pat->d_rev, g->dce,
                                                                            g->dh, g->dz, 0);
   for (int l = kLayers - 1; l >= 0; --l) {
     // h[l+1] = h[l] + u[l]: dh is dL/dh[l+1]
@@ -659,13 +659,13 @@ int backward(hfpx_ctx* c, hfpx_gnn* net, hfpx_gnn_graph* g) {
     lin_dw(c, g, n, kH, 2 * kH, g->cu[l], 2 * kH, g->du, kH, gw(3 + 2 * l), gb(3 + 2 * l));
     lin_dx(c, n, kH, 2 * kH, g->du, kH, w(3 + 2 * l), g->dcu, 2 * kH, false);
     g_launches += 2;
-    mean_concat_bwd_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat.d_ptr, g->pat.d_dst,
+    mean_concat_bwd_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat->d_ptr, g->pat->d_dst,
                                                                                     g->dcu, g->dh2, g->dm);
     relu_bwd_kernel<<<blocks_for(E * kH), 256, 0, c->stream>>>(E * kH, g->m[l], g->dm);
     lin_dw(c, g, E, kH, 3 * kH, g->cm[l], 3 * kH, g->dm, kH, gw(2 + 2 * l), gb(2 + 2 * l));
     lin_dx(c, E, kH, 3 * kH, g->dm, kH, w(2 + 2 * l), g->dce, 3 * kH, false);
     ++g_launches;
-    scatter3_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat.d_ptr, g->pat.d_rev,
+    scatter3_kernel<<<blocks_for(std::max(n, E) * kH), 256, 0, c->stream>>>(n, E, g->pat->d_ptr, g->pat->d_rev,
                                                                              g->dce, g->dh2, g->dz, 1);
     std::swap(g->dh, g->dh2);
   }
@@ -724,13 +724,20 @@ int net_upload(hfpx_ctx* c, hfpx_gnn* net, const float* host) {
 
 void graph_destroy(hfpx_gnn_graph* g);
 
-int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, double G, bool with_targets,
-                 hfpx_gnn_graph** out) {
+// The mesh-only part of a graph: the pattern, the frames and sizes, the
+// geometry columns of the inputs (the operator columns are filled per
+// matrix by graph_fill).
+int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
   *out = nullptr;
   hfpx_gnn_graph* g = new (std::nothrow) hfpx_gnn_graph;
   if (!g) return set_error(c, HFPX_ERR_NOMEM, "graph");
-  int rc = build_pattern(c, mesh, &g->pat);
-  const int64_t n = mesh->n_el, E = g->pat.n_edges;
+  g->pat = mesh_pattern(c, mesh);
+  if (!g->pat) {
+    delete g;
+    return set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
+  }
+  int rc = 0;
+  const int64_t n = mesh->n_el, E = g->pat->n_edges;
   g->n_nodes = n;
   g->n_edges = E;
   // host geometry: frames, sizes, features
@@ -756,10 +763,10 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
       if (a > b) std::swap(a, b);
       if (edge_count[{a, b}] == 1) ++boundary;
     }
-    const int deg = g->pat.ptr[j + 1] - g->pat.ptr[j];
+    const int deg = g->pat->ptr[j + 1] - g->pat->ptr[j];
     double curv = 0.0;
-    for (int32_t e = g->pat.ptr[j]; e < g->pat.ptr[j + 1]; ++e) {
-      const Geo& p = geo[g->pat.idx[e]];
+    for (int32_t e = g->pat->ptr[j]; e < g->pat->ptr[j + 1]; ++e) {
+      const Geo& p = geo[g->pat->idx[e]];
       curv += 1.0 - (p.r[6] * q.r[6] + p.r[7] * q.r[7] + p.r[8] * q.r[8]);
     }
     curv = deg ? curv / deg : 0.0;
@@ -768,8 +775,8 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
     for (int k = 0; k < kGeoN; ++k) xn[(size_t)j * kFN + k] = __float2bfloat16_rn(f[k]);
     for (int k = 0; k < 9; ++k) rot[9 * j + k] = (float)q.r[k];
     size[j] = (float)q.s;
-    for (int32_t e = g->pat.ptr[j]; e < g->pat.ptr[j + 1]; ++e) {
-      const int64_t i = g->pat.idx[e];
+    for (int32_t e = g->pat->ptr[j]; e < g->pat->ptr[j + 1]; ++e) {
+      const int64_t i = g->pat->idx[e];
       const Geo& p = geo[i];
       double d[3] = {(p.c[0] - q.c[0]) / q.s, (p.c[1] - q.c[1]) / q.s, (p.c[2] - q.c[2]) / q.s}, dl[3], nl[3], el[3];
       rot_apply(q.r, d, dl);
@@ -786,35 +793,59 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
   }
   g->d_size = galloc<float>(g, n, &rc, c);
   g->d_rot = galloc<float>(g, 9 * n, &rc, c);
-  g->d_dinv = galloc<double>(g, 324 * n, &rc, c);
-  g->d_neu = galloc<double>(g, 324 * (size_t)g->pat.blocks(), &rc, c);
   g->xn = galloc<__nv_bfloat16>(g, (size_t)n * kFN, &rc, c);
   g->xe = galloc<__nv_bfloat16>(g, (size_t)E * kFE, &rc, c);
-  double* target = nullptr;
-  if (with_targets) {
-    g->tn = galloc<float>(g, (size_t)n * kOut, &rc, c);
-    g->te = galloc<float>(g, (size_t)E * kOut, &rc, c);
-    target = galloc<double>(g, 324 * (size_t)g->pat.blocks(), &rc, c);
-  }
-  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
-  if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_size, size.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "sizes");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_rot, rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, c->stream), "frames");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xn, xn.data(), sizeof(__nv_bfloat16) * xn.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xe, xe.data(), sizeof(__nv_bfloat16) * xe.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
-  if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
-  if (!rc) rc = check_cuda(c, cudaMemsetAsync(g->d_neu, 0, sizeof(double) * 324 * g->pat.blocks(), c->stream), "blocks");
-  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, n, g->d_dinv, err);
-  if (!rc) rc = neumann_blocks(c, m->d_a, m->ld, g->pat, g->d_dinv, g->d_neu, true);
-  if (!rc && target) rc = local_inverse_blocks(c, m->d_a, m->ld, g->pat, target);
-  if (!rc) {
-    ++g_launches;
-    inputs_kernel<<<(unsigned)g->pat.blocks(), 352, 0, c->stream>>>(m->d_a, m->ld, n, g->pat.d_ptr, g->pat.d_idx,
-                                                                    g->pat.d_dst, g->d_dinv, g->d_neu, target,
-                                                                    g->d_rot, g->d_size, G, g->xn, g->xe, g->tn,
-                                                                    g->te);
-    rc = check_cuda(c, cudaGetLastError(), "network inputs");
+  // the host vectors are pageable: finish the copies before they go
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "graph inputs");
+  if (rc) {
+    graph_destroy(g);
+    return rc;
   }
+  *out = g;
+  return 0;
+}
+
+// The operator columns of the inputs (and, with a target, the training
+// targets) of matrix m: dinv and neu are the diagonal-block inverses and the
+// Neumann blocks of m in the pattern's order.
+int graph_fill(hfpx_ctx* c, hfpx_gnn_graph* g, const hfpx_matrix* m, double G, const double* dinv, const double* neu,
+               const double* target) {
+  ++g_launches;
+  inputs_kernel<<<(unsigned)g->pat->blocks(), 352, 0, c->stream>>>(
+      m->d_a, m->ld, g->n_nodes, g->pat->d_ptr, g->pat->d_idx, g->pat->d_dst, dinv, neu, target, g->d_rot, g->d_size,
+      G, g->xn, g->xe, target ? g->tn : nullptr, target ? g->te : nullptr);
+  return check_cuda(c, cudaGetLastError(), "network inputs");
+}
+
+// A training graph: its own diagonal inverses, Neumann blocks and the exact
+// local inverse as the target.
+int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, double G, bool with_targets,
+                 hfpx_gnn_graph** out) {
+  *out = nullptr;
+  hfpx_gnn_graph* g = nullptr;
+  int rc = graph_prepare(c, mesh, &g);
+  if (rc) return rc;
+  const int64_t n = g->n_nodes, E = g->n_edges, nb = g->pat->blocks();
+  g->d_dinv = galloc<double>(g, 324 * n, &rc, c);
+  g->d_neu = galloc<double>(g, 324 * (size_t)nb, &rc, c);
+  double* target = nullptr;
+  if (with_targets) {
+    g->tn = galloc<float>(g, (size_t)n * kOut, &rc, c);
+    g->te = galloc<float>(g, (size_t)E * kOut, &rc, c);
+    target = galloc<double>(g, 324 * (size_t)nb, &rc, c);
+  }
+  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
+  if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(g->d_neu, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
+  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, n, g->d_dinv, err);
+  if (!rc) rc = neumann_blocks(c, m->d_a, m->ld, *g->pat, g->d_dinv, g->d_neu, true);
+  if (!rc && target) rc = local_inverse_blocks(c, m->d_a, m->ld, *g->pat, target);
+  if (!rc) rc = graph_fill(c, g, m, G, g->d_dinv, g->d_neu, target);
   int herr = 0;
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "network inputs");
@@ -829,28 +860,37 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
 
 void graph_destroy(hfpx_gnn_graph* g) {
   if (!g) return;
-  free_pattern(&g->pat);
+  g->pat.reset();
   for (void* p : g->allocs) cudaFree(p);
   delete g;
 }
 
 }  // namespace gnn
 
+// The learned corrections, added to pc's Neumann blocks.  The graph of the
+// mesh (pattern, geometry inputs, activation buffers) is built by the first
+// call and kept with the mesh; each call fills in the operator inputs from
+// pc's diagonal inverses and Neumann blocks and runs one forward pass.
 int gnn_correct_blocks(hfpx_ctx* c, const hfpx_gnn* net, const hfpx_mesh* mesh, const hfpx_matrix* m,
                        hfpx_precond* pc, double shear_m) {
-  hfpx_gnn_graph* g = nullptr;
-  int rc = gnn::graph_create(c, mesh, m, shear_m, false, &g);
+  hfpx_mesh* mm = const_cast<hfpx_mesh*>(mesh);
+  if (!mm->gnn_graph) {
+    int rc = gnn::graph_prepare(c, mesh, &mm->gnn_graph);
+    if (rc) return rc;
+  }
+  hfpx_gnn_graph* g = mm->gnn_graph;
+  int rc = gnn::graph_fill(c, g, m, shear_m, pc->d_dinv, pc->d_blocks, nullptr);
   if (!rc) rc = gnn::forward(c, net, g);
   if (!rc) {
     ++g_launches;
-    gnn::apply_outputs_kernel<<<(unsigned)g->pat.blocks(), 352, 0, c->stream>>>(
-        g->n_nodes, g->pat.d_ptr, g->pat.d_dst, g->on, g->oe, g->d_rot, g->d_size, shear_m, pc->d_blocks);
+    gnn::apply_outputs_kernel<<<(unsigned)g->pat->blocks(), 352, 0, c->stream>>>(
+        g->n_nodes, g->pat->d_ptr, g->pat->d_dst, g->on, g->oe, g->d_rot, g->d_size, shear_m, pc->d_blocks);
     rc = check_cuda(c, cudaGetLastError(), "learned blocks");
   }
-  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "learned blocks");
-  gnn::graph_destroy(g);
   return rc;
 }
+
+void gnn_graph_release(hfpx_gnn_graph* g) { gnn::graph_destroy(g); }
 
 }  // namespace hfpx
 
@@ -1019,8 +1059,8 @@ int hfpx_gnn_graph_data(hfpx_ctx* c, const hfpx_gnn_graph* g, float* xn, float* 
   };
   if (xn) down_bf16(g->xn, n * gnn::kFN, xn);
   if (xe) down_bf16(g->xe, E * gnn::kFE, xe);
-  if (src) std::memcpy(src, g->pat.idx.data(), sizeof(int32_t) * E);
-  if (dst) std::memcpy(dst, g->pat.dst.data(), sizeof(int32_t) * E);
+  if (src) std::memcpy(src, g->pat->idx.data(), sizeof(int32_t) * E);
+  if (dst) std::memcpy(dst, g->pat->dst.data(), sizeof(int32_t) * E);
   if (tn && !rc) rc = check_cuda(c, cudaMemcpy(tn, g->tn, sizeof(float) * n * gnn::kOut, cudaMemcpyDeviceToHost), "targets");
   if (te && !rc) rc = check_cuda(c, cudaMemcpy(te, g->te, sizeof(float) * E * gnn::kOut, cudaMemcpyDeviceToHost), "targets");
   return rc;

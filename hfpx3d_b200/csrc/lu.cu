@@ -2047,6 +2047,7 @@ static void set_math(hfpx_ctx* c, cublasMath_t mode) {
 }
 
 int lu_factor_fp64(hfpx_ctx* c, hfpx_matrix* m) {
+  m->f32_current = 0;
   set_math(c, CUBLAS_DEFAULT_MATH);
   int rc = lu_factor<double>(c, m->d_a, m->ld, m->n, m->d_piv, &m->info);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 1 : 0;
@@ -2061,7 +2062,11 @@ int lu_factor_fp32(hfpx_ctx* c, hfpx_matrix* m) {
     }
   }
   set_math(c, CUBLAS_TF32_TENSOR_OP_MATH);
-  int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info, m->d_a);
+  // the assembly already wrote the FP32 copy when the matrix had one:
+  // nothing to convert; the factors then replace it
+  const double* src = m->f32_current ? nullptr : m->d_a;
+  m->f32_current = 0;
+  int rc = lu_factor<float>(c, m->d_f, m->ld, m->n, m->d_piv, &m->info, src);
   cublasSetSmCountTarget(H(c), 0);
   set_math(c, CUBLAS_DEFAULT_MATH);
   m->factored = rc == 0 || rc == HFPX_ERR_SINGULAR ? 2 : 0;
@@ -2285,7 +2290,8 @@ static int refine_one(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
 constexpr int kGmresMax = 64;
 
 int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
-               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply) {
+               int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply,
+               const float* Af, double relax_below) {
   const int k = std::max(1, std::min(restart, kGmresMax));
   double* V = (double*)ctx_scratch(c, kScrGmresV, sizeof(double) * n * (k + 1));
   double* Z = (double*)ctx_scratch(c, kScrGmresZ, sizeof(double) * n * 2 * k);  // Z, then A Z
@@ -2335,14 +2341,20 @@ int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b
     for (int i = 0; i <= k; ++i) g[i] = 0.0;
     g[0] = rnorm;
     int j = 0;
+    bool cycle_relaxed = false;
     for (; j < k && steps < max_iter; ++j, ++steps) {
       double* vj = V + (size_t)n * j;
       double* zj = Z + (size_t)n * j;
       double* w = V + (size_t)n * (j + 1);
-      // z_j = M v_j (the preconditioner), w = A z_j
+      // z_j = M v_j (the preconditioner), w = A z_j: once the residual is
+      // small the product may be inexact by about tol / |r| (relaxed
+      // Krylov), so below relax_below it reads the FP32 copy of A
       rc = apply(vj, zj);
       if (rc) break;
-      rc = residual_f64(c, A, lda, n, zj, zero, w, part, dmax);  // w = -A z_j
+      const bool relaxed = Af && std::fabs(g[j]) / bnorm2 <= relax_below;
+      cycle_relaxed = cycle_relaxed || relaxed;
+      rc = relaxed ? residual_f32m(c, Af, lda, n, zj, zero, w, part, dmax)   // w = -A z_j
+                   : residual_f64(c, A, lda, n, zj, zero, w, part, dmax);
       if (rc) break;
       const double mone = -1.0, one = 1.0, zero_s = 0.0;
       cublasDscal(h, (int)n, &mone, w, 1);
@@ -2401,9 +2413,14 @@ int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b
     if (rc) break;
     const double one = 1.0, mone = -1.0;
     cublasDgemv(h, CUBLAS_OP_N, (int)n, j, &one, Z, (int)n, dh, 1, &one, x, 1);
-    // r = r_0 - [A z] y (r holds the cycle's starting residual)
-    cublasDgemv(h, CUBLAS_OP_N, (int)n, j, &mone, AZ, (int)n, dh, 1, &one, r, 1);
-    rc = absmax_f64(c, r, n, dmax);
+    if (cycle_relaxed) {
+      // products from the FP32 copy: the cycle's residual is b - A x in FP64
+      rc = residual_f64(c, A, lda, n, x, d_b, r, part, dmax);
+    } else {
+      // r = r_0 - [A z] y (r holds the cycle's starting residual)
+      cublasDgemv(h, CUBLAS_OP_N, (int)n, j, &mone, AZ, (int)n, dh, 1, &one, r, 1);
+      rc = absmax_f64(c, r, n, dmax);
+    }
     double rmax = 0.0;
     if (!rc) rc = read_max(&rmax);
     if (rc) break;

@@ -20,8 +20,10 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <string>
 #include <set>
 #include <vector>
 #include "engine_internal.h"
@@ -273,6 +275,19 @@ int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
   return rc;
 }
 
+std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh) {
+  hfpx_mesh* mm = const_cast<hfpx_mesh*>(mesh);
+  if (!mm->pattern) {
+    std::shared_ptr<NearPattern> p(new (std::nothrow) NearPattern, [](NearPattern* q) {
+      free_pattern(q);
+      delete q;
+    });
+    if (!p || build_pattern(c, mesh, p.get())) return nullptr;
+    mm->pattern = p;
+  }
+  return mm->pattern;
+}
+
 void free_pattern(NearPattern* p) {
   for (int32_t* d : {p->d_ptr, p->d_idx, p->d_dst, p->d_rev, p->d_rptr, p->d_rblk, p->d_rcol})
     if (d) cudaFree(d);
@@ -331,7 +346,7 @@ int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* 
   const int64_t ne = pc->n_el;
   ++g_launches;
   block_spmv_kernel<<<(unsigned)((ne * 32 + 255) / 256), 256, 0, c->stream>>>(
-      pc->d_blocks, pc->pat.d_rptr, pc->pat.d_rblk, pc->pat.d_rcol, ne, v, z);
+      pc->d_blocks, pc->pat->d_rptr, pc->pat->d_rblk, pc->pat->d_rcol, ne, v, z);
   return check_cuda(c, cudaGetLastError(), "preconditioner product");
 }
 
@@ -360,20 +375,21 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
   pc->kind = kind;
   pc->n_el = mesh->n_el;
   pc->n = m->n;
-  int rc = build_pattern(c, mesh, &pc->pat);
+  pc->pat = mesh_pattern(c, mesh);
+  int rc = pc->pat ? 0 : set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
   int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
   if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_blocks, sizeof(double) * 324 * pc->pat.blocks()), "blocks");
-  if (!rc) rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * pc->pat.blocks(), c->stream),
-                           "blocks");
+  const int64_t nb = rc ? 0 : pc->pat->blocks();
+  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_blocks, sizeof(double) * 324 * nb), "blocks");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
   if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_dinv, sizeof(double) * 324 * pc->n_el), "block inverses");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
   if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, pc->n_el, pc->d_dinv, err);
   if (!rc) {
     if (kind == HFPX_PC_LOCAL_INVERSE)
-      rc = local_inverse_blocks(c, m->d_a, m->ld, pc->pat, pc->d_blocks);
+      rc = local_inverse_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_blocks);
     else
-      rc = neumann_blocks(c, m->d_a, m->ld, pc->pat, pc->d_dinv, pc->d_blocks, kind != HFPX_PC_BLOCK_JACOBI);
+      rc = neumann_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_dinv, pc->d_blocks, kind != HFPX_PC_BLOCK_JACOBI);
   }
   if (!rc && kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
   int herr = 0;
@@ -390,7 +406,7 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
 
 int hfpx_precond_destroy(hfpx_precond* pc) {
   if (!pc) return HFPX_OK;
-  free_pattern(&pc->pat);
+  pc->pat.reset();
   if (pc->d_blocks) cudaFree(pc->d_blocks);
   if (pc->d_dinv) cudaFree(pc->d_dinv);
   delete pc;
@@ -401,22 +417,23 @@ int hfpx_precond_blocks(hfpx_ctx* c, const hfpx_precond* pc, int64_t* n_blocks, 
                         int32_t* block_col, double* blocks) {
   if (!c) return HFPX_ERR_ARG;
   if (!pc || !n_blocks) return set_error(c, HFPX_ERR_ARG, "null preconditioner");
-  *n_blocks = pc->pat.blocks();
+  const NearPattern& pat = *pc->pat;
+  *n_blocks = pat.blocks();
   if (!block_row && !block_col && !blocks) return HFPX_OK;
   if (block_row || block_col) {
     for (int64_t j = 0; j < pc->n_el; ++j) {
-      const int64_t base = j + pc->pat.ptr[j];
+      const int64_t base = j + pat.ptr[j];
       if (block_row) block_row[base] = (int32_t)j;
       if (block_col) block_col[base] = (int32_t)j;
-      for (int32_t e = pc->pat.ptr[j]; e < pc->pat.ptr[j + 1]; ++e) {
-        if (block_row) block_row[j + 1 + e] = pc->pat.idx[e];
+      for (int32_t e = pat.ptr[j]; e < pat.ptr[j + 1]; ++e) {
+        if (block_row) block_row[j + 1 + e] = pat.idx[e];
         if (block_col) block_col[j + 1 + e] = (int32_t)j;
       }
     }
   }
   if (blocks) {
     if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
-    int rc = check_cuda(c, cudaMemcpyAsync(blocks, pc->d_blocks, sizeof(double) * 324 * pc->pat.blocks(),
+    int rc = check_cuda(c, cudaMemcpyAsync(blocks, pc->d_blocks, sizeof(double) * 324 * pat.blocks(),
                                            cudaMemcpyDeviceToHost, c->stream),
                         "blocks");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "blocks");
@@ -437,8 +454,29 @@ int hfpx_gmres_precond_device(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_prec
     if (pc) return precond_apply(c, pc, v, z);
     return check_cuda(c, cudaMemcpyAsync(z, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream), "identity");
   };
-  return gmres_core(c, m->d_a, m->ld, n, d_b, tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50,
-                    max_iter > 0 ? max_iter : 1000, info, apply);
+  tol = tol > 0 ? tol : 1e-12;
+  // Relaxed products: once the residual is below tol / 1e-6 the FP32 copy of
+  // the matrix (entries rounded to 2^-24 relative) is accurate enough for
+  // the product, at half the bytes.  The copy is the one the assembly writes
+  // (made here from the FP64 matrix the first time); without room for it, or
+  // with HFPX_GMRES_F32=0, every product is FP64.
+  const float* Af = nullptr;
+  const char* e32 = std::getenv("HFPX_GMRES_F32");
+  if (!(e32 && std::string(e32) == "0")) {
+    hfpx_matrix* mm = const_cast<hfpx_matrix*>(m);
+    if (!mm->d_f && cudaMalloc(&mm->d_f, sizeof(float) * (size_t)mm->ld * mm->n) != cudaSuccess) {
+      mm->d_f = nullptr;
+      cudaGetLastError();
+    }
+    if (mm->d_f && !mm->f32_current) {
+      launch_convert_f32(mm->d_a, mm->ld, mm->n, mm->d_f, c->stream);
+      mm->f32_current = 1;
+      mm->factored = 0;
+    }
+    if (mm->d_f) Af = mm->d_f;
+  }
+  return gmres_core(c, m->d_a, m->ld, n, d_b, tol, restart > 0 ? restart : 50, max_iter > 0 ? max_iter : 1000, info,
+                    apply, Af, std::min(1e-2, tol / 1e-6));
 }
 
 int hfpx_gmres_precond(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_precond* pc, double* b, double tol, int restart,

@@ -402,6 +402,56 @@ __global__ void __launch_bounds__(kGvThreads) resid_partial_kernel(const double*
   if (i0 + 1 < n) part[(int64_t)blockIdx.y * n + i0 + 1] = a1;
 }
 
+// The same partial products from the FP32 copy of the matrix: 4 rows per
+// thread (one 16-byte load per column), products and sums in FP64 with x in
+// FP64, so the only error is the FP32 rounding of the matrix entries.
+constexpr int kGvRows32 = 4 * kGvThreads;
+__global__ void __launch_bounds__(kGvThreads) resid_partial_f32_kernel(const float* __restrict__ A, int64_t lda, int n,
+                                                                       const double* __restrict__ x,
+                                                                       double* __restrict__ part) {
+  __shared__ double s_x[kGvChunk];
+  const int nch = gridDim.y;
+  const int per = (n + nch - 1) / nch;
+  const int c_lo = blockIdx.y * per, c_hi = min(n, c_lo + per);
+  for (int j = c_lo + threadIdx.x; j < c_hi; j += kGvThreads) s_x[j - c_lo] = x[j];
+  __syncthreads();
+  const int i0 = blockIdx.x * kGvRows32 + 4 * threadIdx.x;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i0 + 3 < n) {
+    const float* col = A + i0;
+    int j = c_lo;
+    for (; j + 2 <= c_hi; j += 2) {
+      const float4 v0 = *reinterpret_cast<const float4*>(col + lda * j);
+      const float4 v1 = *reinterpret_cast<const float4*>(col + lda * (j + 1));
+      const double x0 = s_x[j - c_lo], x1 = s_x[j + 1 - c_lo];
+      a[0] = fma((double)v0.x, x0, a[0]);
+      a[1] = fma((double)v0.y, x0, a[1]);
+      a[2] = fma((double)v0.z, x0, a[2]);
+      a[3] = fma((double)v0.w, x0, a[3]);
+      a[0] = fma((double)v1.x, x1, a[0]);
+      a[1] = fma((double)v1.y, x1, a[1]);
+      a[2] = fma((double)v1.z, x1, a[2]);
+      a[3] = fma((double)v1.w, x1, a[3]);
+    }
+    for (; j < c_hi; ++j) {
+      const float4 v = *reinterpret_cast<const float4*>(col + lda * j);
+      const double xj = s_x[j - c_lo];
+      a[0] = fma((double)v.x, xj, a[0]);
+      a[1] = fma((double)v.y, xj, a[1]);
+      a[2] = fma((double)v.z, xj, a[2]);
+      a[3] = fma((double)v.w, xj, a[3]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (i0 + r < n)
+        for (int j = c_lo; j < c_hi; ++j) a[r] = fma((double)A[i0 + r + lda * j], s_x[j - c_lo], a[r]);
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+    if (i0 + r < n) part[(int64_t)blockIdx.y * n + i0 + r] = a[r];
+}
+
 __global__ void resid_finish_kernel(const double* __restrict__ b, const double* __restrict__ part, int n, int nch,
                                     double* __restrict__ r, unsigned long long* __restrict__ rmax) {
   __shared__ double s_m[8];
@@ -445,6 +495,18 @@ int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const dou
   ++g_launches;
   resid_partial_kernel<<<dim3((unsigned)((n + kGvRows - 1) / kGvRows), (unsigned)nch), kGvThreads, 0, c->stream>>>(
       A, lda, (int)n, x, part);
+  ++g_launches;
+  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max);
+  return check_cuda(c, cudaGetLastError(), "residual launch");
+}
+
+int residual_f32m(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
+                  double* part, unsigned long long* d_max) {
+  const int nch = resid_chunks(n);
+  cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
+  ++g_launches;
+  resid_partial_f32_kernel<<<dim3((unsigned)((n + kGvRows32 - 1) / kGvRows32), (unsigned)nch), kGvThreads, 0,
+                             c->stream>>>(A, lda, (int)n, x, part);
   ++g_launches;
   resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max);
   return check_cuda(c, cudaGetLastError(), "residual launch");
