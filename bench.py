@@ -146,6 +146,10 @@ class Forms:
         self.dm, self.dof, self.n, self.A, self.d_rhs, self.d_x = dm, dof, n, A, d_rhs, d_x
         self.info = engine.SolveInfo()
         self.net = None
+        self.host_ms = {}
+
+    def _host(self, key, t0):
+        self.host_ms[key] = self.host_ms.get(key, 0.0) + (time.perf_counter() - t0) * 1e3
 
     def step(self, form, ev=None):
         engine, L, ctx, A, torch = self.engine, self.L, self.ctx, self.A, self.torch
@@ -157,13 +161,19 @@ class Forms:
         if form == 'learned':
             if self.net is None:
                 self.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
+            t0 = time.perf_counter()
             pc = engine.Precond(ctx, self.dm, A, engine.HFPX_PC_LEARNED, net=self.net, shear_m=G)
+            self._host('precond_create', t0)
             rec(2)
             with torch.cuda.stream(self.stream):
                 self.d_x.copy_(self.d_rhs)
+            t0 = time.perf_counter()
             rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, x, self.args.tol, 50, 2000, ctypes.byref(self.info))
+            self._host('gmres', t0)
             rec(3)
+            t0 = time.perf_counter()
             pc.close()
+            self._host('precond_destroy', t0)
             ctx.check(rc)
             return
         mode = engine.HFPX_LU_MIXED if form == 'mixed' else engine.HFPX_LU_FP64
@@ -231,6 +241,7 @@ def run_engine(args, rank, world, local_rank):
     for _ in range(args.warmup):
         F.step(args.mode)
     torch.cuda.synchronize()
+    F.host_ms = {}
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     launches0 = L.hfpx_ctx_launch_count(ctx.h)
     if world > 1:
@@ -240,9 +251,13 @@ def run_engine(args, rank, world, local_rank):
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
         start.record(stream)
+        t_loop = time.perf_counter()
         for k in range(args.steps):
+            t0 = time.perf_counter()
             F.step(args.mode, evs[k])
+            F._host('step', t0)
         end.record(stream)
+        F._host('loop', t_loop)
         torch.cuda.synchronize()
     launches = L.hfpx_ctx_launch_count(ctx.h) - launches0
     total_ms = start.elapsed_time(end)
@@ -327,6 +342,7 @@ def run_engine(args, rank, world, local_rank):
         'steps_ms': {'total': [round(a + b + c, 2) for a, b, c in zip(t_asm, t_fac, t_sol)],
                      'solve': [round(t, 2) for t in t_sol]},
         'solver': {'form': args.mode, 'iterations': iters_main, 'residual': res_main},
+        'host_ms_per_step': {k: v / args.steps for k, v in F.host_ms.items()},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,
         'roofline_assembly': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
