@@ -132,8 +132,10 @@ def replica_max(x, world, local_rank):
 class Forms:
     """The three forms of one step on the device matrix A: FP64 assembly into
     A, then
-      learned: the learned near-field preconditioner (hfpx_precond_create with
-               the trained network) and flexible GMRES(50) on the FP64
+      learned: the learned near-field preconditioner (made by
+               hfpx_precond_create with the trained network on the first step,
+               hfpx_precond_update in its storage on the next ones) and
+               flexible GMRES(50) on the FP64
                operator (hfpx_gmres_precond_device);
       mixed:   the mixed LU (FP32 copy, FP16 tcgen05 updates) and flexible
                GMRES on the FP64 matrix preconditioned by it (hfpx_gmres_device);
@@ -146,6 +148,7 @@ class Forms:
         self.dm, self.dof, self.n, self.A, self.d_rhs, self.d_x = dm, dof, n, A, d_rhs, d_x
         self.info = engine.SolveInfo()
         self.net = None
+        self.pc = None
         self.host_ms = {}
 
     def _host(self, key, t0):
@@ -162,18 +165,21 @@ class Forms:
             if self.net is None:
                 self.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
             t0 = time.perf_counter()
-            pc = engine.Precond(ctx, self.dm, A, engine.HFPX_PC_LEARNED, net=self.net, shear_m=G)
-            self._host('precond_create', t0)
+            # blocks made again from this step's matrix, in the storage of
+            # the first step's preconditioner (hfpx_precond_update)
+            if self.pc is None:
+                self.pc = engine.Precond(ctx, self.dm, A, engine.HFPX_PC_LEARNED, net=self.net, shear_m=G)
+            else:
+                self.pc.update(A, net=self.net, shear_m=G)
+            self._host('precond', t0)
             rec(2)
             with torch.cuda.stream(self.stream):
                 self.d_x.copy_(self.d_rhs)
             t0 = time.perf_counter()
-            rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, x, self.args.tol, 50, 2000, ctypes.byref(self.info))
+            rc = L.hfpx_gmres_precond_device(ctx.h, A.h, self.pc.h, x, self.args.tol, 50, 2000,
+                                             ctypes.byref(self.info))
             self._host('gmres', t0)
             rec(3)
-            t0 = time.perf_counter()
-            pc.close()
-            self._host('precond_destroy', t0)
             ctx.check(rc)
             return
         mode = engine.HFPX_LU_MIXED if form == 'mixed' else engine.HFPX_LU_FP64
@@ -203,6 +209,8 @@ class Forms:
         return best, self.info.iterations, self.info.residual, self.d_x.cpu().numpy()
 
     def close(self):
+        if self.pc is not None:
+            self.pc.close()
         if self.net is not None:
             self.net.close()
 

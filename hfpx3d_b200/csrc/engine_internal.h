@@ -69,6 +69,7 @@ struct hfpx_gnn;
 struct hfpx_precond {
   int kind = 0;
   int64_t n_el = 0, n = 0;
+  const hfpx_mesh* mesh = nullptr;    // the mesh it was made for (updates read it)
   std::shared_ptr<NearPattern> pat;   // the mesh's
   double* d_blocks = nullptr;      // blocks() x 18 x 18, each column-major
   double* d_dinv = nullptr;        // inverses of the diagonal blocks, n_el x 18 x 18

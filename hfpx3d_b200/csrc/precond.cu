@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <set>
 #include <vector>
@@ -355,12 +356,52 @@ int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* 
 // ------------------------------------------------------------------ C-ABI
 using namespace hfpx;
 
-extern "C" {
+namespace {
 
-int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, int kind, const hfpx_gnn* net,
-                        double shear_m, hfpx_precond** out) {
-  if (!c || !out) return HFPX_ERR_ARG;
-  *out = nullptr;
+// Preconditioner storage comes from an engine-owned stream-ordered pool per
+// device whose release threshold keeps freed memory reserved, so a loop that
+// creates and destroys a preconditioner each step (a new mesh each step)
+// maps device memory once instead of every step (cudaMalloc / cudaFree of the
+// blocks cost tens of milliseconds at 4,000 elements).
+cudaMemPool_t block_pool(int dev) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
+int pool_alloc(hfpx_ctx* c, void** p, size_t bytes, const char* what) {
+  cudaMemPool_t pool = block_pool(c->device);
+  if (!pool) return set_error(c, HFPX_ERR_CUDA, "memory pool");
+  return check_cuda(c, cudaMallocFromPoolAsync(p, bytes, pool, c->stream), what);
+}
+
+// After the device is idle (the guarantee cudaFree gives), back to the pool
+// in the legacy stream's order, which is then already complete.
+void pool_free(void* p) {
+  if (!p) return;
+  cudaDeviceSynchronize();
+  if (cudaFreeAsync(p, cudaStreamLegacy) != cudaSuccess) cudaGetLastError();
+}
+
+int precond_check(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, int kind, const hfpx_gnn* net,
+                  double shear_m) {
   if (!mesh || !m) return set_error(c, HFPX_ERR_ARG, "null mesh or matrix");
   if (kind < HFPX_PC_BLOCK_JACOBI || kind > HFPX_PC_LEARNED) return set_error(c, HFPX_ERR_ARG, "unknown preconditioner");
   if (kind == HFPX_PC_LEARNED && !net) return set_error(c, HFPX_ERR_ARG, "the learned preconditioner needs a network");
@@ -369,33 +410,54 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
                                       "no volume-control border)");
   if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "the matrix holds FP64 LU factors, not the operator");
   if (!(shear_m > 0)) return set_error(c, HFPX_ERR_ARG, "bad shear modulus");
+  return HFPX_OK;
+}
+
+// the blocks of pc (storage allocated) from the matrix m of its mesh
+int precond_fill(hfpx_ctx* c, hfpx_precond* pc, const hfpx_mesh* mesh, const hfpx_matrix* m, const hfpx_gnn* net,
+                 double shear_m) {
+  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
+  if (!err) return set_error(c, HFPX_ERR_NOMEM, "status word");
+  const int64_t nb = pc->pat->blocks();
+  int rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
+  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, pc->n_el, pc->d_dinv, err);
+  if (!rc) {
+    if (pc->kind == HFPX_PC_LOCAL_INVERSE)
+      rc = local_inverse_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_blocks);
+    else
+      rc = neumann_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_dinv, pc->d_blocks, pc->kind != HFPX_PC_BLOCK_JACOBI);
+  }
+  if (!rc && pc->kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
+  int herr = 0;
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "preconditioner");
+  if (!rc && herr) rc = set_error(c, HFPX_ERR_SINGULAR, "a diagonal block of the matrix is singular");
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, int kind, const hfpx_gnn* net,
+                        double shear_m, hfpx_precond** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  if (int rc = precond_check(c, mesh, m, kind, net, shear_m)) return rc;
   if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
   hfpx_precond* pc = new (std::nothrow) hfpx_precond;
   if (!pc) return set_error(c, HFPX_ERR_NOMEM, "preconditioner");
   pc->kind = kind;
   pc->n_el = mesh->n_el;
   pc->n = m->n;
+  pc->mesh = mesh;
   pc->pat = mesh_pattern(c, mesh);
   int rc = pc->pat ? 0 : set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
-  int* err = (int*)ctx_scratch(c, kScrTcErr, sizeof(int));
-  if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
   const int64_t nb = rc ? 0 : pc->pat->blocks();
-  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_blocks, sizeof(double) * 324 * nb), "blocks");
-  if (!rc) rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&pc->d_dinv, sizeof(double) * 324 * pc->n_el), "block inverses");
-  if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
-  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, pc->n_el, pc->d_dinv, err);
-  if (!rc) {
-    if (kind == HFPX_PC_LOCAL_INVERSE)
-      rc = local_inverse_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_blocks);
-    else
-      rc = neumann_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_dinv, pc->d_blocks, kind != HFPX_PC_BLOCK_JACOBI);
-  }
-  if (!rc && kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
-  int herr = 0;
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
-  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "preconditioner");
-  if (!rc && herr) rc = set_error(c, HFPX_ERR_SINGULAR, "a diagonal block of the matrix is singular");
+  if (!rc) rc = pool_alloc(c, (void**)&pc->d_blocks, sizeof(double) * 324 * nb, "blocks");
+  if (!rc) rc = pool_alloc(c, (void**)&pc->d_dinv, sizeof(double) * 324 * pc->n_el, "block inverses");
+  if (!rc) rc = precond_fill(c, pc, mesh, m, net, shear_m);
   if (rc) {
     hfpx_precond_destroy(pc);
     return rc;
@@ -404,11 +466,20 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
   return HFPX_OK;
 }
 
+int hfpx_precond_update(hfpx_ctx* c, hfpx_precond* pc, const hfpx_matrix* m, const hfpx_gnn* net, double shear_m) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!pc) return set_error(c, HFPX_ERR_ARG, "null preconditioner");
+  if (int rc = precond_check(c, pc->mesh, m, pc->kind, net, shear_m)) return rc;
+  if (m->n != pc->n) return set_error(c, HFPX_ERR_ARG, "the matrix is not of the preconditioner's mesh");
+  if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  return precond_fill(c, pc, pc->mesh, m, net, shear_m);
+}
+
 int hfpx_precond_destroy(hfpx_precond* pc) {
   if (!pc) return HFPX_OK;
   pc->pat.reset();
-  if (pc->d_blocks) cudaFree(pc->d_blocks);
-  if (pc->d_dinv) cudaFree(pc->d_dinv);
+  pool_free(pc->d_blocks);
+  pool_free(pc->d_dinv);
   delete pc;
   return HFPX_OK;
 }

@@ -64,6 +64,8 @@ SIGNATURES = {
     'hfpx_lu_factor': (_int, [_V, _V, _int, _L]),
     'hfpx_lu_solve': (_int, [_V, _V, _D, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_lu_solve_device': (_int, [_V, _V, _V, _i64, _i64, _f64, _int, ctypes.POINTER(SolveInfo)]),
+    'hfpx_matrix_truncate': (_int, [_V, _V, _L, _i64, _int, ctypes.POINTER(_V)]),
+    'hfpx_lu_solve_fixed': (_int, [_V, _V, _L, _i64, _D, _f64, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres': (_int, [_V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres_device': (_int, [_V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_ctx_launch_count': (_i64, [_V]),
@@ -71,6 +73,7 @@ SIGNATURES = {
     'hfpx_gemm_f16_update': (_int, [_V, _i64, _i64, _i64, _V, _i64, _V, _i64, _V, _i64, _V]),
     'hfpx_precond_create': (_int, [_V, _V, _V, _int, _V, _f64, ctypes.POINTER(_V)]),
     'hfpx_precond_destroy': (_int, [_V]),
+    'hfpx_precond_update': (_int, [_V, _V, _V, _V, _f64]),
     'hfpx_precond_blocks': (_int, [_V, _V, _L, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), _D]),
     'hfpx_gmres_precond': (_int, [_V, _V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres_precond_device': (_int, [_V, _V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
@@ -311,6 +314,66 @@ def add_s_inf_to_3dbem_rhs(ctx, dmesh: DeviceMesh, dof_h, n_dof, s_inf, rhs=None
     return rhs[:, 0].copy() if nr == 1 else rhs
 
 
+def truncate(ctx, matrix: DeviceMatrix, keep, keep_border=True) -> DeviceMatrix:
+    """Device gather of the kept DD unknowns (and the VC border) of a
+    matrix (hfpx_matrix_truncate)."""
+    k = np.ascontiguousarray(keep, dtype=np.int64).reshape(-1)
+    h = _V()
+    ctx.check(lib().hfpx_matrix_truncate(ctx.h, matrix.h, _lp(k), k.size, int(keep_border), ctypes.byref(h)))
+    return DeviceMatrix(ctx, h)
+
+
+def vc_truncation_map(orig_dof_h, dof_h):
+    """keep[t] = the original DoF of truncated DoF t, from the two DoF
+    handles as mod_3dbem_system_vc reads them (system_assembly.cpp:596-606):
+    entry (e, j) maps dof_h(e, j) >= 0 to orig_dof_h(e, j)."""
+    o = np.asarray(orig_dof_h, dtype=np.int64).reshape(-1)
+    t = np.asarray(dof_h, dtype=np.int64).reshape(-1)
+    used = int(t.max()) + 1 if t.size and t.max() >= 0 else 0
+    keep = np.full(used, -1, dtype=np.int64)
+    sel = t >= 0
+    if np.any(o[sel] < 0):
+        raise ValueError('a truncated DoF without an original DoF')
+    if np.unique(t[sel]).size != int(sel.sum()):
+        raise ValueError('a truncated DoF at two element nodes')
+    keep[t[sel]] = o[sel]
+    if np.any(keep < 0):
+        raise ValueError('the truncated numbering has gaps')
+    return keep
+
+
+def vc_rhs(orig_dof_h, dof_h, delta_t, delta_v, orig_ndof):
+    """The right-hand side of mod_3dbem_system_vc (system_assembly.cpp:580-590,
+    612-621): delta_t by the truncated numbering, delta_v last.  delta_t is
+    indexed by the full element-node numbering (n_el * 18), the original DoF
+    numbering or the truncated one, told apart by its length as there."""
+    t = np.asarray(dof_h, dtype=np.int64).reshape(-1)
+    o = np.asarray(orig_dof_h, dtype=np.int64).reshape(-1)
+    used = vc_truncation_map(orig_dof_h, dof_h).size
+    dt = np.asarray(delta_t, dtype=np.float64).reshape(-1)
+    rhs = np.zeros(used + 1)
+    rhs[used] = delta_v
+    sel = t >= 0
+    if dt.size == t.size:
+        rhs[t[sel]] = dt[sel]
+    elif dt.size == orig_ndof:
+        rhs[t[sel]] = dt[o[sel]]
+    elif dt.size == used:
+        rhs[:used] = dt
+    else:
+        raise ValueError('delta_t must have the full, original or truncated DoF count')
+    return rhs
+
+
+def mod_3dbem_system_vc(ctx, matrix: DeviceMatrix, orig_dof_h, dof_h, delta_t, delta_v):
+    """system_assembly.cpp:560-629: the truncated bordered system of the DoF
+    dof_h keeps, gathered on the device from the bordered VC matrix ->
+    (DeviceMatrix of used + 1 unknowns, host rhs)."""
+    keep = vc_truncation_map(orig_dof_h, dof_h)
+    rhs = vc_rhs(orig_dof_h, dof_h, delta_t, delta_v, matrix.n - 1)
+    return truncate(ctx, matrix, keep, True), rhs
+
+
 class LU:
     """il::LU<il::Array2D<double>> (LU.h:46-120) on the device: factor on
     construction (dgetrf), solve(y) (dgetrs).  mode HFPX_LU_MIXED factors an
@@ -335,6 +398,18 @@ class LU:
         self.last_info = info
         self.ctx.check(rc)
         return b[:, 0].copy() if one else b
+
+    def solve_fixed(self, y, fixed, tol=0.0):
+        """x with x[fixed] = 0 solving the rows of A x = y outside `fixed`,
+        from this factorisation (hfpx_lu_solve_fixed): the system that
+        truncating `fixed` away makes, without a new factorisation."""
+        b = np.array(y, dtype=np.float64, copy=True).reshape(-1)
+        fx = np.ascontiguousarray(fixed, dtype=np.int64).reshape(-1)
+        info = SolveInfo()
+        rc = lib().hfpx_lu_solve_fixed(self.ctx.h, self.matrix.h, _lp(fx), fx.size, _dp(b), tol, ctypes.byref(info))
+        self.last_info = info
+        self.ctx.check(rc)
+        return b
 
     def gmres(self, y, tol=0.0, restart=0, max_iter=0):
         """One right-hand side by flexible GMRES on the FP64 matrix,
@@ -430,9 +505,17 @@ class Precond:
 
     def __init__(self, ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, kind, net=None, shear_m=1.0):
         self.ctx = ctx
+        self.dmesh = dmesh  # updates read the mesh
         self.h = _V()
         ctx.check(lib().hfpx_precond_create(ctx.h, dmesh.h, matrix.h, kind, net.h if net is not None else None,
                                             shear_m, ctypes.byref(self.h)))
+
+    def update(self, matrix: DeviceMatrix, net=None, shear_m=1.0):
+        """The blocks made again from a re-assembled matrix of the same mesh,
+        in place (hfpx_precond_update)."""
+        self.ctx.check(lib().hfpx_precond_update(self.ctx.h, self.h, matrix.h, net.h if net is not None else None,
+                                                 shear_m))
+        return self
 
     def blocks(self):
         """(block_row, block_col, blocks[nb, 18, 18]) with blocks[k][r, c] = M[18 row + r, 18 col + c]."""

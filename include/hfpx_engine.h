@@ -133,6 +133,31 @@ int hfpx_matrix_upload_lu(hfpx_ctx *ctx, const double *lu, int64_t n, int64_t ld
 int hfpx_lu_solve_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, int64_t nrhs,
                          int64_t ld_b, double tol, int max_iter, hfpx_solve_info *info);
 
+/* ---- volume-control truncation: mod_3dbem_system_vc,
+ * src/Solvers/system_assembly.cpp:560-629.  *out (new) is the square matrix
+ * of the kept DD unknowns: out(i, j) = matrix(keep[i], keep[j]), keep
+ * distinct indices below n_dd (n_dd = n - 1 when keep_border, else n), in
+ * the truncated numbering's order; with keep_border the volume row and the
+ * pressure column of the bordered matrix (make_3dbem_matrix_vc, :458-557)
+ * follow as row and column n_keep, corner included.  The reference reads the
+ * border one row past an orig_ndof-square matrix; here it is the bordered
+ * matrix's own last row and column.  The matrix must hold the operator (not
+ * FP64 factors); a mixed factorisation keeps it, so truncation can follow.
+ * The right-hand side (delta_t by the truncated numbering, delta_v last) is
+ * a host gather and not part of this call. */
+int hfpx_matrix_truncate(hfpx_ctx *ctx, const hfpx_matrix *matrix, const int64_t *keep, int64_t n_keep,
+                         int keep_border, hfpx_matrix **out);
+/* The truncated system solved with the factors of the full one (no new
+ * factorisation): on return b (host, n) holds x with x[fixed[i]] = 0 and
+ * (A x)[r] = b[r] for every row r not in fixed.  The kept entries of x
+ * solve the system hfpx_matrix_truncate makes from the complement of
+ * `fixed`.  k + 1 solves with the existing factors (tol as in
+ * hfpx_lu_solve) and a k x k capacitance system; at most 4096 distinct
+ * fixed indices.  HFPX_ERR_SINGULAR when the truncated system is singular.
+ * info is that of the solve of b. */
+int hfpx_lu_solve_fixed(hfpx_ctx *ctx, const hfpx_matrix *matrix, const int64_t *fixed, int64_t k, double *b,
+                        double tol, hfpx_solve_info *info);
+
 /* ---- iterative solve: flexible GMRES(restart) on the FP64 matrix,
  * right-preconditioned by the FP32 factors of its mixed factorisation
  * (hfpx_lu_factor with HFPX_LU_MIXED), for one right-hand side b (host, n),
@@ -214,6 +239,13 @@ typedef enum {
 } hfpx_pc_kind;
 int hfpx_precond_create(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix, int kind,
                         const hfpx_gnn *net, double shear_m, hfpx_precond **precond);
+/* The blocks of precond made again from matrix, a re-assembly of the
+ * operator on the same mesh (which must still exist), into the storage the
+ * preconditioner already holds: no device allocation, so a time-stepping
+ * loop that re-assembles into one matrix (hfpx_assemble_into) and updates
+ * one preconditioner allocates nothing per step.  net as for create. */
+int hfpx_precond_update(hfpx_ctx *ctx, hfpx_precond *precond, const hfpx_matrix *matrix, const hfpx_gnn *net,
+                        double shear_m);
 int hfpx_precond_destroy(hfpx_precond *precond);
 /* The blocks (18 x 18 column-major each) and their block row and column:
  * call with null arrays to get n_blocks first. */
