@@ -420,10 +420,12 @@ __global__ void __launch_bounds__(kGvThreads) resid_partial_f32_kernel(const flo
   if (i0 + 3 < n) {
     const float* col = A + i0;
     int j = c_lo;
-    for (; j + 2 <= c_hi; j += 2) {
+    for (; j + 4 <= c_hi; j += 4) {
       const float4 v0 = *reinterpret_cast<const float4*>(col + lda * j);
       const float4 v1 = *reinterpret_cast<const float4*>(col + lda * (j + 1));
-      const double x0 = s_x[j - c_lo], x1 = s_x[j + 1 - c_lo];
+      const float4 v2 = *reinterpret_cast<const float4*>(col + lda * (j + 2));
+      const float4 v3 = *reinterpret_cast<const float4*>(col + lda * (j + 3));
+      const double x0 = s_x[j - c_lo], x1 = s_x[j + 1 - c_lo], x2 = s_x[j + 2 - c_lo], x3 = s_x[j + 3 - c_lo];
       a[0] = fma((double)v0.x, x0, a[0]);
       a[1] = fma((double)v0.y, x0, a[1]);
       a[2] = fma((double)v0.z, x0, a[2]);
@@ -432,6 +434,14 @@ __global__ void __launch_bounds__(kGvThreads) resid_partial_f32_kernel(const flo
       a[1] = fma((double)v1.y, x1, a[1]);
       a[2] = fma((double)v1.z, x1, a[2]);
       a[3] = fma((double)v1.w, x1, a[3]);
+      a[0] = fma((double)v2.x, x2, a[0]);
+      a[1] = fma((double)v2.y, x2, a[1]);
+      a[2] = fma((double)v2.z, x2, a[2]);
+      a[3] = fma((double)v2.w, x2, a[3]);
+      a[0] = fma((double)v3.x, x3, a[0]);
+      a[1] = fma((double)v3.y, x3, a[1]);
+      a[2] = fma((double)v3.z, x3, a[2]);
+      a[3] = fma((double)v3.w, x3, a[3]);
     }
     for (; j < c_hi; ++j) {
       const float4 v = *reinterpret_cast<const float4*>(col + lda * j);
@@ -486,11 +496,41 @@ __global__ void absmax_kernel(const double* __restrict__ v, int n, unsigned long
   }
 }
 
-int resid_chunks(int64_t n) { return (int)std::max<int64_t>(16, (n + kGvChunk - 1) / kGvChunk); }
+// Column chunks: at least n / kGvChunk (the chunk's x fits shared memory)
+// and 16; the partial-sum buffer holds up to 4 times that many.
+static int64_t resid_chunks_min(int64_t n) { return std::max<int64_t>(16, (n + kGvChunk - 1) / kGvChunk); }
+int resid_chunks(int64_t n) { return (int)(4 * resid_chunks_min(n)); }
+
+// The chunk count for a grid of ceil(n / rows) x nch blocks: the one (from
+// the minimum up to 4 times it) whose blocks fill the last wave of resident
+// blocks best, so that the matrix stream keeps every SM's loads in flight to
+// the end.  A function of n and the device only, so sums are reproducible.
+template <class K>
+static int resid_grid_chunks(hfpx_ctx* c, int64_t n, int rows, K kernel) {
+  const int64_t lo = resid_chunks_min(n);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kGvThreads, 0) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    return (int)lo;
+  }
+  const int64_t R = (int64_t)per_sm * std::max(1, c->num_sms);
+  const int64_t gx = (n + rows - 1) / rows;
+  int64_t best = lo;
+  double best_fill = 0.0;
+  for (int64_t nch = lo; nch <= 4 * lo; ++nch) {
+    const int64_t B = gx * nch;
+    const double fill = (double)B / (double)(((B + R - 1) / R) * R);
+    if (fill > best_fill + 1e-3) {
+      best_fill = fill;
+      best = nch;
+    }
+  }
+  return (int)best;
+}
 
 int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
                  double* part, unsigned long long* d_max) {
-  const int nch = resid_chunks(n);
+  const int nch = resid_grid_chunks(c, n, kGvRows, resid_partial_kernel);
   cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
   ++g_launches;
   resid_partial_kernel<<<dim3((unsigned)((n + kGvRows - 1) / kGvRows), (unsigned)nch), kGvThreads, 0, c->stream>>>(
@@ -502,7 +542,7 @@ int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const dou
 
 int residual_f32m(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
                   double* part, unsigned long long* d_max) {
-  const int nch = resid_chunks(n);
+  const int nch = resid_grid_chunks(c, n, kGvRows32, resid_partial_f32_kernel);
   cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
   ++g_launches;
   resid_partial_f32_kernel<<<dim3((unsigned)((n + kGvRows32 - 1) / kGvRows32), (unsigned)nch), kGvThreads, 0,
