@@ -59,10 +59,11 @@ def peaks():
 # the ncu capture of profiles/assemble_kernel_penny1000.md (4.6305 GB for an
 # 18 000 x 18 000 fill; traffic grows with the entries, so it scales by N^2)
 ASM_DRAM_BYTES_PER_ENTRY = 4.630537e9 / 18000 ** 2
-# DRAM bytes per matrix entry of one FP64 operator product (resid_partial_kernel
-# + resid_finish_kernel), from an ncu capture of the product alone; None until
-# measured
-RESID_DRAM_BYTES_PER_ENTRY = None
+# DRAM bytes (read + write) per matrix entry of one FP64 operator product's
+# resid_partial_kernel: 3.7327 GB read + 11.8 MB of partial sums written at
+# N = 21 600 in an ncu capture of one launch (profiles/resid_partial_kernels_penny1200.md);
+# the traffic grows with the entries, so N^2 times this is a launch at any N
+RESID_DRAM_BYTES_PER_ENTRY = (3.732682e9 + 11.813888e6) / 21600.0 ** 2
 
 
 class Clocks:
@@ -325,7 +326,7 @@ def run_engine(args, rank, world, local_rank):
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
     # stresses at observation points (make_3dbem_stress_f_s) on the C1 penny
-    stress = run_stress(ctx, engine) if rank == 0 and args.stress else None
+    stress = run_stress(ctx, engine, torch, stream) if rank == 0 and args.stress else None
     F.close()
 
     if rank != 0:
@@ -402,13 +403,15 @@ def run_engine(args, rank, world, local_rank):
     return line
 
 
-def run_stress(ctx, engine, reps=5):
+def run_stress(ctx, engine, torch, stream, reps=5):
     """Stress at observation points through the C-ABI with host buffers
     (hfpx_stress, make_3dbem_stress_f_s system_assembly.cpp:279-455; and
     hfpx_stress_batch for many load cases at once), on the seeded
     121-element penny: 100 seeded points in [-1.5, 1.5]^3 (the C1 set-up),
     one load case, and 64 load cases (pressures U[0.5, 2] and random in-situ
-    stresses).  Best of `reps` host wall times of the call."""
+    stresses).  Best of `reps` host wall times of the call, and the device
+    time between CUDA events on the engine's stream around it (copies and
+    kernels, without the host-side wrapper)."""
     from hfpx3d_b200 import meshgen
     nods, conn = meshgen.penny(121, seed=4)
     ne = conn.shape[1]
@@ -433,20 +436,27 @@ def run_stress(ctx, engine, reps=5):
 
     def best(fn):
         fn()
-        ts = []
+        ts, ds = [], []
         for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
             t0 = time.perf_counter()
+            e0.record(stream)
             fn()
+            e1.record(stream)
             ts.append(time.perf_counter() - t0)
-        return min(ts)
-    t1 = best(lambda: engine.make_3dbem_stress_f_s(ctx, dm, G, NU, dds[0], pts, S[:, 0]))
-    t64 = best(lambda: engine.make_3dbem_stress_f_s_batch(ctx, dm, G, NU, dds, pts, S))
+            torch.cuda.synchronize()
+            ds.append(e0.elapsed_time(e1) / 1e3)
+        return min(ts), min(ds)
+    t1, d1 = best(lambda: engine.make_3dbem_stress_f_s(ctx, dm, G, NU, dds[0], pts, S[:, 0]))
+    t64, d64 = best(lambda: engine.make_3dbem_stress_f_s_batch(ctx, dm, G, NU, dds, pts, S))
     A.close()
     dm.close()
     npts = pts.shape[1]
     return {'workload': f'penny {ne} el, {npts} seeded points in [-1.5, 1.5]^3; host buffers through the C-ABI',
             'one_case_s': t1, 'points_per_s': npts / t1, 'pair_evaluations_per_s': npts * ne / t1,
-            'cases_64_s': t64, 'point_cases_per_s': 64 * npts / t64}
+            'one_case_device_s': d1, 'cases_64_s': t64, 'cases_64_device_s': d64,
+            'point_cases_per_s': 64 * npts / t64}
 
 
 FORM_TEXT = {'learned': 'learned near-field preconditioner + GMRES(50) on the FP64 operator',

@@ -215,7 +215,7 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
   for (int64_t n = 0; n < n_nodes; ++n)
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(nods[k + ld_nods * n])) return set_error(c, HFPX_ERR_ARG, "non-finite node coordinate");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   ScratchBuf dn(c, kScrHostNods), dc(c, kScrHostConn);
   int rc = check_cuda(c, dn.alloc(sizeof(double) * ld_nods * n_nodes), "nods alloc");
   if (!rc) rc = check_cuda(c, dc.alloc(sizeof(int64_t) * ld_conn * n_el), "conn alloc");
@@ -305,7 +305,7 @@ int hfpx_assemble(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   *out = nullptr;
   int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
   if (rc) return rc;
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   hfpx_matrix* m = nullptr;
   rc = new_matrix(c, n_dof + (vc_border ? 1 : 0), &m);
   if (!rc) rc = assemble_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, vc_border, m);
@@ -323,7 +323,7 @@ int hfpx_assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h,
   int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
   if (rc) return rc;
   if (!m || m->n != n_dof + (vc_border ? 1 : 0)) return set_error(c, HFPX_ERR_ARG, "matrix size does not match n_dof");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   return assemble_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, vc_border, m);
 }
 
@@ -331,7 +331,7 @@ int hfpx_matrix_upload(hfpx_ctx* c, const double* a, int64_t n, int64_t ld_host,
   if (!c || !out) return HFPX_ERR_ARG;
   *out = nullptr;
   if (!a || n < 1 || ld_host < n) return set_error(c, HFPX_ERR_ARG, "bad matrix dimensions");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   hfpx_matrix* m = nullptr;
   int rc = new_matrix(c, n, &m);
   if (rc) return rc;
@@ -351,7 +351,7 @@ int hfpx_matrix_pivots(hfpx_ctx* c, const hfpx_matrix* m, int32_t* ipiv) {
   if (!c) return HFPX_ERR_ARG;
   if (!m || !ipiv) return set_error(c, HFPX_ERR_ARG, "null argument");
   if (m->factored != 1) return set_error(c, HFPX_ERR_STATE, "no FP64 factorisation");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   int rc = check_cuda(c, cudaMemcpyAsync(ipiv, m->d_piv, sizeof(int32_t) * m->n, cudaMemcpyDeviceToHost, c->stream),
                       "pivots");
   return rc ? rc : check_cuda(c, cudaStreamSynchronize(c->stream), "pivots");
@@ -388,7 +388,7 @@ int hfpx_matrix_dims(const hfpx_matrix* m, int64_t* n, int64_t* ld) {
 
 int hfpx_matrix_download(hfpx_ctx* c, const hfpx_matrix* m, double* a, int64_t ld_host) {
   if (!c || !m || !a || ld_host < m->n) return set_error(c, HFPX_ERR_ARG, "bad download arguments");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   int rc = check_cuda(c, cudaMemcpy2DAsync(a, ld_host * sizeof(double), m->d_a, m->ld * sizeof(double), m->n * sizeof(double),
                                            m->n, cudaMemcpyDeviceToHost, c->stream),
                       "matrix download");
@@ -426,7 +426,7 @@ int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   if (!c) return HFPX_ERR_ARG;
   if (!mesh || !dof_h || !s_inf || !rhs || n_rhs < 1 || ld_rhs < n_dof || n_dof < 1)
     return set_error(c, HFPX_ERR_ARG, "bad rhs arguments");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   ScratchBuf ds(c, kScrHostSinf), dr(c, kScrHostRhs);
   int32_t* dd = nullptr;
   int rc = upload_dof(c, dof_h, mesh->n_el, n_dof, &dd);
@@ -446,7 +446,7 @@ int hfpx_lu_factor(hfpx_ctx* c, hfpx_matrix* m, int mode, int64_t* info) {
   if (!m) return set_error(c, HFPX_ERR_ARG, "null matrix");
   if (mode != HFPX_LU_FP64 && mode != HFPX_LU_MIXED) return set_error(c, HFPX_ERR_ARG, "unknown LU mode");
   if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "matrix already factored in place");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   int rc = mode == HFPX_LU_FP64 ? lu_factor_fp64(c, m) : lu_factor_fp32(c, m);
   if (info) *info = m->info;
   return rc;
@@ -458,7 +458,7 @@ int hfpx_lu_solve(hfpx_ctx* c, const hfpx_matrix* m, double* b, int64_t nrhs, in
   if (!m || !b || nrhs < 1 || ld_b < m->n) return set_error(c, HFPX_ERR_ARG, "bad solve arguments");
   if (m->factored == 0) return set_error(c, HFPX_ERR_STATE, "solve before factor");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   ScratchBuf db(c, kScrHostRhs);
   int rc = check_cuda(c, db.alloc(sizeof(double) * m->ld * nrhs), "rhs alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpy2DAsync(db.p, m->ld * sizeof(double), b, ld_b * sizeof(double), m->n * sizeof(double),
@@ -488,7 +488,7 @@ int hfpx_lu_solve_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t
   if (!m || !d_b || nrhs < 1 || ld_b < m->n) return set_error(c, HFPX_ERR_ARG, "bad solve arguments");
   if (m->factored == 0) return set_error(c, HFPX_ERR_STATE, "solve before factor");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   if (m->factored == 1) {
     if (info) { info->iterations = 0; info->residual = 0.0; info->converged = 1; }
     return lu_solve_fp64(c, m, d_b, nrhs, ld_b);
@@ -502,7 +502,7 @@ int hfpx_gmres_device(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, double tol
   if (!m || !d_b) return set_error(c, HFPX_ERR_ARG, "bad GMRES arguments");
   if (m->factored != 2) return set_error(c, HFPX_ERR_STATE, "GMRES needs a mixed factorisation of the matrix");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   return gmres_solve(c, m, d_b, tol > 0 ? tol : 1e-12, restart > 0 ? restart : 50, max_iter > 0 ? max_iter : 200,
                      info);
 }
@@ -513,7 +513,7 @@ int hfpx_gmres(hfpx_ctx* c, const hfpx_matrix* m, double* b, double tol, int res
   if (!m || !b) return set_error(c, HFPX_ERR_ARG, "bad GMRES arguments");
   if (m->factored != 2) return set_error(c, HFPX_ERR_STATE, "GMRES needs a mixed factorisation of the matrix");
   if (m->info != 0) return set_error(c, HFPX_ERR_SINGULAR, "matrix is singular");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   ScratchBuf db(c, kScrHostRhs);
   int rc = check_cuda(c, db.alloc(sizeof(double) * m->n), "rhs alloc");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(db.p, b, sizeof(double) * m->n, cudaMemcpyHostToDevice, c->stream), "rhs");
@@ -577,8 +577,9 @@ int hfpx_stress(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, int is_
   if (!c) return HFPX_ERR_ARG;
   if (!mesh || !dd || !pts || !s_inf || !out || n_pts < 1) return set_error(c, HFPX_ERR_ARG, "bad stress arguments");
   if (!(G > 0) || !(nu > -1.0 && nu < 0.5)) return set_error(c, HFPX_ERR_ARG, "bad elastic constants");
-  cudaSetDevice(c->device);
-  DevBuf ddd, dp, ds, dout;
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
+  // work buffers kept by the context: a loop of stress evaluations allocates nothing
+  ScratchBuf ddd(c, kScrStressDd), dp(c, kScrStressPts), ds(c, kScrStressSinf), dout(c, kScrStressOut);
   const int64_t ne = mesh->n_el;
   int rc = check_cuda(c, ddd.alloc(sizeof(double) * 18 * ne), "dd alloc");
   if (!rc) rc = check_cuda(c, dp.alloc(sizeof(double) * 3 * n_pts), "pts alloc");
@@ -602,9 +603,10 @@ int hfpx_stress_batch(hfpx_ctx* c, const hfpx_mesh* mesh, double G, double nu, i
     return set_error(c, HFPX_ERR_ARG, "bad stress arguments");
   if (!(G > 0) || !(nu > -1.0 && nu < 0.5)) return set_error(c, HFPX_ERR_ARG, "bad elastic constants");
   if (n_cases == 1) return hfpx_stress(c, mesh, G, nu, is_dd_local, dd, pts, n_pts, s_inf, out);
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   const int64_t ne = mesh->n_el, rows = 6 * n_pts, cols = 18 * ne;
-  DevBuf dm, ddd, dvec, dp, ds, dS, dout;
+  ScratchBuf dm(c, kScrStressInfl), ddd(c, kScrStressDd), dvec(c, kScrStressVec), dp(c, kScrStressPts),
+      ds(c, kScrStressSinf), dS(c, kScrStressSum), dout(c, kScrStressOut);
   int rc = check_cuda(c, dm.alloc(sizeof(double) * rows * cols), "influence matrix alloc");
   if (!rc) rc = check_cuda(c, ddd.alloc(sizeof(double) * cols * n_cases), "dd alloc");
   if (!rc) rc = check_cuda(c, dvec.alloc(sizeof(double) * cols * n_cases), "dd vectors alloc");
@@ -637,7 +639,7 @@ int hfpx_local_submatrix(hfpx_ctx* c, double G, double nu, double h, double zr, 
                          const double* sfm, double* out) {
   if (!c) return HFPX_ERR_ARG;
   if (!tau || !sfm || !out) return set_error(c, HFPX_ERR_ARG, "null argument");
-  cudaSetDevice(c->device);
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   DevBuf dt, ds, dout;
   int rc = check_cuda(c, dt.alloc(sizeof(double) * 6), "alloc");
   if (!rc) rc = check_cuda(c, ds.alloc(sizeof(double) * 72), "alloc");

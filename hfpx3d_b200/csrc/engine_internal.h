@@ -22,7 +22,7 @@ struct hfpx_ctx {
   int* d_flags = nullptr;          // device status words (see kernels)
   // device work buffers kept between calls (grown on demand, freed with the
   // context), so repeated factorisations and solves allocate nothing
-  static constexpr int kScratchSlots = 40;
+  static constexpr int kScratchSlots = 48;
   void* scratch[kScratchSlots] = {};
   size_t scratch_bytes[kScratchSlots] = {};
   // tile triangular solves: tiles the flag array covers, epoch of the last
@@ -130,7 +130,8 @@ enum : int {
   kScrLLErr, kScrLinv, kScrA12, kScrL16, kScrU16, kScrAmax, kScrCoef, kScrPerm, kScrSolveTmp, kScrRefX,
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
-  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrCount
+  kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrStressDd, kScrStressPts, kScrStressSinf,
+  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrCount
 };
 
 // assembly.cu

@@ -546,8 +546,16 @@ int hfpx_gmres_precond_device(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_prec
     }
     if (mm->d_f) Af = mm->d_f;
   }
+  // HFPX_GMRES_RELAX sets the product accuracy assumed for the FP32 copy
+  // (default 1e-6, about 16 times its entries' rounding): FP32 products start
+  // once |r| / |b| <= tol / that accuracy.
+  double eps32 = 1e-6;
+  if (const char* er = std::getenv("HFPX_GMRES_RELAX")) {
+    const double v = std::atof(er);
+    if (v > 0.0 && v < 1.0) eps32 = v;
+  }
   return gmres_core(c, m->d_a, m->ld, n, d_b, tol, restart > 0 ? restart : 50, max_iter > 0 ? max_iter : 1000, info,
-                    apply, Af, std::min(1e-2, tol / 1e-6));
+                    apply, Af, std::min(1e-2, tol / eps32));
 }
 
 int hfpx_gmres_precond(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_precond* pc, double* b, double tol, int restart,
