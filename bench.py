@@ -56,13 +56,13 @@ def peaks():
 
 
 # DRAM bytes per matrix entry written by the in-plane assembly kernel, from
-# the ncu capture of profiles/assemble_kernel_penny1000.md (4.6305 GB for an
+# an ncu capture of one launch on the 1000-element penny (4.6305 GB for an
 # 18 000 x 18 000 fill; traffic grows with the entries, so it scales by N^2)
 ASM_DRAM_BYTES_PER_ENTRY = 4.630537e9 / 18000 ** 2
 # DRAM bytes (read + write) per matrix entry of one FP64 operator product's
 # resid_partial_kernel: 3.7327 GB read + 11.8 MB of partial sums written at
-# N = 21 600 in an ncu capture of one launch (profiles/resid_partial_kernels_penny1200.md);
-# the traffic grows with the entries, so N^2 times this is a launch at any N
+# N = 21 600 in an ncu capture of one launch (1200-element penny); the traffic
+# grows with the entries, so N^2 times this is a launch at any N
 RESID_DRAM_BYTES_PER_ENTRY = (3.732682e9 + 11.813888e6) / 21600.0 ** 2
 
 
