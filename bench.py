@@ -169,7 +169,8 @@ class Forms:
             # blocks made again from this step's matrix, in the storage of
             # the first step's preconditioner (hfpx_precond_update)
             if self.pc is None:
-                self.pc = engine.Precond(ctx, self.dm, A, engine.HFPX_PC_LEARNED, net=self.net, shear_m=G)
+                kind = engine.HFPX_PC_LEARNED | (engine.HFPX_PC_COARSE if self.args.coarse else 0)
+                self.pc = engine.Precond(ctx, self.dm, A, kind, net=self.net, shear_m=G)
             else:
                 self.pc.update(A, net=self.net, shear_m=G)
             self._host('precond', t0)
@@ -321,6 +322,7 @@ def run_engine(args, rank, world, local_rank):
     # alone on the engine's stream: N^2 8 bytes of matrix per launch
     resid = None
     if rank == 0:
+        engine.assemble_into(ctx, dm, dof, n, G, NU, A)  # the operator again (an FP64 step leaves factors)
         resid = time_residual(ctx, engine, L, torch, stream, A, d_rhs, d_x, n)
 
     # the 1025-element volume-control ellipse, measured on the engine as well
@@ -549,7 +551,8 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, form, stream, torch, A, F)
         si = engine.SolveInfo()
         if form == 'learned':
             pc = ctypes.c_void_p()
-            ctx.check(L.hfpx_precond_create(ctx.h, mh, A.h, engine.HFPX_PC_LEARNED, F.net.h, G, ctypes.byref(pc)))
+            kind = engine.HFPX_PC_LEARNED | (engine.HFPX_PC_COARSE if args.coarse else 0)
+            ctx.check(L.hfpx_precond_create(ctx.h, mh, A.h, kind, F.net.h, G, ctypes.byref(pc)))
             rc = L.hfpx_gmres_precond(ctx.h, A.h, pc, engine._dp(hr), args.tol, 50, 2000, ctypes.byref(si))
             L.hfpx_precond_destroy(pc)
             ctx.check(rc)
@@ -732,6 +735,9 @@ def main():
                     help='the form of the timed step (the other fast form is timed once beside it)')
     ap.add_argument('--n-el', type=int, default=4000)
     ap.add_argument('--tol', type=float, default=1e-10)
+    ap.add_argument('--coarse', dest='coarse', action='store_true', default=True,
+                    help='learned form: two-level preconditioner (coarse correction over element aggregates)')
+    ap.add_argument('--no-coarse', dest='coarse', action='store_false')
     ap.add_argument('--solver', default='gmres', choices=['refine', 'gmres'],
                     help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
                          'FP32 factors')

@@ -50,6 +50,21 @@ struct NearPattern {
 
 struct hfpx_gnn_graph;
 
+// Coarse space of a mesh for the two-level preconditioner: the elements
+// grouped into aggregates (k-means of their centroids), and on each aggregate
+// the DD components' linear functions 1, xi, eta in the aggregate's tangent
+// plane, sampled at the element nodes.  Coarse unknown 9 a + 3 m + k is
+// basis function m (1, xi, eta) of DD component k on aggregate a; P (n x nc)
+// has P[18 e + 3 node + k, 9 agg(e) + 3 m + k] = w[(6 e + node) 3 + m].
+struct CoarseSpace {
+  int64_t n_el = 0, n_agg = 0, nc = 0;
+  int agg_size = 0, max_agg = 0;
+  std::vector<int32_t> agg_of, ptr, el;   // element -> aggregate; elements of aggregate a: el[ptr[a] .. ptr[a+1])
+  std::vector<double> w;                  // n_el x 6 nodes x 3 basis values
+  int32_t *d_ptr = nullptr, *d_el = nullptr, *d_agg_of = nullptr;
+  double* d_w = nullptr;
+};
+
 struct hfpx_mesh {
   int64_t n_el = 0;
   void* d_elem = nullptr;          // ElemRec[n_el]
@@ -61,6 +76,7 @@ struct hfpx_mesh {
   // built on first use and kept with the mesh: the near-field pattern and the
   // learned preconditioner's graph (geometry inputs and buffers)
   std::shared_ptr<NearPattern> pattern;
+  std::shared_ptr<CoarseSpace> coarse;
   hfpx_gnn_graph* gnn_graph = nullptr;
 };
 
@@ -73,6 +89,14 @@ struct hfpx_precond {
   std::shared_ptr<NearPattern> pat;   // the mesh's
   double* d_blocks = nullptr;      // blocks() x 18 x 18, each column-major
   double* d_dinv = nullptr;        // inverses of the diagonal blocks, n_el x 18 x 18
+  // two-level form (kind with HFPX_PC_COARSE): the coarse space, A P
+  // (n x nc, column-major), the coarse operator P^T A P factored, its
+  // explicit inverse, and work vectors
+  std::shared_ptr<CoarseSpace> cs;
+  double* d_ap = nullptr;
+  hfpx_matrix* ac = nullptr;
+  double* d_acinv = nullptr;
+  double *d_q = nullptr, *d_cc = nullptr, *d_t = nullptr;
 };
 
 struct hfpx_matrix {
@@ -185,6 +209,23 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, 
 // first-order Neumann, exact local inverse, learned) and their product
 int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p);
 void free_pattern(NearPattern* p);
+// the mesh's coarse space with about agg_size elements per aggregate (built
+// on first use and kept with the mesh; rebuilt for another size)
+std::shared_ptr<CoarseSpace> mesh_coarse(hfpx_ctx* c, const hfpx_mesh* mesh, int agg_size);
+// A P, P^T A P and its inverse for pc (storage allocated) from the matrix m
+// (its FP32 copy when current, else the FP64 matrix)
+int coarse_setup(hfpx_ctx* c, hfpx_precond* pc, const hfpx_matrix* m);
+// z = Pc + M (v - A P c), c = (P^T A P)^-1 P^T v: the coarse correction,
+// then the near-field preconditioner M on what it leaves
+int coarse_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z);
+int coarse_alloc(hfpx_ctx* c, hfpx_precond* pc);
+void coarse_free(hfpx_precond* pc);
+int precond_apply_near(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z);
+// device memory from an engine-owned stream-ordered pool that keeps freed
+// blocks reserved (queued on the context's stream); pool_free first waits for
+// the device, as cudaFree does
+int pool_alloc(hfpx_ctx* c, void** p, size_t bytes, const char* what);
+void pool_free(void* p);
 // the mesh's pattern, built on first use (null on failure)
 std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh);
 void gnn_graph_release(hfpx_gnn_graph* g);

@@ -344,6 +344,10 @@ int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPa
 }
 
 int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z) {
+  return pc->cs ? coarse_apply(c, pc, v, z) : precond_apply_near(c, pc, v, z);
+}
+
+int precond_apply_near(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z) {
   const int64_t ne = pc->n_el;
   ++g_launches;
   block_spmv_kernel<<<(unsigned)((ne * 32 + 255) / 256), 256, 0, c->stream>>>(
@@ -351,19 +355,12 @@ int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* 
   return check_cuda(c, cudaGetLastError(), "preconditioner product");
 }
 
-}  // namespace hfpx
-
-// ------------------------------------------------------------------ C-ABI
-using namespace hfpx;
-
-namespace {
-
 // Preconditioner storage comes from an engine-owned stream-ordered pool per
 // device whose release threshold keeps freed memory reserved, so a loop that
 // creates and destroys a preconditioner each step (a new mesh each step)
 // maps device memory once instead of every step (cudaMalloc / cudaFree of the
 // blocks cost tens of milliseconds at 4,000 elements).
-cudaMemPool_t block_pool(int dev) {
+static cudaMemPool_t block_pool(int dev) {
   static std::mutex mu;
   static cudaMemPool_t pools[64] = {};
   if (dev < 0 || dev >= 64) return nullptr;
@@ -400,10 +397,19 @@ void pool_free(void* p) {
   if (cudaFreeAsync(p, cudaStreamLegacy) != cudaSuccess) cudaGetLastError();
 }
 
+}  // namespace hfpx
+
+// ------------------------------------------------------------------ C-ABI
+using namespace hfpx;
+
+namespace {
+
 int precond_check(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, int kind, const hfpx_gnn* net,
                   double shear_m) {
   if (!mesh || !m) return set_error(c, HFPX_ERR_ARG, "null mesh or matrix");
-  if (kind < HFPX_PC_BLOCK_JACOBI || kind > HFPX_PC_LEARNED) return set_error(c, HFPX_ERR_ARG, "unknown preconditioner");
+  if ((kind & ~HFPX_PC_COARSE) < HFPX_PC_BLOCK_JACOBI || (kind & ~HFPX_PC_COARSE) > HFPX_PC_LEARNED)
+    return set_error(c, HFPX_ERR_ARG, "unknown preconditioner");
+  kind &= ~HFPX_PC_COARSE;
   if (kind == HFPX_PC_LEARNED && !net) return set_error(c, HFPX_ERR_ARG, "the learned preconditioner needs a network");
   if (m->n != 18 * mesh->n_el)
     return set_error(c, HFPX_ERR_ARG, "near-field preconditioners need a matrix of 18 DoF per element (no fixed DoF, "
@@ -429,6 +435,7 @@ int precond_fill(hfpx_ctx* c, hfpx_precond* pc, const hfpx_mesh* mesh, const hfp
       rc = neumann_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_dinv, pc->d_blocks, pc->kind != HFPX_PC_BLOCK_JACOBI);
   }
   if (!rc && pc->kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
+  if (!rc && pc->cs) rc = coarse_setup(c, pc, m);
   int herr = 0;
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "preconditioner");
@@ -448,7 +455,7 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
   if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
   hfpx_precond* pc = new (std::nothrow) hfpx_precond;
   if (!pc) return set_error(c, HFPX_ERR_NOMEM, "preconditioner");
-  pc->kind = kind;
+  pc->kind = kind & ~HFPX_PC_COARSE;
   pc->n_el = mesh->n_el;
   pc->n = m->n;
   pc->mesh = mesh;
@@ -457,6 +464,7 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
   const int64_t nb = rc ? 0 : pc->pat->blocks();
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_blocks, sizeof(double) * 324 * nb, "blocks");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_dinv, sizeof(double) * 324 * pc->n_el, "block inverses");
+  if (!rc && (kind & HFPX_PC_COARSE)) rc = coarse_alloc(c, pc);
   if (!rc) rc = precond_fill(c, pc, mesh, m, net, shear_m);
   if (rc) {
     hfpx_precond_destroy(pc);
@@ -480,6 +488,7 @@ int hfpx_precond_destroy(hfpx_precond* pc) {
   pc->pat.reset();
   pool_free(pc->d_blocks);
   pool_free(pc->d_dinv);
+  coarse_free(pc);
   delete pc;
   return HFPX_OK;
 }

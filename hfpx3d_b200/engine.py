@@ -74,6 +74,7 @@ SIGNATURES = {
     'hfpx_precond_create': (_int, [_V, _V, _V, _int, _V, _f64, ctypes.POINTER(_V)]),
     'hfpx_precond_destroy': (_int, [_V]),
     'hfpx_precond_update': (_int, [_V, _V, _V, _V, _f64]),
+    'hfpx_precond_coarse': (_int, [_V, _V, _L, ctypes.POINTER(ctypes.c_int32), _D, _D, _D]),
     'hfpx_precond_blocks': (_int, [_V, _V, _L, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32), _D]),
     'hfpx_gmres_precond': (_int, [_V, _V, _V, _D, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
     'hfpx_gmres_precond_device': (_int, [_V, _V, _V, _V, _f64, _int, _int, ctypes.POINTER(SolveInfo)]),
@@ -488,6 +489,7 @@ def write_dd_vector_to_md(sol, dof_h, n_el):
 
 # ------------------------------------------------- near-field preconditioners
 HFPX_PC_BLOCK_JACOBI, HFPX_PC_NEUMANN, HFPX_PC_LOCAL_INVERSE, HFPX_PC_LEARNED = 0, 1, 2, 3
+HFPX_PC_COARSE = 16  # or'ed with a kind: the two-level form
 # the trained network shipped with the engine (HFPX_PC_WEIGHTS overrides the path)
 WEIGHTS_PATH = os.environ.get('HFPX_PC_WEIGHTS') or os.path.join(_HERE, 'data', 'pc_gnn.bin')
 
@@ -509,6 +511,22 @@ class Precond:
         self.h = _V()
         ctx.check(lib().hfpx_precond_create(ctx.h, dmesh.h, matrix.h, kind, net.h if net is not None else None,
                                             shear_m, ctypes.byref(self.h)))
+
+    def coarse(self, with_ap=False):
+        """The coarse level (two-level kinds): (agg_of_el, weights[n_el, 6, 3],
+        A P or None, inverse of P^T A P or None)."""
+        na = _i64()
+        self.ctx.check(lib().hfpx_precond_coarse(self.ctx.h, self.h, ctypes.byref(na), None, None, None, None))
+        ne = self.dmesh.n_el
+        n = 18 * ne
+        nc = 9 * na.value
+        agg = np.empty(ne, dtype=np.int32)
+        w = np.empty(ne * 18)
+        ap = np.empty((n, nc), order='F') if with_ap else None
+        inv = np.empty((nc, nc), order='F') if with_ap else None
+        self.ctx.check(lib().hfpx_precond_coarse(self.ctx.h, self.h, ctypes.byref(na), _ip(agg), _dp(w),
+                                                 _dp(ap) if with_ap else None, _dp(inv) if with_ap else None))
+        return agg, w.reshape(ne, 6, 3), ap, inv
 
     def update(self, matrix: DeviceMatrix, net=None, shear_m=1.0):
         """The blocks made again from a re-assembled matrix of the same mesh,

@@ -11,9 +11,11 @@
 // (system_assembly.cpp:39-42, 287-290, 468-471) and every engine error abort
 // with a message.  There is no CPU fallback.
 //
-// mod_3dbem_system_vc (system_assembly.cpp:560-640) re-indexes a host matrix
-// for the Development/ fixed-point loop; it is host bookkeeping outside the
-// engine and is not defined here, so a program that calls it fails to link.
+// mod_3dbem_system_vc (system_assembly.cpp:560-629) is defined for the
+// bordered matrix its one caller passes (Development/c_f_iteration.cpp:285):
+// the reference version requires an orig_ndof-square matrix and then reads
+// its border one row past the end; here the border is the bordered matrix's
+// own last row and column, gathered on the device (hfpx_matrix_truncate).
 //
 //   HFPX_DEVICE   GPU to use (default 0)
 #include <cstdint>
@@ -185,6 +187,55 @@ il::Array2D<double> make_3dbem_stress_f_s(double shear_m, double poiss_r, const 
   for (int j = 0; j < 6; ++j)
     for (il::int_t p = 0; p < n_pts; ++p) out(p, j) = res[(size_t)(p + n_pts * j)];
   return out;
+}
+
+// mod_3dbem_system_vc (system_assembly.cpp:560-629): the truncated bordered
+// system of the DoF that dof_hndl keeps (dof_h >= 0), from orig_matrix, the
+// (orig_ndof + 1)-square matrix make_3dbem_matrix_vc returns for
+// orig_dof_hndl.  The corner stays 0 as the reference leaves it; delta_t is
+// indexed by the full element-node, the original or the truncated numbering,
+// told apart by its size as there; delta_v is the last right-hand side entry.
+SAE_T mod_3dbem_system_vc(const il::Array2D<double>& orig_matrix, const DoF_Handle_T& orig_dof_hndl,
+                          const DoF_Handle_T& dof_hndl, const il::Array<double>& delta_t, const double delta_v) {
+  expect(orig_matrix.size(0) == orig_matrix.size(1), "orig_matrix.size(0) == orig_matrix.size(1)");
+  const il::int_t num_of_ele = orig_dof_hndl.dof_h.size(0);
+  const il::int_t ndpe = orig_dof_hndl.dof_h.size(1);
+  expect(num_of_ele > 0, "num_of_ele > 0");
+  const il::int_t full_ndof = num_of_ele * ndpe;
+  const il::int_t orig_ndof = orig_dof_hndl.n_dof;
+  expect(orig_ndof > 0 && orig_ndof <= full_ndof, "orig_ndof > 0 && orig_ndof <= full_ndof");
+  expect(orig_ndof + 1 == orig_matrix.size(0), "orig_matrix is the bordered matrix (orig_ndof + 1 square)");
+  const il::int_t used_ndof = dof_hndl.n_dof;
+  expect(used_ndof > 0 && used_ndof <= orig_ndof, "used_ndof > 0 && used_ndof <= orig_ndof");
+  expect(dof_hndl.dof_h.size(0) == num_of_ele && dof_hndl.dof_h.size(1) == ndpe, "dof_hndl matches orig_dof_hndl");
+  const il::int_t tsize = delta_t.size();
+  expect(tsize == full_ndof || tsize == orig_ndof || tsize == used_ndof, "delta_t size");
+  std::vector<int64_t> keep((size_t)used_ndof, -1);
+  SAE_T sys;
+  sys.rhs_v = il::Array<double>{used_ndof + 1, 0.0};
+  sys.rhs_v[used_ndof] = delta_v;
+  for (il::int_t e = 0; e < num_of_ele; ++e)
+    for (il::int_t j = 0; j < ndpe; ++j) {
+      const il::int_t t = dof_hndl.dof_h(e, j);
+      if (t < 0) continue;
+      expect(t < used_ndof && keep[(size_t)t] < 0, "each truncated DoF at one element node");
+      const il::int_t o = orig_dof_hndl.dof_h(e, j);
+      expect(o >= 0 && o < orig_ndof, "a truncated DoF has an original DoF");
+      keep[(size_t)t] = o;
+      sys.rhs_v[t] = tsize == full_ndof ? delta_t[e * ndpe + j] : (tsize == orig_ndof ? delta_t[o] : delta_t[t]);
+    }
+  for (int64_t o : keep) expect(o >= 0, "the truncated numbering has no gaps");
+  hfpx_matrix *a = nullptr, *t = nullptr;
+  check(hfpx_matrix_upload(ctx(), orig_matrix.data(), orig_matrix.size(0), orig_matrix.stride(1), &a),
+        "matrix upload");
+  const int rc = hfpx_matrix_truncate(ctx(), a, keep.data(), used_ndof, 1, &t);
+  hfpx_matrix_destroy(a);
+  check(rc, "truncation");
+  sys.matrix = il::Array2D<double>{used_ndof + 1, used_ndof + 1};
+  const int rc2 = hfpx_matrix_download(ctx(), t, sys.matrix.data(), sys.matrix.stride(1));
+  hfpx_matrix_destroy(t);
+  check(rc2, "matrix download");
+  return sys;
 }
 
 }  // namespace hfp3d

@@ -235,7 +235,12 @@ typedef enum {
   HFPX_PC_BLOCK_JACOBI = 0,
   HFPX_PC_NEUMANN = 1,
   HFPX_PC_LOCAL_INVERSE = 2,
-  HFPX_PC_LEARNED = 3
+  HFPX_PC_LEARNED = 3,
+  /* or'ed with a kind above: the two-level form, a coarse correction over
+   * aggregates of about 30 elements (HFPX_PC_AGG overrides the size) with
+   * linear DD on each, before the near-field preconditioner:
+   * z = P c + M (v - A P c), c = (P^T A P)^-1 P^T v */
+  HFPX_PC_COARSE = 16
 } hfpx_pc_kind;
 int hfpx_precond_create(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix, int kind,
                         const hfpx_gnn *net, double shear_m, hfpx_precond **precond);
@@ -247,6 +252,13 @@ int hfpx_precond_create(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix 
 int hfpx_precond_update(hfpx_ctx *ctx, hfpx_precond *precond, const hfpx_matrix *matrix, const hfpx_gnn *net,
                         double shear_m);
 int hfpx_precond_destroy(hfpx_precond *precond);
+/* The coarse level of a two-level preconditioner (HFPX_PC_COARSE): the number
+ * of aggregates, each element's aggregate (n_el), the basis values
+ * (n_el x 6 nodes x 3: 1, xi, eta), A P (n x 9 n_agg, column-major, from the
+ * last create or update) and the coarse operator's inverse (9 n_agg square);
+ * null arrays are skipped. */
+int hfpx_precond_coarse(hfpx_ctx *ctx, const hfpx_precond *precond, int64_t *n_agg, int32_t *agg_of_el,
+                        double *weights, double *ap, double *acinv);
 /* The blocks (18 x 18 column-major each) and their block row and column:
  * call with null arrays to get n_blocks first. */
 int hfpx_precond_blocks(hfpx_ctx *ctx, const hfpx_precond *precond, int64_t *n_blocks, int32_t *block_row,
