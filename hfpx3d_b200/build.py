@@ -27,7 +27,7 @@ NVCC = os.path.join(CUDA, 'bin', 'nvcc')
 CXX = os.environ.get('CXX', 'g++')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3', '-std=c++17',
          '-Xcompiler', '-fPIC', '-shared', '--expt-relaxed-constexpr', '-I' + INCLUDE]
-LIBS = ['-L' + os.path.join(CUDA, 'lib64'), '-lcublas', '-Xlinker', '-rpath=' + os.path.join(CUDA, 'lib64')]
+LIBS = ['-L' + os.path.join(CUDA, 'lib64'), '-lcublas', '-lcusolver', '-Xlinker', '-rpath=' + os.path.join(CUDA, 'lib64')]
 # --exclude-libs: a toolchain that links its C++ runtime statically must not
 # re-export it from these libraries into the programs that load them
 HOST_FLAGS = ['-O2', '-std=c++17', '-Wall', '-I' + INCLUDE, '-I' + HOST, '-Wl,--exclude-libs,ALL']

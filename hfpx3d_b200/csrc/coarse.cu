@@ -20,8 +20,11 @@
 // read again.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <type_traits>
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <vector>
 #include "engine_internal.h"
@@ -53,32 +56,52 @@ __global__ void __launch_bounds__(kApThreads) ap_kernel(const T* __restrict__ A,
   for (int i = 0; i < R; ++i)
 #pragma unroll
     for (int j = 0; j < 9; ++j) acc[i][j] = 0.0;
-  const bool full = r0 + R <= n;
-  for (int le = 0; le < cnt; ++le) {
-    const T* col = A + r0 + lda * (18 * (int64_t)s_el[le]);
-    const double* wl = s_w + 18 * le;
+  if (r0 + R <= n) {
+    // whole rows: each element's 18 column loads issued before their products
+    using V = typename std::conditional<R == 4, float4, double2>::type;
+    for (int le = 0; le < cnt; ++le) {
+      const T* col = A + r0 + lda * (18 * (int64_t)s_el[le]);
+      const double* wl = s_w + 18 * le;
 #pragma unroll
-    for (int cidx = 0; cidx < 18; ++cidx) {
-      const int k = cidx % 3, node = cidx / 3;
-      double v[R];
-      if (full) {
-        if constexpr (R == 4) {
-          const float4 q = *reinterpret_cast<const float4*>(col + lda * cidx);
-          v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-        } else {
-          const double2 q = *reinterpret_cast<const double2*>(col + lda * cidx);
-          v[0] = q.x; v[1] = q.y;
+      for (int half = 0; half < 2; ++half) {  // nodes 0-2, then 3-5: 9 loads in flight
+        V q[9];
+#pragma unroll
+        for (int u = 0; u < 9; ++u) q[u] = __ldcs(reinterpret_cast<const V*>(col + lda * (9 * half + u)));
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+          const int k = u % 3, node = 3 * half + u / 3;
+          double v[R];
+          if constexpr (R == 4) {
+            v[0] = q[u].x; v[1] = q[u].y; v[2] = q[u].z; v[3] = q[u].w;
+          } else {
+            v[0] = q[u].x; v[1] = q[u].y;
+          }
+          const double w0 = wl[3 * node], w1 = wl[3 * node + 1], w2 = wl[3 * node + 2];
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            acc[i][k] = fma(v[i], w0, acc[i][k]);
+            acc[i][3 + k] = fma(v[i], w1, acc[i][3 + k]);
+            acc[i][6 + k] = fma(v[i], w2, acc[i][6 + k]);
+          }
         }
-      } else {
-#pragma unroll
-        for (int i = 0; i < R; ++i) v[i] = r0 + i < n ? (double)col[lda * cidx + i] : 0.0;
       }
-      const double w0 = wl[3 * node], w1 = wl[3 * node + 1], w2 = wl[3 * node + 2];
+    }
+  } else {
+    for (int le = 0; le < cnt; ++le) {
+      const T* col = A + r0 + lda * (18 * (int64_t)s_el[le]);
+      const double* wl = s_w + 18 * le;
 #pragma unroll
-      for (int i = 0; i < R; ++i) {
-        acc[i][k] = fma(v[i], w0, acc[i][k]);
-        acc[i][3 + k] = fma(v[i], w1, acc[i][3 + k]);
-        acc[i][6 + k] = fma(v[i], w2, acc[i][6 + k]);
+      for (int cidx = 0; cidx < 18; ++cidx) {
+        const int k = cidx % 3, node = cidx / 3;
+        const double w0 = wl[3 * node], w1 = wl[3 * node + 1], w2 = wl[3 * node + 2];
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+          if (r0 + i < n) {
+            const double v = (double)col[lda * cidx + i];
+            acc[i][k] = fma(v, w0, acc[i][k]);
+            acc[i][3 + k] = fma(v, w1, acc[i][3 + k]);
+            acc[i][6 + k] = fma(v, w2, acc[i][6 + k]);
+          }
       }
     }
   }
@@ -360,40 +383,62 @@ int coarse_alloc(hfpx_ctx* c, hfpx_precond* pc) {
   pc->cs = mesh_coarse(c, pc->mesh, env_agg_size());
   if (!pc->cs) return set_error(c, HFPX_ERR_NOMEM, "coarse space");
   const int64_t n = pc->n, nc = pc->cs->nc;
-  hfpx_matrix* ac = new (std::nothrow) hfpx_matrix;
-  if (!ac) return set_error(c, HFPX_ERR_NOMEM, "coarse operator");
-  ac->n = nc;
-  ac->ld = (nc + 31) / 32 * 32;
-  pc->ac = ac;
+  if (!c->cusolver) {
+    cusolverDnHandle_t h = nullptr;
+    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return set_error(c, HFPX_ERR_CUDA, "cuSOLVER handle");
+    cusolverDnSetStream(h, c->stream);
+    c->cusolver = h;
+  }
+  int lwork = 0;
+  if (cusolverDnDgetrf_bufferSize(static_cast<cusolverDnHandle_t>(c->cusolver), (int)nc, (int)nc, nullptr, (int)nc,
+                                  &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return set_error(c, HFPX_ERR_CUDA, "coarse LU workspace");
+  pc->acwork_bytes = sizeof(double) * (size_t)std::max(1, lwork);
   int rc = pool_alloc(c, (void**)&pc->d_ap, sizeof(double) * n * nc, "A P");
+  if (!rc) rc = pool_alloc(c, (void**)&pc->d_ac, sizeof(double) * nc * nc, "coarse operator");
+  if (!rc) rc = pool_alloc(c, (void**)&pc->d_acpiv, sizeof(int32_t) * nc, "coarse pivots");
+  if (!rc) rc = pool_alloc(c, (void**)&pc->d_acinfo, sizeof(int), "coarse status");
+  if (!rc) rc = pool_alloc(c, &pc->d_acwork, pc->acwork_bytes, "coarse LU workspace");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_acinv, sizeof(double) * nc * nc, "coarse inverse");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_q, sizeof(double) * nc, "coarse vectors");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_cc, sizeof(double) * nc, "coarse vectors");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_t, sizeof(double) * n, "coarse vectors");
-  if (!rc) rc = pool_alloc(c, (void**)&ac->d_a, sizeof(double) * ac->ld * nc, "coarse operator");
-  if (!rc) rc = pool_alloc(c, (void**)&ac->d_piv, sizeof(int32_t) * nc, "coarse pivots");
   return rc;
 }
 
 void coarse_free(hfpx_precond* pc) {
-  for (double* p : {pc->d_ap, pc->d_acinv, pc->d_q, pc->d_cc, pc->d_t}) pool_free(p);
-  pc->d_ap = pc->d_acinv = pc->d_q = pc->d_cc = pc->d_t = nullptr;
-  if (hfpx_matrix* ac = pc->ac) {
-    pool_free(ac->d_a);
-    pool_free(ac->d_piv);
-    ac->d_a = nullptr;
-    ac->d_piv = nullptr;
-    hfpx_matrix_destroy(ac);  // whatever else the solves attached to it
-  }
-  pc->ac = nullptr;
+  for (void* p : {(void*)pc->d_ap, (void*)pc->d_ac, (void*)pc->d_acpiv, (void*)pc->d_acinfo, pc->d_acwork,
+                  (void*)pc->d_acinv, (void*)pc->d_q, (void*)pc->d_cc, (void*)pc->d_t})
+    pool_free(p);
+  pc->d_ap = pc->d_ac = pc->d_acinv = pc->d_q = pc->d_cc = pc->d_t = nullptr;
+  pc->d_acpiv = nullptr;
+  pc->d_acinfo = nullptr;
+  pc->d_acwork = nullptr;
   pc->cs.reset();
+}
+
+// HFPX_PROFILE=1: event times of the coarse set-up's phases to stderr
+static bool coarse_profile() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_PROFILE");
+    return e && *e == '1';
+  }();
+  return on;
 }
 
 int coarse_setup(hfpx_ctx* c, hfpx_precond* pc, const hfpx_matrix* m) {
   const CoarseSpace& cs = *pc->cs;
-  const int64_t n = pc->n, nc = cs.nc;
   const size_t smem = sizeof(double) * 18 * cs.max_agg + sizeof(int32_t) * cs.max_agg;
   if (smem > 200 * 1024) return set_error(c, HFPX_ERR_ARG, "an aggregate too large for the coarse pass");
+  cudaEvent_t ev[5] = {};
+  const bool prof = coarse_profile();
+  if (prof)
+    for (auto& e : ev) cudaEventCreate(&e);
+  auto mark = [&](int i) {
+    if (prof) cudaEventRecord(ev[i], c->stream);
+  };
+  mark(0);
+  const int64_t n = pc->n, nc = cs.nc;
   ++g_launches;
   if (m->d_f && m->f32_current) {
     constexpr int R = 4;
@@ -410,28 +455,44 @@ int coarse_setup(hfpx_ctx* c, hfpx_precond* pc, const hfpx_matrix* m) {
                                                                 pc->d_ap);
   }
   int rc = check_cuda(c, cudaGetLastError(), "A P");
-  hfpx_matrix* ac = pc->ac;
+  mark(1);
   if (!rc) {
     ++g_launches;
     coarse_matrix_kernel<<<dim3((unsigned)((nc + 127) / 128), (unsigned)cs.n_agg), 128, 0, c->stream>>>(
-        pc->d_ap, n, nc, cs.d_ptr, cs.d_el, cs.d_w, ac->d_a, ac->ld);
+        pc->d_ap, n, nc, cs.d_ptr, cs.d_el, cs.d_w, pc->d_ac, nc);
     rc = check_cuda(c, cudaGetLastError(), "coarse operator");
   }
-  // the engine's FP64 LU of the coarse operator, then its explicit inverse
-  if (!rc) {
-    ac->factored = 0;
-    ac->info = 0;
-    ac->dinv_valid = 0;
-    ac->f32_current = 0;
-    int64_t info = 0;
-    rc = hfpx_lu_factor(c, ac, HFPX_LU_FP64, &info);
-    if (rc == HFPX_ERR_SINGULAR) rc = set_error(c, HFPX_ERR_SINGULAR, "the coarse operator is singular");
-  }
+  mark(2);
+  // LU of the coarse operator (cuSOLVER's dense getrf: a library
+  // factorisation of an nc x nc matrix that lives in L2), then its explicit
+  // inverse by getrs on the identity
+  cusolverDnHandle_t hs = static_cast<cusolverDnHandle_t>(c->cusolver);
+  cusolverDnSetStream(hs, c->stream);
+  if (!rc && cusolverDnDgetrf(hs, (int)nc, (int)nc, pc->d_ac, (int)nc, static_cast<double*>(pc->d_acwork),
+                              pc->d_acpiv, pc->d_acinfo) != CUSOLVER_STATUS_SUCCESS)
+    rc = set_error(c, HFPX_ERR_CUDA, "coarse LU");
+  int hinfo = 0;
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&hinfo, pc->d_acinfo, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                           "coarse status");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(pc->d_acinv, 0, sizeof(double) * nc * nc, c->stream), "coarse inverse");
   if (!rc) {
     ++g_launches;
     identity_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, c->stream>>>(pc->d_acinv, nc);
-    rc = hfpx_lu_solve_device(c, ac, pc->d_acinv, nc, nc, 0.0, 0, nullptr);
+    rc = check_cuda(c, cudaStreamSynchronize(c->stream), "coarse LU");
+  }
+  if (!rc && hinfo != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "the coarse operator is singular");
+  mark(3);
+  if (!rc && cusolverDnDgetrs(hs, CUBLAS_OP_N, (int)nc, (int)nc, pc->d_ac, (int)nc, pc->d_acpiv, pc->d_acinv, (int)nc,
+                              pc->d_acinfo) != CUSOLVER_STATUS_SUCCESS)
+    rc = set_error(c, HFPX_ERR_CUDA, "coarse inverse");
+  mark(4);
+  if (prof) {
+    cudaEventSynchronize(ev[4]);
+    float t[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
+    std::fprintf(stderr, "[hfpx profile] coarse set-up (%lld aggregates, nc %lld): A P %.3f ms, P^T A P %.3f ms, "
+                 "LU %.3f ms, inverse %.3f ms\n", (long long)cs.n_agg, (long long)nc, t[0], t[1], t[2], t[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
   }
   return rc;
 }

@@ -1,6 +1,7 @@
 // C-ABI of the engine (include/hfpx_engine.h): objects, argument checks,
 // host<->device copies around the kernels of assembly.cu and lu.cu.
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -143,6 +144,7 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   if (c->stream_left) cudaStreamSynchronize(c->stream_left);
   if (c->cublas) cublasDestroy(static_cast<cublasHandle_t>(c->cublas));
   if (c->cublas_panel) cublasDestroy(static_cast<cublasHandle_t>(c->cublas_panel));
+  if (c->cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(c->cusolver));
   if (c->d_flags) cudaFree(c->d_flags);
   for (void* p : c->scratch)
     if (p) cudaFree(p);

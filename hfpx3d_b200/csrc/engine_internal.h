@@ -18,6 +18,7 @@ struct hfpx_ctx {
   // handle, deferred left-side row swaps on a third stream
   cudaStream_t stream_panel = nullptr, stream_left = nullptr;
   void* cublas_panel = nullptr;
+  void* cusolver = nullptr;        // cusolverDnHandle_t (small dense LU), made on first use
   std::string last_error;
   int* d_flags = nullptr;          // device status words (see kernels)
   // device work buffers kept between calls (grown on demand, freed with the
@@ -94,7 +95,11 @@ struct hfpx_precond {
   // explicit inverse, and work vectors
   std::shared_ptr<CoarseSpace> cs;
   double* d_ap = nullptr;
-  hfpx_matrix* ac = nullptr;
+  double* d_ac = nullptr;          // P^T A P, then its LU factors (nc x nc)
+  int32_t* d_acpiv = nullptr;
+  int* d_acinfo = nullptr;
+  void* d_acwork = nullptr;        // the factorisation's workspace
+  size_t acwork_bytes = 0;
   double* d_acinv = nullptr;
   double *d_q = nullptr, *d_cc = nullptr, *d_t = nullptr;
 };
@@ -155,7 +160,7 @@ enum : int {
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
   kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrStressDd, kScrStressPts, kScrStressSinf,
-  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrCount
+  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrGmresEst, kScrCount
 };
 
 // assembly.cu
