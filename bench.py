@@ -538,23 +538,35 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, form, stream, torch, A, F)
     if form == 'learned' and F.net is None:
         F.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
     times = []
+    host = {}
+
+    def tick(key, t0):
+        if k >= args.e2e_warmup:
+            host[key] = host.get(key, 0.0) + (time.perf_counter() - t0) * 1e3
+        return time.perf_counter()
     for k in range(args.e2e_warmup + args.e2e_steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
+        t0 = time.perf_counter()
         mh = ctypes.c_void_p()
         ctx.check(L.hfpx_mesh_create(ctx.h, engine._dp(hn), nods.shape[0], nods.shape[1], engine._lp(hc),
                                      conn.shape[0], conn.shape[1], BETA, ctypes.byref(mh)))
+        t0 = tick('mesh_create', t0)
         ctx.check(L.hfpx_assemble_into(ctx.h, mh, engine._lp(hd), n, G, NU, 0, 0, A.h))
         hr[:] = 0.0
         ctx.check(L.hfpx_rhs_sinf(ctx.h, mh, engine._lp(hd), n, engine._dp(s), 1, engine._dp(hr), n))
+        t0 = tick('assemble_rhs', t0)
         si = engine.SolveInfo()
         if form == 'learned':
             pc = ctypes.c_void_p()
             kind = engine.HFPX_PC_LEARNED | (engine.HFPX_PC_COARSE if args.coarse else 0)
             ctx.check(L.hfpx_precond_create(ctx.h, mh, A.h, kind, F.net.h, G, ctypes.byref(pc)))
+            t0 = tick('precond_create', t0)
             rc = L.hfpx_gmres_precond(ctx.h, A.h, pc, engine._dp(hr), args.tol, 50, 2000, ctypes.byref(si))
+            t0 = tick('gmres', t0)
             L.hfpx_precond_destroy(pc)
+            t0 = tick('precond_destroy', t0)
             ctx.check(rc)
         else:
             info_ = ctypes.c_int64()
@@ -566,12 +578,15 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, form, stream, torch, A, F)
                 ctx.check(L.hfpx_lu_solve(ctx.h, A.h, engine._dp(hr), 1, n, args.tol, 50, ctypes.byref(si)))
         e1.record(stream)
         torch.cuda.synchronize()
+        t0 = time.perf_counter()
         L.hfpx_mesh_destroy(mh)
+        tick('mesh_destroy (after the timed region)', t0)
         if k >= args.e2e_warmup:
             times.append(e0.elapsed_time(e1))
     h2d = hn.nbytes + hc.nbytes + 2 * hd.nbytes + hr.nbytes + s.nbytes  # dof_h goes up twice
     return {'value': statistics.mean(times) / 1e3, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d),
-            'd2h_bytes_per_step': int(hr.nbytes), 'steps': len(times), 'steps_ms': [round(t, 2) for t in times]}
+            'd2h_bytes_per_step': int(hr.nbytes), 'steps': len(times), 'steps_ms': [round(t, 2) for t in times],
+            'host_ms_per_step': {key: round(v / max(1, len(times)), 2) for key, v in host.items()}}
 
 
 # ------------------------------------------------------------- CPU reference
@@ -752,7 +767,7 @@ def main():
     ap.add_argument('--no-c2-ref', dest='c2_ref', action='store_false',
                     help='skip the CPU reference run of the 1025-element VC ellipse')
     ap.add_argument('--e2e-steps', type=int, default=3)
-    ap.add_argument('--e2e-warmup', type=int, default=1)
+    ap.add_argument('--e2e-warmup', type=int, default=3)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

@@ -240,7 +240,7 @@ bool build_coarse(const hfpx_mesh* m, int agg_size, CoarseSpace* cs) {
   std::vector<int32_t> lab(ne, 0);
   std::vector<double> sum(3 * na);
   std::vector<int64_t> cnt(na);
-  for (int it = 0; it < 12; ++it) {
+  for (int it = 0; it < 6; ++it) {  // a few Lloyd steps: the aggregates need to be compact, not optimal
     bool moved = false;
     for (int64_t e = 0; e < ne; ++e) {
       int32_t best = 0;
@@ -345,15 +345,15 @@ bool build_coarse(const hfpx_mesh* m, int agg_size, CoarseSpace* cs) {
 }
 
 void free_coarse(CoarseSpace* cs) {
-  for (void* p : {(void*)cs->d_ptr, (void*)cs->d_el, (void*)cs->d_agg_of, (void*)cs->d_w})
-    if (p) cudaFree(p);
+  void* ps[] = {(void*)cs->d_ptr, (void*)cs->d_el, (void*)cs->d_agg_of, (void*)cs->d_w};
+  pool_free_many(ps, 4);
   cs->d_ptr = cs->d_el = cs->d_agg_of = nullptr;
   cs->d_w = nullptr;
 }
 
 template <class T>
 int upload(hfpx_ctx* c, T** d, const std::vector<T>& h, const char* what) {
-  int rc = check_cuda(c, cudaMalloc(d, sizeof(T) * std::max<size_t>(1, h.size())), what);
+  int rc = pool_alloc(c, (void**)d, sizeof(T) * std::max<size_t>(1, h.size()), what);
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream), what);
   return rc;
 }
@@ -407,9 +407,9 @@ int coarse_alloc(hfpx_ctx* c, hfpx_precond* pc) {
 }
 
 void coarse_free(hfpx_precond* pc) {
-  for (void* p : {(void*)pc->d_ap, (void*)pc->d_ac, (void*)pc->d_acpiv, (void*)pc->d_acinfo, pc->d_acwork,
-                  (void*)pc->d_acinv, (void*)pc->d_q, (void*)pc->d_cc, (void*)pc->d_t})
-    pool_free(p);
+  void* ps[] = {(void*)pc->d_ap, (void*)pc->d_ac, (void*)pc->d_acpiv, (void*)pc->d_acinfo, pc->d_acwork,
+                (void*)pc->d_acinv, (void*)pc->d_q, (void*)pc->d_cc, (void*)pc->d_t};
+  pool_free_many(ps, 9);
   pc->d_ap = pc->d_ac = pc->d_acinv = pc->d_q = pc->d_cc = pc->d_t = nullptr;
   pc->d_acpiv = nullptr;
   pc->d_acinfo = nullptr;

@@ -234,7 +234,7 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
       m->h_vid[3 * e + j] = v;
       for (int k = 0; k < 3; ++k) m->h_vert[9 * e + 3 * j + k] = nods[k + ld_nods * v];
     }
-  if (!rc) rc = check_cuda(c, cudaMalloc(&m->d_elem, elem_record_bytes() * n_el), "element records");
+  if (!rc) rc = pool_alloc(c, &m->d_elem, elem_record_bytes() * n_el, "element records");
   if (!rc) launch_element_precompute(dn.as<double>(), ld_nods, dc.as<int64_t>(), ld_conn, n_el, beta, m->d_elem, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "element precompute");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "element precompute");
@@ -250,7 +250,7 @@ int hfpx_mesh_destroy(hfpx_mesh* m) {
   if (!m) return HFPX_OK;
   if (m->gnn_graph) gnn_graph_release(m->gnn_graph);
   m->pattern.reset();
-  if (m->d_elem) cudaFree(m->d_elem);
+  pool_free(m->d_elem);
   delete m;
   return HFPX_OK;
 }

@@ -231,6 +231,7 @@ int precond_apply_near(hfpx_ctx* c, const hfpx_precond* pc, const double* v, dou
 // the device, as cudaFree does
 int pool_alloc(hfpx_ctx* c, void** p, size_t bytes, const char* what);
 void pool_free(void* p);
+void pool_free_many(void* const* p, size_t count);
 // the mesh's pattern, built on first use (null on failure)
 std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh);
 void gnn_graph_release(hfpx_gnn_graph* g);

@@ -492,7 +492,7 @@ template <class T>
 T* galloc(hfpx_gnn_graph* g, size_t count, int* rc, hfpx_ctx* c) {
   if (*rc) return nullptr;
   void* p = nullptr;
-  *rc = check_cuda(c, cudaMalloc(&p, sizeof(T) * std::max<size_t>(1, count)), "network buffers");
+  *rc = pool_alloc(c, &p, sizeof(T) * std::max<size_t>(1, count), "network buffers");
   if (!*rc) g->allocs.push_back(p);
   return static_cast<T*>(p);
 }
@@ -861,7 +861,7 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
 void graph_destroy(hfpx_gnn_graph* g) {
   if (!g) return;
   g->pat.reset();
-  for (void* p : g->allocs) cudaFree(p);
+  pool_free_many(g->allocs.data(), g->allocs.size());
   delete g;
 }
 
@@ -1048,6 +1048,8 @@ int hfpx_gnn_graph_data(hfpx_ctx* c, const hfpx_gnn_graph* g, float* xn, float* 
   if (!g) return set_error(c, HFPX_ERR_ARG, "null graph");
   if ((tn || te) && !g->tn) return set_error(c, HFPX_ERR_STATE, "the graph has no targets");
   if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  // the graph's buffers are written on the context's stream
+  if (int rc = check_cuda(c, cudaStreamSynchronize(c->stream), "graph")) return rc;
   const int64_t n = g->n_nodes, E = g->n_edges;
   std::vector<__nv_bfloat16> b;
   int rc = 0;

@@ -209,7 +209,7 @@ template <class T>
 T* dev_copy(hfpx_ctx* c, const std::vector<T>& h, int* rc) {
   if (*rc) return nullptr;
   T* d = nullptr;
-  *rc = check_cuda(c, cudaMalloc(&d, sizeof(T) * std::max<size_t>(1, h.size())), "pattern alloc");
+  *rc = pool_alloc(c, (void**)&d, sizeof(T) * std::max<size_t>(1, h.size()), "pattern alloc");
   if (!*rc && !h.empty())
     *rc = check_cuda(c, cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, c->stream),
                      "pattern copy");
@@ -290,8 +290,8 @@ std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh) {
 }
 
 void free_pattern(NearPattern* p) {
-  for (int32_t* d : {p->d_ptr, p->d_idx, p->d_dst, p->d_rev, p->d_rptr, p->d_rblk, p->d_rcol})
-    if (d) cudaFree(d);
+  void* ds[] = {p->d_ptr, p->d_idx, p->d_dst, p->d_rev, p->d_rptr, p->d_rblk, p->d_rcol};
+  pool_free_many(ds, 7);
   p->d_ptr = p->d_idx = p->d_dst = p->d_rev = p->d_rptr = p->d_rblk = p->d_rcol = nullptr;
 }
 
@@ -315,12 +315,12 @@ int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPa
   const int64_t ne = p.n_el;
   double *L = nullptr, *E = nullptr, **Lp = nullptr, **Ep = nullptr;
   int *piv = nullptr, *info = nullptr;
-  int rc = check_cuda(c, cudaMalloc(&L, sizeof(double) * Q * Q * ne), "local systems");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&E, sizeof(double) * Q * kB * ne), "local right-hand sides");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&Lp, sizeof(double*) * ne), "local pointers");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&Ep, sizeof(double*) * ne), "local pointers");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&piv, sizeof(int) * Q * ne), "local pivots");
-  if (!rc) rc = check_cuda(c, cudaMalloc(&info, sizeof(int) * ne), "local info");
+  int rc = pool_alloc(c, (void**)&L, sizeof(double) * Q * Q * ne, "local systems");
+  if (!rc) rc = pool_alloc(c, (void**)&E, sizeof(double) * Q * kB * ne, "local right-hand sides");
+  if (!rc) rc = pool_alloc(c, (void**)&Lp, sizeof(double*) * ne, "local pointers");
+  if (!rc) rc = pool_alloc(c, (void**)&Ep, sizeof(double*) * ne, "local pointers");
+  if (!rc) rc = pool_alloc(c, (void**)&piv, sizeof(int) * Q * ne, "local pivots");
+  if (!rc) rc = pool_alloc(c, (void**)&info, sizeof(int) * ne, "local info");
   if (!rc) {
     g_launches += 4;
     local_system_kernel<<<dim3((unsigned)ne, slots, slots), 352, 0, c->stream>>>(A, lda, p.d_ptr, p.d_idx, slots,
@@ -338,8 +338,8 @@ int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPa
     if (!rc) rc = check_cuda(c, cudaGetLastError(), "local inverse");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "local inverse");
   }
-  for (void* q : {(void*)L, (void*)E, (void*)Lp, (void*)Ep, (void*)piv, (void*)info})
-    if (q) cudaFree(q);
+  void* qs[] = {(void*)L, (void*)E, (void*)Lp, (void*)Ep, (void*)piv, (void*)info};
+  pool_free_many(qs, 6);
   return rc;
 }
 
@@ -391,10 +391,15 @@ int pool_alloc(hfpx_ctx* c, void** p, size_t bytes, const char* what) {
 
 // After the device is idle (the guarantee cudaFree gives), back to the pool
 // in the legacy stream's order, which is then already complete.
-void pool_free(void* p) {
-  if (!p) return;
+void pool_free(void* p) { pool_free_many(&p, 1); }
+
+void pool_free_many(void* const* p, size_t count) {
+  bool any = false;
+  for (size_t i = 0; i < count; ++i) any = any || p[i];
+  if (!any) return;
   cudaDeviceSynchronize();
-  if (cudaFreeAsync(p, cudaStreamLegacy) != cudaSuccess) cudaGetLastError();
+  for (size_t i = 0; i < count; ++i)
+    if (p[i] && cudaFreeAsync(p[i], cudaStreamLegacy) != cudaSuccess) cudaGetLastError();
 }
 
 }  // namespace hfpx
