@@ -111,8 +111,13 @@ class Clocks:
                 'reasons': reasons, 'samples': len(self.samples)}
 
 
-def workload(n_el, seed=2026):
+def workload(n_el, seed=2026, mesh='penny'):
+    """The timed crack: the C3 penny, or (mesh='wavy') a non-planar elliptical
+    crack like the learned preconditioner's evaluation set (aspect 2, waviness
+    0.12), whose pairs all take the off-plane (quadrature) path."""
     from hfpx3d_b200 import meshgen
+    if mesh == 'wavy':
+        return meshgen.wavy(n_el, aspect=2.0, amp=0.12, seed=seed)
     return meshgen.penny(n_el, seed=seed)
 
 
@@ -169,7 +174,7 @@ class Forms:
             # blocks made again from this step's matrix, in the storage of
             # the first step's preconditioner (hfpx_precond_update)
             if self.pc is None:
-                kind = engine.HFPX_PC_LEARNED | (engine.HFPX_PC_COARSE if self.args.coarse else 0)
+                kind = PC_KINDS[self.args.pc] | (engine.HFPX_PC_COARSE if self.args.coarse else 0)
                 self.pc = engine.Precond(ctx, self.dm, A, kind, net=self.net, shear_m=G)
             else:
                 self.pc.update(A, net=self.net, shear_m=G)
@@ -236,7 +241,7 @@ def run_engine(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     ctx = engine.Context(local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream, device=f'cuda:{local_rank}')
-    nods, conn = workload(args.n_el)
+    nods, conn = workload(args.n_el, mesh=args.mesh)
     mesh = engine.MeshGeom(nods, conn)
     dof, n = engine.make_dof_h_crack(mesh, 0)
     dm = engine.DeviceMesh(ctx, mesh, BETA)
@@ -343,9 +348,11 @@ def run_engine(args, rank, world, local_rank):
         'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': dtype,
-        'data': 'synthetic (seeded 4000-triangle penny mesh, pressure 1)',
-        'config': {'workload': f'penny crack {args.n_el} el, N={n} DoF, assembly + {FORM_TEXT[args.mode]} to rel '
+        'data': f'synthetic (seeded {args.n_el}-triangle {args.mesh} mesh, pressure 1)',
+        'config': {'workload': f'{args.mesh} crack {args.n_el} el, N={n} DoF, assembly + {FORM_TEXT[args.mode]} to rel '
                                f'residual {args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'form': args.mode,
+                   'preconditioner': ((args.pc + (' + coarse' if args.coarse else ''))
+                                      if args.mode == 'learned' else None),
                    'parallelism': f'replicas x{world}',
                    'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
         'phases_ms': {'assembly': asm_ms, 'preconditioner' if args.mode == 'learned' else 'factor': fac_ms,
@@ -461,7 +468,11 @@ def run_stress(ctx, engine, torch, stream, reps=5):
             'point_cases_per_s': 64 * npts / t64}
 
 
-FORM_TEXT = {'learned': 'learned near-field preconditioner + GMRES(50) on the FP64 operator',
+# near-field part of the learned form's preconditioner (hfpx_pc_kind)
+PC_KINDS = {'learned': 3, 'neumann': 1, 'local': 2, 'jacobi': 0}
+
+FORM_TEXT = {'learned': 'two-level preconditioner (learned near-field blocks + coarse correction over element '
+                        'aggregates) + GMRES(50) on the FP64 operator',
              'mixed': 'mixed LU (FP16 tcgen05 updates) + GMRES on the FP64 operator',
              'fp64': 'FP64 LU + triangular solves'}
 
@@ -560,7 +571,7 @@ def run_e2e(args, ctx, engine, L, nods, conn, dof, n, form, stream, torch, A, F)
         si = engine.SolveInfo()
         if form == 'learned':
             pc = ctypes.c_void_p()
-            kind = engine.HFPX_PC_LEARNED | (engine.HFPX_PC_COARSE if args.coarse else 0)
+            kind = PC_KINDS[args.pc] | (engine.HFPX_PC_COARSE if args.coarse else 0)
             ctx.check(L.hfpx_precond_create(ctx.h, mh, A.h, kind, F.net.h, G, ctypes.byref(pc)))
             t0 = tick('precond_create', t0)
             rc = L.hfpx_gmres_precond(ctx.h, A.h, pc, engine._dp(hr), args.tol, 50, 2000, ctypes.byref(si))
@@ -760,10 +771,14 @@ def main():
     ap.add_argument('--mode', default='learned', choices=['learned', 'mixed', 'fp64'],
                     help='the form of the timed step (the other fast form is timed once beside it)')
     ap.add_argument('--n-el', type=int, default=4000)
+    ap.add_argument('--mesh', choices=['penny', 'wavy'], default='penny',
+                    help='penny: the C3 crack (timed by default); wavy: a non-planar crack (off-plane pairs)')
     ap.add_argument('--tol', type=float, default=1e-10)
     ap.add_argument('--coarse', dest='coarse', action='store_true', default=True,
                     help='learned form: two-level preconditioner (coarse correction over element aggregates)')
     ap.add_argument('--no-coarse', dest='coarse', action='store_false')
+    ap.add_argument('--pc', choices=sorted(PC_KINDS), default='learned',
+                    help='learned form: the near-field part of the preconditioner (the network by default)')
     ap.add_argument('--solver', default='gmres', choices=['refine', 'gmres'],
                     help='mixed mode: FP64 iterative refinement or flexible GMRES, both preconditioned by the '
                          'FP32 factors')
