@@ -137,17 +137,19 @@ __global__ void __launch_bounds__(352) neumann_kernel(const double* __restrict__
 }
 
 // Local systems of the exact local inverse: L_j (Q x Q, column-major) =
-// A[P(j), P(j)] padded with the identity to Q = 18 (1 + maxdeg) rows, and
-// its right-hand side E_j = the first 18 columns of the identity.  One CTA
-// per (column j, pattern block a, pattern block b).
+// A[P(j), P(j)] (Q = 18 |P(j)|; padded with the identity up to the group's Q
+// when a shorter pattern shares the group), and its right-hand side E_j = the
+// first 18 columns of the identity.  Elements come in groups of one pattern
+// size; CTA (g, a, b) fills pattern blocks (a, b) of the group's element g.
 __global__ void local_system_kernel(const double* __restrict__ A, int64_t lda, const int32_t* __restrict__ ptr,
-                                    const int32_t* __restrict__ idx, int slots, double* __restrict__ L,
-                                    double* __restrict__ E) {
-  const int64_t j = blockIdx.x;
+                                    const int32_t* __restrict__ idx, const int32_t* __restrict__ elems, int slots,
+                                    double* __restrict__ L, double* __restrict__ E) {
+  const int64_t g = blockIdx.x;
+  const int64_t j = elems[g];
   const int a = blockIdx.y, bsl = blockIdx.z;
   const int Q = kB * slots;
   const int deg = ptr[j + 1] - ptr[j];
-  double* Lj = L + (size_t)Q * Q * j;
+  double* Lj = L + (size_t)Q * Q * g;
   const int t = threadIdx.x;
   if (t >= kBB) return;
   const int r = t % kB, c = t / kB;
@@ -160,12 +162,13 @@ __global__ void local_system_kernel(const double* __restrict__ A, int64_t lda, c
     v = (a == bsl && r == c) ? 1.0 : 0.0;
   }
   Lj[(kB * a + r) + (size_t)Q * (kB * bsl + c)] = v;
-  if (bsl == 0) E[(size_t)Q * kB * j + (kB * a + r) + (size_t)Q * c] = (a == 0 && r == c) ? 1.0 : 0.0;
+  if (bsl == 0) E[(size_t)Q * kB * g + (kB * a + r) + (size_t)Q * c] = (a == 0 && r == c) ? 1.0 : 0.0;
 }
 
-__global__ void local_scatter_kernel(const double* __restrict__ E, const int32_t* __restrict__ ptr, int slots,
-                                     double* __restrict__ blocks) {
-  const int64_t j = blockIdx.x;
+__global__ void local_scatter_kernel(const double* __restrict__ E, const int32_t* __restrict__ ptr,
+                                     const int32_t* __restrict__ elems, int slots, double* __restrict__ blocks) {
+  const int64_t g = blockIdx.x;
+  const int64_t j = elems[g];
   const int s = blockIdx.y;
   const int deg = ptr[j + 1] - ptr[j];
   if (s > deg) return;
@@ -174,7 +177,7 @@ __global__ void local_scatter_kernel(const double* __restrict__ E, const int32_t
   if (t >= kBB) return;
   const int r = t % kB, c = t / kB;
   const int64_t blk = s == 0 ? j + ptr[j] : j + 1 + ptr[j] + (s - 1);
-  blocks[(size_t)kBB * blk + t] = E[(size_t)Q * kB * j + (kB * s + r) + (size_t)Q * c];
+  blocks[(size_t)kBB * blk + t] = E[(size_t)Q * kB * g + (kB * s + r) + (size_t)Q * c];
 }
 
 __global__ void ptr_array_kernel(double* base, int64_t stride, int64_t count, double** out) {
@@ -310,36 +313,62 @@ int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern&
 }
 
 int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks) {
-  const int slots = 1 + p.maxdeg;
-  const int Q = kB * slots;
+  // elements grouped by pattern size (1 + neighbours), each group one batched
+  // LU of its own size: padding every system to the largest pattern made the
+  // factorisation about 4 times the work on a penny mesh
   const int64_t ne = p.n_el;
+  std::vector<std::vector<int32_t>> groups((size_t)p.maxdeg + 2);
+  for (int64_t j = 0; j < ne; ++j) groups[(size_t)(1 + p.ptr[j + 1] - p.ptr[j])].push_back((int32_t)j);
+  std::vector<int32_t> order;
+  std::vector<size_t> goff(groups.size() + 1, 0), loff(groups.size() + 1, 0), eoff(groups.size() + 1, 0);
+  for (size_t sl = 0; sl < groups.size(); ++sl) {
+    const size_t Q = (size_t)kB * sl, cnt = groups[sl].size();
+    order.insert(order.end(), groups[sl].begin(), groups[sl].end());
+    goff[sl + 1] = goff[sl] + cnt;
+    loff[sl + 1] = loff[sl] + cnt * Q * Q;
+    eoff[sl + 1] = eoff[sl] + cnt * Q * kB;
+  }
   double *L = nullptr, *E = nullptr, **Lp = nullptr, **Ep = nullptr;
   int *piv = nullptr, *info = nullptr;
-  int rc = pool_alloc(c, (void**)&L, sizeof(double) * Q * Q * ne, "local systems");
-  if (!rc) rc = pool_alloc(c, (void**)&E, sizeof(double) * Q * kB * ne, "local right-hand sides");
+  int32_t* d_order = nullptr;
+  const size_t qmax = (size_t)kB * (p.maxdeg + 1);
+  int rc = pool_alloc(c, (void**)&L, sizeof(double) * std::max<size_t>(1, loff.back()), "local systems");
+  if (!rc) rc = pool_alloc(c, (void**)&E, sizeof(double) * std::max<size_t>(1, eoff.back()), "local right-hand sides");
   if (!rc) rc = pool_alloc(c, (void**)&Lp, sizeof(double*) * ne, "local pointers");
   if (!rc) rc = pool_alloc(c, (void**)&Ep, sizeof(double*) * ne, "local pointers");
-  if (!rc) rc = pool_alloc(c, (void**)&piv, sizeof(int) * Q * ne, "local pivots");
+  if (!rc) rc = pool_alloc(c, (void**)&piv, sizeof(int) * qmax * ne, "local pivots");
   if (!rc) rc = pool_alloc(c, (void**)&info, sizeof(int) * ne, "local info");
-  if (!rc) {
+  if (!rc) rc = pool_alloc(c, (void**)&d_order, sizeof(int32_t) * ne, "local groups");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(d_order, order.data(), sizeof(int32_t) * ne, cudaMemcpyHostToDevice,
+                                              c->stream), "local groups");
+  cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
+  cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+  for (size_t sl = 1; !rc && sl < groups.size(); ++sl) {
+    const int64_t cnt = (int64_t)groups[sl].size();
+    if (!cnt) continue;
+    const int Q = kB * (int)sl;
+    double* Lg = L + loff[sl];
+    double* Eg = E + eoff[sl];
+    double** Lpg = Lp + goff[sl];
+    double** Epg = Ep + goff[sl];
+    const int32_t* eg = d_order + goff[sl];
     g_launches += 4;
-    local_system_kernel<<<dim3((unsigned)ne, slots, slots), 352, 0, c->stream>>>(A, lda, p.d_ptr, p.d_idx, slots,
-                                                                                  L, E);
-    ptr_array_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, c->stream>>>(L, (int64_t)Q * Q, ne, Lp);
-    ptr_array_kernel<<<(unsigned)((ne + 255) / 256), 256, 0, c->stream>>>(E, (int64_t)Q * kB, ne, Ep);
-    cublasHandle_t h = static_cast<cublasHandle_t>(c->cublas);
-    cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+    local_system_kernel<<<dim3((unsigned)cnt, (unsigned)sl, (unsigned)sl), 352, 0, c->stream>>>(
+        A, lda, p.d_ptr, p.d_idx, eg, (int)sl, Lg, Eg);
+    ptr_array_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, c->stream>>>(Lg, (int64_t)Q * Q, cnt, Lpg);
+    ptr_array_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, c->stream>>>(Eg, (int64_t)Q * kB, cnt, Epg);
     int hinfo = 0;
-    if (cublasDgetrfBatched(h, Q, Lp, Q, piv, info, (int)ne) != CUBLAS_STATUS_SUCCESS ||
-        cublasDgetrsBatched(h, CUBLAS_OP_N, Q, kB, (const double* const*)Lp, Q, piv, Ep, Q, &hinfo, (int)ne) !=
-            CUBLAS_STATUS_SUCCESS)
+    if (cublasDgetrfBatched(h, Q, Lpg, Q, piv + qmax * goff[sl], info + goff[sl], (int)cnt) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgetrsBatched(h, CUBLAS_OP_N, Q, kB, (const double* const*)Lpg, Q, piv + qmax * goff[sl], Epg, Q, &hinfo,
+                            (int)cnt) != CUBLAS_STATUS_SUCCESS)
       rc = set_error(c, HFPX_ERR_CUDA, "batched local solves");
-    if (!rc) local_scatter_kernel<<<dim3((unsigned)ne, slots), 352, 0, c->stream>>>(E, p.d_ptr, slots, blocks);
+    if (!rc)
+      local_scatter_kernel<<<dim3((unsigned)cnt, (unsigned)sl), 352, 0, c->stream>>>(Eg, p.d_ptr, eg, (int)sl, blocks);
     if (!rc) rc = check_cuda(c, cudaGetLastError(), "local inverse");
-    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "local inverse");
   }
-  void* qs[] = {(void*)L, (void*)E, (void*)Lp, (void*)Ep, (void*)piv, (void*)info};
-  pool_free_many(qs, 6);
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "local inverse");
+  void* qs[] = {(void*)L, (void*)E, (void*)Lp, (void*)Ep, (void*)piv, (void*)info, (void*)d_order};
+  pool_free_many(qs, 7);
   return rc;
 }
 
