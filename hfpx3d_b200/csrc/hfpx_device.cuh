@@ -65,11 +65,10 @@ static_assert(sizeof(ElemRec) % 16 == 0, "bulk copy size");
 __device__ __forceinline__ void lim_moments_diff(double chi_m, double chi_n, cplx d,
                                                  cplx* P, cplx* Q) {
   const double D = cabs_(d);
-  double se, ce;
-  sincos(carg_(d), &se, &ce);
-  const cplx e = mk(ce, se), e2 = e * e, e3 = e2 * e, e4 = e2 * e2;
-  const cplx ec = conj(e), e2c = conj(e2);
   const double iD = 1.0 / D;
+  // e^{i arg d} = d / |d| (the unit foot direction; no angle round trip)
+  const cplx e = mk(d.re * iD, d.im * iD), e2 = e * e, e3 = e2 * e, e4 = e2 * e2;
+  const cplx ec = conj(e), e2c = conj(e2);
   // Both ends go through the same code into separate arrays and are
   // subtracted explicitly: for an edge whose two ends are seen under the same
   // angle (the point on the edge line) the terms, of size 1/|d|, cancel
@@ -157,9 +156,7 @@ __device__ __forceinline__ void radial_F(double X, double h, double* F) {
 __device__ inline void gen_moments_edge(double chi_m, double chi_n, cplx d, double h, bool upper,
                                         const GL12& gl, cplx* W) {
   const double D = cabs_(d);
-  double se, ce;
-  sincos(carg_(d), &se, &ce);
-  const cplx e = mk(ce, se);
+  const cplx e = mk(d.re / D, d.im / D);  // e^{i arg d}
   const double tm = asinh(tan(chi_m)), tn = asinh(tan(chi_n));
   int npan = (int)ceil(fabs(tn - tm) / 1.5);
   npan = npan < 1 ? 1 : (npan > 64 ? 64 : npan);
