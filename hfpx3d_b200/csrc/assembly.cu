@@ -194,7 +194,7 @@ __global__ void element_precompute_kernel(const double* __restrict__ nods, int64
     }
   }
   E.area = 0.5 * norm3_rn(a3) * n1;
-  E.pad[0] = E.pad[1] = 0.0;
+  edge_directions(E.tau, E.nt2);
   out[el] = E;
 }
 
@@ -206,7 +206,7 @@ struct InPlaneBlock {
 
 __device__ __forceinline__ void inplane_moments(const ElemRec& S, cplx z, cplx* P, cplx* Q) {
   EdgeSet E;
-  edge_setup(S.tau, z, E);
+  edge_setup(S.tau, S.nt2, z, E);
   for (int j = 0; j < 6; ++j) { P[j] = mk(0.0); Q[j] = mk(0.0); }
   for (int m = 0; m < 3; ++m)
     if (E.use[m]) lim_moments_diff(E.chi[0][m], E.chi[1][m], E.d[m], P, Q);
@@ -255,7 +255,7 @@ __device__ __forceinline__ void inplane_nodes(const ElemRec& S, cplx z, const cp
 __device__ __noinline__ void offplane_smon(const ElemRec& S, cplx z, double h, double nu,
                                            cplx* smon) {
   EdgeSet E;
-  edge_setup(S.tau, z, E);
+  edge_setup(S.tau, S.nt2, z, E);
   // Points below the element's span integrate the regular parts F_p and add
   // the h-singular lower-limit parts in closed form (exact vertex cancellation
   // around the contour); points higher up integrate I_p directly.
@@ -712,6 +712,7 @@ __global__ void local_block_kernel(double G, double nu, double h, double zr, dou
   ElemRec S;
   for (int i = 0; i < 6; ++i) S.tau[i] = tau[i];
   for (int i = 0; i < 72; ++i) S.sfm[i] = sfm[i];
+  edge_directions(S.tau, S.nt2);
   const cplx z = mk(zr, zi);
   const double scale = -G / (4.0 * kPi * (1.0 - nu));
   auto sink = [&](int a, const double Sx[6][3]) {

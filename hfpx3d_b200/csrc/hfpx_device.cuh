@@ -55,7 +55,8 @@ struct alignas(16) ElemRec {
   double cp[18];        // collocation points (6 x xyz)
   double nrm[3];        // target normal -e3
   double area;          // element area
-  double pad[2];
+  double nt2[6];        // per edge j (tau_j -> tau_j+1): dt / conj(dt), the edge's doubled-angle
+                        // direction that reflects z across the edge line (re,im), by Smith's quotient
 };
 static_assert(sizeof(ElemRec) % 16 == 0, "bulk copy size");
 
@@ -219,16 +220,28 @@ __device__ __forceinline__ cplx div_smith(cplx x, cplx y) {
           __ddiv_rn(__dsub_rn(b, __dmul_rn(d, __ddiv_rn(a, c))), den)};
 }
 
-__device__ __forceinline__ void edge_setup(const double* tau6, cplx z, EdgeSet& E) {
-  cplx tz[3];
-  double phi[3], psi[3];
+// dt / conj(dt) of each edge (tau_j -> tau_j+1): a property of the element,
+// made once per element with the same arithmetic the point loop used
+__device__ __forceinline__ void edge_directions(const double* tau6, double* nt2_6) {
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int q = (j + 1) % 3;
     const cplx tj = mk(tau6[2 * j], tau6[2 * j + 1]), tq = mk(tau6[2 * q], tau6[2 * q + 1]);
-    tz[j] = mk(__dsub_rn(tj.re, z.re), __dsub_rn(tj.im, z.im));
     const cplx dt = mk(__dsub_rn(tq.re, tj.re), __dsub_rn(tq.im, tj.im));
     const cplx nt2 = div_smith(dt, conj(dt));
+    nt2_6[2 * j] = nt2.re;
+    nt2_6[2 * j + 1] = nt2.im;
+  }
+}
+
+__device__ __forceinline__ void edge_setup(const double* tau6, const double* nt2_6, cplx z, EdgeSet& E) {
+  cplx tz[3];
+  double phi[3], psi[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const cplx tj = mk(tau6[2 * j], tau6[2 * j + 1]);
+    tz[j] = mk(__dsub_rn(tj.re, z.re), __dsub_rn(tj.im, z.im));
+    const cplx nt2 = mk(nt2_6[2 * j], nt2_6[2 * j + 1]);
     const cplx pr = mul_rn(nt2, conj(tz[j]));
     E.d[j] = mk(__dmul_rn(0.5, __dsub_rn(tz[j].re, pr.re)), __dmul_rn(0.5, __dsub_rn(tz[j].im, pr.im)));
   }
