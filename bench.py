@@ -9,9 +9,12 @@ internal pressure 1 (sigma_zz = 1).  Synthetic seeded mesh (the reference has
 no mesher).  One step = assemble the FP64 collocation matrix in HBM
 (41.5 GB) + solve to a relative residual <= 1e-10 in one of three forms:
 
-  --mode learned (default): the learned near-field preconditioner (a graph
-        network over element adjacency, hfpx3d_b200/data/pc_gnn.bin) and
-        flexible GMRES(50) on the FP64 operator;
+  --mode learned (default): the two-level preconditioner with the learned
+        near-field blocks (a graph network over element adjacency,
+        hfpx3d_b200/data/pc_gnn.bin) and flexible GMRES(50) on the operator,
+        held by default in mixed precision (--operator mixed: FP32 entries,
+        near-field blocks kept to ~2^-48 by FP32 low parts, products in FP64;
+        --operator fp64: the FP64 matrix);
   --mode mixed: the FP32 LU of a copy with FP16 tcgen05 trailing updates and
         flexible GMRES on the FP64 operator preconditioned by it (--solver
         gmres, the default) or FP64 iterative refinement (--solver refine);
@@ -64,6 +67,15 @@ ASM_DRAM_BYTES_PER_ENTRY = 4.630537e9 / 18000 ** 2
 # N = 21 600 in an ncu capture of one launch (1200-element penny); the traffic
 # grows with the entries, so N^2 times this is a launch at any N
 RESID_DRAM_BYTES_PER_ENTRY = (3.732682e9 + 11.813888e6) / 21600.0 ** 2
+# the same for the FP32 entries' product (resid_partial_f32_kernel, the
+# mixed-precision operator's dense part): 1.8664 GB read + 9.5 MB written at
+# N = 21 600 in the same capture
+RESID32_DRAM_BYTES_PER_ENTRY = (1.8664e9 + 9.5e6) / 21600.0 ** 2
+# DRAM bytes per matrix entry of the mixed-precision operator's fill (FP32
+# entries + near-field low parts): 2.0153 GB written (2.8 MB read) for an
+# 18 000 x 18 000 fill in an ncu capture of one launch on the 1000-element
+# penny; scaled by N^2 like the FP64 fill's
+ASM32_DRAM_BYTES_PER_ENTRY = (2.015346e9 + 2.779e6) / 18000 ** 2
 
 
 class Clocks:
@@ -154,8 +166,18 @@ class Forms:
         self.dm, self.dof, self.n, self.A, self.d_rhs, self.d_x = dm, dof, n, A, d_rhs, d_x
         self.info = engine.SolveInfo()
         self.net = None
-        self.pc = None
+        self.pcs = {}
+        self.Am = None   # the mixed-precision operator (made on first use)
         self.host_ms = {}
+
+    def operator(self, form):
+        """The matrix a form works on: the learned form's operator is the
+        mixed-precision one unless --operator fp64 ('learned64': always FP64)."""
+        if form == 'learned' and self.args.operator == 'mixed':
+            if self.Am is None:
+                self.Am = self.engine.assemble_mixed(self.ctx, self.dm, self.dof, self.n, G, NU)
+            return self.Am
+        return self.A
 
     def _host(self, key, t0):
         self.host_ms[key] = self.host_ms.get(key, 0.0) + (time.perf_counter() - t0) * 1e3
@@ -163,27 +185,29 @@ class Forms:
     def step(self, form, ev=None):
         engine, L, ctx, A, torch = self.engine, self.L, self.ctx, self.A, self.torch
         rec = (lambda k: ev[k].record(self.stream)) if ev else (lambda k: None)
+        A = self.operator(form)
         rec(0)
         engine.assemble_into(ctx, self.dm, self.dof, self.n, G, NU, A)
         rec(1)
         x = ctypes.c_void_p(self.d_x.data_ptr())
-        if form == 'learned':
+        if form in ('learned', 'learned64'):
             if self.net is None:
                 self.net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
             t0 = time.perf_counter()
             # blocks made again from this step's matrix, in the storage of
             # the first step's preconditioner (hfpx_precond_update)
-            if self.pc is None:
+            pc = self.pcs.get(form)
+            if pc is None:
                 kind = PC_KINDS[self.args.pc] | (engine.HFPX_PC_COARSE if self.args.coarse else 0)
-                self.pc = engine.Precond(ctx, self.dm, A, kind, net=self.net, shear_m=G)
+                pc = self.pcs[form] = engine.Precond(ctx, self.dm, A, kind, net=self.net, shear_m=G)
             else:
-                self.pc.update(A, net=self.net, shear_m=G)
+                pc.update(A, net=self.net, shear_m=G)
             self._host('precond', t0)
             rec(2)
             with torch.cuda.stream(self.stream):
                 self.d_x.copy_(self.d_rhs)
             t0 = time.perf_counter()
-            rc = L.hfpx_gmres_precond_device(ctx.h, A.h, self.pc.h, x, self.args.tol, 50, 2000,
+            rc = L.hfpx_gmres_precond_device(ctx.h, A.h, pc.h, x, self.args.tol, 50, 2000,
                                              ctypes.byref(self.info))
             self._host('gmres', t0)
             rec(3)
@@ -216,10 +240,22 @@ class Forms:
         return best, self.info.iterations, self.info.residual, self.d_x.cpu().numpy()
 
     def close(self):
-        if self.pc is not None:
-            self.pc.close()
+        for pc in self.pcs.values():
+            pc.close()
         if self.net is not None:
             self.net.close()
+        if self.Am is not None:
+            self.Am.close()
+
+
+def near_blocks(conn):
+    """Blocks of the near-field pattern: every element with itself and with
+    each element sharing a vertex with it."""
+    v2e = {}
+    for e in range(conn.shape[1]):
+        for v in conn[:3, e]:
+            v2e.setdefault(int(v), set()).add(e)
+    return sum(len(set().union(*[v2e[int(v)] for v in conn[:3, e]])) for e in range(conn.shape[1]))
 
 
 def opening(x):
@@ -288,7 +324,7 @@ def run_engine(args, rank, world, local_rank):
     # seconds-long FP64 comparison heats the GPU
     e2e = None
     if rank == 0 and args.e2e_steps > 0:
-        e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, args.mode, stream, torch, A, F)
+        e2e = run_e2e(args, ctx, engine, L, nods, conn, dof, n, args.mode, stream, torch, F.operator(args.mode), F)
 
     # the plain FP64 GPU path, once, for the speed-up and the opening error
     other_s, rel_err, x64 = None, None, None
@@ -301,15 +337,20 @@ def run_engine(args, rank, world, local_rank):
         x64 = d_x.cpu().numpy()
         rel_err = rel_opening_err(x_main, x64)
 
-    # the other fast form (mixed LU or learned), best of 2 after a warm-up
-    second = None
-    second_form = {'learned': 'mixed', 'mixed': 'learned'}.get(args.mode)
-    if rank == 0 and args.second and second_form:
+    # the other fast forms (mixed LU, or learned; and the learned form on the
+    # FP64 operator beside the mixed-precision one), best of 2 after a warm-up
+    seconds = {}
+    others = {'learned': ['mixed'] + (['learned64'] if args.operator == 'mixed' else []),
+              'mixed': ['learned']}.get(args.mode, [])
+    for second_form in (others if rank == 0 and args.second else []):
         t, it, res, xs = F.timed(second_form, 2)
-        second = {'value': t[2] / 1e3, 'unit': UNIT,
-                  'phases_ms': {'assembly': t[0], 'factor' if second_form == 'mixed' else 'preconditioner': t[1] - t[0],
-                                'solve': t[2] - t[1]},
-                  'iterations': it, 'residual': res}
+        second = seconds[second_form] = {
+            'value': t[2] / 1e3, 'unit': UNIT,
+            'phases_ms': {'assembly': t[0], 'factor' if second_form == 'mixed' else 'preconditioner': t[1] - t[0],
+                          'solve': t[2] - t[1]},
+            'iterations': it, 'residual': res}
+        if second_form == 'learned64':
+            second['operator'] = 'FP64 matrix (41.5 GB), FP32 copy for products once the residual is small'
         if x64 is not None:
             second['opening_rel_err_vs_fp64'] = rel_opening_err(xs, x64)
             second['speedup_vs_plain_fp64'] = other_s / second['value']
@@ -327,8 +368,9 @@ def run_engine(args, rank, world, local_rank):
     # alone on the engine's stream: N^2 8 bytes of matrix per launch
     resid = None
     if rank == 0:
-        engine.assemble_into(ctx, dm, dof, n, G, NU, A)  # the operator again (an FP64 step leaves factors)
-        resid = time_residual(ctx, engine, L, torch, stream, A, d_rhs, d_x, n)
+        Aop = F.operator(args.mode)
+        engine.assemble_into(ctx, dm, dof, n, G, NU, Aop)  # the operator again (an FP64 step leaves factors)
+        resid = time_residual(ctx, engine, L, torch, stream, Aop, d_rhs, d_x, n)
 
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
@@ -341,20 +383,29 @@ def run_engine(args, rank, world, local_rank):
     hbm, tensor_peak, peak_src = peaks()
     asm_ms = statistics.mean(t_asm)
     fac_ms = statistics.mean(t_fac)
-    bytes_asm = float(n) * n * 8
+    op_mixed = args.mode == 'learned' and args.operator == 'mixed'
+    n_blocks = near_blocks(conn) if op_mixed else 0
+    # algorithmic bytes of one assembly / one operator product: the matrix
+    # entries once (FP64, or FP32 plus the near-field blocks' FP32 low parts)
+    bytes_op = float(n) * n * 4 + 324.0 * 4 * n_blocks if op_mixed else float(n) * n * 8
+    bytes_asm = bytes_op
     flops_lu = 2.0 / 3.0 * float(n) ** 3
-    dtype = {'learned': 'f64 operator + bf16 network', 'mixed': 'f64+f32+f16', 'fp64': 'f64'}[args.mode]
+    dtype = {'learned': ('f32 far field + near field to 2^-48 (f64 products) + bf16 network' if op_mixed
+                         else 'f64 operator + bf16 network'), 'mixed': 'f64+f32+f16', 'fp64': 'f64'}[args.mode]
     line = {
         'metric': METRIC, 'value': ms / 1e3, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': False, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': dtype,
         'data': f'synthetic (seeded {args.n_el}-triangle {args.mesh} mesh, pressure 1)',
-        'config': {'workload': f'{args.mesh} crack {args.n_el} el, N={n} DoF, assembly + {FORM_TEXT[args.mode]} to rel '
+        'config': {'workload': f'{args.mesh} crack {args.n_el} el, N={n} DoF, assembly + '
+                               f'{FORM_TEXT[args.mode].replace("OPERATOR", OPERATOR_TEXT[args.operator])} to rel '
                                f'residual {args.tol:g}', 'n_el': args.n_el, 'n_dof': n, 'form': args.mode,
+                   'operator': args.operator if args.mode == 'learned' else 'fp64',
                    'preconditioner': ((args.pc + (' + coarse' if args.coarse else ''))
                                       if args.mode == 'learned' else None),
                    'parallelism': f'replicas x{world}',
-                   'l2': 'inputs larger than L2 (41.5 GB matrix rewritten each step)'},
+                   'l2': ('inputs larger than L2 (the 20.7 GB mixed-precision operator rewritten each step)'
+                          if op_mixed else 'inputs larger than L2 (41.5 GB matrix rewritten each step)')},
         'phases_ms': {'assembly': asm_ms, 'preconditioner' if args.mode == 'learned' else 'factor': fac_ms,
                       'solve': statistics.mean(t_sol)},
         'steps_ms': {'total': [round(a + b + c, 2) for a, b, c in zip(t_asm, t_fac, t_sol)],
@@ -363,22 +414,29 @@ def run_engine(args, rank, world, local_rank):
         'host_ms_per_step': {k: v / args.steps for k, v in F.host_ms.items()},
         'assemblies_per_s': 1e3 / asm_ms,
         'solves_per_s': 1e3 / ms,
-        'roofline_assembly': {'kernel': 'assemble_kernel<in-plane> (FP64 matrix fill)', 'bound': 'hbm',
+        'roofline_assembly': {'kernel': ('assemble_kernel<in-plane> (mixed-precision operator fill: FP32 entries + '
+                                         'near-field low parts)' if op_mixed else
+                                         'assemble_kernel<in-plane> (FP64 matrix fill)'), 'bound': 'hbm',
                               'achieved': bytes_asm / (asm_ms / 1e3) / 1e9, 'peak': hbm, 'unit': 'GB/s',
                               'frac': bytes_asm / (asm_ms / 1e3) / 1e9 / hbm,
-                              'traffic': ASM_DRAM_BYTES_PER_ENTRY * float(n) * n,
+                              'traffic': (ASM32_DRAM_BYTES_PER_ENTRY * float(n) * n if op_mixed and
+                                          ASM32_DRAM_BYTES_PER_ENTRY else
+                                          None if op_mixed else ASM_DRAM_BYTES_PER_ENTRY * float(n) * n),
                               'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm},
         'gpu_launches': int(launches),
         'clocks': clk.summary(),
         'e2e': e2e,
     }
     if args.mode == 'learned' and resid is not None:
-        line['roofline'] = {'kernel': 'resid_partial_kernel + resid_finish_kernel (FP64 operator product, one per '
-                                      'GMRES step)', 'bound': 'hbm', 'achieved': resid['gbs'], 'peak': hbm,
-                            'unit': 'GB/s', 'frac': resid['gbs'] / hbm,
-                            'traffic': (RESID_DRAM_BYTES_PER_ENTRY * float(n) * n
-                                        if RESID_DRAM_BYTES_PER_ENTRY else None),
-                            'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_asm,
+        gbs = bytes_op / (resid['ms'] / 1e3) / 1e9
+        line['roofline'] = {'kernel': ('resid_partial_f32_kernel + near_lo_kernel + resid_finish_kernel (the mixed-'
+                                       'precision operator product, one per GMRES step)' if op_mixed else
+                                       'resid_partial_kernel + resid_finish_kernel (FP64 operator product, one per '
+                                       'GMRES step)'), 'bound': 'hbm', 'achieved': gbs, 'peak': hbm,
+                            'unit': 'GB/s', 'frac': gbs / hbm,
+                            'traffic': ((RESID32_DRAM_BYTES_PER_ENTRY if op_mixed else RESID_DRAM_BYTES_PER_ENTRY)
+                                        * float(n) * n),
+                            'peak_source': f'{peak_src} hbm_gbs', 'algorithmic_bytes': bytes_op,
                             'launch_ms': resid['ms']}
     else:
         line['roofline'] = {'kernel': 'LU factorisation (panel_ll_kernel chain + tcgen05 FP16 updates)',
@@ -390,8 +448,8 @@ def run_engine(args, rank, world, local_rank):
         line['plain_fp64_s'] = other_s
         line['speedup_vs_plain_fp64'] = other_s / (ms / 1e3)
         line['opening_rel_err_vs_fp64'] = rel_err
-    if second is not None:
-        line[second_form] = second
+    for k, v in seconds.items():
+        line['learned_fp64_operator' if k == 'learned64' else k] = v
     if args.cpu_baseline:
         cb = cpu_baseline(args)
         x_ref = cb.pop('_c2_x', None)
@@ -470,9 +528,11 @@ def run_stress(ctx, engine, torch, stream, reps=5):
 
 # near-field part of the learned form's preconditioner (hfpx_pc_kind)
 PC_KINDS = {'learned': 3, 'neumann': 1, 'local': 2, 'jacobi': 0}
+OPERATOR_TEXT = {'mixed': 'mixed-precision operator (FP32 entries, near-field blocks to 2^-48, FP64 products)',
+                 'fp64': 'FP64 operator'}
 
 FORM_TEXT = {'learned': 'two-level preconditioner (learned near-field blocks + coarse correction over element '
-                        'aggregates) + GMRES(50) on the FP64 operator',
+                        'aggregates) + GMRES(50) on the OPERATOR',
              'mixed': 'mixed LU (FP16 tcgen05 updates) + GMRES on the FP64 operator',
              'fp64': 'FP64 LU + triangular solves'}
 
@@ -774,6 +834,9 @@ def main():
     ap.add_argument('--mesh', choices=['penny', 'wavy'], default='penny',
                     help='penny: the C3 crack (timed by default); wavy: a non-planar crack (off-plane pairs)')
     ap.add_argument('--tol', type=float, default=1e-10)
+    ap.add_argument('--operator', choices=['mixed', 'fp64'], default='mixed',
+                    help='learned form: the operator in mixed precision (FP32 far field, near-field blocks to '
+                         '2^-48) or the FP64 matrix')
     ap.add_argument('--coarse', dest='coarse', action='store_true', default=True,
                     help='learned form: two-level preconditioner (coarse correction over element aggregates)')
     ap.add_argument('--no-coarse', dest='coarse', action='store_false')

@@ -339,7 +339,25 @@ struct AsmSmem {
   int32_t cols[18];
   int32_t rows[kStageRows];
   double wbuf[kTile / 32][96];
+  // mixed-precision operator: the source element's near-field column (its
+  // neighbours, sorted, and the index of its self block)
+  int32_t nb[kMaxNearDeg];
+  int32_t ndeg;
+  int64_t nbase;
 };
+
+// Block index of (target t, source s) in the near-field block store, or -1
+// for a far pair (self block s + ptr[s], neighbour k at s + ptr[s] + 1 + k).
+__device__ __forceinline__ int64_t near_block(const AsmSmem& sm, int64_t t, int64_t s) {
+  if (t == s) return sm.nbase;
+  for (int k = 0; k < sm.ndeg; ++k)
+    if (sm.nb[k] == t) return sm.nbase + 1 + k;
+  return -1;
+}
+
+// The low part of a near-field entry: what rounding v to FP32 lost, itself
+// rounded to FP32 (hi + lo carries about 48 bits of v).
+__device__ __forceinline__ float low_part(double v) { return (float)(v - (double)(float)v); }
 
 template <bool GENERAL>
 __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const ElemRec* __restrict__ elems,
@@ -348,18 +366,34 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
                                                          double G, double nu, int is_dd_local,
                                                          double* __restrict__ A, int64_t ld,
                                                          float* __restrict__ Af,
-                                                         int* __restrict__ status) {
+                                                         int* __restrict__ status,
+                                                         float* __restrict__ lo,
+                                                         const int32_t* __restrict__ np_ptr,
+                                                         const int32_t* __restrict__ np_idx,
+                                                         const int32_t* __restrict__ slist,
+                                                         const int32_t* __restrict__ tlist, int64_t n_t) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
   if (GENERAL && status[1] == 0) return;  // first pass met no off-plane pair
-  const int64_t s = blockIdx.y;
+  // source element of this CTA and the target elements of the grid's x
+  // range: all of them, or the lists of a partial (incremental) assembly
+  const int64_t s = slist ? slist[blockIdx.y] : blockIdx.y;
   const int tid = threadIdx.x;
   if (!stage_bulk(&sm.src, elems + s, sizeof(ElemRec), &sm.bar, status)) return;
   if (tid < 18) sm.cols[tid] = dof[s + n_el * tid];
+  if (lo) {
+    const int32_t p0 = np_ptr[s], deg = min(np_ptr[s + 1] - p0, kMaxNearDeg);
+    for (int k = tid; k < deg; k += kTile) sm.nb[k] = np_idx[p0 + k];
+    if (tid == 0) {
+      sm.ndeg = deg;
+      sm.nbase = s + p0;
+    }
+  }
   const int64_t g = (int64_t)blockIdx.x * kTile + tid;
-  const bool valid = g < 6 * n_el;
-  const int64_t t = valid ? g / 6 : 0;
-  const int nt = (int)(g - 6 * t);
+  const bool valid = g < 6 * n_t;
+  const int64_t tg = valid ? g / 6 : 0;
+  const int nt = (int)(g - 6 * tg);
+  const int64_t t = tlist ? tlist[tg] : tg;
   double pt[3] = {0.0, 0.0, 0.0}, nrm[3] = {0.0, 0.0, 0.0};
   if (valid) {
     const ElemRec* T = elems + t;
@@ -387,6 +421,10 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
 #pragma unroll
     for (int q = 0; q < 3; ++q) trow[q] = sm.rows[96 * warp + lane + 32 * q];
     double* wb = sm.wbuf[warp];
+    // mixed-precision operator: this lane's block in the near-field store
+    // (the sm.nb list was staged before the barrier above)
+    const int64_t blk = (lo && mine) ? near_block(sm, t, s) : -1;
+    float* lob = blk >= 0 ? lo + blk * 324 + 3 * nt : nullptr;
     // every lane runs the in-plane form (the warp stays converged for the
     // per-warp transpose); rows of lanes that are not in-plane pairs are -1
     cplx P[6], Q[6];
@@ -399,12 +437,18 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
         const int32_t col = sm.cols[3 * a + j];
 #pragma unroll
         for (int i = 0; i < 3; ++i) wb[3 * lane + i] = B[i][j];
+        if (lob) {
+#pragma unroll
+          for (int i = 0; i < 3; ++i) lob[18 * (3 * a + j) + i] = low_part(B[i][j]);
+        }
         __syncwarp();
         if (col >= 0) {
-          double* colp = A + (int64_t)col * ld;
+          if (A) {
+            double* colp = A + (int64_t)col * ld;
 #pragma unroll
-          for (int q = 0; q < 3; ++q)
-            if (trow[q] >= 0) colp[trow[q]] = wb[lane + 32 * q];
+            for (int q = 0; q < 3; ++q)
+              if (trow[q] >= 0) colp[trow[q]] = wb[lane + 32 * q];
+          }
           if (Af) {
             float* colf = Af + (int64_t)col * ld;
 #pragma unroll
@@ -422,15 +466,19 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
     offplane_smon(S, z, h, nu, smon);
     int32_t rows[3];
     for (int k = 0; k < 3; ++k) rows[k] = dof[t + n_el * (3 * nt + k)];
+    const int64_t blk = lo ? near_block(sm, t, s) : -1;
+    float* lob = blk >= 0 ? lo + blk * 324 + 3 * nt : nullptr;
     contract_nodes(S.sfm, z, smon, scale, [&](int a, const double Sx[6][3]) {
       double B[3][3];
       traction_3x3(S.r, nl, Sx, is_dd_local, B);
       for (int j = 0; j < 3; ++j) {
+        if (lob)
+          for (int i = 0; i < 3; ++i) lob[18 * (3 * a + j) + i] = low_part(B[i][j]);
         const int32_t col = sm.cols[3 * a + j];
         if (col < 0) continue;
         for (int i = 0; i < 3; ++i)
           if (rows[i] >= 0) {
-            A[(int64_t)col * ld + rows[i]] = B[i][j];
+            if (A) A[(int64_t)col * ld + rows[i]] = B[i][j];
             if (Af) Af[(int64_t)col * ld + rows[i]] = (float)B[i][j];
           }
       }
@@ -450,20 +498,71 @@ void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int6
       d_nods, ld_nods, d_conn, ld_conn, n_el, beta, static_cast<ElemRec*>(d_elem));
 }
 
-void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
-                     int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s) {
+static void launch_assemble_pairs(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                                  int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s,
+                                  float* d_lo, const int32_t* np_ptr, const int32_t* np_idx, const int32_t* slist,
+                                  int64_t n_s, const int32_t* tlist, int64_t n_t) {
   gl_host_init(s);
   const size_t smem = sizeof(AsmSmem);
   static PerDeviceOnce attr0, attr1;
   smem_attr_once(attr0, assemble_kernel<false>, (int)smem);
   smem_attr_once(attr1, assemble_kernel<true>, (int)smem);
   cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
-  const dim3 grid((unsigned)((6 * n_el + kTile - 1) / kTile), (unsigned)n_el);
+  if (n_s <= 0 || n_t <= 0) return;
+  const dim3 grid((unsigned)((6 * n_t + kTile - 1) / kTile), (unsigned)n_s);
   const ElemRec* e = static_cast<const ElemRec*>(d_elem);
   ++g_launches;
-  assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status);
+  assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, d_lo,
+                                                   np_ptr, np_idx, slist, tlist, n_t);
   ++g_launches;
-  assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status);
+  assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, d_lo,
+                                                  np_ptr, np_idx, slist, tlist, n_t);
+}
+
+void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                     int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s,
+                     float* d_lo, const int32_t* np_ptr, const int32_t* np_idx) {
+  launch_assemble_pairs(d_elem, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, s, d_lo, np_ptr, np_idx,
+                        nullptr, n_el, nullptr, n_el);
+}
+
+// The pairs of an incremental assembly: every target of the sources in
+// slist (n_s), then the targets in tlist (n_t) of the sources in slist2
+// (n_s2).  The status words are cleared once; the off-plane passes run when
+// either in-plane pass met an off-plane pair.
+void launch_assemble_partial(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                             int is_dd_local, double* d_a, int64_t ld, int* d_status, cudaStream_t s,
+                             const int32_t* slist, int64_t n_s, const int32_t* slist2, int64_t n_s2,
+                             const int32_t* tlist, int64_t n_t) {
+  gl_host_init(s);
+  const size_t smem = sizeof(AsmSmem);
+  static PerDeviceOnce attr0, attr1;
+  smem_attr_once(attr0, assemble_kernel<false>, (int)smem);
+  smem_attr_once(attr1, assemble_kernel<true>, (int)smem);
+  cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
+  const ElemRec* e = static_cast<const ElemRec*>(d_elem);
+  for (int pass = 0; pass < 2; ++pass) {
+    const int32_t* sl = pass == 0 ? slist : slist2;
+    const int64_t ns = pass == 0 ? n_s : n_s2;
+    const int32_t* tl = pass == 0 ? nullptr : tlist;
+    const int64_t nt = pass == 0 ? n_el : n_t;
+    if (ns <= 0 || nt <= 0) continue;
+    const dim3 grid((unsigned)((6 * nt + kTile - 1) / kTile), (unsigned)ns);
+    ++g_launches;
+    assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, nullptr, d_status,
+                                                     nullptr, nullptr, nullptr, sl, tl, nt);
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    const int32_t* sl = pass == 0 ? slist : slist2;
+    const int64_t ns = pass == 0 ? n_s : n_s2;
+    const int32_t* tl = pass == 0 ? nullptr : tlist;
+    const int64_t nt = pass == 0 ? n_el : n_t;
+    if (ns <= 0 || nt <= 0) continue;
+    const dim3 grid((unsigned)((6 * nt + kTile - 1) / kTile), (unsigned)ns);
+    ++g_launches;
+    assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, nullptr, d_status,
+                                                    nullptr, nullptr, nullptr, sl, tl, nt);
+  }
 }
 
 // ----------------------------------------------------------- VC border

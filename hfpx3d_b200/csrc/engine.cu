@@ -301,6 +301,82 @@ static int assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_
   return rc;
 }
 
+// The mixed-precision operator: every entry in FP32 (no FP64 matrix), the
+// near-field blocks' low parts on the mesh's pattern.  The pattern indexes
+// blocks by element, so the DoF must be the default numbering of a mesh
+// without fixed DoF (18 e + 3 node + component), as for the near-field
+// preconditioners.
+static int assemble_mixed_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G,
+                               double nu, int is_dd_local, hfpx_matrix* m) {
+  const int64_t ne = mesh->n_el;
+  if (n_dof != 18 * ne) return set_error(c, HFPX_ERR_ARG, "the mixed-precision operator needs 18 DoF per element");
+  for (int64_t l = 0; l < 18; ++l)
+    for (int64_t e = 0; e < ne; ++e)
+      if (dof_h[e + ne * l] != 18 * e + l)
+        return set_error(c, HFPX_ERR_ARG, "the mixed-precision operator needs the default DoF numbering (no fixed DoF)");
+  std::shared_ptr<NearPattern> pat = mesh_pattern(c, mesh);
+  if (!pat) return set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
+  if (pat->maxdeg > kMaxNearDeg) return set_error(c, HFPX_ERR_ARG, "an element has more than 64 vertex neighbours");
+  if (m->lo_blocks != pat->blocks()) {
+    if (m->d_lo) cudaFree(m->d_lo);
+    m->d_lo = nullptr;
+    m->lo_blocks = 0;
+    if (int rc = check_cuda(c, cudaMalloc(&m->d_lo, sizeof(float) * 324 * (size_t)pat->blocks()), "near-field low parts"))
+      return rc;
+    m->lo_blocks = pat->blocks();
+  }
+  m->pat = pat;
+  int32_t* dd = nullptr;
+  int rc = upload_dof(c, dof_h, ne, n_dof, &dd);
+  if (rc) return rc;
+  m->factored = 0;
+  m->info = 0;
+  m->dinv_valid = 0;
+  launch_assemble(mesh->d_elem, ne, dd, G, nu, is_dd_local, nullptr, m->ld, m->d_f, c->d_flags, c->stream, m->d_lo,
+                  pat->d_ptr, pat->d_idx);
+  m->f32_current = 1;
+  rc = check_cuda(c, cudaGetLastError(), "assembly launch");
+  int flags[2] = {0, 0};
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(flags, c->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream), "flags");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "assembly");
+  if (!rc && (flags[0] & 1)) rc = set_error(c, HFPX_ERR_CUDA, "element staging copy timed out");
+  return rc;
+}
+
+// entries (i0 + r, j0 + q) of a mixed-precision operator, hi + lo, into a
+// column-major block (ld_out)
+__global__ void compose_block_kernel(const OpView V, int64_t i0, int64_t j0, int64_t rows, int64_t cols,
+                                     double* __restrict__ out, int64_t ld_out) {
+  const int64_t q = blockIdx.y;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    out[r + ld_out * q] = V.at(i0 + r, j0 + q);
+  (void)cols;
+}
+
+// a block of a mixed-precision operator to the host, in column chunks of at
+// most 32 MB through a context buffer
+static int download_mixed(hfpx_ctx* c, const hfpx_matrix* m, int64_t i0, int64_t j0, int64_t rows, int64_t cols,
+                          double* a, int64_t ld_host) {
+  const int64_t per = std::max<int64_t>(1, std::min<int64_t>(cols, ((int64_t)32 << 20) / (8 * rows)));
+  double* buf = (double*)ctx_scratch(c, kScrMixedBlk, sizeof(double) * rows * per);
+  if (!buf) return set_error(c, HFPX_ERR_NOMEM, "download buffer");
+  const OpView V = op_view(m);
+  int rc = 0;
+  for (int64_t q0 = 0; !rc && q0 < cols; q0 += per) {
+    const int64_t nq = std::min(per, cols - q0);
+    ++g_launches;
+    compose_block_kernel<<<dim3((unsigned)std::min<int64_t>(64, (rows + 255) / 256), (unsigned)nq), 256, 0, c->stream>>>(
+        V, i0, j0 + q0, rows, nq, buf, rows);
+    rc = check_cuda(c, cudaGetLastError(), "compose block");
+    if (!rc)
+      rc = check_cuda(c, cudaMemcpy2DAsync(a + ld_host * q0, ld_host * sizeof(double), buf, rows * sizeof(double),
+                                           rows * sizeof(double), nq, cudaMemcpyDeviceToHost, c->stream),
+                      "block download");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "block download");
+  }
+  return rc;
+}
+
 int hfpx_assemble(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
                   int is_dd_local, int vc_border, hfpx_matrix** out) {
   if (!c || !out) return HFPX_ERR_ARG;
@@ -326,7 +402,102 @@ int hfpx_assemble_into(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h,
   if (rc) return rc;
   if (!m || m->n != n_dof + (vc_border ? 1 : 0)) return set_error(c, HFPX_ERR_ARG, "matrix size does not match n_dof");
   if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
+  if (m->op_mixed) {
+    if (vc_border) return set_error(c, HFPX_ERR_ARG, "a mixed-precision operator has no volume-control border");
+    return assemble_mixed_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, m);
+  }
   return assemble_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, vc_border, m);
+}
+
+int hfpx_assemble_mixed(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int64_t n_dof, double G, double nu,
+                        int is_dd_local, hfpx_matrix** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
+  if (rc) return rc;
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
+  hfpx_matrix* m = new (std::nothrow) hfpx_matrix;
+  if (!m) return set_error(c, HFPX_ERR_NOMEM, "matrix");
+  m->n = n_dof;
+  m->ld = round_ld(n_dof);
+  m->op_mixed = 1;
+  rc = check_cuda(c, cudaMalloc(&m->d_f, sizeof(float) * (size_t)m->ld * n_dof), "matrix alloc");
+  if (!rc) rc = assemble_mixed_into(c, mesh, dof_h, n_dof, G, nu, is_dd_local, m);
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
+}
+
+int hfpx_matrix_is_mixed(const hfpx_matrix* m) { return m && m->op_mixed ? 1 : 0; }
+
+int hfpx_assemble_grow(hfpx_ctx* c, const hfpx_mesh* mesh, int64_t n_el_old, const int64_t* dof_h, int64_t n_dof,
+                       double G, double nu, int is_dd_local, const hfpx_matrix* old, hfpx_matrix** out) {
+  if (!c || !out) return HFPX_ERR_ARG;
+  *out = nullptr;
+  int rc = check_assembly_args(c, mesh, dof_h, n_dof, G, nu);
+  if (rc) return rc;
+  if (!old) return set_error(c, HFPX_ERR_ARG, "null old matrix");
+  if (old->op_mixed || !old->d_a) return set_error(c, HFPX_ERR_STATE, "the old matrix must be an FP64 operator");
+  if (old->factored == 1) return set_error(c, HFPX_ERR_STATE, "the old matrix holds FP64 LU factors, not the operator");
+  const int64_t ne = mesh->n_el, n_old = old->n;
+  if (n_el_old < 1 || n_el_old > ne) return set_error(c, HFPX_ERR_ARG, "n_el_old out of range");
+  if (n_old > n_dof) return set_error(c, HFPX_ERR_ARG, "the old matrix is larger than the new one");
+  // The old block is copied as it is, so the old elements must keep their
+  // DoF numbers: exactly the old matrix's n_old DoF belong to them, and the
+  // appended elements' DoF come after.
+  int64_t free_old = 0;
+  for (int64_t l = 0; l < 18; ++l)
+    for (int64_t e = 0; e < ne; ++e) {
+      const int64_t d = dof_h[e + ne * l];
+      if (d < -1 || d >= n_dof) return set_error(c, HFPX_ERR_ARG, "dof_h entry out of range");
+      if (d < 0) continue;
+      if (e < n_el_old) {
+        if (d >= n_old) return set_error(c, HFPX_ERR_ARG, "an old element's DoF is not one of the old matrix's");
+        ++free_old;
+      } else if (d < n_old) {
+        return set_error(c, HFPX_ERR_ARG, "an appended element's DoF falls inside the old matrix");
+      }
+    }
+  if (free_old != n_old) return set_error(c, HFPX_ERR_ARG, "the old elements' DoF do not number the old matrix");
+  if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
+  hfpx_matrix* m = nullptr;
+  rc = new_matrix(c, n_dof, &m);
+  if (rc) return rc;
+  // element lists: appended sources (all targets), then old sources with
+  // the appended targets
+  const int64_t n_new = ne - n_el_old;
+  std::vector<int32_t> lists(n_new + n_el_old);
+  for (int64_t i = 0; i < n_new; ++i) lists[i] = (int32_t)(n_el_old + i);
+  for (int64_t i = 0; i < n_el_old; ++i) lists[n_new + i] = (int32_t)i;
+  int32_t* dl = (int32_t*)ctx_scratch(c, kScrGrowList, sizeof(int32_t) * std::max<size_t>(1, lists.size()));
+  if (!dl) rc = set_error(c, HFPX_ERR_NOMEM, "element lists");
+  if (!rc)
+    rc = check_cuda(c, cudaMemcpyAsync(dl, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice,
+                                       c->stream), "element lists");
+  int32_t* dd = nullptr;
+  if (!rc) rc = upload_dof(c, dof_h, ne, n_dof, &dd);
+  if (!rc)
+    rc = check_cuda(c, cudaMemcpy2DAsync(m->d_a, m->ld * sizeof(double), old->d_a, old->ld * sizeof(double),
+                                         n_old * sizeof(double), n_old, cudaMemcpyDeviceToDevice, c->stream),
+                    "old block");
+  if (!rc) {
+    launch_assemble_partial(mesh->d_elem, ne, dd, G, nu, is_dd_local, m->d_a, m->ld, c->d_flags, c->stream, dl, n_new,
+                            dl + n_new, n_el_old, dl, n_new);
+    rc = check_cuda(c, cudaGetLastError(), "assembly launch");
+  }
+  int flags[2] = {0, 0};
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(flags, c->d_flags, sizeof(flags), cudaMemcpyDeviceToHost, c->stream), "flags");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "assembly");
+  if (!rc && (flags[0] & 1)) rc = set_error(c, HFPX_ERR_CUDA, "element staging copy timed out");
+  if (rc) {
+    hfpx_matrix_destroy(m);
+    return rc;
+  }
+  *out = m;
+  return HFPX_OK;
 }
 
 int hfpx_matrix_upload(hfpx_ctx* c, const double* a, int64_t n, int64_t ld_host, hfpx_matrix** out) {
@@ -391,6 +562,7 @@ int hfpx_matrix_dims(const hfpx_matrix* m, int64_t* n, int64_t* ld) {
 int hfpx_matrix_download(hfpx_ctx* c, const hfpx_matrix* m, double* a, int64_t ld_host) {
   if (!c || !m || !a || ld_host < m->n) return set_error(c, HFPX_ERR_ARG, "bad download arguments");
   if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
+  if (m->op_mixed) return download_mixed(c, m, 0, 0, m->n, m->n, a, ld_host);
   int rc = check_cuda(c, cudaMemcpy2DAsync(a, ld_host * sizeof(double), m->d_a, m->ld * sizeof(double), m->n * sizeof(double),
                                            m->n, cudaMemcpyDeviceToHost, c->stream),
                       "matrix download");
@@ -406,6 +578,7 @@ int hfpx_matrix_download_block(hfpx_ctx* c, const hfpx_matrix* m, int64_t i0, in
     return set_error(c, HFPX_ERR_ARG, "bad block download arguments");
   if (rows == 0 || cols == 0) return HFPX_OK;
   if (int rc = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc;
+  if (m->op_mixed) return download_mixed(c, m, i0, j0, rows, cols, a, ld_host);
   int rc = check_cuda(c, cudaMemcpy2DAsync(a, ld_host * sizeof(double), m->d_a + i0 + m->ld * j0, m->ld * sizeof(double),
                                            rows * sizeof(double), cols, cudaMemcpyDeviceToHost, c->stream),
                       "block download");
@@ -417,6 +590,8 @@ int hfpx_matrix_destroy(hfpx_matrix* m) {
   if (!m) return HFPX_OK;
   if (m->d_a) cudaFree(m->d_a);
   if (m->d_f) cudaFree(m->d_f);
+  if (m->d_lo) cudaFree(m->d_lo);
+  m->pat.reset();
   if (m->d_dinv) cudaFree(m->d_dinv);
   if (m->d_piv) cudaFree(m->d_piv);
   delete m;
@@ -448,6 +623,8 @@ int hfpx_lu_factor(hfpx_ctx* c, hfpx_matrix* m, int mode, int64_t* info) {
   if (!m) return set_error(c, HFPX_ERR_ARG, "null matrix");
   if (mode != HFPX_LU_FP64 && mode != HFPX_LU_MIXED) return set_error(c, HFPX_ERR_ARG, "unknown LU mode");
   if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "matrix already factored in place");
+  if (m->op_mixed)
+    return set_error(c, HFPX_ERR_STATE, "a mixed-precision operator is solved by GMRES (assemble in FP64 to factor)");
   if (int rc_dev = check_cuda(c, cudaSetDevice(c->device), "set device")) return rc_dev;
   int rc = mode == HFPX_LU_FP64 ? lu_factor_fp64(c, m) : lu_factor_fp32(c, m);
   if (info) *info = m->info;
@@ -562,6 +739,7 @@ int hfpx_residual_device(hfpx_ctx* c, const hfpx_matrix* m, const double* d_x, c
     if (zero) cudaMemsetAsync(zero, 0, sizeof(double) * n, c->stream);
   }
   if (!part || !dmax || (!d_b && !zero)) return set_error(c, HFPX_ERR_NOMEM, "residual buffers");
+  if (m->op_mixed) return residual_mixed(c, m, d_x, d_b ? d_b : zero, d_r, part, dmax);
   return residual_f64(c, m->d_a, m->ld, n, d_x, d_b ? d_b : zero, d_r, part, dmax);
 }
 

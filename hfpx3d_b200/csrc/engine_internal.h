@@ -23,7 +23,7 @@ struct hfpx_ctx {
   int* d_flags = nullptr;          // device status words (see kernels)
   // device work buffers kept between calls (grown on demand, freed with the
   // context), so repeated factorisations and solves allocate nothing
-  static constexpr int kScratchSlots = 48;
+  static constexpr int kScratchSlots = 64;
   void* scratch[kScratchSlots] = {};
   size_t scratch_bytes[kScratchSlots] = {};
   // tile triangular solves: tiles the flag array covers, epoch of the last
@@ -50,6 +50,47 @@ struct NearPattern {
 };
 
 struct hfpx_gnn_graph;
+
+// Read-only view of an operator for the kernels that gather its entries (the
+// near-field preconditioners, the network's inputs): the FP64 matrix A, or a
+// mixed-precision operator (Af every entry in FP32, lo the low parts of the
+// near-field blocks on the pattern ptr/idx: block (i, j) of column j is
+// j + ptr[j] for i == j, j + 1 + e for idx[e] == i).
+struct OpView {
+  const double* A = nullptr;
+  const float* Af = nullptr;
+  int64_t ld = 0;
+  const float* lo = nullptr;
+  const int32_t* ptr = nullptr;
+  const int32_t* idx = nullptr;
+#ifdef __CUDACC__
+  // entry (r, c) whose near-field block index is known (blk < 0: none)
+  __device__ __forceinline__ double at_blk(int64_t r, int64_t c, int64_t blk) const {
+    if (A) return A[r + ld * c];
+    double v = (double)Af[r + ld * c];
+    if (lo && blk >= 0) v += (double)lo[blk * 324 + 18 * (c % 18) + (r % 18)];
+    return v;
+  }
+  // any entry: the block is looked up in column c / 18's pattern
+  __device__ __forceinline__ double at(int64_t r, int64_t c) const {
+    if (A) return A[r + ld * c];
+    int64_t blk = -1;
+    if (lo) {
+      const int64_t i = r / 18, j = c / 18;
+      if (i == j) {
+        blk = j + ptr[j];
+      } else {
+        for (int32_t e = ptr[j]; e < ptr[j + 1]; ++e)
+          if (idx[e] == i) {
+            blk = j + 1 + e;
+            break;
+          }
+      }
+    }
+    return at_blk(r, c, blk);
+  }
+#endif
+};
 
 // Coarse space of a mesh for the two-level preconditioner: the elements
 // grouped into aggregates (k-means of their centroids), and on each aggregate
@@ -106,9 +147,18 @@ struct hfpx_precond {
 
 struct hfpx_matrix {
   int64_t n = 0, ld = 0;
-  double* d_a = nullptr;           // FP64 n x n column-major (ld)
+  double* d_a = nullptr;           // FP64 n x n column-major (ld); null for a mixed-precision operator
   float* d_f = nullptr;            // FP32 working copy (mixed mode), ld
   int f32_current = 0;             // d_f holds the operator (written by the assembly), not factors
+  // Mixed-precision operator (hfpx_assemble_mixed): d_f holds every entry
+  // rounded to FP32 and d_lo, on the near-field blocks of `pat` (each
+  // element with itself and with the elements sharing a vertex, 18 x 18
+  // column-major blocks in the pattern's block order), the FP32 rounding of
+  // what that rounding lost, so hi + lo is the FP64 entry to about 2^-48.
+  int op_mixed = 0;
+  float* d_lo = nullptr;
+  int64_t lo_blocks = 0;
+  std::shared_ptr<NearPattern> pat;
   int32_t* d_piv = nullptr;        // pivots (0-based global rows), n
   int factored = 0;                // 0 none, 1 fp64 in place, 2 fp32 copy
   int64_t info = 0;
@@ -160,7 +210,7 @@ enum : int {
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
   kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrStressDd, kScrStressPts, kScrStressSinf,
-  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrGmresEst, kScrCount
+  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrGmresEst, kScrMixedY, kScrMixedBlk, kScrGrowList, kScrCount
 };
 
 // assembly.cu
@@ -168,10 +218,22 @@ size_t elem_record_bytes();
 void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int64_t* d_conn,
                                int64_t ld_conn, int64_t n_el, double beta, void* d_elem,
                                cudaStream_t s);
-// d_f (optional): an FP32 copy of the matrix written in the same pass
+// d_f (optional): an FP32 copy of the matrix written in the same pass.
+// d_a null: the mixed-precision operator, d_f every entry in FP32 and d_lo
+// (on the near-field pattern np_ptr/np_idx, at most kMaxNearDeg neighbours
+// per element) the low parts of the near-field blocks.
+constexpr int kMaxNearDeg = 64;
 void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
                      int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_general_count,
-                     cudaStream_t s);
+                     cudaStream_t s, float* d_lo = nullptr, const int32_t* np_ptr = nullptr,
+                     const int32_t* np_idx = nullptr);
+// the pairs of an incremental assembly (FP64 only): every target of the
+// sources slist[0..n_s), and the targets tlist[0..n_t) of the sources
+// slist2[0..n_s2)
+void launch_assemble_partial(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
+                             int is_dd_local, double* d_a, int64_t ld, int* d_status, cudaStream_t s,
+                             const int32_t* slist, int64_t n_s, const int32_t* slist2, int64_t n_s2,
+                             const int32_t* tlist, int64_t n_t);
 void launch_vc_border(const void* d_elem, int64_t n_el, const int32_t* d_dof, int64_t n_dof,
                       int is_dd_local, double* d_a, int64_t ld, cudaStream_t s);
 void launch_rhs(const void* d_elem, int64_t n_el, const int32_t* d_dof, const double* d_sinf,
@@ -236,21 +298,24 @@ void pool_free_many(void* const* p, size_t count);
 std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh);
 void gnn_graph_release(hfpx_gnn_graph* g);
 int precond_apply(hfpx_ctx* c, const hfpx_precond* pc, const double* v, double* z);
-int gather_diag_inverse(hfpx_ctx* c, const double* A, int64_t lda, int64_t n_el, double* dinv, int* d_err);
-int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, const double* dinv, double* blocks,
+// the view of the operator a matrix holds (FP64, or mixed precision)
+OpView op_view(const hfpx_matrix* m);
+int gather_diag_inverse(hfpx_ctx* c, const OpView& A, const NearPattern& p, double* dinv, int* d_err);
+int neumann_blocks(hfpx_ctx* c, const OpView& A, const NearPattern& p, const double* dinv, double* blocks,
                    bool offdiag);
 // gnn.cu: the learned corrections added to the Neumann blocks of pc
 int gnn_correct_blocks(hfpx_ctx* c, const hfpx_gnn* net, const hfpx_mesh* mesh, const hfpx_matrix* m,
                        hfpx_precond* pc, double shear_m);
-int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks);
+int local_inverse_blocks(hfpx_ctx* c, const OpView& A, const NearPattern& p, double* blocks);
 // lu.cu: flexible GMRES on the FP64 matrix with a right preconditioner
 // apply(v, z): z = M v (FP64, device), for one right-hand side
 // Af (optional): the FP32 copy of A; products use it once the rotated
 // residual is below relax_below (relative), with an FP64 residual at the end
-// of such a cycle
+// of such a cycle.  mixed_op (optional): a mixed-precision operator; every
+// product and residual is then its own (A and Af unused)
 int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
                int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply,
-               const float* Af = nullptr, double relax_below = 0.0);
+               const float* Af = nullptr, double relax_below = 0.0, const hfpx_matrix* mixed_op = nullptr);
 
 // solve.cu: one right-hand side of the refinement
 int trsv_tiles(int64_t n);
@@ -264,4 +329,8 @@ int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const dou
 int residual_f32m(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const double* x, const double* b, double* r,
                   double* part, unsigned long long* d_max);
 int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max);
+// r = b - A x for a mixed-precision operator: the FP32 entries (products and
+// sums in FP64) plus the near-field blocks' low parts
+int residual_mixed(hfpx_ctx* c, const hfpx_matrix* m, const double* x, const double* b, double* r, double* part,
+                   unsigned long long* d_max);
 }  // namespace hfpx

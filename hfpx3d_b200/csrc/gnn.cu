@@ -402,7 +402,7 @@ __device__ void rotate18(const float* R, const double* X, double* Y, bool invers
 // One CTA per block b (self blocks first, then edges, as NearPattern): the
 // normalised operator input (X row, after its geometry features) and, when
 // `target` is given, the normalised target (local inverse minus Neumann).
-__global__ void __launch_bounds__(352) inputs_kernel(const double* __restrict__ A, int64_t lda, int64_t n_el,
+__global__ void __launch_bounds__(352) inputs_kernel(const OpView A, int64_t n_el,
                                                      const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                                      const int32_t* __restrict__ dst, const double* __restrict__ dinv,
                                                      const double* __restrict__ neu,
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(352) inputs_kernel(const double* __restrict__ 
       // D_i^-1 A_ij
       const int r = t % 18, c = t / 18;
       double s = 0.0;
-      for (int k = 0; k < 18; ++k) s += dinv[(size_t)324 * i + r + 18 * k] * A[(18 * i + k) + lda * (18 * j + c)];
+      for (int k = 0; k < 18; ++k) s += dinv[(size_t)324 * i + r + 18 * k] * A.at_blk(18 * i + k, 18 * j + c, blk);
       s_x[t] = s;
     }
   }
@@ -816,7 +816,7 @@ int graph_fill(hfpx_ctx* c, hfpx_gnn_graph* g, const hfpx_matrix* m, double G, c
                const double* target) {
   ++g_launches;
   inputs_kernel<<<(unsigned)g->pat->blocks(), 352, 0, c->stream>>>(
-      m->d_a, m->ld, g->n_nodes, g->pat->d_ptr, g->pat->d_idx, g->pat->d_dst, dinv, neu, target, g->d_rot, g->d_size,
+      op_view(m), g->n_nodes, g->pat->d_ptr, g->pat->d_idx, g->pat->d_dst, dinv, neu, target, g->d_rot, g->d_size,
       G, g->xn, g->xe, target ? g->tn : nullptr, target ? g->te : nullptr);
   return check_cuda(c, cudaGetLastError(), "network inputs");
 }
@@ -842,9 +842,10 @@ int graph_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m, doubl
   if (!rc && !err) rc = set_error(c, HFPX_ERR_NOMEM, "status word");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(g->d_neu, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
-  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, n, g->d_dinv, err);
-  if (!rc) rc = neumann_blocks(c, m->d_a, m->ld, *g->pat, g->d_dinv, g->d_neu, true);
-  if (!rc && target) rc = local_inverse_blocks(c, m->d_a, m->ld, *g->pat, target);
+  const OpView A = op_view(m);
+  if (!rc) rc = gather_diag_inverse(c, A, *g->pat, g->d_dinv, err);
+  if (!rc) rc = neumann_blocks(c, A, *g->pat, g->d_dinv, g->d_neu, true);
+  if (!rc && target) rc = local_inverse_blocks(c, A, *g->pat, target);
   if (!rc) rc = graph_fill(c, g, m, G, g->d_dinv, g->d_neu, target);
   int herr = 0;
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");

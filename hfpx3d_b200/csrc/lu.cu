@@ -2291,7 +2291,8 @@ constexpr int kGmresMax = 64;
 
 int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b, double tol, int restart,
                int max_iter, hfpx_solve_info* info, const std::function<int(const double*, double*)>& apply,
-               const float* Af, double relax_below) {
+               const float* Af, double relax_below, const hfpx_matrix* mixed_op) {
+  if (mixed_op) Af = nullptr;  // the operator is the mixed one: no relaxed products
   const int k = std::max(1, std::min(restart, kGmresMax));
   double* V = (double*)ctx_scratch(c, kScrGmresV, sizeof(double) * n * (k + 1));
   double* Z = (double*)ctx_scratch(c, kScrGmresZ, sizeof(double) * n * 2 * k);  // Z, then A Z
@@ -2355,8 +2356,9 @@ int gmres_core(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, double* d_b
       if (rc) break;
       const bool relaxed = Af && std::fabs(g[j]) / bnorm2 <= relax_below;
       cycle_relaxed = cycle_relaxed || relaxed;
-      rc = relaxed ? residual_f32m(c, Af, lda, n, zj, zero, w, part, dmax)   // w = -A z_j
-                   : residual_f64(c, A, lda, n, zj, zero, w, part, dmax);
+      rc = relaxed    ? residual_f32m(c, Af, lda, n, zj, zero, w, part, dmax)   // w = -A z_j
+           : mixed_op ? residual_mixed(c, mixed_op, zj, zero, w, part, dmax)
+                      : residual_f64(c, A, lda, n, zj, zero, w, part, dmax);
       if (rc) break;
       const double mone = -1.0, one = 1.0, zero_s = 0.0;
       cublasDscal(h, (int)n, &mone, w, 1);

@@ -37,16 +37,17 @@ constexpr int kBB = kB * kB;
 
 // Gauss-Jordan inverse of each 18 x 18 diagonal block, partial pivoting, in
 // shared memory (one CTA per element).  A zero pivot sets *err.
-__global__ void __launch_bounds__(128) diag_inverse_kernel(const double* __restrict__ A, int64_t lda, int64_t n_el,
-                                                           double* __restrict__ dinv, int* __restrict__ err) {
+__global__ void __launch_bounds__(128) diag_inverse_kernel(const OpView A, const int32_t* __restrict__ ptr,
+                                                           int64_t n_el, double* __restrict__ dinv,
+                                                           int* __restrict__ err) {
   __shared__ double a[kB][2 * kB + 1];
   __shared__ double f[kB];
   __shared__ int piv;
   const int64_t e = blockIdx.x;
-  const double* Ae = A + kB * e + lda * kB * e;
+  const int64_t blk = e + ptr[e];  // the self block in the near-field block order
   for (int t = threadIdx.x; t < kB * 2 * kB; t += blockDim.x) {
     const int r = t % kB, c = t / kB;
-    a[r][c] = c < kB ? Ae[r + lda * c] : (c - kB == r ? 1.0 : 0.0);
+    a[r][c] = c < kB ? A.at_blk(kB * e + r, kB * e + c, blk) : (c - kB == r ? 1.0 : 0.0);
   }
   __syncthreads();
   for (int c = 0; c < kB; ++c) {
@@ -105,7 +106,7 @@ __device__ __forceinline__ void mul18(const double* X, const double* Y, double* 
 }
 
 // Neumann blocks: M_jj = D_j^-1, M_ij = -D_i^-1 A_ij D_j^-1 (one CTA per block)
-__global__ void __launch_bounds__(352) neumann_kernel(const double* __restrict__ A, int64_t lda, int64_t n_el,
+__global__ void __launch_bounds__(352) neumann_kernel(const OpView A, int64_t n_el,
                                                       const int32_t* __restrict__ ptr,
                                                       const int32_t* __restrict__ idx,
                                                       const int32_t* __restrict__ dst,
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(352) neumann_kernel(const double* __restrict__
   const int64_t i = idx[e], j = dst[e];
   if (t < kBB) {
     const int r = t % kB, c = t / kB;
-    s_a[t] = A[(kB * i + r) + lda * (kB * j + c)];
+    s_a[t] = A.at_blk(kB * i + r, kB * j + c, j + 1 + e);
     s_di[t] = dinv[(size_t)kBB * i + t];
     s_dj[t] = dinv[(size_t)kBB * j + t];
   }
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(352) neumann_kernel(const double* __restrict__
 // when a shorter pattern shares the group), and its right-hand side E_j = the
 // first 18 columns of the identity.  Elements come in groups of one pattern
 // size; CTA (g, a, b) fills pattern blocks (a, b) of the group's element g.
-__global__ void local_system_kernel(const double* __restrict__ A, int64_t lda, const int32_t* __restrict__ ptr,
+__global__ void local_system_kernel(const OpView A, const int32_t* __restrict__ ptr,
                                     const int32_t* __restrict__ idx, const int32_t* __restrict__ elems, int slots,
                                     double* __restrict__ L, double* __restrict__ E) {
   const int64_t g = blockIdx.x;
@@ -157,7 +158,7 @@ __global__ void local_system_kernel(const double* __restrict__ A, int64_t lda, c
   if (a <= deg && bsl <= deg) {
     const int64_t pa = a == 0 ? j : idx[ptr[j] + a - 1];
     const int64_t pb = bsl == 0 ? j : idx[ptr[j] + bsl - 1];
-    v = A[(kB * pa + r) + lda * (kB * pb + c)];
+    v = A.at(kB * pa + r, kB * pb + c);
   } else {
     v = (a == bsl && r == c) ? 1.0 : 0.0;
   }
@@ -298,21 +299,35 @@ void free_pattern(NearPattern* p) {
   p->d_ptr = p->d_idx = p->d_dst = p->d_rev = p->d_rptr = p->d_rblk = p->d_rcol = nullptr;
 }
 
-int gather_diag_inverse(hfpx_ctx* c, const double* A, int64_t lda, int64_t n_el, double* dinv, int* d_err) {
+OpView op_view(const hfpx_matrix* m) {
+  OpView v;
+  v.ld = m->ld;
+  if (m->op_mixed) {
+    v.Af = m->d_f;
+    v.lo = m->d_lo;
+    v.ptr = m->pat->d_ptr;
+    v.idx = m->pat->d_idx;
+  } else {
+    v.A = m->d_a;
+  }
+  return v;
+}
+
+int gather_diag_inverse(hfpx_ctx* c, const OpView& A, const NearPattern& p, double* dinv, int* d_err) {
   ++g_launches;
-  diag_inverse_kernel<<<(unsigned)n_el, 128, 0, c->stream>>>(A, lda, n_el, dinv, d_err);
+  diag_inverse_kernel<<<(unsigned)p.n_el, 128, 0, c->stream>>>(A, p.d_ptr, p.n_el, dinv, d_err);
   return check_cuda(c, cudaGetLastError(), "diagonal block inverses");
 }
 
-int neumann_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, const double* dinv,
+int neumann_blocks(hfpx_ctx* c, const OpView& A, const NearPattern& p, const double* dinv,
                    double* blocks, bool offdiag) {
   ++g_launches;
   neumann_kernel<<<(unsigned)(offdiag ? p.blocks() : p.n_el), 352, 0, c->stream>>>(
-      A, lda, p.n_el, p.d_ptr, p.d_idx, p.d_dst, dinv, blocks, offdiag ? 1 : 0);
+      A, p.n_el, p.d_ptr, p.d_idx, p.d_dst, dinv, blocks, offdiag ? 1 : 0);
   return check_cuda(c, cudaGetLastError(), "Neumann blocks");
 }
 
-int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPattern& p, double* blocks) {
+int local_inverse_blocks(hfpx_ctx* c, const OpView& A, const NearPattern& p, double* blocks) {
   // elements grouped by pattern size (1 + neighbours), each group one batched
   // LU of its own size: padding every system to the largest pattern made the
   // factorisation about 4 times the work on a penny mesh
@@ -354,7 +369,7 @@ int local_inverse_blocks(hfpx_ctx* c, const double* A, int64_t lda, const NearPa
     const int32_t* eg = d_order + goff[sl];
     g_launches += 4;
     local_system_kernel<<<dim3((unsigned)cnt, (unsigned)sl, (unsigned)sl), 352, 0, c->stream>>>(
-        A, lda, p.d_ptr, p.d_idx, eg, (int)sl, Lg, Eg);
+        A, p.d_ptr, p.d_idx, eg, (int)sl, Lg, Eg);
     ptr_array_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, c->stream>>>(Lg, (int64_t)Q * Q, cnt, Lpg);
     ptr_array_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, c->stream>>>(Eg, (int64_t)Q * kB, cnt, Epg);
     int hinfo = 0;
@@ -461,12 +476,13 @@ int precond_fill(hfpx_ctx* c, hfpx_precond* pc, const hfpx_mesh* mesh, const hfp
   const int64_t nb = pc->pat->blocks();
   int rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
-  if (!rc) rc = gather_diag_inverse(c, m->d_a, m->ld, pc->n_el, pc->d_dinv, err);
+  const OpView A = op_view(m);
+  if (!rc) rc = gather_diag_inverse(c, A, *pc->pat, pc->d_dinv, err);
   if (!rc) {
     if (pc->kind == HFPX_PC_LOCAL_INVERSE)
-      rc = local_inverse_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_blocks);
+      rc = local_inverse_blocks(c, A, *pc->pat, pc->d_blocks);
     else
-      rc = neumann_blocks(c, m->d_a, m->ld, *pc->pat, pc->d_dinv, pc->d_blocks, pc->kind != HFPX_PC_BLOCK_JACOBI);
+      rc = neumann_blocks(c, A, *pc->pat, pc->d_dinv, pc->d_blocks, pc->kind != HFPX_PC_BLOCK_JACOBI);
   }
   if (!rc && pc->kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
   if (!rc && pc->cs) rc = coarse_setup(c, pc, m);
@@ -574,6 +590,9 @@ int hfpx_gmres_precond_device(hfpx_ctx* c, const hfpx_matrix* m, const hfpx_prec
   // the product, at half the bytes.  The copy is the one the assembly writes
   // (made here from the FP64 matrix the first time); without room for it, or
   // with HFPX_GMRES_F32=0, every product is FP64.
+  if (m->op_mixed)  // every product is the mixed-precision operator's own
+    return gmres_core(c, nullptr, m->ld, n, d_b, tol, restart > 0 ? restart : 50, max_iter > 0 ? max_iter : 1000,
+                      info, apply, nullptr, 0.0, m);
   const float* Af = nullptr;
   const char* e32 = std::getenv("HFPX_GMRES_F32");
   if (!(e32 && std::string(e32) == "0")) {

@@ -462,14 +462,18 @@ __global__ void __launch_bounds__(kGvThreads) resid_partial_f32_kernel(const flo
     if (i0 + r < n) part[(int64_t)blockIdx.y * n + i0 + r] = a[r];
 }
 
+// extra (optional): one more term of each row's product, added after the
+// chunk sums (the near-field low parts of a mixed-precision operator)
 __global__ void resid_finish_kernel(const double* __restrict__ b, const double* __restrict__ part, int n, int nch,
-                                    double* __restrict__ r, unsigned long long* __restrict__ rmax) {
+                                    double* __restrict__ r, unsigned long long* __restrict__ rmax,
+                                    const double* __restrict__ extra) {
   __shared__ double s_m[8];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double m = 0.0;
   if (i < n) {
     double s = 0.0;
     for (int k = 0; k < nch; ++k) s += part[(int64_t)k * n + i];
+    if (extra) s += extra[i];
     const double v = b[i] - s;
     r[i] = v;
     m = fabs(v);
@@ -536,7 +540,7 @@ int residual_f64(hfpx_ctx* c, const double* A, int64_t lda, int64_t n, const dou
   resid_partial_kernel<<<dim3((unsigned)((n + kGvRows - 1) / kGvRows), (unsigned)nch), kGvThreads, 0, c->stream>>>(
       A, lda, (int)n, x, part);
   ++g_launches;
-  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max);
+  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max, nullptr);
   return check_cuda(c, cudaGetLastError(), "residual launch");
 }
 
@@ -548,8 +552,49 @@ int residual_f32m(hfpx_ctx* c, const float* A, int64_t lda, int64_t n, const dou
   resid_partial_f32_kernel<<<dim3((unsigned)((n + kGvRows32 - 1) / kGvRows32), (unsigned)nch), kGvThreads, 0,
                              c->stream>>>(A, lda, (int)n, x, part);
   ++g_launches;
-  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max);
+  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max, nullptr);
   return check_cuda(c, cudaGetLastError(), "residual launch");
+}
+
+// y = L x for the near-field low parts of a mixed-precision operator, one
+// warp per block row (element i): lane r < 18 sums row 18 i + r over the
+// row's blocks (row view rptr/rblk/rcol) in a fixed order, in FP64.
+__global__ void __launch_bounds__(256) near_lo_kernel(const float* __restrict__ lo, int64_t n_el,
+                                                      const int32_t* __restrict__ rptr,
+                                                      const int32_t* __restrict__ rblk,
+                                                      const int32_t* __restrict__ rcol,
+                                                      const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n_el || lane >= 18) return;
+  double s = 0.0;
+  for (int32_t k = rptr[i]; k < rptr[i + 1]; ++k) {
+    const float* B = lo + (int64_t)rblk[k] * 324 + lane;
+    const double* xc = x + 18 * (int64_t)rcol[k];
+#pragma unroll 6
+    for (int c = 0; c < 18; ++c) s = fma((double)B[18 * c], xc[c], s);
+  }
+  y[18 * i + lane] = s;
+}
+
+int residual_mixed(hfpx_ctx* c, const hfpx_matrix* m, const double* x, const double* b, double* r, double* part,
+                   unsigned long long* d_max) {
+  const int64_t n = m->n;
+  if (!m->op_mixed || !m->d_f || !m->d_lo || !m->pat) return set_error(c, HFPX_ERR_STATE, "not a mixed-precision operator");
+  double* y = (double*)ctx_scratch(c, kScrMixedY, sizeof(double) * n);
+  if (!y) return set_error(c, HFPX_ERR_NOMEM, "mixed product buffer");
+  const NearPattern& p = *m->pat;
+  ++g_launches;
+  near_lo_kernel<<<(unsigned)((p.n_el * 32 + 255) / 256), 256, 0, c->stream>>>(m->d_lo, p.n_el, p.d_rptr, p.d_rblk,
+                                                                              p.d_rcol, x, y);
+  const int nch = resid_grid_chunks(c, n, kGvRows32, resid_partial_f32_kernel);
+  cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), c->stream);
+  ++g_launches;
+  resid_partial_f32_kernel<<<dim3((unsigned)((n + kGvRows32 - 1) / kGvRows32), (unsigned)nch), kGvThreads, 0,
+                             c->stream>>>(m->d_f, m->ld, (int)n, x, part);
+  ++g_launches;
+  resid_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(b, part, (int)n, nch, r, d_max, y);
+  return check_cuda(c, cudaGetLastError(), "mixed residual launch");
 }
 
 int absmax_f64(hfpx_ctx* c, const double* v, int64_t n, unsigned long long* d_max) {

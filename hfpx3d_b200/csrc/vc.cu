@@ -106,6 +106,7 @@ int hfpx_matrix_truncate(hfpx_ctx* c, const hfpx_matrix* m, const int64_t* keep,
   *out = nullptr;
   if (!m || !keep || n_keep < 1) return set_error(c, HFPX_ERR_ARG, "bad truncation arguments");
   if (m->factored == 1) return set_error(c, HFPX_ERR_STATE, "the matrix holds FP64 LU factors, not the operator");
+  if (m->op_mixed) return set_error(c, HFPX_ERR_STATE, "truncation needs the FP64 matrix");
   const int64_t n_dd = keep_border ? m->n - 1 : m->n;
   if (n_dd < 1 || n_keep > n_dd) return set_error(c, HFPX_ERR_ARG, "more kept DoF than the matrix has");
   {

@@ -55,6 +55,9 @@ SIGNATURES = {
     'hfpx_mesh_destroy': (_int, [_V]),
     'hfpx_assemble': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, _int, ctypes.POINTER(_V)]),
     'hfpx_assemble_into': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, _int, _V]),
+    'hfpx_assemble_mixed': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, ctypes.POINTER(_V)]),
+    'hfpx_matrix_is_mixed': (_int, [_V]),
+    'hfpx_assemble_grow': (_int, [_V, _V, _i64, _L, _i64, _f64, _f64, _int, _V, ctypes.POINTER(_V)]),
     'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
     'hfpx_matrix_dims': (_int, [_V, _L, _L]),
     'hfpx_matrix_download': (_int, [_V, _V, _D, _i64]),
@@ -233,6 +236,7 @@ class DeviceMatrix:
         n, ld = _i64(), _i64()
         lib().hfpx_matrix_dims(self.h, ctypes.byref(n), ctypes.byref(ld))
         self.n, self.ld = n.value, ld.value
+        self.mixed = bool(lib().hfpx_matrix_is_mixed(self.h))
 
     @classmethod
     def upload(cls, ctx, a):
@@ -270,6 +274,27 @@ def assemble(ctx, dmesh: DeviceMesh, dof_h, n_dof, G, nu, is_dd_local=False, vc=
     dof_h = _f(dof_h, np.int64)
     ctx.check(lib().hfpx_assemble(ctx.h, dmesh.h, _lp(dof_h), n_dof, G, nu, int(is_dd_local), int(vc),
                                   ctypes.byref(h)))
+    return DeviceMatrix(ctx, h)
+
+
+def assemble_mixed(ctx, dmesh: DeviceMesh, dof_h, n_dof, G, nu, is_dd_local=False) -> DeviceMatrix:
+    """The operator of assemble() in mixed precision: FP32 entries, near-field
+    blocks (self and vertex neighbours) kept to ~2^-48 by FP32 low parts."""
+    h = _V()
+    dof_h = _f(dof_h, np.int64)
+    ctx.check(lib().hfpx_assemble_mixed(ctx.h, dmesh.h, _lp(dof_h), n_dof, G, nu, int(is_dd_local), ctypes.byref(h)))
+    return DeviceMatrix(ctx, h)
+
+
+def assemble_grow(ctx, dmesh: DeviceMesh, n_el_old, dof_h, n_dof, G, nu, old: DeviceMatrix,
+                  is_dd_local=False) -> DeviceMatrix:
+    """The operator of a mesh grown by appending elements to the one `old`
+    was assembled for: the old block copied, only new rows and columns
+    assembled (hfpx_assemble_grow)."""
+    h = _V()
+    dof_h = _f(dof_h, np.int64)
+    ctx.check(lib().hfpx_assemble_grow(ctx.h, dmesh.h, n_el_old, _lp(dof_h), n_dof, G, nu, int(is_dd_local), old.h,
+                                       ctypes.byref(h)))
     return DeviceMatrix(ctx, h)
 
 

@@ -88,6 +88,37 @@ int hfpx_assemble(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, in
 int hfpx_assemble_into(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, int64_t n_dof,
                        double shear_m, double poiss_r, int is_dd_local, int vc_border,
                        hfpx_matrix *matrix);
+/* The same operator as hfpx_assemble (make_3dbem_matrix_s,
+ * system_assembly.cpp:30-219) held in mixed precision: every entry rounded
+ * to FP32 (4 bytes per entry instead of 8), and on the near-field blocks
+ * (each element with itself and with every element sharing a vertex: the
+ * log/atan-singular pairs) the FP32 rounding of what that rounding lost, so
+ * those entries keep about 48 bits.  The far field, whose entries decay as
+ * the cube of the distance, carries the FP32 rounding only.  Products and
+ * residuals with it accumulate in FP64 (hfpx_residual_device,
+ * hfpx_gmres_precond); the near-field preconditioners and the network read
+ * its near blocks to about 2^-48.  It needs 18 DoF per element in the
+ * default numbering (no fixed DoF) and has no volume-control border; it
+ * cannot be LU-factored or truncated (HFPX_ERR_STATE).  hfpx_assemble_into
+ * on it re-assembles in the same form; hfpx_matrix_download gives hi + lo. */
+int hfpx_assemble_mixed(hfpx_ctx *ctx, const hfpx_mesh *mesh, const int64_t *dof_h, int64_t n_dof,
+                        double shear_m, double poiss_r, int is_dd_local, hfpx_matrix **matrix);
+/* 1 for a mixed-precision operator (hfpx_assemble_mixed), else 0. */
+int hfpx_matrix_is_mixed(const hfpx_matrix *matrix);
+/* Incremental assembly of a growing crack, the step the reference leaves as
+ * "todo: growing mesh" (src/Development/c_f_iteration.cpp:289) around its
+ * full re-assembly (make_3dbem_matrix_s, system_assembly.cpp:30-219):
+ * `mesh` is the mesh `old` was assembled for with elements appended (its
+ * first n_el_old elements unchanged), dof_h its DoF handle (n_dof).  The
+ * old elements must keep their DoF numbers (they number the old matrix's
+ * n_old DoF; the appended elements' DoF come after), as the default
+ * numbering does.  *out (new, FP64) is the whole mesh's operator: the old
+ * block copied on the device, and only the new block rows and columns
+ * assembled (pairs with an appended source or target).  Removing elements is
+ * hfpx_matrix_truncate with the DoF of the elements that stay. */
+int hfpx_assemble_grow(hfpx_ctx *ctx, const hfpx_mesh *mesh, int64_t n_el_old, const int64_t *dof_h,
+                       int64_t n_dof, double shear_m, double poiss_r, int is_dd_local, const hfpx_matrix *old,
+                       hfpx_matrix **out);
 /* Upload a caller matrix (n x n, column-major, ld_host) for il::LU use. */
 int hfpx_matrix_upload(hfpx_ctx *ctx, const double *a, int64_t n, int64_t ld_host,
                        hfpx_matrix **matrix);
