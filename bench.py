@@ -376,6 +376,8 @@ def run_engine(args, rank, world, local_rank):
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
     # stresses at observation points (make_3dbem_stress_f_s) on the C1 penny
     stress = run_stress(ctx, engine, torch, stream) if rank == 0 and args.stress else None
+    # the batched workload: 256 uneven meshes x 64 load cases in one graph
+    c5 = run_c5(args, ctx, engine, torch, stream) if rank == 0 and args.batch else None
     F.close()
 
     if rank != 0:
@@ -467,6 +469,18 @@ def run_engine(args, rank, world, local_rank):
         line['c2'] = c2
     if stress is not None:
         line['stress'] = stress
+    if c5 is not None:
+        cb = line.get('cpu_baseline') or {}
+        fit = cb.get('fit')
+        if fit:
+            # the reference per mesh: assembly a Ne^2 + LU b N^3 (the fit of
+            # the measured sizes), the 64 load cases' dgetrs neglected
+            ref = sum(fit['a'] * ne ** 2 + fit['b'] * (18.0 * ne) ** 3 for ne in c5.pop('_n_el'))
+            c5['reference_cpu_s'] = ref
+            c5['reference_cpu_note'] = ('extrapolated per mesh from the fit of the measured CPU reference '
+                                        '(a Ne^2 + b N^3, summed over the meshes)')
+        c5.pop('_n_el', None)
+        line['c5'] = c5
     return line
 
 
@@ -535,6 +549,64 @@ FORM_TEXT = {'learned': 'two-level preconditioner (learned near-field blocks + c
                         'aggregates) + GMRES(50) on the OPERATOR',
              'mixed': 'mixed LU (FP16 tcgen05 updates) + GMRES on the FP64 operator',
              'fp64': 'FP64 LU + triangular solves'}
+
+
+def run_c5(args, ctx, engine, torch, stream, reps=3):
+    """The batched workload: 256 seeded penny / 2:1
+    ellipse meshes of 24-550 elements, 64 load cases each (pressures U[0.5, 2],
+    random in-situ stresses), assembly + factorisation + solves of every mesh
+    and load case in one CUDA-graph launch (hfpx_batch_run), best of `reps`
+    replays after the capturing run; beside it the same meshes one by one
+    through the per-mesh C-ABI (FP64 assembly, mixed LU, refined solves of
+    the 64 load cases)."""
+    from hfpx3d_b200 import meshgen
+    meshes, S = meshgen.batch_workload(256, 64)
+    n_el = [c.shape[1] for _, c in meshes]
+    dms = [engine.DeviceMesh(ctx, engine.MeshGeom(nods, conn), BETA) for nods, conn in meshes]
+    t0 = time.perf_counter()
+    B = engine.Batch(ctx, dms, G, NU)
+    B.set_loads(S)
+    info = B.run(tol=args.tol)
+    setup_s = time.perf_counter() - t0
+    best = float('inf')
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        info = B.run(tol=args.tol)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    flops = sum(2.0 / 3.0 * (18.0 * ne) ** 3 for ne in n_el)
+    out = {'workload': '256 seeded penny / 2:1 ellipse meshes, 24-550 elements (meshgen.batch_workload), 64 load '
+                       'cases each; one CUDA graph: assembly (mixed-precision operators) + FP32 tournament-pivoted '
+                       'LU + solves of the 6 unit stress states + FP64 refinement + the 64 combinations',
+           'n_mesh': len(meshes), 'elements': int(sum(n_el)), 'load_cases': int(S.shape[2]),
+           'tiles': {'nb': B.nb, 'leaf_rows': B.leaf_rows}, 'graph_launches': B.launches,
+           'batch_s': best, 'meshes_per_s': len(meshes) / best,
+           'load_case_solves_per_s': len(meshes) * S.shape[2] / best,
+           'lu_tflops': flops / best / 1e12, 'residual': info.residual, 'converged': bool(info.converged),
+           'first_run_s (capture + instantiate + run)': setup_s, '_n_el': n_el}
+    B.close()
+    # the same meshes one by one through the per-mesh C-ABI
+    if args.c5_per_mesh:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for m, (nods, conn) in enumerate(meshes):
+            mesh = engine.MeshGeom(nods, conn)
+            dof, n = engine.make_dof_h_crack(mesh, 0)
+            A = engine.assemble(ctx, dms[m], dof, n, G, NU)
+            rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dms[m], dof, n, S[m])
+            engine.LU(ctx, A, engine.HFPX_LU_MIXED).solve(np.asfortranarray(rhs), tol=args.tol)
+            A.close()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out['per_mesh_path_s'] = e0.elapsed_time(e1) / 1e3
+        out['speedup_vs_per_mesh_path'] = out['per_mesh_path_s'] / best
+    for d in dms:
+        d.close()
+    return out
 
 
 def time_residual(ctx, engine, L, torch, stream, A, d_b, d_x, n, reps=5):
@@ -855,6 +927,10 @@ def main():
                     help='penny sizes (elements) the CPU reference is measured at and fitted from')
     ap.add_argument('--no-c2-ref', dest='c2_ref', action='store_false',
                     help='skip the CPU reference run of the 1025-element VC ellipse')
+    ap.add_argument('--no-batch', dest='batch', action='store_false',
+                    help='skip the batched workload (256 uneven meshes x 64 load cases in one graph)')
+    ap.add_argument('--no-c5-per-mesh', dest='c5_per_mesh', action='store_false',
+                    help='skip the per-mesh C-ABI timing of the batched workload')
     ap.add_argument('--e2e-steps', type=int, default=3)
     ap.add_argument('--e2e-warmup', type=int, default=3)
     args = ap.parse_args()

@@ -359,25 +359,18 @@ __device__ __forceinline__ int64_t near_block(const AsmSmem& sm, int64_t t, int6
 // rounded to FP32 (hi + lo carries about 48 bits of v).
 __device__ __forceinline__ float low_part(double v) { return (float)(v - (double)(float)v); }
 
+// One CTA's work: source element s against the targets of tile bx (all
+// n_t targets, or those listed in tlist).  A (FP64) and the FP32 arrays Af,
+// Af2 (any may be null) receive every entry; lo the near-field low parts.
 template <bool GENERAL>
-__global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const ElemRec* __restrict__ elems,
-                                                         int64_t n_el,
-                                                         const int32_t* __restrict__ dof,
-                                                         double G, double nu, int is_dd_local,
-                                                         double* __restrict__ A, int64_t ld,
-                                                         float* __restrict__ Af,
-                                                         int* __restrict__ status,
-                                                         float* __restrict__ lo,
-                                                         const int32_t* __restrict__ np_ptr,
-                                                         const int32_t* __restrict__ np_idx,
-                                                         const int32_t* __restrict__ slist,
-                                                         const int32_t* __restrict__ tlist, int64_t n_t) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
-  if (GENERAL && status[1] == 0) return;  // first pass met no off-plane pair
-  // source element of this CTA and the target elements of the grid's x
-  // range: all of them, or the lists of a partial (incremental) assembly
-  const int64_t s = slist ? slist[blockIdx.y] : blockIdx.y;
+__device__ __forceinline__ void assemble_body(AsmSmem& sm, const ElemRec* __restrict__ elems, int64_t n_el,
+                                              const int32_t* __restrict__ dof, double G, double nu,
+                                              int is_dd_local, double* __restrict__ A, int64_t ld,
+                                              float* __restrict__ Af, float* __restrict__ Af2,
+                                              int* __restrict__ status, float* __restrict__ lo,
+                                              const int32_t* __restrict__ np_ptr,
+                                              const int32_t* __restrict__ np_idx, int64_t s, int64_t bx,
+                                              const int32_t* __restrict__ tlist, int64_t n_t) {
   const int tid = threadIdx.x;
   if (!stage_bulk(&sm.src, elems + s, sizeof(ElemRec), &sm.bar, status)) return;
   if (tid < 18) sm.cols[tid] = dof[s + n_el * tid];
@@ -389,7 +382,7 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
       sm.nbase = s + p0;
     }
   }
-  const int64_t g = (int64_t)blockIdx.x * kTile + tid;
+  const int64_t g = bx * kTile + tid;
   const bool valid = g < 6 * n_t;
   const int64_t tg = valid ? g / 6 : 0;
   const int nt = (int)(g - 6 * tg);
@@ -455,6 +448,12 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
             for (int q = 0; q < 3; ++q)
               if (trow[q] >= 0) colf[trow[q]] = (float)wb[lane + 32 * q];
           }
+          if (Af2) {
+            float* colf = Af2 + (int64_t)col * ld;
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+              if (trow[q] >= 0) colf[trow[q]] = (float)wb[lane + 32 * q];
+          }
         }
         __syncwarp();
       }
@@ -480,10 +479,81 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
           if (rows[i] >= 0) {
             if (A) A[(int64_t)col * ld + rows[i]] = B[i][j];
             if (Af) Af[(int64_t)col * ld + rows[i]] = (float)B[i][j];
+            if (Af2) Af2[(int64_t)col * ld + rows[i]] = (float)B[i][j];
           }
       }
     });
   }
+}
+
+template <bool GENERAL>
+__global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const ElemRec* __restrict__ elems,
+                                                         int64_t n_el,
+                                                         const int32_t* __restrict__ dof,
+                                                         double G, double nu, int is_dd_local,
+                                                         double* __restrict__ A, int64_t ld,
+                                                         float* __restrict__ Af,
+                                                         int* __restrict__ status,
+                                                         float* __restrict__ lo,
+                                                         const int32_t* __restrict__ np_ptr,
+                                                         const int32_t* __restrict__ np_idx,
+                                                         const int32_t* __restrict__ slist,
+                                                         const int32_t* __restrict__ tlist, int64_t n_t) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
+  if (GENERAL && status[1] == 0) return;  // first pass met no off-plane pair
+  // source element of this CTA and the target elements of the grid's x
+  // range: all of them, or the lists of a partial (incremental) assembly
+  const int64_t s = slist ? slist[blockIdx.y] : blockIdx.y;
+  assemble_body<GENERAL>(sm, elems, n_el, dof, G, nu, is_dd_local, A, ld, Af, nullptr, status, lo, np_ptr, np_idx, s,
+                         blockIdx.x, tlist, n_t);
+}
+
+// Many meshes in one launch: CTA i takes task i = (mesh, source element,
+// target tile) and writes that mesh's mixed-precision operator (FP32
+// entries and near-field low parts) and its FP32 copy for the factorisation.
+__global__ void __launch_bounds__(kTile, 4) batch_assemble_kernel(const BatchAsmMesh* __restrict__ meshes,
+                                                                  const int4* __restrict__ tasks, double G,
+                                                                  double nu, int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
+  const int4 tk = tasks[blockIdx.x];
+  const BatchAsmMesh M = meshes[tk.x];
+  assemble_body<false>(sm, static_cast<const ElemRec*>(M.elems), M.n_el, M.dof, G, nu, 0, nullptr, M.ld, M.A, M.F, status, M.lo, M.np_ptr,
+                       M.np_idx, tk.y, tk.z, nullptr, M.n_el);
+}
+__global__ void __launch_bounds__(kTile, 1) batch_assemble_general_kernel(const BatchAsmMesh* __restrict__ meshes,
+                                                                          const int4* __restrict__ tasks, double G,
+                                                                          double nu, int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
+  if (status[1] == 0) return;  // the in-plane pass met no off-plane pair
+  const int4 tk = tasks[blockIdx.x];
+  const BatchAsmMesh M = meshes[tk.x];
+  assemble_body<true>(sm, static_cast<const ElemRec*>(M.elems), M.n_el, M.dof, G, nu, 0, nullptr, M.ld, M.A, M.F, status, M.lo, M.np_ptr,
+                      M.np_idx, tk.y, tk.z, nullptr, M.n_el);
+}
+
+// set-up of the batched assembly kernels on the current device (before a
+// stream capture records their launches)
+static PerDeviceOnce g_batch_attr0, g_batch_attr1;
+int batch_assemble_setup(cudaStream_t s) {
+  gl_host_init(s);
+  const size_t smem = sizeof(AsmSmem);
+  cudaError_t e = smem_attr_once(g_batch_attr0, batch_assemble_kernel, (int)smem);
+  if (e == cudaSuccess) e = smem_attr_once(g_batch_attr1, batch_assemble_general_kernel, (int)smem);
+  return e == cudaSuccess ? 0 : 1;
+}
+
+void launch_batch_assemble(const BatchAsmMesh* d_meshes, const void* d_tasks, int64_t n_tasks, double G, double nu,
+                           int* d_status, cudaStream_t s) {
+  const size_t smem = sizeof(AsmSmem);
+  cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
+  const int4* t = static_cast<const int4*>(d_tasks);
+  ++g_launches;
+  batch_assemble_kernel<<<(unsigned)n_tasks, kTile, smem, s>>>(d_meshes, t, G, nu, d_status);
+  ++g_launches;
+  batch_assemble_general_kernel<<<(unsigned)n_tasks, kTile, smem, s>>>(d_meshes, t, G, nu, d_status);
 }
 
 size_t elem_record_bytes() { return sizeof(ElemRec); }
@@ -613,6 +683,35 @@ __global__ void rhs_kernel(const ElemRec* __restrict__ elems, int64_t n_el,
   else if (l == 1) t = n[1] * si[1] + n[0] * si[3] + n[2] * si[5];
   else t = n[2] * si[2] + n[0] * si[4] + n[1] * si[5];
   rhs[d + ld * c] -= t;
+}
+
+// The right-hand sides of the 6 unit in-situ stress states of many meshes
+// without fixed DoF (rhs = -(n . e_c) per collocation point and component,
+// DoF 18 e + 3 node + l): block y is mesh y, its n x 6 block at B + boff[y].
+__global__ void batch_basis_rhs_kernel(const BatchAsmMesh* __restrict__ meshes, double* __restrict__ B,
+                                       const int64_t* __restrict__ boff) {
+  const BatchAsmMesh M = meshes[blockIdx.y];
+  const ElemRec* E = static_cast<const ElemRec*>(M.elems);
+  const int64_t n = 18 * M.n_el;
+  double* b = B + boff[blockIdx.y];
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 6 * n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / n, d = t - c * n, el = d / 18;
+    const int l = (int)(d % 3);
+    const double* nr = E[el].nrm;
+    double si[6] = {0, 0, 0, 0, 0, 0};
+    si[c] = 1.0;
+    double v;
+    if (l == 0) v = nr[0] * si[0] + nr[1] * si[3] + nr[2] * si[4];
+    else if (l == 1) v = nr[1] * si[1] + nr[0] * si[3] + nr[2] * si[5];
+    else v = nr[2] * si[2] + nr[0] * si[4] + nr[1] * si[5];
+    b[t] = -v;
+  }
+}
+
+void launch_batch_basis_rhs(const BatchAsmMesh* d_meshes, int64_t n_mesh, double* d_B, const int64_t* d_boff,
+                            cudaStream_t s) {
+  ++g_launches;
+  batch_basis_rhs_kernel<<<dim3(64, (unsigned)n_mesh), 256, 0, s>>>(d_meshes, d_B, d_boff);
 }
 
 void launch_rhs(const void* d_elem, int64_t n_el, const int32_t* d_dof, const double* d_sinf,

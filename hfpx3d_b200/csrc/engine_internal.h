@@ -227,6 +227,29 @@ void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, dou
                      int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_general_count,
                      cudaStream_t s, float* d_lo = nullptr, const int32_t* np_ptr = nullptr,
                      const int32_t* np_idx = nullptr);
+// One mesh of a batched assembly: its element records, DoF map, the FP32
+// operator A (hi parts) with its near-field low parts lo on the pattern
+// np_ptr/np_idx, and the FP32 copy F the factorisation overwrites (ld rows).
+struct BatchAsmMesh {
+  const void* elems;
+  const int32_t* dof;
+  float* A;
+  float* F;
+  float* lo;
+  const int32_t* np_ptr;
+  const int32_t* np_idx;
+  int64_t n_el;
+  int64_t ld;
+};
+// tasks: n_tasks int4 (mesh, source element, target tile of 128
+// collocation points, 0), one CTA each
+int batch_assemble_setup(cudaStream_t s);
+void launch_batch_assemble(const BatchAsmMesh* d_meshes, const void* d_tasks, int64_t n_tasks, double G, double nu,
+                           int* d_status, cudaStream_t s);
+// the 6 unit in-situ stress states' right-hand sides of every mesh (no
+// fixed DoF), mesh m's n x 6 block at d_B + d_boff[m]
+void launch_batch_basis_rhs(const BatchAsmMesh* d_meshes, int64_t n_mesh, double* d_B, const int64_t* d_boff,
+                            cudaStream_t s);
 // the pairs of an incremental assembly (FP64 only): every target of the
 // sources slist[0..n_s), and the targets tlist[0..n_t) of the sources
 // slist2[0..n_s2)
@@ -271,6 +294,23 @@ bool tc_update_supported(int64_t lda_k, int64_t ldb_k, const void* A, const void
 int tc_update_f16(hfpx_ctx* c, cudaStream_t s, int64_t m, int64_t n, int64_t k, const void* A, int64_t lda_k,
                   const void* B, int64_t ldb_k, float* C, int64_t ldc, const float* d_alpha, const float* d_row_scale,
                   int* d_err, int max_ctas);
+
+// the grouped form (the batched LU's trailing updates): problem p is
+// C += alpha s_i (A B^T), m x n x k, its operand maps at maps[map], maps[map + 1]
+// (tensor maps of 128 bytes each in device memory, made by
+// tc_make_operand_map with box rows 128 for A and 256 for B), its tiles
+// tile_start[p] .. tile_start[p + 1) (128 x 256 outputs each)
+struct TcProblem {
+  float* C;
+  int64_t ldc;
+  int32_t m, n, k, map;
+  const float* alpha;
+  const float* row_scale;
+};
+bool tc_make_operand_map(void* map, const void* base, int64_t rows, int64_t k, int64_t ld_k, int box_rows);
+int tc_grouped_setup(hfpx_ctx* c);
+void tc_update_grouped(cudaStream_t st, int grid, const void* d_maps, const TcProblem* d_probs,
+                       const int64_t* d_tile_start, int n_probs, int* d_err);
 
 // precond.cu: near-field preconditioners on the FP64 matrix (block-Jacobi,
 // first-order Neumann, exact local inverse, learned) and their product

@@ -604,6 +604,192 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   }
 }
 
+// ------------------------------------------------------ grouped form
+// Many independent updates in one persistent launch (the batched LU's
+// trailing updates, one problem per mesh): problem p is C_p += alpha_p s_i
+// (A_p B_p^T) with its tensor maps at maps[map_p], maps[map_p + 1] (in
+// global memory, written before the launch), its output tiles numbered
+// tile_start[p] .. tile_start[p + 1).  The roles and the pipeline are the
+// 1-SM kernel's; each tile looks its problem up.
+__device__ __forceinline__ int tile_problem(const int64_t* __restrict__ tile_start, int n_probs, int64_t t) {
+  int lo = 0, hi = n_probs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    update_tc_grouped_kernel(const CUtensorMap* __restrict__ maps, const TcProblem* __restrict__ probs,
+                             const int64_t* __restrict__ tile_start, int n_probs, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t tiles = tile_start[n_probs];
+  volatile int* abort = &s.abort;
+  auto tile_of = [&](int64_t t, int& p, int64_t& mb, int64_t& nb) {
+    p = tile_problem(tile_start, n_probs, t);
+    const int64_t l = t - tile_start[p];
+    const int64_t tn = (probs[p].n + kBN - 1) / kBN;
+    mb = l / tn;
+    nb = l - mb * tn;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(&s.full[i], 1);
+      mbar_init(&s.empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&s.tfull[i], 1);
+      mbar_init(&s.tempty[i], kEpiWarps);
+    }
+    mbar_init(&s.drain, 1);
+    s.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem_base;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t armed = 0, armed_par = 0;
+      for (int64_t t = blockIdx.x; t < tiles && !*abort; t += gridDim.x) {
+        int p;
+        int64_t mb, nb;
+        tile_of(t, p, mb, nb);
+        const CUtensorMap* ma = maps + probs[p].map;
+        const int nk = (probs[p].k + kBK - 1) / kBK;
+        // the maps were written to global memory before the launch: acquire
+        // them for the tensor-map proxy before the copies read them
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(ma))
+                     : "memory");
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(ma + 1))
+                     : "memory");
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.empty[stage], phase ^ 1u, abort, err, 0x301)) break;
+          armed &= ~(1u << stage);
+          mbar_expect_tx(&s.full[stage], kStageA + kStageB);
+          tma_load_2d(s.a[stage], ma, &s.full[stage], kb * kBK, (int)(mb * kBM));
+          tma_load_2d(s.b[stage], ma + 1, &s.full[stage], kb * kBK, (int)(nb * kBN));
+          armed |= 1u << stage;
+          armed_par = (armed_par & ~(1u << stage)) | (phase << stage);
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (*abort)
+        for (int i = 0; i < kStages; ++i)
+          if (armed & (1u << i)) drain_phase(&s.full[i], (armed_par >> i) & 1u);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      bool issued = false;
+      for (int64_t t = blockIdx.x; t < tiles && !*abort; t += gridDim.x, ++it) {
+        int p;
+        int64_t mb, nb;
+        tile_of(t, p, mb, nb);
+        const int nk = (probs[p].k + kBK - 1) / kBK;
+        const int acc = it & 1;
+        const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+        if (!wait_phase(&s.tempty[acc], acc_phase ^ 1u, abort, err, 0x302)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * kBN);
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!wait_phase(&s.full[stage], phase, abort, err, 0x303)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll
+          for (int k16 = 0; k16 < kBK / 16; ++k16)
+            mma_f16(d, smem_desc(s.a[stage], k16), smem_desc(s.b[stage], k16), (kb | k16) != 0);
+          issued = true;
+          mma_commit(&s.empty[stage]);
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&s.tfull[acc]);
+      }
+      if (*abort && issued) {
+        mma_commit(&s.drain);
+        drain_phase(&s.drain, 0);
+      }
+    }
+    __syncwarp();
+  } else {
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int acc = it & 1;
+      const uint32_t acc_phase = (uint32_t)(it >> 1) & 1u;
+      bool ok = wait_phase(&s.tfull[acc], acc_phase, abort, err, 0x304);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      tc_fence_after();
+      int p;
+      int64_t mb, nb;
+      tile_of(t, p, mb, nb);
+      const TcProblem& P = probs[p];
+      const float alpha = *P.alpha;
+      const int64_t row = mb * kBM + q * 32 + lane;
+      const bool row_ok = row < P.m;
+      const float ra = row_ok && P.row_scale ? alpha * P.row_scale[row] : alpha;
+      const int64_t col0 = nb * kBN + half * 128;
+#pragma unroll 1
+      for (int ch = 0; ch < 4; ++ch) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
+        const int64_t cb = col0 + ch * 32;
+        const int ncol = row_ok ? (int)min((int64_t)32, max((int64_t)0, (int64_t)P.n - cb)) : 0;
+        float* pc = P.C + row + P.ldc * cb;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float c[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(pc + P.ldc * (16 * h + j)) : 0.f;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (16 * h + j < ncol) __stcg(pc + P.ldc * (16 * h + j), fmaf(ra, v[16 * h + j], c[j]));
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&s.tempty[acc]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* p = nullptr;
@@ -698,6 +884,22 @@ int tc_update_f16(hfpx_ctx* c, cudaStream_t st, int64_t m, int64_t n, int64_t k,
                                                          d_alpha, d_row_scale, d_err);
   }
   return check_cuda(c, cudaGetLastError(), "tensor-core update launch");
+}
+
+bool tc_make_operand_map(void* map, const void* base, int64_t rows, int64_t k, int64_t ld_k, int box_rows) {
+  return make_map(static_cast<CUtensorMap*>(map), base, rows, k, ld_k, (uint32_t)box_rows);
+}
+
+int tc_grouped_setup(hfpx_ctx* c) {
+  static PerDeviceOnce attr;
+  return check_cuda(c, smem_attr_once(attr, update_tc_grouped_kernel, (int)kSmemBytes), "grouped update attribute");
+}
+
+void tc_update_grouped(cudaStream_t st, int grid, const void* d_maps, const TcProblem* d_probs,
+                       const int64_t* d_tile_start, int n_probs, int* d_err) {
+  ++g_launches;
+  update_tc_grouped_kernel<<<(unsigned)grid, kThreads, kSmemBytes, st>>>(
+      static_cast<const CUtensorMap*>(d_maps), d_probs, d_tile_start, n_probs, d_err);
 }
 
 }  // namespace hfpx

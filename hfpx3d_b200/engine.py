@@ -58,6 +58,13 @@ SIGNATURES = {
     'hfpx_assemble_mixed': (_int, [_V, _V, _L, _i64, _f64, _f64, _int, ctypes.POINTER(_V)]),
     'hfpx_matrix_is_mixed': (_int, [_V]),
     'hfpx_assemble_grow': (_int, [_V, _V, _i64, _L, _i64, _f64, _f64, _int, _V, ctypes.POINTER(_V)]),
+    'hfpx_batch_create': (_int, [_V, _i64, ctypes.POINTER(_V), _f64, _f64, _int, _int, ctypes.POINTER(_V)]),
+    'hfpx_batch_set_loads': (_int, [_V, _V, _D, _i64]),
+    'hfpx_batch_run': (_int, [_V, _V, _f64, _int, _V]),
+    'hfpx_batch_solution': (_int, [_V, _V, _i64, _D]),
+    'hfpx_batch_residuals': (_int, [_V, _V, _D]),
+    'hfpx_batch_launches': (_i64, [_V]),
+    'hfpx_batch_destroy': (_int, [_V]),
     'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
     'hfpx_matrix_dims': (_int, [_V, _L, _L]),
     'hfpx_matrix_download': (_int, [_V, _V, _D, _i64]),
@@ -680,6 +687,85 @@ class GnnGraph:
     def close(self):
         if self.h:
             lib().hfpx_gnn_graph_destroy(self.h)
+            self.h = _V()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [('n_mesh', ctypes.c_int64), ('residual', ctypes.c_double), ('converged', ctypes.c_int),
+                ('singular_mesh', ctypes.c_int64), ('off_plane_pairs', ctypes.c_int)]
+
+
+BATCH_TILES_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data', 'batch_tiles.json')
+
+
+def batch_tiles():
+    """The autotuner's choice of (block size, leaf rows) for the batched
+    factorisation (hfpx3d_b200/data/batch_tiles.json), or the defaults."""
+    import json
+    try:
+        with open(BATCH_TILES_PATH) as f:
+            best = json.load(f)['best']
+        return int(best['nb']), int(best['leaf_rows'])
+    except (OSError, KeyError, ValueError):
+        return 128, 512
+
+
+class Batch:
+    """Many meshes (DeviceMesh, no fixed DoF) assembled, factored and solved
+    in one CUDA-graph launch (hfpx_batch_*); load cases are in-situ stress
+    tensors (6 x n_cases per mesh)."""
+
+    def __init__(self, ctx, dmeshes, G, nu, nb=None, leaf_rows=None):
+        self.ctx = ctx
+        self.dmeshes = list(dmeshes)  # the batch reads them: keep them alive
+        if nb is None or leaf_rows is None:
+            t_nb, t_leaf = batch_tiles()
+            nb = t_nb if nb is None else nb
+            leaf_rows = t_leaf if leaf_rows is None else leaf_rows
+        self.nb, self.leaf_rows = nb, leaf_rows
+        arr = (_V * len(self.dmeshes))(*[d.h for d in self.dmeshes])
+        self.h = _V()
+        ctx.check(lib().hfpx_batch_create(ctx.h, len(self.dmeshes), arr, G, nu, nb, leaf_rows, ctypes.byref(self.h)))
+        self.n = [18 * d.n_el for d in self.dmeshes]
+        self.n_cases = 0
+
+    def set_loads(self, s_inf):
+        """s_inf: (n_mesh, 6, n_cases) in-situ stress tensors (Voigt)."""
+        s = np.ascontiguousarray(np.asarray(s_inf, dtype=np.float64).transpose(0, 2, 1))  # mesh, case, component
+        self.n_cases = s.shape[1]
+        self.ctx.check(lib().hfpx_batch_set_loads(self.ctx.h, self.h, _dp(s), self.n_cases))
+
+    def run(self, tol=1e-10, max_iter=10):
+        info = BatchInfo()
+        rc = lib().hfpx_batch_run(self.ctx.h, self.h, tol, max_iter, ctypes.byref(info))
+        if rc not in (HFPX_OK, HFPX_ERR_NOT_CONVERGED):
+            self.ctx.check(rc)
+        return info
+
+    def solution(self, m):
+        cols = self.n_cases if self.n_cases else 6
+        x = np.empty((self.n[m], cols), order='F')
+        self.ctx.check(lib().hfpx_batch_solution(self.ctx.h, self.h, m, _dp(x)))
+        return x
+
+    def residuals(self):
+        r = np.empty(len(self.n))
+        self.ctx.check(lib().hfpx_batch_residuals(self.ctx.h, self.h, _dp(r)))
+        return r
+
+    @property
+    def launches(self):
+        return int(lib().hfpx_batch_launches(self.h))
+
+    def close(self):
+        if self.h:
+            lib().hfpx_batch_destroy(self.h)
             self.h = _V()
 
     def __del__(self):

@@ -154,3 +154,35 @@ def observation_points(n: int, seed: int, box: float = 1.5, nods=None, conn=None
             continue
         pts.append(p)
     return np.asfortranarray(np.array(pts).T)
+
+
+def in_situ_stress(rng, lo: float = -1.0, hi: float = 0.0):
+    """A random in-situ stress tensor (Voigt xx, yy, zz, xy, xz, yz): principal
+    values uniform in [lo, hi], Haar-random principal axes."""
+    q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+    q = q * np.sign(np.diag(r))
+    s = q @ np.diag(rng.uniform(lo, hi, 3)) @ q.T
+    return np.array([s[0, 0], s[1, 1], s[2, 2], s[0, 1], s[0, 2], s[1, 2]])
+
+
+def batch_workload(n_mesh: int = 256, n_cases: int = 64, seed: int = 2027, el_min: int = 24, el_max: int = 550):
+    """The batched workload: n_mesh seeded penny or 2:1 elliptical cracks of
+    uneven sizes (elements uniform in [el_min, el_max]), each with n_cases
+    load cases: uniform pressures in [0.5, 2] (sigma_zz, even cases) and random
+    in-situ stress tensors (odd cases).  Returns ([(nods, conn)], S) with S
+    of shape (n_mesh, 6, n_cases)."""
+    rng = np.random.default_rng(seed)
+    meshes = []
+    S = np.zeros((n_mesh, 6, n_cases))
+    for m in range(n_mesh):
+        ne = int(rng.integers(el_min, el_max + 1))
+        if rng.random() < 0.5:
+            meshes.append(penny(ne, seed=seed + 1 + m))
+        else:
+            meshes.append(ellipse(ne, seed=seed + 1 + m))
+        for j in range(n_cases):
+            if j % 2 == 0:
+                S[m, 2, j] = rng.uniform(0.5, 2.0)
+            else:
+                S[m, :, j] = in_situ_stress(rng)
+    return meshes, S

@@ -362,6 +362,49 @@ int hfpx_stress_batch(hfpx_ctx *ctx, const hfpx_mesh *mesh, double shear_m, doub
                       int is_dd_local, const double *dd, int64_t n_cases, const double *pts,
                       int64_t n_pts, const double *s_inf, double *out);
 
+/* ---- the batched workload: many meshes of uneven sizes (no fixed DoF,
+ * 18 DoF per element in the default numbering), each with many load cases,
+ * assembled, factored and solved in one CUDA-graph launch.  Per mesh this is
+ * the reference's make_3dbem_matrix_s (system_assembly.cpp:30-219),
+ * add_s_inf_to_3dbem_rhs (:222-274) and il::LU factor + solve
+ * (il/linear_algebra/dense/factorization/LU.h:79-120) once per load case.
+ * The right-hand side is linear in the in-situ stress, so the 6 unit stress
+ * states are solved to the tolerance and each load case is their
+ * combination.  The operator of each mesh is held in mixed precision (FP32
+ * entries, near-field blocks to about 2^-48, as hfpx_assemble_mixed); the
+ * factorisation is FP32 with tournament-pivoted panels; the solutions are
+ * refined in FP64 against the operator.  The meshes (hfpx_mesh_create) must
+ * outlive the batch; at most 611 elements per mesh.  nb: block size (a
+ * multiple of 32, <= 0: 128), leaf_rows: rows per panel chunk (256 or 512,
+ * <= 0: 512); both are tile choices of the autotuner. */
+typedef struct hfpx_batch hfpx_batch;
+typedef struct {
+  int64_t n_mesh;
+  double residual;          /* max over meshes and unit states of |b - A x|_inf / |b|_inf */
+  int converged;
+  int64_t singular_mesh;    /* first mesh with a zero pivot, -1 none */
+  int off_plane_pairs;      /* pairs evaluated by the off-plane path */
+} hfpx_batch_info;
+int hfpx_batch_create(hfpx_ctx *ctx, int64_t n_mesh, const hfpx_mesh *const *meshes, double shear_m,
+                      double poiss_r, int nb, int leaf_rows, hfpx_batch **batch);
+/* Load cases: s_inf is 6 x n_cases per mesh (Voigt, tension positive),
+ * mesh after mesh; each case's solution is the combination of the unit
+ * states' solutions. */
+int hfpx_batch_set_loads(hfpx_ctx *ctx, hfpx_batch *batch, const double *s_inf, int64_t n_cases);
+/* One run: assembly, right-hand sides, factorisation, solves and FP64
+ * refinement to |b - A x|_inf / |b|_inf <= tol (<= 0: 1e-10) in at most
+ * max_iter steps (<= 0: 10), and the load cases' solutions, as one CUDA
+ * graph (captured by the first run, replayed after). */
+int hfpx_batch_run(hfpx_ctx *ctx, hfpx_batch *batch, double tol, int max_iter, hfpx_batch_info *info);
+/* Mesh `mesh`'s solutions: n x n_cases (or n x 6 unit states without load
+ * cases), column-major. */
+int hfpx_batch_solution(hfpx_ctx *ctx, const hfpx_batch *batch, int64_t mesh, double *x);
+/* Each mesh's final relative residual (n_mesh). */
+int hfpx_batch_residuals(hfpx_ctx *ctx, const hfpx_batch *batch, double *res);
+/* Launches of the factorisation's schedule (plus the fixed ones). */
+int64_t hfpx_batch_launches(const hfpx_batch *batch);
+int hfpx_batch_destroy(hfpx_batch *batch);
+
 /* ---- one element at one point: make_local_3dbem_submatrix,
  * src/Elasticity/elasticity_kernel_integration.cpp:34-205 (kernel 1).
  * tau: 3 complex (re,im), sfm: 6x6 complex row-major (re,im); out 6x18
