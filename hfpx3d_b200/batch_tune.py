@@ -44,15 +44,20 @@ def main():
     ap.add_argument('--n-cases', type=int, default=64)
     ap.add_argument('--reps', type=int, default=2)
     ap.add_argument('--out', default=engine.BATCH_TILES_PATH)
+    ap.add_argument('--candidates', default='', help='comma-separated NBxLEAF (default: all)')
     args = ap.parse_args()
+    cands = CANDIDATES
+    if args.candidates:
+        cands = [tuple(int(v) for v in c.split('x')) for c in args.candidates.split(',')]
     ctx = engine.Context(0)
     meshes, S = meshgen.batch_workload(args.n_mesh, args.n_cases)
     dms = [engine.DeviceMesh(ctx, engine.MeshGeom(n, c), BETA) for n, c in meshes]
-    res = time_candidates(ctx, dms, S, reps=args.reps)
+    res = time_candidates(ctx, dms, S, candidates=cands, reps=args.reps)
     ok = {k: v for k, v in res.items() if v['converged']}
     best = min(ok.values(), key=lambda v: v['seconds'])
     table = {'workload': f'{args.n_mesh} seeded penny/2:1 ellipse meshes, 24-550 elements, {args.n_cases} load cases '
                          'each (meshgen.batch_workload)',
+             'trailing_update': 'tcgen05 FP16 grouped' if os.environ.get('HFPX_BATCH_TC') == '1' else 'SIMT FP32',
              'candidates': res, 'best': {'nb': best['nb'], 'leaf_rows': best['leaf_rows']}}
     with open(args.out, 'w') as f:
         json.dump(table, f, indent=1)

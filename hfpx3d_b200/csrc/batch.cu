@@ -530,11 +530,41 @@ __global__ void __launch_bounds__(256) perm_kernel(BMesh* __restrict__ meshes, i
 }
 
 // W = P r in FP32 (r = B, the current residual), then W = U^-1 L^-1 W, and
-// X += W in FP64.  One CTA of 1024 threads per mesh; the triangles are taken
+// X += W in FP64.  One CTA of 512 threads per mesh; the triangles are taken
 // in 32-row blocks: the block's 32 x 32 triangle by one warp per right-hand
 // side (shuffles), then the rows beyond it by all threads.
-constexpr int kSt = 1024;
-__global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, int first) {
+constexpr int kSt = 512;
+
+// rows [r0, r1) of W (n x 6) -= T[rows, c0 .. c0 + bw) Y (Y = yb, bw x 6),
+// T the factor; all 32 loads of a row issued together when bw is 32
+__device__ __forceinline__ void rows_update(const float* __restrict__ F, int64_t ld, float* __restrict__ W, int n,
+                                            int r0, int r1, int c0, int bw, const float (*yb)[kBasis]) {
+  for (int i = r0 + threadIdx.x; i < r1; i += kSt) {
+    float acc[kBasis];
+#pragma unroll
+    for (int c = 0; c < kBasis; ++c) acc[c] = W[i + (int64_t)n * c];
+    const float* row = F + i + ld * (int64_t)c0;
+    if (bw == kPw) {
+      float l[kPw];
+#pragma unroll
+      for (int k = 0; k < kPw; ++k) l[k] = row[ld * k];
+#pragma unroll
+      for (int k = 0; k < kPw; ++k)
+#pragma unroll
+        for (int c = 0; c < kBasis; ++c) acc[c] = fmaf(-l[k], yb[k][c], acc[c]);
+    } else {
+      for (int k = 0; k < bw; ++k) {
+        const float l = row[ld * k];
+#pragma unroll
+        for (int c = 0; c < kBasis; ++c) acc[c] = fmaf(-l, yb[k][c], acc[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kBasis; ++c) W[i + (int64_t)n * c] = acc[c];
+  }
+}
+
+__global__ void __launch_bounds__(kSt, 1) solve_kernel(BMesh* __restrict__ meshes, int first) {
   BMesh& M = meshes[blockIdx.x];
   if (!first && M.done) return;
   const int n = (int)M.n;
@@ -543,6 +573,7 @@ __global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, 
   float* W = M.W;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ float yb[kPw][kBasis];
+  __shared__ float Db[kPw][kPw + 1];  // the current 32 x 32 diagonal block
   for (int t = tid; t < n * kBasis; t += kSt) {
     const int i = t % n, c = t / n;
     W[i + (int64_t)n * c] = (float)M.B[M.perm[i] + (int64_t)n * c];
@@ -551,11 +582,16 @@ __global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, 
   // forward: unit lower L
   for (int b0 = 0; b0 < n; b0 += kPw) {
     const int bw = min(kPw, n - b0);
+    for (int t = tid; t < kPw * kPw; t += kSt) {
+      const int r = t % kPw, k = t / kPw;
+      if (r < bw && k < bw) Db[r][k] = F[(b0 + r) + ld * (b0 + k)];
+    }
+    __syncthreads();
     if (warp < kBasis) {
       float y = lane < bw ? W[b0 + lane + (int64_t)n * warp] : 0.f;
       for (int k = 0; k < bw; ++k) {
         const float yk = __shfl_sync(0xffffffffu, y, k);
-        if (lane > k && lane < bw) y = fmaf(-F[(b0 + lane) + ld * (b0 + k)], yk, y);
+        if (lane > k && lane < bw) y = fmaf(-Db[lane][k], yk, y);
       }
       if (lane < bw) {
         W[b0 + lane + (int64_t)n * warp] = y;
@@ -563,18 +599,7 @@ __global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, 
       }
     }
     __syncthreads();
-    for (int i = b0 + bw + tid; i < n; i += kSt) {
-      float acc[kBasis];
-#pragma unroll
-      for (int c = 0; c < kBasis; ++c) acc[c] = W[i + (int64_t)n * c];
-      for (int k = 0; k < bw; ++k) {
-        const float l = F[i + ld * (b0 + k)];
-#pragma unroll
-        for (int c = 0; c < kBasis; ++c) acc[c] = fmaf(-l, yb[k][c], acc[c]);
-      }
-#pragma unroll
-      for (int c = 0; c < kBasis; ++c) W[i + (int64_t)n * c] = acc[c];
-    }
+    rows_update(F, ld, W, n, b0 + bw, n, b0, bw, yb);
     __syncthreads();
   }
   // backward: upper U, blocks from the bottom; rows above the block take
@@ -582,13 +607,20 @@ __global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, 
   const int nb_blocks = (n + kPw - 1) / kPw;
   for (int bb = nb_blocks - 1; bb >= 0; --bb) {
     const int b0 = bb * kPw, bw = min(kPw, n - b0);
+    for (int t = tid; t < kPw * kPw; t += kSt) {
+      const int r = t % kPw, k = t / kPw;
+      if (r < bw && k < bw) Db[r][k] = F[(b0 + r) + ld * (b0 + k)];
+    }
+    __syncthreads();
     if (warp < kBasis) {
       float y = lane < bw ? W[b0 + lane + (int64_t)n * warp] : 0.f;
       for (int k = bw - 1; k >= 0; --k) {
-        const float u = lane == k ? F[(b0 + k) + ld * (b0 + k)] : 1.f;
-        if (lane == k) y = u != 0.f ? y / u : 0.f;
+        if (lane == k) {
+          const float u = Db[k][k];
+          y = u != 0.f ? y / u : 0.f;
+        }
         const float yk = __shfl_sync(0xffffffffu, y, k);
-        if (lane < k) y = fmaf(-F[(b0 + lane) + ld * (b0 + k)], yk, y);
+        if (lane < k) y = fmaf(-Db[lane][k], yk, y);
       }
       if (lane < bw) {
         W[b0 + lane + (int64_t)n * warp] = y;
@@ -596,18 +628,7 @@ __global__ void __launch_bounds__(kSt) solve_kernel(BMesh* __restrict__ meshes, 
       }
     }
     __syncthreads();
-    for (int i = tid; i < b0; i += kSt) {
-      float acc[kBasis];
-#pragma unroll
-      for (int c = 0; c < kBasis; ++c) acc[c] = W[i + (int64_t)n * c];
-      for (int k = 0; k < bw; ++k) {
-        const float u = F[i + ld * (b0 + k)];
-#pragma unroll
-        for (int c = 0; c < kBasis; ++c) acc[c] = fmaf(-u, yb[k][c], acc[c]);
-      }
-#pragma unroll
-      for (int c = 0; c < kBasis; ++c) W[i + (int64_t)n * c] = acc[c];
-    }
+    rows_update(F, ld, W, n, 0, b0, b0, bw, yb);
     __syncthreads();
   }
   for (int t = tid; t < n * kBasis; t += kSt) {
@@ -797,8 +818,10 @@ struct hfpx_batch {
   double *d_S = nullptr, *d_Xc = nullptr;
   int64_t* d_xoff = nullptr;
   std::vector<int64_t> xoff;
-  // the captured run
+  // the captured run, with events after the assembly (and right-hand
+  // sides), the factorisation and the solves
   cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double tol = 0.0;
   int max_iter = 0, graph_cases = -1;
 };
@@ -955,6 +978,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
   cudaStream_t s = c->stream;
   BMesh* bm = static_cast<BMesh*>(b->d_bm);
   const unsigned nm = (unsigned)b->n_mesh;
+  cudaEventRecordWithFlags(b->ev[0], s, cudaEventRecordExternal);
   launch_batch_assemble(b->d_am, b->d_tasks, b->n_tasks, b->G, b->nu, b->d_status, s);
   int64_t nbs = 0;
   for (int64_t m = 0; m < b->n_mesh; ++m) nbs += b->n[m] * kBasis;
@@ -962,6 +986,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
   cudaMemcpyAsync(b->d_B, b->d_Bs, sizeof(double) * nbs, cudaMemcpyDeviceToDevice, s);
   ++g_launches;
   bmax_kernel<<<nm, 256, 0, s>>>(bm);
+  cudaEventRecordWithFlags(b->ev[1], s, cudaEventRecordExternal);
   const unsigned char* items = static_cast<const unsigned char*>(b->d_items);
   for (const auto& L : b->sched) {
     const void* it = items + L.off;
@@ -1007,6 +1032,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
         break;
     }
   }
+  cudaEventRecordWithFlags(b->ev[2], s, cudaEventRecordExternal);
   ++g_launches;
   perm_kernel<<<nm, 256, sizeof(int32_t) * b->max_n, s>>>(bm, (int)b->max_n);
   ++g_launches;
@@ -1024,10 +1050,13 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
     ++g_launches;
     combine_kernel<<<dim3(16, nm), 256, 0, s>>>(bm, b->d_S, b->n_cases, b->d_Xc, b->d_xoff);
   }
+  cudaEventRecordWithFlags(b->ev[3], s, cudaEventRecordExternal);
 }
 
 void batch_free(hfpx_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
   void* ps[] = {b->d_am, b->d_bm, b->d_tasks, b->d_A, b->d_F, b->d_lo, b->d_W, b->d_diag, b->d_ints, b->d_dof,
                 b->d_B, b->d_Bs, b->d_X, b->d_res, b->d_boff, b->d_status, b->d_items, b->d_res_items, b->d_S,
                 b->d_Xc, b->d_xoff, b->d_l16, b->d_u16, b->d_rs, b->d_alpha, b->d_amax, b->d_maps, b->d_tcerr,
@@ -1068,11 +1097,11 @@ int hfpx_batch_create(hfpx_ctx* c, int64_t n_mesh, const hfpx_mesh* const* meshe
   b->G = G;
   b->nu = nu;
   b->num_sms = std::max(1, c->num_sms);
-  // trailing updates on the tensor cores (the FP16 grouped kernel) with
-  // HFPX_BATCH_TC=1, when the block is a multiple of its 64-deep k-steps;
-  // otherwise the SIMT FP32 update
+  // trailing updates on the tensor cores (the FP16 grouped kernel) when the
+  // block is a multiple of its 64-deep k-steps; otherwise, or with
+  // HFPX_BATCH_TC=0, the SIMT FP32 update
   const char* etc = std::getenv("HFPX_BATCH_TC");
-  b->use_tc = nb % 64 == 0 && etc && std::string(etc) == "1";
+  b->use_tc = nb % 64 == 0 && !(etc && std::string(etc) == "0");
   int rc = 0;
   for (int64_t m = 0; m < n_mesh && !rc; ++m) {
     const hfpx_mesh* me = meshes[m];
@@ -1231,6 +1260,7 @@ int hfpx_batch_create(hfpx_ctx* c, int64_t n_mesh, const hfpx_mesh* const* meshe
                       "residual items");
   }
   if (!rc) rc = batch_setup(c, b);
+  for (int i = 0; i < 4 && !rc; ++i) rc = check_cuda(c, cudaEventCreate(&b->ev[i]), "batch events");
   if (rc) {
     batch_free(b);
     return rc;
@@ -1349,6 +1379,17 @@ int hfpx_batch_residuals(hfpx_ctx* c, const hfpx_batch* b, double* res) {
 }
 
 int64_t hfpx_batch_launches(const hfpx_batch* b) { return b ? (int64_t)b->sched.size() + 3 : -1; }
+
+int hfpx_batch_phases(hfpx_ctx* c, const hfpx_batch* b, double* ms) {
+  if (!c) return HFPX_ERR_ARG;
+  if (!b || !ms || !b->exec) return set_error(c, HFPX_ERR_STATE, "no run yet");
+  for (int i = 0; i < 3; ++i) {
+    float t = 0.f;
+    if (int rc = check_cuda(c, cudaEventElapsedTime(&t, b->ev[i], b->ev[i + 1]), "batch phases")) return rc;
+    ms[i] = t;
+  }
+  return HFPX_OK;
+}
 
 int hfpx_batch_destroy(hfpx_batch* b) {
   if (b) batch_free(b);

@@ -64,6 +64,7 @@ SIGNATURES = {
     'hfpx_batch_solution': (_int, [_V, _V, _i64, _D]),
     'hfpx_batch_residuals': (_int, [_V, _V, _D]),
     'hfpx_batch_launches': (_i64, [_V]),
+    'hfpx_batch_phases': (_int, [_V, _V, _D]),
     'hfpx_batch_destroy': (_int, [_V]),
     'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
     'hfpx_matrix_dims': (_int, [_V, _L, _L]),
@@ -762,6 +763,12 @@ class Batch:
     @property
     def launches(self):
         return int(lib().hfpx_batch_launches(self.h))
+
+    def phases(self):
+        """Device ms of the last run: assembly (+ right-hand sides), factorisation, solves."""
+        ms = np.empty(3)
+        self.ctx.check(lib().hfpx_batch_phases(self.ctx.h, self.h, _dp(ms)))
+        return {'assembly': ms[0], 'factor': ms[1], 'solve': ms[2]}
 
     def close(self):
         if self.h:

@@ -403,6 +403,9 @@ int hfpx_batch_solution(hfpx_ctx *ctx, const hfpx_batch *batch, int64_t mesh, do
 int hfpx_batch_residuals(hfpx_ctx *ctx, const hfpx_batch *batch, double *res);
 /* Launches of the factorisation's schedule (plus the fixed ones). */
 int64_t hfpx_batch_launches(const hfpx_batch *batch);
+/* Device times (ms) of the last run's phases: assembly with the right-hand
+ * sides, factorisation, solves with refinement and the load cases. */
+int hfpx_batch_phases(hfpx_ctx *ctx, const hfpx_batch *batch, double *ms);
 int hfpx_batch_destroy(hfpx_batch *batch);
 
 /* ---- one element at one point: make_local_3dbem_submatrix,
