@@ -77,18 +77,25 @@ struct LeafItem {
   int32_t mesh, r0, rows, chunk, c0, w;
 };
 
-// Partial pivoting on one chunk of rows (rows x w in shared memory): the w
-// rows it would choose, in order, as proposals for the tournament.
-// Ties go to the lower row index (the first maximum, as LAPACK's idamax).
-__device__ void chunk_gepp(float* a, int lda, int32_t* rid, int rows, int w, float* s_val, int* s_idx) {
+// Partial pivoting on one chunk of rows (rows x w in shared memory, row i
+// of the chunk at a + i lda): the w rows it chooses, in order, go to cho[].
+// Rows are not moved: a chosen row is marked and left out of later steps,
+// so each column takes two CTA barriers (the candidates' maxima, then the
+// elimination).  After the call a chosen row j holds its multipliers in
+// columns < j and its U row from column j on (L11\U11 row j).  Ties go to
+// the lower row id (the first maximum, as LAPACK's idamax).
+__device__ void chunk_gepp(float* a, int lda, const int32_t* rid, int rows, int w, unsigned char* chosen, int* cho) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ int s_pos[kBt / 32 + 1];
+  __shared__ float s_val[kBt / 32];
+  __shared__ int s_id[kBt / 32], s_pos[kBt / 32];
+  for (int i = tid; i < rows; i += kBt) chosen[i] = 0;
+  __syncthreads();
   const int steps = min(rows, w);
   for (int j = 0; j < steps; ++j) {
-    // (|a|, row id, position) maximum over the CTA, ties to the lower row id
     float best = -1.f;
-    int bi = 0x7fffffff, bp = j;
-    for (int i = j + tid; i < rows; i += kBt) {
+    int bi = 0x7fffffff, bp = 0;
+    for (int i = tid; i < rows; i += kBt) {
+      if (chosen[i]) continue;
       const float v = fabsf(a[i * lda + j]);
       const int r = rid[i];
       if (v > best || (v == best && r < bi)) {
@@ -109,42 +116,32 @@ __device__ void chunk_gepp(float* a, int lda, int32_t* rid, int rows, int w, flo
     }
     if (lane == 0) {
       s_val[warp] = best;
-      s_idx[warp] = bi;
+      s_id[warp] = bi;
       s_pos[warp] = bp;
     }
     __syncthreads();
+    // every thread finds the same winner
+    float b = s_val[0];
+    int id = s_id[0], p = s_pos[0];
+    for (int k = 1; k < kBt / 32; ++k)
+      if (s_val[k] > b || (s_val[k] == b && s_id[k] < id)) {
+        b = s_val[k];
+        id = s_id[k];
+        p = s_pos[k];
+      }
     if (tid == 0) {
-      float b = s_val[0];
-      int id = s_idx[0], pos = s_pos[0];
-      for (int k = 1; k < kBt / 32; ++k)
-        if (s_val[k] > b || (s_val[k] == b && s_idx[k] < id)) {
-          b = s_val[k];
-          id = s_idx[k];
-          pos = s_pos[k];
-        }
-      s_pos[kBt / 32] = pos;
+      cho[j] = p;
+      chosen[p] = 1;
     }
-    __syncthreads();
-    const int p = s_pos[kBt / 32];
-    if (p != j) {
-      for (int c = tid; c < w; c += kBt) {
-        const float t = a[j * lda + c];
-        a[j * lda + c] = a[p * lda + c];
-        a[p * lda + c] = t;
-      }
-      if (tid == 0) {
-        const int t = rid[j];
-        rid[j] = rid[p];
-        rid[p] = t;
-      }
-    }
-    __syncthreads();
-    const float piv = a[j * lda + j];
+    const float piv = a[p * lda + j];
     const float inv = piv != 0.f ? 1.f / piv : 0.f;
-    for (int i = j + 1 + tid; i < rows; i += kBt) {
-      const float l = a[i * lda + j] * inv;
-      a[i * lda + j] = l;
-      for (int c = j + 1; c < w; ++c) a[i * lda + c] = fmaf(-l, a[j * lda + c], a[i * lda + c]);
+    const float* pr = a + p * lda;
+    for (int i = tid; i < rows; i += kBt) {
+      if (i == p || chosen[i]) continue;
+      float* ar = a + i * lda;
+      const float l = ar[j] * inv;
+      ar[j] = l;
+      for (int c = j + 1; c < w; ++c) ar[c] = fmaf(-l, pr[c], ar[c]);
     }
     __syncthreads();
   }
@@ -158,17 +155,17 @@ __global__ void __launch_bounds__(kBt) leaf_kernel(BMesh* __restrict__ meshes, c
   float* a = reinterpret_cast<float*>(smem);
   const int lda = kPw + 1;
   int32_t* rid = reinterpret_cast<int32_t*>(a + (size_t)leaf_rows * lda);
-  __shared__ float s_val[kBt / 32];
-  __shared__ int s_idx[kBt / 32 + 1];
+  unsigned char* chosen = reinterpret_cast<unsigned char*>(rid + leaf_rows);
+  __shared__ int cho[kPw];
   for (int t = threadIdx.x; t < it.rows * it.w; t += kBt) {
     const int i = t % it.rows, c = t / it.rows;
     a[i * lda + c] = M.F[(int64_t)(it.r0 + i) + M.ld * (it.c0 + c)];
   }
   for (int i = threadIdx.x; i < it.rows; i += kBt) rid[i] = it.r0 + i;
   __syncthreads();
-  chunk_gepp(a, lda, rid, it.rows, it.w, s_val, s_idx);
+  chunk_gepp(a, lda, rid, it.rows, it.w, chosen, cho);
   for (int j = threadIdx.x; j < kPw; j += kBt)
-    M.cand[it.chunk * kPw + j] = j < min(it.rows, it.w) ? rid[j] : -1;
+    M.cand[it.chunk * kPw + j] = j < min(it.rows, it.w) ? rid[cho[j]] : -1;
 }
 
 // --------------------------------------------------- panel: tournament
@@ -188,8 +185,8 @@ __global__ void __launch_bounds__(kBt) tourn_kernel(BMesh* __restrict__ meshes, 
   const int lda = kPw + 1;
   float* a = reinterpret_cast<float*>(smem);  // cap candidate rows (the launch's largest chunk count x 32)
   int32_t* rid = reinterpret_cast<int32_t*>(a + (size_t)cap * lda);
-  __shared__ float s_val[kBt / 32];
-  __shared__ int s_idx[kBt / 32 + 1];
+  unsigned char* chosen = reinterpret_cast<unsigned char*>(rid + cap);
+  __shared__ int cho[kPw];
   __shared__ int n_rows;
   if (threadIdx.x == 0) {
     int k = 0;
@@ -207,16 +204,16 @@ __global__ void __launch_bounds__(kBt) tourn_kernel(BMesh* __restrict__ meshes, 
     a[i * lda + c] = M.F[(int64_t)rid[i] + M.ld * (it.c0 + c)];
   }
   __syncthreads();
-  chunk_gepp(a, lda, rid, rows, it.w, s_val, s_idx);
-  // L11\U11 (column-major 32 x 32) and the pivot rows
+  chunk_gepp(a, lda, rid, rows, it.w, chosen, cho);
+  // L11\U11 (column-major 32 x 32): row j is the j-th chosen row; the pivot rows
   for (int t = threadIdx.x; t < it.w * it.w; t += kBt) {
     const int i = t % it.w, c = t / it.w;
-    M.diag[i + kPw * c] = a[i * lda + c];
+    M.diag[i + kPw * c] = a[cho[i] * lda + c];
   }
-  for (int j = threadIdx.x; j < it.w; j += kBt) M.prow[j] = rid[j];
+  for (int j = threadIdx.x; j < it.w; j += kBt) M.prow[j] = rid[cho[j]];
   if (threadIdx.x == 0) {
     for (int j = 0; j < it.w; ++j)
-      if (a[j * lda + j] == 0.f && M.info == 0) M.info = it.c0 + j + 1;
+      if (a[cho[j] * lda + j] == 0.f && M.info == 0) M.info = it.c0 + j + 1;
     // interchanges: position c0 + j receives pivot row prow[j]; rows moved
     // earlier are tracked in a small map (position -> original row)
     int pos[2 * kPw], org[2 * kPw], n_map = 0;
@@ -236,7 +233,7 @@ __global__ void __launch_bounds__(kBt) tourn_kernel(BMesh* __restrict__ meshes, 
       ++n_map;
     };
     for (int j = 0; j < it.w; ++j) {
-      const int target = rid[j];
+      const int target = rid[cho[j]];
       int where = target;
       for (int k = 0; k < n_map; ++k)
         if (org[k] == target) {
@@ -888,8 +885,8 @@ void build_schedule(hfpx_batch* b, std::vector<unsigned char>& bytes) {
         // the block's own columns, all rows below the panel
         gemm_tiles(gm, m, c0 + w, n, c0 + w, bend, c0, w);
       }
-      push_items(bytes, b->sched, kLeaf, leaf, (int)(R * ((kPw + 1) * 4 + 4)));
-      push_items(bytes, b->sched, kTourn, tourn, (int)(max_chunks * kPw * ((kPw + 1) * 4 + 4)));
+      push_items(bytes, b->sched, kLeaf, leaf, (int)(R * ((kPw + 1) * 4 + 4 + 1)));
+      push_items(bytes, b->sched, kTourn, tourn, (int)(max_chunks * kPw * ((kPw + 1) * 4 + 4 + 1)));
       push_items(bytes, b->sched, kSwap, swp, 0);
       push_items(bytes, b->sched, kL21, l21, 0);
       push_items(bytes, b->sched, kU12, u12, 0);
@@ -964,8 +961,8 @@ PerDeviceOnce g_attr_leaf, g_attr_tourn, g_attr_perm, g_attr_half;
 
 int batch_setup(hfpx_ctx* c, const hfpx_batch* b) {
   if (batch_assemble_setup(c->stream)) return set_error(c, HFPX_ERR_CUDA, "batched assembly set-up");
-  cudaError_t e = smem_attr_once(g_attr_leaf, leaf_kernel, 512 * ((kPw + 1) * 4 + 4));
-  if (e == cudaSuccess) e = smem_attr_once(g_attr_tourn, tourn_kernel, kMaxChunks * kPw * ((kPw + 1) * 4 + 4));
+  cudaError_t e = smem_attr_once(g_attr_leaf, leaf_kernel, 512 * ((kPw + 1) * 4 + 4 + 1));
+  if (e == cudaSuccess) e = smem_attr_once(g_attr_tourn, tourn_kernel, kMaxChunks * kPw * ((kPw + 1) * 4 + 4 + 1));
   if (e == cudaSuccess) e = smem_attr_once(g_attr_perm, perm_kernel, 48 * 1024);
   if (e == cudaSuccess) e = smem_attr_once(g_attr_half, l21_half_kernel, (int)(sizeof(float) * kHr * (1024 + 1)));
   int rc = check_cuda(c, e, "batched kernel attributes");
@@ -997,7 +994,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
         leaf_kernel<<<grid, kBt, L.aux, s>>>(bm, static_cast<const LeafItem*>(it), b->leaf_rows);
         break;
       case kTourn:
-        tourn_kernel<<<grid, kBt, L.aux, s>>>(bm, static_cast<const PanelItem*>(it), L.aux / ((kPw + 1) * 4 + 4));
+        tourn_kernel<<<grid, kBt, L.aux, s>>>(bm, static_cast<const PanelItem*>(it), L.aux / ((kPw + 1) * 4 + 4 + 1));
         break;
       case kSwap:
         swap_rows_kernel<<<grid, 256, 0, s>>>(bm, static_cast<const ColItem*>(it));
