@@ -588,6 +588,7 @@ def run_c5(args, ctx, engine, torch, stream, reps=3):
            'batch_s': best, 'phases_ms': phases, 'meshes_per_s': len(meshes) / best,
            'load_case_solves_per_s': len(meshes) * S.shape[2] / best,
            'lu_tflops': flops / best / 1e12, 'residual': info.residual, 'converged': bool(info.converged),
+           'refinement_steps': info.iterations,
            'first_run_s (capture + instantiate + run)': setup_s, '_n_el': n_el}
     B.close()
     # the same meshes one by one through the per-mesh C-ABI

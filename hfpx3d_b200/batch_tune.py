@@ -57,7 +57,7 @@ def main():
     best = min(ok.values(), key=lambda v: v['seconds'])
     table = {'workload': f'{args.n_mesh} seeded penny/2:1 ellipse meshes, 24-550 elements, {args.n_cases} load cases '
                          'each (meshgen.batch_workload)',
-             'trailing_update': 'tcgen05 FP16 grouped' if os.environ.get('HFPX_BATCH_TC') == '1' else 'SIMT FP32',
+             'trailing_update': 'SIMT FP32' if os.environ.get('HFPX_BATCH_TC') == '0' else 'tcgen05 FP16 grouped (nb a multiple of 64)',
              'candidates': res, 'best': {'nb': best['nb'], 'leaf_rows': best['leaf_rows']}}
     with open(args.out, 'w') as f:
         json.dump(table, f, indent=1)

@@ -68,6 +68,7 @@ struct BMesh {
   int64_t n, ld, n_el;
   int info;          // first zero pivot (1-based column), 0 none
   int done;          // refinement converged
+  int iters;         // refinement corrections applied
   double bmax[kBasis];
 };
 
@@ -351,31 +352,32 @@ __global__ void __launch_bounds__(256) u12_kernel(BMesh* __restrict__ meshes, co
 }
 
 // --------------------------------------------------------- tiled GEMM
-// C -= L U on 128 x 128 tiles of one mesh's factor: C = F[r0.., q0..],
+// C -= L U on 64 x 64 tiles of one mesh's factor: C = F[r0.., q0..],
 // L = F[r0.., k0 .. k0 + K), U = F[k0 .., q0..]; rows < r_end, columns <
-// q_end.  256 threads, 8 x 8 outputs each, K in steps of 16 staged in
-// shared memory.
+// q_end.  256 threads, 4 x 4 outputs each, K in steps of 32 staged in
+// shared memory; each thread's 16 entries of C are loaded together before
+// they are written back.  Small tiles keep many CTAs per SM in flight: the
+// rank-32 updates of the panels are bound by the latency of their loads.
 struct GemmItem {
   int32_t mesh, r0, q0, r_end, q_end, k0, K;
 };
-constexpr int kGm = 128, kGk = 16;
+constexpr int kGm = 64, kGk = 32;
 
 __global__ void __launch_bounds__(256) bgemm_kernel(BMesh* __restrict__ meshes, const GemmItem* __restrict__ items) {
   const GemmItem it = items[blockIdx.x];
   const BMesh& M = meshes[it.mesh];
-  __shared__ float Ls[kGk][kGm + 4];
-  __shared__ float Us[kGk][kGm + 4];
+  __shared__ float Ls[kGk][kGm + 1];
+  __shared__ float Us[kGk][kGm + 1];
   const int tid = threadIdx.x;
-  const int tr = tid % 16, tc = tid / 16;  // thread's rows tr + 16 i, columns tc + 16 j
-  float acc[8][8];
+  const int tr = tid % 16, tc = tid / 16;  // rows tr + 16 i, columns tc + 16 j
+  float acc[4][4];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
   const int64_t ld = M.ld;
-  const float* F = M.F;
+  float* F = M.F;
   for (int kk = 0; kk < it.K; kk += kGk) {
-    // L tile: 128 rows x 16 k (coalesced along rows); U tile: 16 k x 128 columns
     for (int t = tid; t < kGm * kGk; t += 256) {
       const int r = t % kGm, k = t / kGm;
       const int64_t gr = it.r0 + r;
@@ -389,29 +391,37 @@ __global__ void __launch_bounds__(256) bgemm_kernel(BMesh* __restrict__ meshes, 
       Us[k][q] = (gq < it.q_end && gk < it.K) ? F[(it.k0 + gk) + ld * gq] : 0.f;
     }
     __syncthreads();
-#pragma unroll
+#pragma unroll 8
     for (int k = 0; k < kGk; ++k) {
-      float lv[8], uv[8];
+      float lv[4], uv[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) lv[i] = Ls[k][tr + 16 * i];
+      for (int i = 0; i < 4; ++i) lv[i] = Ls[k][tr + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) uv[j] = Us[k][tc + 16 * j];
+      for (int j = 0; j < 4; ++j) uv[j] = Us[k][tc + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
     }
     __syncthreads();
   }
-  float* C = M.F;
+  float c[4][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < 4; ++j) {
     const int64_t gq = it.q0 + tc + 16 * j;
-    if (gq >= it.q_end) continue;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < 4; ++i) {
       const int64_t gr = it.r0 + tr + 16 * i;
-      if (gr < it.r_end) C[gr + ld * gq] -= acc[i][j];
+      c[i][j] = (gq < it.q_end && gr < it.r_end) ? F[gr + ld * gq] : 0.f;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t gq = it.q0 + tc + 16 * j;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int64_t gr = it.r0 + tr + 16 * i;
+      if (gq < it.q_end && gr < it.r_end) F[gr + ld * gq] = c[i][j] - acc[i][j];
     }
   }
 }
@@ -527,10 +537,14 @@ __global__ void __launch_bounds__(256) perm_kernel(BMesh* __restrict__ meshes, i
 }
 
 // W = P r in FP32 (r = B, the current residual), then W = U^-1 L^-1 W, and
-// X += W in FP64.  One CTA of 512 threads per mesh; the triangles are taken
-// in 32-row blocks: the block's 32 x 32 triangle by one warp per right-hand
-// side (shuffles), then the rows beyond it by all threads.
-constexpr int kSt = 512;
+// X += W in FP64.  One thread-block cluster of kSc CTAs per mesh (meshes
+// largest first, so the longest solves start first).  The triangles are
+// taken in 32-row blocks: every CTA of the cluster solves the block's 32 x 32
+// triangle itself (a warp per right-hand side, shuffles, the block staged in
+// shared memory), then updates its slice of the rows beyond the block; a
+// cluster barrier (release / acquire at cluster scope) separates the blocks,
+// so the cluster's SMs share the factor's bandwidth.
+constexpr int kSt = 256, kSc = 4;
 
 // rows [r0, r1) of W (n x 6) -= T[rows, c0 .. c0 + bw) Y (Y = yb, bw x 6),
 // T the factor; all 32 loads of a row issued together when bw is 32
@@ -561,9 +575,29 @@ __device__ __forceinline__ void rows_update(const float* __restrict__ F, int64_t
   }
 }
 
-__global__ void __launch_bounds__(kSt, 1) solve_kernel(BMesh* __restrict__ meshes, int first) {
-  BMesh& M = meshes[blockIdx.x];
-  if (!first && M.done) return;
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank_u() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// this CTA's slice of rows [r0, r1) (contiguous, in 32-row units)
+__device__ __forceinline__ void cta_slice(int r0, int r1, unsigned rank, int& s0, int& s1) {
+  const int span = r1 - r0;
+  const int per = ((span + kSc - 1) / kSc + 31) / 32 * 32;
+  s0 = min(r1, r0 + (int)rank * per);
+  s1 = min(r1, s0 + per);
+}
+
+__global__ void __cluster_dims__(kSc, 1, 1) __launch_bounds__(kSt, 2)
+    solve_kernel(BMesh* __restrict__ meshes, const int32_t* __restrict__ order, int first) {
+  BMesh& M = meshes[order[blockIdx.x / kSc]];
+  if (!first && M.done) return;  // the whole cluster returns together
+  const unsigned rank = cluster_rank_u();
+  if (!first && threadIdx.x == 0 && rank == 0) ++M.iters;
   const int n = (int)M.n;
   const int64_t ld = M.ld;
   const float* F = M.F;
@@ -571,11 +605,15 @@ __global__ void __launch_bounds__(kSt, 1) solve_kernel(BMesh* __restrict__ meshe
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ float yb[kPw][kBasis];
   __shared__ float Db[kPw][kPw + 1];  // the current 32 x 32 diagonal block
-  for (int t = tid; t < n * kBasis; t += kSt) {
-    const int i = t % n, c = t / n;
-    W[i + (int64_t)n * c] = (float)M.B[M.perm[i] + (int64_t)n * c];
+  {
+    int s0, s1;
+    cta_slice(0, n, rank, s0, s1);
+    for (int t = tid; t < (s1 - s0) * kBasis; t += kSt) {
+      const int i = s0 + t % (s1 - s0), c = t / (s1 - s0);
+      W[i + (int64_t)n * c] = (float)M.B[M.perm[i] + (int64_t)n * c];
+    }
   }
-  __syncthreads();
+  cluster_barrier();
   // forward: unit lower L
   for (int b0 = 0; b0 < n; b0 += kPw) {
     const int bw = min(kPw, n - b0);
@@ -590,15 +628,16 @@ __global__ void __launch_bounds__(kSt, 1) solve_kernel(BMesh* __restrict__ meshe
         const float yk = __shfl_sync(0xffffffffu, y, k);
         if (lane > k && lane < bw) y = fmaf(-Db[lane][k], yk, y);
       }
-      if (lane < bw) {
-        W[b0 + lane + (int64_t)n * warp] = y;
-        yb[lane][warp] = y;
-      }
+      if (lane < bw) yb[lane][warp] = y;
     }
     __syncthreads();
-    rows_update(F, ld, W, n, b0 + bw, n, b0, bw, yb);
-    __syncthreads();
+    int s0, s1;
+    cta_slice(b0 + bw, n, rank, s0, s1);
+    rows_update(F, ld, W, n, s0, s1, b0, bw, yb);
+    cluster_barrier();  // every CTA has read W[b0 .. b0 + bw) and updated its rows
+    if (rank == 0 && warp < kBasis && lane < bw) W[b0 + lane + (int64_t)n * warp] = yb[lane][warp];
   }
+  cluster_barrier();
   // backward: upper U, blocks from the bottom; rows above the block take
   // the block's contribution
   const int nb_blocks = (n + kPw - 1) / kPw;
@@ -619,19 +658,24 @@ __global__ void __launch_bounds__(kSt, 1) solve_kernel(BMesh* __restrict__ meshe
         const float yk = __shfl_sync(0xffffffffu, y, k);
         if (lane < k) y = fmaf(-Db[lane][k], yk, y);
       }
-      if (lane < bw) {
-        W[b0 + lane + (int64_t)n * warp] = y;
-        yb[lane][warp] = y;
-      }
+      if (lane < bw) yb[lane][warp] = y;
     }
     __syncthreads();
-    rows_update(F, ld, W, n, 0, b0, b0, bw, yb);
-    __syncthreads();
+    int s0, s1;
+    cta_slice(0, b0, rank, s0, s1);
+    rows_update(F, ld, W, n, s0, s1, b0, bw, yb);
+    cluster_barrier();
+    if (rank == 0 && warp < kBasis && lane < bw) W[b0 + lane + (int64_t)n * warp] = yb[lane][warp];
   }
-  for (int t = tid; t < n * kBasis; t += kSt) {
-    const int64_t i = t % n, c = t / n;
-    const double v = (double)W[i + n * c];
-    M.X[i + n * c] = first ? v : M.X[i + n * c] + v;
+  cluster_barrier();
+  {
+    int s0, s1;
+    cta_slice(0, n, rank, s0, s1);
+    for (int t = tid; t < (s1 - s0) * kBasis; t += kSt) {
+      const int64_t i = s0 + t % (s1 - s0), c = t / (s1 - s0);
+      const double v = (double)W[i + n * c];
+      M.X[i + n * c] = first ? v : M.X[i + n * c] + v;
+    }
   }
 }
 
@@ -744,6 +788,7 @@ __global__ void __launch_bounds__(256) bmax_kernel(BMesh* __restrict__ meshes) {
     }
     M.done = 0;
     M.info = 0;
+    M.iters = 0;
   }
 }
 
@@ -810,6 +855,7 @@ struct hfpx_batch {
   void* d_items = nullptr;
   std::vector<hfpx::ResItem> res_items;
   hfpx::ResItem* d_res_items = nullptr;
+  int32_t* d_order = nullptr;  // meshes by size, largest first
   // load cases
   int n_cases = 0;
   double *d_S = nullptr, *d_Xc = nullptr;
@@ -1033,7 +1079,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
   ++g_launches;
   perm_kernel<<<nm, 256, sizeof(int32_t) * b->max_n, s>>>(bm, (int)b->max_n);
   ++g_launches;
-  solve_kernel<<<nm, kSt, 0, s>>>(bm, 1);
+  solve_kernel<<<nm * kSc, kSt, 0, s>>>(bm, b->d_order, 1);
   const unsigned nr = (unsigned)b->res_items.size();
   for (int it = 0; it <= b->max_iter; ++it) {
     g_launches += 2;
@@ -1041,7 +1087,7 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
     converge_kernel<<<nm, 256, 0, s>>>(bm, b->tol, b->d_res);
     if (it == b->max_iter) break;
     ++g_launches;
-    solve_kernel<<<nm, kSt, 0, s>>>(bm, 0);
+    solve_kernel<<<nm * kSc, kSt, 0, s>>>(bm, b->d_order, 0);
   }
   if (b->n_cases > 0) {
     ++g_launches;
@@ -1057,7 +1103,7 @@ void batch_free(hfpx_batch* b) {
   void* ps[] = {b->d_am, b->d_bm, b->d_tasks, b->d_A, b->d_F, b->d_lo, b->d_W, b->d_diag, b->d_ints, b->d_dof,
                 b->d_B, b->d_Bs, b->d_X, b->d_res, b->d_boff, b->d_status, b->d_items, b->d_res_items, b->d_S,
                 b->d_Xc, b->d_xoff, b->d_l16, b->d_u16, b->d_rs, b->d_alpha, b->d_amax, b->d_maps, b->d_tcerr,
-                b->d_hoff, b->d_rsoff};
+                b->d_hoff, b->d_rsoff, b->d_order};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete b;
@@ -1248,8 +1294,15 @@ int hfpx_batch_create(hfpx_ctx* c, int64_t n_mesh, const hfpx_mesh* const* meshe
     rc = check_cuda(c, cudaMalloc(&b->d_items, std::max<size_t>(16, bytes.size())), "schedule");
     if (!rc && !bytes.empty())
       rc = check_cuda(c, cudaMemcpy(b->d_items, bytes.data(), bytes.size(), cudaMemcpyHostToDevice), "schedule");
-    for (int64_t m = 0; m < n_mesh; ++m)
-      for (int64_t r0 = 0; r0 < b->n[m]; r0 += kRt) b->res_items.push_back({(int32_t)m, (int32_t)r0});
+    std::vector<int32_t> order(n_mesh);
+    for (int64_t m = 0; m < n_mesh; ++m) order[m] = (int32_t)m;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return b->n[x] > b->n[y]; });
+    for (int32_t m : order)
+      for (int64_t r0 = 0; r0 < b->n[m]; r0 += kRt) b->res_items.push_back({m, (int32_t)r0});
+    if (!rc) rc = dalloc(c, &b->d_order, n_mesh, "mesh order");
+    if (!rc)
+      rc = check_cuda(c, cudaMemcpy(b->d_order, order.data(), sizeof(int32_t) * n_mesh, cudaMemcpyHostToDevice),
+                      "mesh order");
     if (!rc) rc = dalloc(c, &b->d_res_items, b->res_items.size(), "residual items");
     if (!rc)
       rc = check_cuda(c, cudaMemcpy(b->d_res_items, b->res_items.data(), sizeof(ResItem) * b->res_items.size(),
@@ -1339,8 +1392,10 @@ int hfpx_batch_run(hfpx_ctx* c, hfpx_batch* b, double tol, int max_iter, hfpx_ba
   }
   double worst = 0.0;
   int64_t singular = -1;
+  int iters = 0;
   for (int64_t m = 0; m < b->n_mesh; ++m) {
     worst = std::max(worst, res[m]);
+    iters = std::max(iters, bm[m].iters);
     if (bm[m].info && singular < 0) singular = m;
   }
   if (info) {
@@ -1349,6 +1404,7 @@ int hfpx_batch_run(hfpx_ctx* c, hfpx_batch* b, double tol, int max_iter, hfpx_ba
     info->converged = worst <= tol;
     info->singular_mesh = singular;
     info->off_plane_pairs = status[1];
+    info->iterations = iters;
   }
   if (singular >= 0) return set_error(c, HFPX_ERR_SINGULAR, "a mesh's matrix is singular");
   if (!(worst <= tol)) return set_error(c, HFPX_ERR_NOT_CONVERGED, "refinement did not reach the tolerance");

@@ -699,7 +699,7 @@ class GnnGraph:
 
 class BatchInfo(ctypes.Structure):
     _fields_ = [('n_mesh', ctypes.c_int64), ('residual', ctypes.c_double), ('converged', ctypes.c_int),
-                ('singular_mesh', ctypes.c_int64), ('off_plane_pairs', ctypes.c_int)]
+                ('singular_mesh', ctypes.c_int64), ('off_plane_pairs', ctypes.c_int), ('iterations', ctypes.c_int)]
 
 
 BATCH_TILES_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data', 'batch_tiles.json')

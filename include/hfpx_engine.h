@@ -384,6 +384,7 @@ typedef struct {
   int converged;
   int64_t singular_mesh;    /* first mesh with a zero pivot, -1 none */
   int off_plane_pairs;      /* pairs evaluated by the off-plane path */
+  int iterations;           /* most refinement corrections any mesh took */
 } hfpx_batch_info;
 int hfpx_batch_create(hfpx_ctx *ctx, int64_t n_mesh, const hfpx_mesh *const *meshes, double shear_m,
                       double poiss_r, int nb, int leaf_rows, hfpx_batch **batch);
