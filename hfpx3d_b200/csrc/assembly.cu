@@ -24,10 +24,21 @@ namespace hfpx {
 __constant__ GL12 c_gl;
 static PerDeviceOnce g_gl_ready;
 
-static void gl_host_init(cudaStream_t s) {
-  if (!g_gl_ready.pending()) return;
-  GL12 g;
-  const int n = 12;
+// Far-field quadrature over a source triangle (the mixed-precision
+// operator's far pairs): the collapsed (Duffy) product of 4-point
+// Gauss-Legendre rules, 16 points, barycentric (l1, l2) and, per node a
+// (vertices, then the edge node opposite vertex v), the weight times the
+// quadratic shape function: wn[a][q] = w_q N_a(l_q).  Weights sum to 1 over
+// the triangle (times its area).
+constexpr int kFarQ = 16;
+struct FarRule {
+  float l1[kFarQ], l2[kFarQ];
+  float wn[6][kFarQ];
+};
+__constant__ FarRule c_far;
+
+// Gauss-Legendre nodes and weights on [-1, 1] (Newton on P_n)
+static void gauss_legendre(int n, double* x_out, double* w_out) {
   for (int i = 0; i < n; ++i) {
     double x = std::cos(kPi * (i + 0.75) / (n + 0.5)), dp = 1.0;
     for (int it = 0; it < 100; ++it) {
@@ -42,9 +53,33 @@ static void gl_host_init(cudaStream_t s) {
       x -= dx;
       if (std::fabs(dx) < 1e-16) break;
     }
-    g.x[i] = x;
-    g.w[i] = 2.0 / ((1.0 - x * x) * dp * dp);
+    x_out[i] = x;
+    w_out[i] = 2.0 / ((1.0 - x * x) * dp * dp);
   }
+}
+
+static void gl_host_init(cudaStream_t s) {
+  if (!g_gl_ready.pending()) return;
+  GL12 g;
+  gauss_legendre(12, g.x, g.w);
+  // the triangle rule: (u, v) on [0,1]^2 -> l1 = u, l2 = v (1 - u), weight
+  // 2 (1 - u) w_u w_v (the reference triangle has area 1/2)
+  FarRule fr;
+  double x4[4], w4[4];
+  gauss_legendre(4, x4, w4);
+  for (int iu = 0; iu < 4; ++iu)
+    for (int iv = 0; iv < 4; ++iv) {
+      const int q = 4 * iu + iv;
+      const double u = 0.5 * (x4[iu] + 1.0), v = 0.5 * (x4[iv] + 1.0);
+      const double w = 2.0 * (1.0 - u) * (0.5 * w4[iu]) * (0.5 * w4[iv]);
+      const double l1 = u, l2 = v * (1.0 - u), l0 = 1.0 - l1 - l2;
+      const double lam[3] = {l0, l1, l2};
+      fr.l1[q] = (float)l1;
+      fr.l2[q] = (float)l2;
+      for (int a = 0; a < 3; ++a) fr.wn[a][q] = (float)(w * lam[a] * (2.0 * lam[a] - 1.0));
+      for (int a = 0; a < 3; ++a) fr.wn[3 + a][q] = (float)(w * 4.0 * lam[(a + 1) % 3] * lam[(a + 2) % 3]);
+    }
+  if (cudaMemcpyToSymbolAsync(c_far, &fr, sizeof(fr), 0, cudaMemcpyHostToDevice, s) != cudaSuccess) return;
   if (cudaMemcpyToSymbolAsync(c_gl, &g, sizeof(g), 0, cudaMemcpyHostToDevice, s) == cudaSuccess) g_gl_ready.mark();
 }
 
@@ -251,6 +286,77 @@ __device__ __forceinline__ void inplane_nodes(const ElemRec& S, cplx z, const cp
   }
 }
 
+// The far field in FP32: the in-plane (h = 0) stress of each node's shape
+// function at z by the 16-point triangle rule, for a target at least
+// kFarRatio element sizes from the source (there the rule's error is below
+// 1e-7 of the block and the FP32 sums keep the block to about 2e-7).  The
+// point kernel of a DD on the plane x3 = 0, at r = (r1, r2, 0) from the
+// source point, is K = P(r1, r2) / R^7 with P of degree 4 (Kelvin's solution
+// differentiated through Volterra's formula); only eight (stress, DD
+// component) pairs are non-zero in the plane.  sink(a, S[6][3]) as for
+// inplane_nodes.
+constexpr double kFarRatio = 8.0;
+
+__device__ __forceinline__ bool far_pair(const ElemRec& S, const double* pt) {
+  // the source centroid is the mean of its three vertex collocation points
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const double c = (S.cp[k] + S.cp[3 + k] + S.cp[6 + k]) * (1.0 / 3.0);
+    d2 += (pt[k] - c) * (pt[k] - c);
+  }
+  // largest edge (tau of vertex j at tau[2 j], tau[2 j + 1]; vertex 0 is the origin)
+  const double e1 = S.tau[2] * S.tau[2] + S.tau[3] * S.tau[3];
+  const double e2 = S.tau[4] * S.tau[4] + S.tau[5] * S.tau[5];
+  const double dx = S.tau[4] - S.tau[2], dy = S.tau[5] - S.tau[3];
+  const double e3 = dx * dx + dy * dy;
+  const double L2 = fmax(e1, fmax(e2, e3));
+  return d2 >= kFarRatio * kFarRatio * L2;
+}
+
+template <class F>
+__device__ __forceinline__ void quad_nodes(const ElemRec& S, cplx z, double nu, double G, F&& sink) {
+  const float zr = (float)z.re, zi = (float)z.im;
+  const float t1r = (float)S.tau[2], t1i = (float)S.tau[3], t2r = (float)S.tau[4], t2i = (float)S.tau[5];
+  const float fn = (float)nu;
+  const float a11 = 2.f - 2.f * fn, b11 = 2.f * fn + 1.f, c11 = 4.f * fn - 1.f;   // S11 (normal DD)
+  const float c12 = 3.f - 6.f * fn;                                               // S12 (normal DD)
+  const float a13 = 1.f + fn, b13 = 2.f - fn, c13 = 1.f - 2.f * fn;               // S13 (DD 0), S23 (DD 1) mirrored
+  const float d13 = 3.f * fn;                                                     // S13 (DD 1), S23 (DD 0)
+  const double scale = G / (4.0 * kPi * (1.0 - nu)) * S.area;
+  for (int a = 0; a < 6; ++a) {
+    float s11 = 0.f, s22 = 0.f, s33 = 0.f, s12 = 0.f, s13_0 = 0.f, s13_1 = 0.f, s23_0 = 0.f, s23_1 = 0.f;
+#pragma unroll 4
+    for (int q = 0; q < kFarQ; ++q) {
+      const float l1 = c_far.l1[q], l2 = c_far.l2[q];
+      const float r1 = zr - (l1 * t1r + l2 * t2r), r2 = zi - (l1 * t1i + l2 * t2i);
+      const float u = r1 * r1, v = r2 * r2, w = r1 * r2, R2 = u + v;
+      const float ri = rsqrtf(R2), ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2, ri7 = ri5 * ri2;
+      const float c = c_far.wn[a][q];
+      const float cu = c * ri7;
+      s11 = fmaf(cu, fmaf(a11, u * u, fmaf(b11, u * v, c11 * v * v)), s11);
+      s22 = fmaf(cu, fmaf(c11, u * u, fmaf(b11, u * v, a11 * v * v)), s22);
+      s33 = fmaf(c, ri3, s33);
+      const float cw = c * w * ri5;
+      s12 = fmaf(c12, cw, s12);
+      s13_0 = fmaf(cu, fmaf(a13, u * u, fmaf(b13, u * v, c13 * v * v)), s13_0);
+      s13_1 = fmaf(d13, cw, s13_1);
+      s23_0 = fmaf(d13, cw, s23_0);
+      s23_1 = fmaf(cu, fmaf(c13, u * u, fmaf(b13, u * v, a13 * v * v)), s23_1);
+    }
+    double Sx[6][3];
+    for (int k = 0; k < 6; ++k) Sx[k][0] = Sx[k][1] = Sx[k][2] = 0.0;
+    Sx[0][2] = scale * s11;
+    Sx[1][2] = scale * s22;
+    Sx[2][2] = scale * s33;
+    Sx[3][2] = scale * s12;
+    Sx[4][0] = scale * s13_0;
+    Sx[4][1] = scale * s13_1;
+    Sx[5][0] = scale * s23_0;
+    Sx[5][1] = scale * s23_1;
+    sink(a, Sx);
+  }
+}
+
 // Off-plane monomial tensor (6x4x3) from the quadrature moments.
 __device__ __noinline__ void offplane_smon(const ElemRec& S, cplx z, double h, double nu,
                                            cplx* smon) {
@@ -370,7 +476,7 @@ __device__ __forceinline__ void assemble_body(AsmSmem& sm, const ElemRec* __rest
                                               int* __restrict__ status, float* __restrict__ lo,
                                               const int32_t* __restrict__ np_ptr,
                                               const int32_t* __restrict__ np_idx, int64_t s, int64_t bx,
-                                              const int32_t* __restrict__ tlist, int64_t n_t) {
+                                              const int32_t* __restrict__ tlist, int64_t n_t, bool far32) {
   const int tid = threadIdx.x;
   if (!stage_bulk(&sm.src, elems + s, sizeof(ElemRec), &sm.bar, status)) return;
   if (tid < 18) sm.cols[tid] = dof[s + n_el * tid];
@@ -418,11 +524,14 @@ __device__ __forceinline__ void assemble_body(AsmSmem& sm, const ElemRec* __rest
     // (the sm.nb list was staged before the barrier above)
     const int64_t blk = (lo && mine) ? near_block(sm, t, s) : -1;
     float* lob = blk >= 0 ? lo + blk * 324 + 3 * nt : nullptr;
-    // every lane runs the in-plane form (the warp stays converged for the
-    // per-warp transpose); rows of lanes that are not in-plane pairs are -1
-    cplx P[6], Q[6];
-    inplane_moments(S, z, P, Q);
-    inplane_nodes(S, z, P, Q, nu, scale, [&](int a, const double Sx[6][3]) {
+    // every lane runs the same form (the warp stays converged for the
+    // per-warp transpose); rows of lanes that are not in-plane pairs are -1.
+    // With far32 a warp whose pairs are all far from the source (and none
+    // in its near-field pattern) takes the FP32 quadrature instead of the
+    // closed form.
+    const bool lane_far = !mine || (far32 && blk < 0 && far_pair(S, pt));
+    const bool warp_far = far32 && __all_sync(0xffffffffu, lane_far) && __any_sync(0xffffffffu, mine);
+    auto sink = [&](int a, const double Sx[6][3]) {
       double B[3][3];
       traction_3x3(S.r, nl, Sx, is_dd_local, B);
 #pragma unroll
@@ -457,7 +566,14 @@ __device__ __forceinline__ void assemble_body(AsmSmem& sm, const ElemRec* __rest
         }
         __syncwarp();
       }
-    });
+    };
+    if (warp_far) {
+      quad_nodes(S, z, nu, G, sink);
+    } else {
+      cplx P[6], Q[6];
+      inplane_moments(S, z, P, Q);
+      inplane_nodes(S, z, P, Q, nu, scale, sink);
+    }
   } else {
     __syncthreads();
     if (!(valid && !inplane)) return;
@@ -498,7 +614,8 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
                                                          const int32_t* __restrict__ np_ptr,
                                                          const int32_t* __restrict__ np_idx,
                                                          const int32_t* __restrict__ slist,
-                                                         const int32_t* __restrict__ tlist, int64_t n_t) {
+                                                         const int32_t* __restrict__ tlist, int64_t n_t,
+                                                         int far32) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
   if (GENERAL && status[1] == 0) return;  // first pass met no off-plane pair
@@ -506,7 +623,7 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
   // range: all of them, or the lists of a partial (incremental) assembly
   const int64_t s = slist ? slist[blockIdx.y] : blockIdx.y;
   assemble_body<GENERAL>(sm, elems, n_el, dof, G, nu, is_dd_local, A, ld, Af, nullptr, status, lo, np_ptr, np_idx, s,
-                         blockIdx.x, tlist, n_t);
+                         blockIdx.x, tlist, n_t, far32 != 0);
 }
 
 // Many meshes in one launch: CTA i takes task i = (mesh, source element,
@@ -514,13 +631,13 @@ __global__ void __launch_bounds__(kTile, GENERAL ? 1 : 4) assemble_kernel(const 
 // entries and near-field low parts) and its FP32 copy for the factorisation.
 __global__ void __launch_bounds__(kTile, 4) batch_assemble_kernel(const BatchAsmMesh* __restrict__ meshes,
                                                                   const int4* __restrict__ tasks, double G,
-                                                                  double nu, int* __restrict__ status) {
+                                                                  double nu, int* __restrict__ status, int far32) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AsmSmem& sm = *reinterpret_cast<AsmSmem*>(smem_raw);
   const int4 tk = tasks[blockIdx.x];
   const BatchAsmMesh M = meshes[tk.x];
   assemble_body<false>(sm, static_cast<const ElemRec*>(M.elems), M.n_el, M.dof, G, nu, 0, nullptr, M.ld, M.A, M.F, status, M.lo, M.np_ptr,
-                       M.np_idx, tk.y, tk.z, nullptr, M.n_el);
+                       M.np_idx, tk.y, tk.z, nullptr, M.n_el, far32 != 0);
 }
 __global__ void __launch_bounds__(kTile, 1) batch_assemble_general_kernel(const BatchAsmMesh* __restrict__ meshes,
                                                                           const int4* __restrict__ tasks, double G,
@@ -531,7 +648,7 @@ __global__ void __launch_bounds__(kTile, 1) batch_assemble_general_kernel(const 
   const int4 tk = tasks[blockIdx.x];
   const BatchAsmMesh M = meshes[tk.x];
   assemble_body<true>(sm, static_cast<const ElemRec*>(M.elems), M.n_el, M.dof, G, nu, 0, nullptr, M.ld, M.A, M.F, status, M.lo, M.np_ptr,
-                      M.np_idx, tk.y, tk.z, nullptr, M.n_el);
+                      M.np_idx, tk.y, tk.z, nullptr, M.n_el, false);
 }
 
 // set-up of the batched assembly kernels on the current device (before a
@@ -546,12 +663,12 @@ int batch_assemble_setup(cudaStream_t s) {
 }
 
 void launch_batch_assemble(const BatchAsmMesh* d_meshes, const void* d_tasks, int64_t n_tasks, double G, double nu,
-                           int* d_status, cudaStream_t s) {
+                           int* d_status, cudaStream_t s, int far32) {
   const size_t smem = sizeof(AsmSmem);
   cudaMemsetAsync(d_status, 0, 2 * sizeof(int), s);
   const int4* t = static_cast<const int4*>(d_tasks);
   ++g_launches;
-  batch_assemble_kernel<<<(unsigned)n_tasks, kTile, smem, s>>>(d_meshes, t, G, nu, d_status);
+  batch_assemble_kernel<<<(unsigned)n_tasks, kTile, smem, s>>>(d_meshes, t, G, nu, d_status, far32);
   ++g_launches;
   batch_assemble_general_kernel<<<(unsigned)n_tasks, kTile, smem, s>>>(d_meshes, t, G, nu, d_status);
 }
@@ -571,7 +688,7 @@ void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int6
 static void launch_assemble_pairs(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
                                   int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s,
                                   float* d_lo, const int32_t* np_ptr, const int32_t* np_idx, const int32_t* slist,
-                                  int64_t n_s, const int32_t* tlist, int64_t n_t) {
+                                  int64_t n_s, const int32_t* tlist, int64_t n_t, int far32) {
   gl_host_init(s);
   const size_t smem = sizeof(AsmSmem);
   static PerDeviceOnce attr0, attr1;
@@ -583,17 +700,17 @@ static void launch_assemble_pairs(const void* d_elem, int64_t n_el, const int32_
   const ElemRec* e = static_cast<const ElemRec*>(d_elem);
   ++g_launches;
   assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, d_lo,
-                                                   np_ptr, np_idx, slist, tlist, n_t);
+                                                   np_ptr, np_idx, slist, tlist, n_t, far32);
   ++g_launches;
   assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, d_lo,
-                                                  np_ptr, np_idx, slist, tlist, n_t);
+                                                  np_ptr, np_idx, slist, tlist, n_t, 0);
 }
 
 void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
                      int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_status, cudaStream_t s,
-                     float* d_lo, const int32_t* np_ptr, const int32_t* np_idx) {
+                     float* d_lo, const int32_t* np_ptr, const int32_t* np_idx, int far32) {
   launch_assemble_pairs(d_elem, n_el, d_dof, G, nu, is_dd_local, d_a, ld, d_f, d_status, s, d_lo, np_ptr, np_idx,
-                        nullptr, n_el, nullptr, n_el);
+                        nullptr, n_el, nullptr, n_el, far32);
 }
 
 // The pairs of an incremental assembly: every target of the sources in
@@ -620,7 +737,7 @@ void launch_assemble_partial(const void* d_elem, int64_t n_el, const int32_t* d_
     const dim3 grid((unsigned)((6 * nt + kTile - 1) / kTile), (unsigned)ns);
     ++g_launches;
     assemble_kernel<false><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, nullptr, d_status,
-                                                     nullptr, nullptr, nullptr, sl, tl, nt);
+                                                     nullptr, nullptr, nullptr, sl, tl, nt, 0);
   }
   for (int pass = 0; pass < 2; ++pass) {
     const int32_t* sl = pass == 0 ? slist : slist2;
@@ -631,7 +748,7 @@ void launch_assemble_partial(const void* d_elem, int64_t n_el, const int32_t* d_
     const dim3 grid((unsigned)((6 * nt + kTile - 1) / kTile), (unsigned)ns);
     ++g_launches;
     assemble_kernel<true><<<grid, kTile, smem, s>>>(e, n_el, d_dof, G, nu, is_dd_local, d_a, ld, nullptr, d_status,
-                                                    nullptr, nullptr, nullptr, sl, tl, nt);
+                                                    nullptr, nullptr, nullptr, sl, tl, nt, 0);
   }
 }
 

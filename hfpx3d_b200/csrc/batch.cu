@@ -1022,7 +1022,11 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
   BMesh* bm = static_cast<BMesh*>(b->d_bm);
   const unsigned nm = (unsigned)b->n_mesh;
   cudaEventRecordWithFlags(b->ev[0], s, cudaEventRecordExternal);
-  launch_batch_assemble(b->d_am, b->d_tasks, b->n_tasks, b->G, b->nu, b->d_status, s);
+  // far pairs in FP32 by quadrature only with HFPX_FAR32=1 (as for
+  // hfpx_assemble_mixed: the default keeps the reference's closed form)
+  const char* ef = std::getenv("HFPX_FAR32");
+  launch_batch_assemble(b->d_am, b->d_tasks, b->n_tasks, b->G, b->nu, b->d_status, s,
+                        (ef && std::string(ef) == "1") ? 1 : 0);
   int64_t nbs = 0;
   for (int64_t m = 0; m < b->n_mesh; ++m) nbs += b->n[m] * kBasis;
   launch_batch_basis_rhs(b->d_am, b->n_mesh, b->d_Bs, b->d_boff, s);

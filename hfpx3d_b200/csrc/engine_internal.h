@@ -221,12 +221,14 @@ void launch_element_precompute(const double* d_nods, int64_t ld_nods, const int6
 // d_f (optional): an FP32 copy of the matrix written in the same pass.
 // d_a null: the mixed-precision operator, d_f every entry in FP32 and d_lo
 // (on the near-field pattern np_ptr/np_idx, at most kMaxNearDeg neighbours
-// per element) the low parts of the near-field blocks.
+// per element) the low parts of the near-field blocks.  far32: in-plane
+// pairs at least 8 source-element sizes apart, outside the near-field
+// pattern, are integrated in FP32 by a 16-point rule (mixed operator only).
 constexpr int kMaxNearDeg = 64;
 void launch_assemble(const void* d_elem, int64_t n_el, const int32_t* d_dof, double G, double nu,
                      int is_dd_local, double* d_a, int64_t ld, float* d_f, int* d_general_count,
                      cudaStream_t s, float* d_lo = nullptr, const int32_t* np_ptr = nullptr,
-                     const int32_t* np_idx = nullptr);
+                     const int32_t* np_idx = nullptr, int far32 = 0);
 // One mesh of a batched assembly: its element records, DoF map, the FP32
 // operator A (hi parts) with its near-field low parts lo on the pattern
 // np_ptr/np_idx, and the FP32 copy F the factorisation overwrites (ld rows).
@@ -245,7 +247,7 @@ struct BatchAsmMesh {
 // collocation points, 0), one CTA each
 int batch_assemble_setup(cudaStream_t s);
 void launch_batch_assemble(const BatchAsmMesh* d_meshes, const void* d_tasks, int64_t n_tasks, double G, double nu,
-                           int* d_status, cudaStream_t s);
+                           int* d_status, cudaStream_t s, int far32);
 // the 6 unit in-situ stress states' right-hand sides of every mesh (no
 // fixed DoF), mesh m's n x 6 block at d_B + d_boff[m]
 void launch_batch_basis_rhs(const BatchAsmMesh* d_meshes, int64_t n_mesh, double* d_B, const int64_t* d_boff,

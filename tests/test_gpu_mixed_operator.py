@@ -3,10 +3,15 @@ make_3dbem_matrix_s (src/Solvers/system_assembly.cpp:30-219) held as FP32
 entries, with the near-field blocks (each element with itself and with the
 elements sharing a vertex) kept to ~2^-48 by FP32 low parts.
 
-* entries against the FP64 assembly of the same kernel: far entries are
-  exactly the FP32 rounding of the FP64 entries, near entries within 1e-14
-  relative, on a planar penny (in-plane path) and a wavy crack (off-plane
-  path);
+* entries against the FP64 assembly of the same kernel: near-field entries
+  within 1e-14 relative, every other entry exactly the FP32 rounding of the
+  FP64 entry, on a planar penny (in-plane path) and a wavy crack (off-plane
+  path); with HFPX_FAR32=1 the in-plane pairs at least 8 source-element
+  sizes apart are integrated in FP32 by a 16-point rule: against an
+  accurate FP64 quadrature of the same integrals they are never further off
+  than the FP64 closed form by more than 2e-6 of the block scale (the closed
+  form itself cancels between the ends of an edge whose line passes near
+  the point);
 * its product r = b - A x against numpy with the composed matrix (1e-13);
 * GMRES on it (near-field and learned two-level preconditioners) against the
   FP64 LU solution of the FP64 matrix: the opening within 1e-8 of the
@@ -35,6 +40,111 @@ def near_mask(conn):
     return np.kron(m, np.ones((18, 18), dtype=bool))
 
 
+def far_mask(nods, conn, beta=0.125, margin=0.02):
+    """(far, ambiguous) masks over the 18 n_el x 18 n_el entries: the
+    collocation point of the row at least 8 (1 + margin) sizes (largest edge)
+    from the source element's centroid, and within the margin of 8."""
+    ne = conn.shape[1]
+    V = np.asarray(nods)[:3, np.asarray(conn)[:3]]          # 3 x 3 x ne (coord, vertex, element)
+    cen = V.mean(axis=1)                                   # 3 x ne
+    L = np.max([np.linalg.norm(V[:, (k + 1) % 3] - V[:, k], axis=0) for k in range(3)], axis=0)
+    cps = []
+    for k in range(3):                                     # vertex points, then edge points opposite vertex k
+        cps.append((1 - beta) * V[:, k] + beta * cen)
+    for k in range(3):
+        cps.append((1 - beta) * 0.5 * (V[:, (k + 1) % 3] + V[:, (k + 2) % 3]) + beta * cen)
+    far = np.zeros((18 * ne, 18 * ne), dtype=bool)
+    amb = np.zeros_like(far)
+    for nt in range(6):
+        d = np.linalg.norm(cps[nt][:, :, None] - cen[:, None, :], axis=0) / L[None, :]   # target x source
+        rows = np.arange(ne) * 18 + 3 * nt
+        for i in range(3):
+            far[rows + i] |= np.kron(d >= 8 * (1 + margin), np.ones((1, 18), dtype=bool))
+            amb[rows + i] |= np.kron(np.abs(d - 8) < 8 * margin, np.ones((1, 18), dtype=bool))
+    return far, amb
+
+
+def _local_block_quad(V, pt, nu=NU, G=G, n=10):
+    """6 x 18 local stress block of an in-plane target far from the flat
+    triangle V (3 x 3): FP64 collapsed Gauss rule (n x n) of the point kernel
+    of a DD on the plane, K = P(r1, r2) / R^7 (stress rows S11, S22, S33,
+    S12, S13, S23; columns 3 node + DD component)."""
+    e1 = V[:, 1] - V[:, 0]
+    e1 = e1 / np.linalg.norm(e1)
+    e3 = np.cross(V[:, 1] - V[:, 0], V[:, 2] - V[:, 0])
+    area = 0.5 * np.linalg.norm(e3)
+    e3 = e3 / np.linalg.norm(e3)
+    e2 = np.cross(e3, e1)
+    R = np.array([e1, e2, e3])
+    loc = lambda x: R @ (x - V[:, 0])
+    t = [loc(V[:, k])[:2] for k in range(3)]
+    p = loc(pt)[:2]
+    x, w = np.polynomial.legendre.leggauss(n)
+    x = 0.5 * (x + 1)
+    w = 0.5 * w
+    B = np.zeros((6, 18))
+    for u, wu in zip(x, w):
+        for v, wv in zip(x, w):
+            l1, l2 = u, v * (1 - u)
+            lam = [1 - l1 - l2, l1, l2]
+            wt = 2 * (1 - u) * wu * wv * area
+            xi = lam[0] * t[0] + lam[1] * t[1] + lam[2] * t[2]
+            r1, r2 = p - xi
+            a, b, c = r1 * r1, r2 * r2, r1 * r2
+            R2 = a + b
+            i7, i5, i3 = R2 ** -3.5, R2 ** -2.5, R2 ** -1.5
+            K = np.zeros((6, 3))
+            K[0, 2] = ((2 - 2 * nu) * a * a + (2 * nu + 1) * a * b + (4 * nu - 1) * b * b) * i7
+            K[1, 2] = ((4 * nu - 1) * a * a + (2 * nu + 1) * a * b + (2 - 2 * nu) * b * b) * i7
+            K[2, 2] = i3
+            K[3, 2] = (3 - 6 * nu) * c * i5
+            K[4, 0] = ((1 + nu) * a * a + (2 - nu) * a * b + (1 - 2 * nu) * b * b) * i7
+            K[4, 1] = 3 * nu * c * i5
+            K[5, 0] = 3 * nu * c * i5
+            K[5, 1] = ((1 - 2 * nu) * a * a + (2 - nu) * a * b + (1 + nu) * b * b) * i7
+            N = [lam[k] * (2 * lam[k] - 1) for k in range(3)] + [4 * lam[(k + 1) % 3] * lam[(k + 2) % 3]
+                                                                 for k in range(3)]
+            for nd in range(6):
+                B[:, 3 * nd:3 * nd + 3] += wt * N[nd] * K
+    return B * G / (4 * np.pi * (1 - nu)), R
+
+
+def far_field_truth_errors(nods, conn, M, A64, far, scale, beta=BETA, samples=400, seed=5):
+    """Largest |M - T| and |A64 - T| over a seeded sample of far (target
+    point, source element) pairs, relative to the block scale, T the global
+    traction entries of the accurate quadrature (traction = n . sigma with
+    the target normal in the source frame, back to global, DD global)."""
+    rng = np.random.default_rng(seed)
+    rows, cols = np.nonzero(far[::3, ::18])
+    pick = rng.choice(len(rows), size=min(samples, len(rows)), replace=False)
+    e_q = e_c = excess = 0.0
+    for k in pick:
+        row0, s_ = 3 * rows[k], cols[k]
+        t_, nt = divmod(row0 // 3, 6)
+        Vs, Vt = nods[:3, conn[:3, s_]], nods[:3, conn[:3, t_]]
+        cen = Vt.mean(axis=1)
+        pt = ((1 - beta) * Vt[:, nt] + beta * cen if nt < 3 else
+              (1 - beta) * 0.5 * (Vt[:, (nt + 1) % 3] + Vt[:, (nt + 2) % 3]) + beta * cen)
+        B, R = _local_block_quad(Vs, pt)
+        nt_ = np.cross(Vt[:, 1] - Vt[:, 0], Vt[:, 2] - Vt[:, 0])
+        nrm = -nt_ / np.linalg.norm(nt_)
+        nl = R @ nrm
+        T = np.zeros((3, 18))
+        for nd in range(6):
+            S = B[:, 3 * nd:3 * nd + 3]
+            tl = np.array([nl[0] * S[0] + nl[1] * S[3] + nl[2] * S[4],
+                           nl[1] * S[1] + nl[0] * S[3] + nl[2] * S[5],
+                           nl[2] * S[2] + nl[0] * S[4] + nl[1] * S[5]])
+            T[:, 3 * nd:3 * nd + 3] = R.T @ tl @ R
+        r = slice(row0, row0 + 3)
+        c = slice(18 * s_, 18 * s_ + 18)
+        sc = scale[row0, 18 * s_]
+        q = np.abs(M[r, c] - T).max() / sc
+        cf = np.abs(A64[r, c] - T).max() / sc
+        e_q, e_c, excess = max(e_q, q), max(e_c, cf), max(excess, q - cf)
+    return e_q, e_c, excess
+
+
 def build(ctx, kind, args, kwargs):
     from hfpx3d_b200 import engine, meshgen
     nods, conn = getattr(meshgen, kind)(*args, **kwargs)
@@ -44,20 +154,43 @@ def build(ctx, kind, args, kwargs):
     return nods, conn, dm, dof, n
 
 
-@pytest.mark.parametrize('kind,args,kwargs', [('penny', (200,), dict(seed=11)),
-                                              ('wavy', (120,), dict(aspect=1.5, amp=0.15, seed=12))])
-def test_entries_are_the_fp64_entries_rounded(ctx, kind, args, kwargs):
+@pytest.mark.parametrize('kind,args,kwargs,far32', [('penny', (200,), dict(seed=11), False),
+                                                    ('wavy', (120,), dict(aspect=1.5, amp=0.15, seed=12), False),
+                                                    ('penny', (200,), dict(seed=11), True)])
+def test_entries_are_the_fp64_entries_rounded(ctx, kind, args, kwargs, far32, monkeypatch):
     from hfpx3d_b200 import engine
     nods, conn, dm, dof, n = build(ctx, kind, args, kwargs)
     A64 = engine.assemble(ctx, dm, dof, n, G, NU).download()
+    if far32:
+        monkeypatch.setenv('HFPX_FAR32', '1')
     Am = engine.assemble_mixed(ctx, dm, dof, n, G, NU)
     assert Am.mixed
     M = Am.download()
     near = near_mask(conn)
-    far = ~near
-    assert np.array_equal(M[far], A64[far].astype(np.float32).astype(np.float64))
+    far, amb = far_mask(nods, conn)
+    far &= ~near
+    loose = (far | (amb & ~near)) if far32 else np.zeros_like(far)
+    rest = ~near & ~loose
+    assert np.array_equal(M[rest], A64[rest].astype(np.float32).astype(np.float64))
     rel = np.abs(M[near] - A64[near]) / np.maximum(np.abs(A64[near]), 1e-300)
     assert rel.max() <= 1e-14, rel.max()
+    # far pairs: against the FP64 closed form within 1e-4 of the block scale
+    # (the closed form itself cancels between the ends of an edge whose line
+    # passes near the point: up to ~7e-5 there), and against an accurate
+    # FP64 quadrature of the same integrals within 2e-6
+    ne = conn.shape[1]
+    blk = np.abs(A64).reshape(ne, 18, ne, 18).max(axis=(1, 3))
+    scale = np.kron(blk, np.ones((18, 18)))
+    err = np.where(loose, np.abs(M - A64) / np.maximum(scale, 1e-300), 0.0)
+    assert err.max() <= 1e-4, err.max()
+    if far32:
+        # a warp whose pairs are not all far keeps the closed form, so every
+        # far entry is checked to be no further from the accurate value than
+        # the closed form's, up to 2e-6 of the block scale
+        e_q, e_c, excess = far_field_truth_errors(nods, conn, M, A64, far, scale)
+        print(f'{kind}: far pairs {far.sum() // 18}: the operator vs an accurate FP64 quadrature {e_q:.2e}, '
+              f'the FP64 closed form vs the same {e_c:.2e}, largest excess {excess:.2e} (of the block scale)')
+        assert excess <= 2e-6, excess
     # the near entries carry more than the FP32 rounding alone would
     assert np.abs(M[near] - A64[near]).max() < 1e-3 * np.abs(A64[near].astype(np.float32) - A64[near]).max()
     # a block of the same, and re-assembly into it
@@ -65,6 +198,7 @@ def test_entries_are_the_fp64_entries_rounded(ctx, kind, args, kwargs):
     assert np.array_equal(blk, M[90:130, 126:156])
     engine.assemble_into(ctx, dm, dof, n, G, NU, Am)
     assert np.array_equal(Am.download(), M)
+    monkeypatch.delenv('HFPX_FAR32', raising=False)
 
 
 def test_product_matches_numpy(ctx):
