@@ -850,6 +850,14 @@ struct hfpx_batch {
   unsigned* d_amax = nullptr;
   void* d_maps = nullptr;
   int* d_tcerr = nullptr;
+  // C's tensor maps of every trailing update (the reduce-add epilogue),
+  // 128 bytes each, 64-byte aligned
+  struct alignas(64) Map128 {
+    unsigned char bytes[128];
+  };
+  std::vector<Map128> cmaps;
+  void* d_cmaps = nullptr;
+  bool tc_reduce = true;
   int64_t *d_hoff = nullptr, *d_rsoff = nullptr;
   std::vector<Launch> sched;
   void* d_items = nullptr;
@@ -981,6 +989,17 @@ void build_schedule(hfpx_batch* b, std::vector<unsigned char>& bytes) {
         P.alpha = b->d_alpha + m;
         P.row_scale = b->d_rs + b->rsoff[mi];
         P.C = b->d_F + b->aoff[mi] + bend * (b->ld[mi] + 1);
+        P.cmap = -1;
+        P.pad = 0;
+        if (b->tc_reduce) {
+          hfpx_batch::Map128 cm;
+          if (tc_make_c_map(&cm, P.C, rest, rest, b->ld[mi])) {
+            P.cmap = (int32_t)b->cmaps.size();
+            b->cmaps.push_back(cm);
+          } else {
+            b->tc_reduce = false;  // fall back to the reading epilogue everywhere
+          }
+        }
         probs.push_back(P);
         tstart.push_back(tstart.back() + ((rest + 127) / 128) * ((rest + 255) / 256));
       }
@@ -1075,7 +1094,8 @@ void batch_launches(hfpx_ctx* c, hfpx_batch* b) {
       default:  // kTcUpdate
         --g_launches;  // counted by the launcher
         tc_update_grouped(s, L.aux, b->d_maps, static_cast<const TcProblem*>(it),
-                          reinterpret_cast<const int64_t*>(items + L.off2), (int)L.count, b->d_tcerr);
+                          reinterpret_cast<const int64_t*>(items + L.off2), (int)L.count, b->d_tcerr,
+                          b->tc_reduce ? b->d_cmaps : nullptr);
         break;
     }
   }
@@ -1107,7 +1127,7 @@ void batch_free(hfpx_batch* b) {
   void* ps[] = {b->d_am, b->d_bm, b->d_tasks, b->d_A, b->d_F, b->d_lo, b->d_W, b->d_diag, b->d_ints, b->d_dof,
                 b->d_B, b->d_Bs, b->d_X, b->d_res, b->d_boff, b->d_status, b->d_items, b->d_res_items, b->d_S,
                 b->d_Xc, b->d_xoff, b->d_l16, b->d_u16, b->d_rs, b->d_alpha, b->d_amax, b->d_maps, b->d_tcerr,
-                b->d_hoff, b->d_rsoff, b->d_order};
+                b->d_hoff, b->d_rsoff, b->d_order, b->d_cmaps};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete b;
@@ -1149,6 +1169,9 @@ int hfpx_batch_create(hfpx_ctx* c, int64_t n_mesh, const hfpx_mesh* const* meshe
   // HFPX_BATCH_TC=0, the SIMT FP32 update
   const char* etc = std::getenv("HFPX_BATCH_TC");
   b->use_tc = nb % 64 == 0 && !(etc && std::string(etc) == "0");
+  // the reduce-add epilogue (HFPX_BATCH_TC_REDUCE=0: the epilogue reads and writes C)
+  const char* etr = std::getenv("HFPX_BATCH_TC_REDUCE");
+  b->tc_reduce = !(etr && std::string(etr) == "0");
   int rc = 0;
   for (int64_t m = 0; m < n_mesh && !rc; ++m) {
     const hfpx_mesh* me = meshes[m];
@@ -1295,7 +1318,15 @@ int hfpx_batch_create(hfpx_ctx* c, int64_t n_mesh, const hfpx_mesh* const* meshe
   if (!rc) {
     std::vector<unsigned char> bytes;
     build_schedule(b, bytes);
-    rc = check_cuda(c, cudaMalloc(&b->d_items, std::max<size_t>(16, bytes.size())), "schedule");
+    if (b->use_tc && b->tc_reduce && !b->cmaps.empty()) {
+      rc = check_cuda(c, cudaMalloc(&b->d_cmaps, 128 * b->cmaps.size()), "C tensor maps");
+      if (!rc)
+        rc = check_cuda(c, cudaMemcpy(b->d_cmaps, b->cmaps.data(), 128 * b->cmaps.size(), cudaMemcpyHostToDevice),
+                        "C tensor maps");
+    } else {
+      b->tc_reduce = false;
+    }
+    if (!rc) rc = check_cuda(c, cudaMalloc(&b->d_items, std::max<size_t>(16, bytes.size())), "schedule");
     if (!rc && !bytes.empty())
       rc = check_cuda(c, cudaMemcpy(b->d_items, bytes.data(), bytes.size(), cudaMemcpyHostToDevice), "schedule");
     std::vector<int32_t> order(n_mesh);

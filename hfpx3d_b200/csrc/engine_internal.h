@@ -308,11 +308,16 @@ struct TcProblem {
   int32_t m, n, k, map;
   const float* alpha;
   const float* row_scale;
+  int32_t cmap, pad;  // C's tensor map (32 x 32 boxes) for the reduce-add epilogue
 };
 bool tc_make_operand_map(void* map, const void* base, int64_t rows, int64_t k, int64_t ld_k, int box_rows);
+// C (m x n FP32, column-major, ldc) for the reduce-add epilogue: 32 x 32 boxes
+bool tc_make_c_map(void* map, const float* C, int64_t m, int64_t n, int64_t ldc);
 int tc_grouped_setup(hfpx_ctx* c);
+// d_cmaps (optional): the problems' C maps; the epilogue then adds into C
+// with TMA reduce-add copies instead of reading and writing C
 void tc_update_grouped(cudaStream_t st, int grid, const void* d_maps, const TcProblem* d_probs,
-                       const int64_t* d_tile_start, int n_probs, int* d_err);
+                       const int64_t* d_tile_start, int n_probs, int* d_err, const void* d_cmaps = nullptr);
 
 // precond.cu: near-field preconditioners on the FP64 matrix (block-Jacobi,
 // first-order Neumann, exact local inverse, learned) and their product

@@ -621,11 +621,33 @@ __device__ __forceinline__ int tile_problem(const int64_t* __restrict__ tile_sta
   return lo;
 }
 
+// REDUCE: the epilogue adds the scaled accumulator into C with TMA
+// reduce-add copies (cp.reduce.async.bulk.tensor, 32 x 32 boxes staged in
+// shared memory per epilogue warp, C's tensor map at cmaps[cmap]): the SMs
+// never read C, L2 applies the additions.
+struct alignas(1024) TcSmemR {
+  TcSmem base;
+  float red[kEpiWarps][32 * 32];
+};
+constexpr size_t kSmemBytesR = sizeof(TcSmemR) + 1024;
+static_assert(kSmemBytesR <= 232448, "shared memory of the reduce-add epilogue");
+
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+template <bool REDUCE>
 __global__ void __launch_bounds__(kThreads, 1)
     update_tc_grouped_kernel(const CUtensorMap* __restrict__ maps, const TcProblem* __restrict__ probs,
-                             const int64_t* __restrict__ tile_start, int n_probs, int* __restrict__ err) {
+                             const int64_t* __restrict__ tile_start, int n_probs, int* __restrict__ err,
+                             const CUtensorMap* __restrict__ cmaps) {
   extern __shared__ uint8_t smem_raw[];
-  TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  TcSmemR& sr = *reinterpret_cast<TcSmemR*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  TcSmem& s = sr.base;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t tiles = tile_start[n_probs];
   volatile int* abort = &s.abort;
@@ -759,27 +781,53 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool row_ok = row < P.m;
       const float ra = row_ok && P.row_scale ? alpha * P.row_scale[row] : alpha;
       const int64_t col0 = nb * kBN + half * 128;
+      if (REDUCE) {
+        // this warp's 32 rows x 32 columns per chunk, column-major in its
+        // staging box, added into C by one TMA reduce-add per chunk
+        float* box = sr.red[warp - 2];
+        const int64_t row0 = mb * kBM + q * 32;
+        const CUtensorMap* cm = cmaps + P.cmap;
 #pragma unroll 1
-      for (int ch = 0; ch < 4; ++ch) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
-        const int64_t cb = col0 + ch * 32;
-        const int ncol = row_ok ? (int)min((int64_t)32, max((int64_t)0, (int64_t)P.n - cb)) : 0;
-        float* pc = P.C + row + P.ldc * cb;
+        for (int ch = 0; ch < 4; ++ch) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
+          const int64_t cb = col0 + ch * 32;
+          // the previous chunk's copy has read the box
+          if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          __syncwarp();
+          const float sc = row_ok ? ra : 0.f;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          float c[16];
+          for (int j = 0; j < 32; ++j) box[32 * j + lane] = sc * v[j];
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0 && row0 < P.m && cb < P.n) tma_reduce_add_2d(cm, box, (int)row0, (int)cb);
+        }
+      } else {
+#pragma unroll 1
+        for (int ch = 0; ch < 4; ++ch) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN + half * 128 + ch * 32), v);
+          const int64_t cb = col0 + ch * 32;
+          const int ncol = row_ok ? (int)min((int64_t)32, max((int64_t)0, (int64_t)P.n - cb)) : 0;
+          float* pc = P.C + row + P.ldc * cb;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(pc + P.ldc * (16 * h + j)) : 0.f;
+          for (int h = 0; h < 2; ++h) {
+            float c[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (16 * h + j < ncol) __stcg(pc + P.ldc * (16 * h + j), fmaf(ra, v[16 * h + j], c[j]));
+            for (int j = 0; j < 16; ++j) c[j] = 16 * h + j < ncol ? __ldcg(pc + P.ldc * (16 * h + j)) : 0.f;
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (16 * h + j < ncol) __stcg(pc + P.ldc * (16 * h + j), fmaf(ra, v[16 * h + j], c[j]));
+          }
         }
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&s.tempty[acc]);
     }
+    // the reduce-add copies complete before the CTA's shared memory goes away
+    if (REDUCE && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
   }
 
   tc_fence_before();
@@ -891,15 +939,37 @@ bool tc_make_operand_map(void* map, const void* base, int64_t rows, int64_t k, i
 }
 
 int tc_grouped_setup(hfpx_ctx* c) {
-  static PerDeviceOnce attr;
-  return check_cuda(c, smem_attr_once(attr, update_tc_grouped_kernel, (int)kSmemBytes), "grouped update attribute");
+  static PerDeviceOnce attr, attr_r;
+  int rc = check_cuda(c, smem_attr_once(attr, update_tc_grouped_kernel<false>, (int)kSmemBytes),
+                      "grouped update attribute");
+  if (!rc)
+    rc = check_cuda(c, smem_attr_once(attr_r, update_tc_grouped_kernel<true>, (int)kSmemBytesR),
+                    "grouped update attribute");
+  return rc;
+}
+
+bool tc_make_c_map(void* map, const float* C, int64_t m, int64_t n, int64_t ldc) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ldc * 4)};
+  const cuuint32_t box[2] = {32, 32};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(static_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(C), dims, strides,
+            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 void tc_update_grouped(cudaStream_t st, int grid, const void* d_maps, const TcProblem* d_probs,
-                       const int64_t* d_tile_start, int n_probs, int* d_err) {
+                       const int64_t* d_tile_start, int n_probs, int* d_err, const void* d_cmaps) {
   ++g_launches;
-  update_tc_grouped_kernel<<<(unsigned)grid, kThreads, kSmemBytes, st>>>(
-      static_cast<const CUtensorMap*>(d_maps), d_probs, d_tile_start, n_probs, d_err);
+  if (d_cmaps)
+    update_tc_grouped_kernel<true><<<(unsigned)grid, kThreads, kSmemBytesR, st>>>(
+        static_cast<const CUtensorMap*>(d_maps), d_probs, d_tile_start, n_probs, d_err,
+        static_cast<const CUtensorMap*>(d_cmaps));
+  else
+    update_tc_grouped_kernel<false><<<(unsigned)grid, kThreads, kSmemBytes, st>>>(
+        static_cast<const CUtensorMap*>(d_maps), d_probs, d_tile_start, n_probs, d_err, nullptr);
 }
 
 }  // namespace hfpx

@@ -11,9 +11,11 @@
 * the 4000-triangle penny of the headline step (72 000 DoF,
   make_3dbem_matrix_s, :30-219): 198 rows and 198 columns of the device FP64
   matrix against the reference's, the full blocks of each sampled element
-  with its nearest neighbours, entry samples; the mixed solution's opening
-  against the FP64 GPU solution (<= 1e-8), and both against Sneddon's closed
-  form for r < 0.9 (test_radial_crack_static.cpp:316-337).
+  with its nearest neighbours, entry samples; the openings of the mixed LU's
+  solution and of the timed form's (learned two-level GMRES on the
+  mixed-precision operator) against the FP64 GPU solution (<= 1e-8), and all
+  against Sneddon's closed form for r < 0.9
+  (test_radial_crack_static.cpp:316-337).
 
 Tolerances.  In far pairs whose collocation point lies near the line of one
 of the source element's edges the in-plane closed form cancels, and the
@@ -125,18 +127,31 @@ def test_c3_matrix_rows_and_columns(c3):
     assert errs['near_blocks'] <= 1e-11
 
 
-def test_c3_mixed_vs_fp64_and_sneddon(c3, ora):
+def test_c3_mixed_and_learned_vs_fp64_and_sneddon(c3, ora):
     from hfpx3d_b200 import engine
     A, n, dof, dm, nods, conn = c3['A'], c3['n'], c3['dof'], c3['dm'], c3['nods'], c3['conn']
     ne = conn.shape[1]
-    rhs = engine.add_s_inf_to_3dbem_rhs(ctx_of(A), dm, dof, n, [0, 0, 1.0, 0, 0, 0])
-    x_mixed = engine.LU(ctx_of(A), A, engine.HFPX_LU_MIXED).gmres(rhs, tol=1e-12)
-    x_fp64 = engine.LU(ctx_of(A), A, engine.HFPX_LU_FP64).solve(rhs)       # factors A in place: last
+    ctx = ctx_of(A)
+    rhs = engine.add_s_inf_to_3dbem_rhs(ctx, dm, dof, n, [0, 0, 1.0, 0, 0, 0])
+    # the timed form: the learned two-level preconditioner and GMRES on the
+    # mixed-precision operator (FP32 entries, near-field blocks to 2^-48)
+    Am = engine.assemble_mixed(ctx, dm, dof, n, G, NU)
+    net = engine.Gnn(ctx, path=engine.WEIGHTS_PATH)
+    P = engine.Precond(ctx, dm, Am, engine.HFPX_PC_LEARNED | engine.HFPX_PC_COARSE, net=net, shear_m=G)
+    x_learned, info = engine.gmres(ctx, Am, rhs, P, tol=1e-10, restart=50, max_iter=500)
+    assert info.converged, info.residual
+    P.close()
+    net.close()
+    Am.close()
+    x_mixed = engine.LU(ctx, A, engine.HFPX_LU_MIXED).gmres(rhs, tol=1e-12)
+    x_fp64 = engine.LU(ctx, A, engine.HFPX_LU_FP64).solve(rhs)       # factors A in place: last
     dd_m = engine.write_dd_vector_to_md(x_mixed, dof, ne)
     dd_f = engine.write_dd_vector_to_md(x_fp64, dof, ne)
+    dd_l = engine.write_dd_vector_to_md(x_learned, dof, ne)
     open_err = rel(dd_m[:, 2], dd_f[:, 2], np.abs(dd_f[:, 2]).max())
+    open_err_l = rel(dd_l[:, 2], dd_f[:, 2], np.abs(dd_f[:, 2]).max())
     # Sneddon's opening at every node with r < 0.9 (pressure 1, unit radius)
-    xs, ws_m, ws_f = [], [], []
+    xs, ws_m, ws_f, ws_l = [], [], [], []
     for e in range(ne):
         v = nods[:3, conn[:3, e]]
         nodes = list(v.T) + [0.5 * (v[:, (a + 1) % 3] + v[:, (a + 2) % 3]) for a in range(3)]
@@ -145,12 +160,15 @@ def test_c3_mixed_vs_fp64_and_sneddon(c3, ora):
                 xs.append(ora.sneddon_dd(G, NU, 1.0, 1.0, x)[2])
                 ws_m.append(dd_m[6 * e + k, 2])
                 ws_f.append(dd_f[6 * e + k, 2])
+                ws_l.append(dd_l[6 * e + k, 2])
     xs = np.array(xs)
     sn_m = rel(ws_m, xs, np.abs(xs).max())
     sn_f = rel(ws_f, xs, np.abs(xs).max())
-    print(f'C3 opening: mixed vs FP64 {open_err:.1e}; vs Sneddon (r < 0.9) mixed {sn_m:.1e}, FP64 {sn_f:.1e}')
-    assert open_err <= 1e-8
-    assert sn_m <= 1e-2 and sn_f <= 1e-2
+    sn_l = rel(ws_l, xs, np.abs(xs).max())
+    print(f'C3 opening vs FP64: mixed LU {open_err:.1e}, learned on the mixed-precision operator {open_err_l:.1e}; '
+          f'vs Sneddon (r < 0.9) mixed {sn_m:.1e}, learned {sn_l:.1e}, FP64 {sn_f:.1e}')
+    assert open_err <= 1e-8 and open_err_l <= 1e-8
+    assert sn_m <= 1e-2 and sn_f <= 1e-2 and sn_l <= 1e-2
 
 
 def ctx_of(matrix):
