@@ -39,3 +39,29 @@ def test_ellipse_and_wavy():
     assert np.allclose((nods[0, tips] / 2.0) ** 2 + nods[1, tips] ** 2, 1.0)
     nw, cw = meshgen.wavy(200, aspect=2.0, amp=0.2, k=np.pi, seed=3)
     assert np.abs(nw[2]).max() > 0.1
+
+
+def test_batch_workload_is_seeded_and_uneven():
+    from hfpx3d_b200 import meshgen
+    m1, S1 = meshgen.batch_workload(16, 8, seed=5)
+    m2, S2 = meshgen.batch_workload(16, 8, seed=5)
+    assert len(m1) == 16 and S1.shape == (16, 6, 8)
+    assert all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(m1, m2))
+    assert np.array_equal(S1, S2)
+    sizes = [c.shape[1] for _, c in m1]
+    assert min(sizes) >= 24 and max(sizes) <= 550 and len(set(sizes)) > 8
+    # even cases: uniform pressure in [0.5, 2] (sigma_zz only); odd: in-situ
+    # stress tensors with principal values in [-1, 0]
+    assert np.all((S1[:, 2, 0::2] >= 0.5) & (S1[:, 2, 0::2] <= 2.0))
+    assert np.all(S1[:, [0, 1, 3, 4, 5]][:, :, 0::2] == 0.0)
+    for m in range(16):
+        s = S1[m, :, 1]
+        T = np.array([[s[0], s[3], s[4]], [s[3], s[1], s[5]], [s[4], s[5], s[2]]])
+        ev = np.linalg.eigvalsh(T)
+        assert np.all(ev >= -1 - 1e-12) and np.all(ev <= 1e-12)
+
+
+def test_batch_tile_table_is_read():
+    from hfpx3d_b200 import engine
+    nb, leaf = engine.batch_tiles()
+    assert nb % 32 == 0 and leaf in (256, 512)
