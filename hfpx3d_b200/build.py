@@ -21,7 +21,7 @@ HOST_LIB = os.path.join(HERE, 'libhfpx_host.so')
 LAPACKE_LIB = os.path.join(HERE, 'libhfpx_lapacke.so')
 MAIN = os.path.join(HERE, 'bin', 'hfpx_main')
 SOURCES = ['engine.cu', 'assembly.cu', 'lu.cu', 'solve.cu', 'gemm_tc.cu', 'precond.cu', 'gnn.cu', 'vc.cu', 'batch.cu',
-           'coarse.cu']
+           'coarse.cu', 'cf.cu']
 CUDA = os.environ.get('CUDA_HOME', '/usr/local/cuda')
 NVCC = os.path.join(CUDA, 'bin', 'nvcc')
 CXX = os.environ.get('CXX', 'g++')

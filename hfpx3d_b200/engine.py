@@ -36,6 +36,30 @@ class SolveInfo(ctypes.Structure):
     _fields_ = [('iterations', ctypes.c_int), ('residual', ctypes.c_double), ('converged', ctypes.c_int)]
 
 
+class CfMaterial(ctypes.Structure):
+    """F_C_Param_T (src/Core/model_parameters.h:22-31) with the contact model
+    ids of Properties_T::c_model_id (cohesion: 0 box, 1 linear weakening;
+    friction: 0 constant, 1 linear slip weakening)."""
+    _fields_ = [('cr_open', ctypes.c_double), ('peak_ts', ctypes.c_double), ('cr_slip', ctypes.c_double),
+                ('peak_sc', ctypes.c_double), ('peak_sf', ctypes.c_double), ('res_sf', ctypes.c_double),
+                ('cohesion_model', ctypes.c_int), ('friction_model', ctypes.c_int)]
+
+
+class _CfStateC(ctypes.Structure):
+    _fields_ = [('dd', ctypes.POINTER(ctypes.c_double)), ('pp', ctypes.POINTER(ctypes.c_double)),
+                ('mr_open', ctypes.POINTER(ctypes.c_double)), ('mr_slip', ctypes.POINTER(ctypes.c_double)),
+                ('friction_coef', ctypes.POINTER(ctypes.c_double)),
+                ('slip_cohesion', ctypes.POINTER(ctypes.c_double)),
+                ('open_cohesion', ctypes.POINTER(ctypes.c_double)),
+                ('mat_id', ctypes.POINTER(ctypes.c_int32)), ('dof_h', ctypes.POINTER(ctypes.c_int64))]
+
+
+class CfInfo(ctypes.Structure):
+    _fields_ = [('residual', ctypes.c_double), ('volume', ctypes.c_double), ('pressure', ctypes.c_double),
+                ('delta_p', ctypes.c_double), ('n_dof', ctypes.c_int64), ('n_fixed', ctypes.c_int64),
+                ('solver', ctypes.c_int), ('refinement', ctypes.c_int)]
+
+
 _D = ctypes.POINTER(ctypes.c_double)
 _L = ctypes.POINTER(ctypes.c_int64)
 _V = ctypes.c_void_p
@@ -66,6 +90,10 @@ SIGNATURES = {
     'hfpx_batch_launches': (_i64, [_V]),
     'hfpx_batch_phases': (_int, [_V, _V, _D]),
     'hfpx_batch_destroy': (_int, [_V]),
+    'hfpx_cf_match': (_int, [_V, _i64, ctypes.POINTER(CfMaterial), _int, ctypes.POINTER(_CfStateC)]),
+    'hfpx_cf_update_mrd': (_int, [_V, _i64, ctypes.POINTER(CfMaterial), _int, ctypes.POINTER(_CfStateC)]),
+    'hfpx_vc_cf_iteration': (_int, [_V, _V, _V, _L, _i64, ctypes.POINTER(CfMaterial), _int, _D, _i64, _f64, _int,
+                                    _int, _f64, ctypes.POINTER(_CfStateC), ctypes.POINTER(CfInfo)]),
     'hfpx_matrix_upload': (_int, [_V, _D, _i64, _i64, ctypes.POINTER(_V)]),
     'hfpx_matrix_dims': (_int, [_V, _L, _L]),
     'hfpx_matrix_download': (_int, [_V, _V, _D, _i64]),
@@ -780,3 +808,97 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ---- the volume-control iteration with cohesion and friction
+# (vc_cf_iteration, src/Development/c_f_iteration.cpp:27-436; match_f_c and
+# update_mrd, src/Development/cohesion_friction.cpp:22-194)
+
+class CfState:
+    """The solution part of the reference's Mesh_Data_T
+    (src/Core/surface_mesh_utilities.h:51-101) per collocation point
+    (n_cp = 6 n_el, point 6 el + local node): dd (n_cp x 3), pp, the
+    Frac_State_T arrays, the material ids, and the step's truncated DoF
+    handle dof_h (dof_h_dd) with its DoF count n_dof."""
+
+    def __init__(self, n_el, dd=None, pp=None, mr_open=None, mr_slip=None, mat_id=None):
+        n_cp = 6 * int(n_el)
+        self.n_el = int(n_el)
+        self.dd = np.asfortranarray(np.zeros((n_cp, 3)) if dd is None else dd, dtype=np.float64).copy(order='F')
+        self.pp = np.ascontiguousarray(np.zeros(n_cp) if pp is None else pp, dtype=np.float64).copy()
+        self.mr_open = np.ascontiguousarray(np.zeros(n_cp) if mr_open is None else mr_open, dtype=np.float64).copy()
+        self.mr_slip = np.ascontiguousarray(np.zeros(n_cp) if mr_slip is None else mr_slip, dtype=np.float64).copy()
+        self.mat_id = np.ascontiguousarray(np.zeros(n_cp) if mat_id is None else mat_id, dtype=np.int32).copy()
+        self.friction_coef = np.zeros(n_cp)
+        self.slip_cohesion = np.zeros(n_cp)
+        self.open_cohesion = np.zeros(n_cp)
+        self.dof_h = np.full((self.n_el, 18), -1, dtype=np.int64, order='F')
+        self.n_dof = 0
+        for a in (self.pp, self.mr_open, self.mr_slip, self.mat_id):
+            if a.shape != (n_cp,):
+                raise ValueError('per-point arrays must hold 6 n_el entries')
+        if self.dd.shape != (n_cp, 3):
+            raise ValueError('dd must be (6 n_el) x 3')
+
+    def _c(self):
+        d = lambda a: a.ctypes.data_as(_D)
+        return _CfStateC(d(self.dd), d(self.pp), d(self.mr_open), d(self.mr_slip), d(self.friction_coef),
+                         d(self.slip_cohesion), d(self.open_cohesion),
+                         self.mat_id.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _lp(self.dof_h))
+
+    def copy(self):
+        s = CfState(self.n_el, self.dd, self.pp, self.mr_open, self.mr_slip, self.mat_id)
+        for k in ('friction_coef', 'slip_cohesion', 'open_cohesion', 'dof_h'):
+            setattr(s, k, getattr(self, k).copy(order='K'))
+        s.n_dof = self.n_dof
+        return s
+
+
+def _materials(materials):
+    mats = (CfMaterial * len(materials))()
+    for i, m in enumerate(materials):
+        if isinstance(m, CfMaterial):
+            mats[i] = m
+        else:
+            mats[i] = CfMaterial(**m)
+    return mats
+
+
+def match_f_c(ctx, materials, state: CfState):
+    """cohesion_friction.cpp:22-130: cohesion and friction of every point."""
+    mats = _materials(materials)
+    st = state._c()
+    ctx.check(lib().hfpx_cf_match(ctx.h, 6 * state.n_el, mats, len(mats), ctypes.byref(st)))
+
+
+def update_mrd(ctx, materials, state: CfState):
+    """cohesion_friction.cpp:134-194: the maximum relative opening and slip."""
+    mats = _materials(materials)
+    st = state._c()
+    ctx.check(lib().hfpx_cf_update_mrd(ctx.h, 6 * state.n_el, mats, len(mats), ctypes.byref(st)))
+
+
+def vc_cf_iteration(ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, orig_dof_h, n_dof, materials, state: CfState,
+                    s_inf, inj_cp, new_vol, is_dd_local=False, all_components=False, release_sign=False,
+                    tol=1e-12) -> CfInfo:
+    """One volume-control iteration with cohesion and friction
+    (c_f_iteration.cpp:27-436) on the bordered matrix of orig_dof_h
+    (unfactored, or factored with HFPX_LU_MIXED); updates `state` in place
+    and returns the step's CfInfo (residual as the reference's return value).
+    all_components adds the normal traction adjustment to the right-hand side
+    too (the reference adds the first two components); release_sign adds the
+    adjustments with the sign that removes the excess traction (the
+    reference's sign doubles it)."""
+    mats = _materials(materials)
+    dof = _f(orig_dof_h, np.int64)
+    si = np.ascontiguousarray(s_inf, dtype=np.float64)
+    if si.shape != (6,):
+        raise ValueError('s_inf must hold 6 Voigt components')
+    st = state._c()
+    info = CfInfo()
+    ctx.check(lib().hfpx_vc_cf_iteration(ctx.h, dmesh.h, matrix.h, _lp(dof), int(n_dof), mats, len(mats), _dp(si),
+                                         int(inj_cp), float(new_vol), int(is_dd_local),
+                                         (1 if all_components else 0) | (2 if release_sign else 0),
+                                         float(tol), ctypes.byref(st), ctypes.byref(info)))
+    state.n_dof = int(info.n_dof)
+    return info

@@ -409,6 +409,83 @@ int64_t hfpx_batch_launches(const hfpx_batch *batch);
 int hfpx_batch_phases(hfpx_ctx *ctx, const hfpx_batch *batch, double *ms);
 int hfpx_batch_destroy(hfpx_batch *batch);
 
+/* ---- the volume-control iteration with cohesion and friction:
+ * vc_cf_iteration, src/Development/c_f_iteration.cpp:27-436, with match_f_c
+ * and update_mrd (src/Development/cohesion_friction.cpp:22-130, :134-194).
+ * The state is the reference's Mesh_Data_T solution part
+ * (src/Core/surface_mesh_utilities.h:51-101), per collocation point
+ * (n_cp = 6 n_el, point 6 el + local node): dd n_cp x 3 column-major (the
+ * nodal DD), pp the nodal pressures, the Frac_State_T arrays and the
+ * material ids; dof_h (n_el x 18, written by the iteration) is the
+ * truncated DoF handle of the step, dof_h_dd.  Materials are the
+ * reference's F_C_Param_T (model_parameters.h:22-31) with its contact
+ * model ids (Properties_T::c_model_id(mat, 0 / 1)). */
+typedef struct {
+  double cr_open;      /* critical opening */
+  double peak_ts;      /* peak tensile stress */
+  double cr_slip;      /* critical slip */
+  double peak_sc;      /* peak shear cohesion */
+  double peak_sf;      /* peak friction coefficient */
+  double res_sf;       /* residual friction coefficient */
+  int cohesion_model;  /* 0 box (Dugdale), 1 linear weakening, other: none */
+  int friction_model;  /* 0 constant (peak), 1 linear slip weakening, other: residual */
+} hfpx_cf_material;
+
+typedef struct {
+  double *dd;                 /* n_cp x 3, ld n_cp (in/out) */
+  double *pp;                 /* n_cp (in/out) */
+  double *mr_open, *mr_slip;  /* max. relative opening / slip (in; update_mrd writes) */
+  double *friction_coef, *slip_cohesion, *open_cohesion;  /* written by match_f_c */
+  const int32_t *mat_id;      /* n_cp, 0 .. n_mat - 1 */
+  int64_t *dof_h;             /* n_el x 18 column-major (out; may be null) */
+} hfpx_cf_state;
+
+typedef struct {
+  double residual;    /* |increments|_1 + |traction adjustments|_1 (:430-433) */
+  double volume;      /* crack volume before the step (the volume row times dd) */
+  double pressure;    /* injection pressure after the step */
+  double delta_p;     /* its increment */
+  int64_t n_dof;      /* active DD unknowns of the step (dof_h_dd.n_dof) */
+  int64_t n_fixed;    /* unknowns fixed at intact collocation points */
+  int solver;         /* 0: solved with the full system's factors, 1: truncated system factored */
+  int refinement;     /* refinement steps of the solve */
+} hfpx_cf_info;
+
+/* match_f_c on the device: cohesion and friction of every point from its
+ * DD (read as local, as the reference reads them) and damage state. */
+int hfpx_cf_match(hfpx_ctx *ctx, int64_t n_cp, const hfpx_cf_material *mats, int n_mat, hfpx_cf_state *state);
+/* update_mrd on the device: the maximum relative opening and slip reached. */
+int hfpx_cf_update_mrd(hfpx_ctx *ctx, int64_t n_cp, const hfpx_cf_material *mats, int n_mat,
+                       hfpx_cf_state *state);
+/* One iteration: match_f_c, the elastic tractions of the current DD (one
+ * product with the bordered matrix, whose volume row gives the volume),
+ * per point the traction check (opening, cohesion, slip, intact) and the
+ * traction adjustments, the truncated system (the DoF of intact points
+ * fixed; mod_3dbem_system_vc, system_assembly.cpp:560-629) solved for the
+ * DD increments and the pressure increment that injects new_vol, then the
+ * DD (negative openings clamped) and the pressures of opened points.
+ * `matrix` is the bordered matrix of orig_dof_h (make_3dbem_matrix_vc,
+ * n_dof + 1 unknowns): unfactored, or factored with HFPX_LU_MIXED, which
+ * keeps the operator.  With mixed factors and at most 1024 fixed DoF the
+ * step reuses them (hfpx_lu_solve_fixed); otherwise it factors the
+ * truncated system (hfpx_matrix_truncate, HFPX_LU_MIXED).  inj_cp is the
+ * injection point (6 el + node, load.inj_loc(0, 0..1)).  flags bit 0: add
+ * all three components of the traction adjustments to the right-hand side
+ * (the reference adds the first two, :262-268); bit 1: add them with the
+ * opposite sign.  The reference's sign adds A dd = dt with dt = -(excess
+ * traction) to the traction A dd it subtracts, which doubles the excess,
+ * and its iteration grows; with bit 1 the excess is removed and the
+ * iteration settles.  Where the reference's
+ * statements disagree with each other the engine takes one reading:
+ * DoF renumbering in element order (the reference's shared counter races
+ * under OpenMP), DoF untouched by the checks stay active, tractions and the
+ * volume from the original numbering, the clamped DD left in local
+ * coordinates.  HFPX_ERR_SINGULAR when every DoF is fixed. */
+int hfpx_vc_cf_iteration(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix,
+                         const int64_t *orig_dof_h, int64_t n_dof, const hfpx_cf_material *mats, int n_mat,
+                         const double *s_inf, int64_t inj_cp, double new_vol, int is_dd_local, int flags,
+                         double tol, hfpx_cf_state *state, hfpx_cf_info *info);
+
 /* ---- one element at one point: make_local_3dbem_submatrix,
  * src/Elasticity/elasticity_kernel_integration.cpp:34-205 (kernel 1).
  * tau: 3 complex (re,im), sfm: 6x6 complex row-major (re,im); out 6x18
