@@ -374,6 +374,8 @@ def run_engine(args, rank, world, local_rank):
 
     # the 1025-element volume-control ellipse, measured on the engine as well
     c2 = run_c2(args, ctx, engine, L, torch, stream, local_rank) if rank == 0 and args.compare else None
+    # one volume-control iteration with cohesion and friction on the same ellipse
+    cf = run_cf(ctx, engine) if rank == 0 and args.cf else None
     # stresses at observation points (make_3dbem_stress_f_s) on the C1 penny
     stress = run_stress(ctx, engine, torch, stream) if rank == 0 and args.stress else None
     # the batched workload: 256 uneven meshes x 64 load cases in one graph
@@ -467,6 +469,8 @@ def run_engine(args, rank, world, local_rank):
         for k in ('mixed', 'fp64'):
             c2.pop('_x_' + k, None)
         line['c2'] = c2
+    if cf is not None:
+        line['cf_iteration'] = cf
     if stress is not None:
         line['stress'] = stress
     if c5 is not None:
@@ -748,6 +752,69 @@ FIT_SIZES = (600, 900, 1200)
 C2_NEL, C2_SEED = 1025, 1025
 
 
+def run_cf(ctx, engine, steps=3):
+    """Steps of the volume-control iteration with cohesion and friction
+    (hfpx_vc_cf_iteration) on the 1025-element ellipse's bordered matrix (DD
+    in local coordinates): opened within rho < 0.5 of the ellipse's scaled
+    radius (fully within 0.3), earlier slip in 0.5 < rho < `ring`, pressure 1
+    where opened, two materials; 10 % more volume each step.  Host arrays in
+    and out through the C-ABI; wall time per step (each call synchronises).
+    Once with the mixed factors of the full system (few intact points: the
+    capacitance solve), once with many intact points (the truncated system
+    factored)."""
+    nods, conn, s_inf, _ = c2_case()
+    mesh = engine.MeshGeom(nods, conn)
+    dof, n = engine.make_dof_h_crack(mesh, 1)
+    dm = engine.DeviceMesh(ctx, mesh, BETA)
+    A = engine.assemble(ctx, dm, dof, n, G, NU, is_dd_local=True, vc=True)
+    vrow = A.block(n, 0, 1, n + 1)[0]
+    lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+    ne = conn.shape[1]
+    pos = np.zeros((6 * ne, 2))
+    for a in range(3):
+        pos[a::6] = nods[:2, conn[a]].T
+        pos[3 + a::6] = 0.5 * (nods[:2, conn[(a + 1) % 3]] + nods[:2, conn[(a + 2) % 3]]).T
+    ax = np.abs(nods[:2]).max(axis=1)
+    rho = np.hypot(pos[:, 0] / ax[0], pos[:, 1] / ax[1])
+    rng = np.random.default_rng(9)
+    mats = [dict(cr_open=0.02, peak_ts=0.8, cr_slip=0.02, peak_sc=0.2, peak_sf=0.6, res_sf=0.3, cohesion_model=1,
+                 friction_model=1),
+            dict(cr_open=0.03, peak_ts=1.2, cr_slip=0.03, peak_sc=0.1, peak_sf=0.5, res_sf=0.5, cohesion_model=0,
+                 friction_model=0)]
+    out = {'workload': f'VC 2:1 ellipse {C2_NEL} el, N={n}+1, DD local, tip vertices fixed; {steps} steps, '
+                       'all traction components, releasing sign',
+           'runs': []}
+    for ring in (0.995, 0.8):
+        dd = np.zeros((6 * ne, 3))
+        dd[:, 2] = 0.02 * np.sqrt(np.clip(1 - (rho / 0.5) ** 2, 0, None))
+        st = engine.CfState(ne, dd=dd, pp=np.where(rho < 0.5, 1.0, 0.0),
+                            mr_open=np.where(rho < 0.3, 1.0, np.where(rho < 0.5, 0.5, 0.0)),
+                            mr_slip=np.where((rho > 0.5) & (rho < ring), 0.3, 0.0),
+                            mat_id=(rng.random(6 * ne) < 0.3).astype(np.int32))
+        x = np.zeros(n + 1)
+        for l in range(18):
+            kept = dof[:, l] >= 0
+            x[dof[kept, l]] = st.dd[6 * np.arange(ne)[kept] + l // 3, l % 3]
+        vol = float(vrow @ x)
+        run = {'slip_ring': ring, 'steps_s': [], 'n_fixed': [], 'solver': [], 'residual': []}
+        for k in range(steps + 1):   # step 0 warms up
+            t0 = time.perf_counter()
+            info = engine.vc_cf_iteration(ctx, dm, A, dof, n, mats, st, s_inf, int(np.argmin(rho)), 1.1 * vol,
+                                          is_dd_local=True, all_components=True, release_sign=True)
+            dt = time.perf_counter() - t0
+            if k == 0:
+                continue
+            run['steps_s'].append(round(dt, 5))
+            run['n_fixed'].append(int(info.n_fixed))
+            run['solver'].append('full factors + capacitance' if info.solver == 0 else 'truncated system factored')
+            run['residual'].append(float(info.residual))
+        out['runs'].append(run)
+    del lu
+    A.close()
+    dm.close()
+    return out
+
+
 def c2_case():
     """The 1025-element 2:1 volume-control ellipse: mesh, Haar in-situ stress, V = 1."""
     from hfpx3d_b200 import meshgen
@@ -930,6 +997,8 @@ def main():
                     help='penny sizes (elements) the CPU reference is measured at and fitted from')
     ap.add_argument('--no-c2-ref', dest='c2_ref', action='store_false',
                     help='skip the CPU reference run of the 1025-element VC ellipse')
+    ap.add_argument('--no-cf', dest='cf', action='store_false',
+                    help='skip the cohesion/friction iteration steps on the ellipse')
     ap.add_argument('--no-batch', dest='batch', action='store_false',
                     help='skip the batched workload (256 uneven meshes x 64 load cases in one graph)')
     ap.add_argument('--no-c5-per-mesh', dest='c5_per_mesh', action='store_false',

@@ -46,17 +46,34 @@ struct DoF_Handle_T {
   int64_t n_dof = 0;
   Array2D<int64_t> dof_h;  // Ne x 18, -1 = fixed
 };
+// surface_mesh_utilities.h:51-62: "damage state" and forces per collocation point
+struct Frac_State_T {
+  std::vector<double> mr_open, mr_slip;                               // max. relative opening / slip
+  std::vector<double> friction_coef, slip_cohesion, open_cohesion;   // instant forces
+};
 struct Mesh_Data_T {
   Mesh_Geom_T mesh;
   DoF_Handle_T dof_h_dd;
   Array2D<double> dd;      // (6 Ne) x 3
+  // the volume-control iteration's state (surface_mesh_utilities.h:66-101),
+  // per collocation point (6 el + local node)
+  std::vector<int> mat_id;
+  std::vector<double> pp;
+  Frac_State_T frac_state;
+};
+// src/Core/model_parameters.h:22-31
+struct F_C_Param_T {
+  double cr_open = 1.0, peak_ts = 0.0, cr_slip = 1.0, peak_sc = 0.0, peak_sf = 0.0, res_sf = 0.0;
 };
 // src/Core/model_parameters.h:34-102
 struct Properties_T {
   double shear_m = 1.0, poiss_r = 0.0;
+  Array2D<int> c_model_id;              // n_surface x 2: cohesion, friction model ids
+  std::vector<F_C_Param_T> f_c_param;   // per surface (material) id
 };
 struct Load_T {
   double s_inf[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, xz, yz (tension positive)
+  Array2D<int64_t> inj_loc;              // injection points: (element, local node) rows
 };
 struct Num_Param_T {
   double beta = 0.125;
@@ -143,6 +160,24 @@ class LU {
  private:
   DeviceMatrix& a_;
 };
+
+// src/Development/cohesion_friction.cpp:22-130, :134-194 (on the device)
+void match_f_c(const Properties_T& prop, const std::vector<int>& mat_id, const Array2D<double>& dd,
+               bool is_dd_local, Frac_State_T& f_state);
+void update_mrd(const Properties_T& prop, const std::vector<int>& mat_id, const Array2D<double>& dd,
+                bool is_dd_local, Frac_State_T& f_state);
+// src/Development/c_f_iteration.cpp:27-436: one step of the volume-control
+// scheme with cohesion and friction on the device-resident bordered matrix of
+// orig_dof_h (make_3dbem_matrix_vc; unfactored, or factored with
+// HFPX_LU_MIXED).  m_data (dd, pp, frac_state, mat_id) is updated and its
+// dof_h_dd set to the step's truncated handle; returns the reference's
+// residual (|increments|_1 + |traction adjustments|_1).  cf_flags are
+// hfpx_vc_cf_iteration's (bit 0 all traction components, bit 1 the
+// releasing sign); 0 reproduces the reference.  m_data_p (the previous time
+// step) is unused, as in the reference.
+double vc_cf_iteration(const Mesh_Data_T& m_data_p, const DeviceMatrix& orig_vc_sys, const DoF_Handle_T& orig_dof_h,
+                       const DeviceMesh& mesh, const Properties_T& prop, const Num_Param_T& n_par, const Load_T& load,
+                       double new_vol, Mesh_Data_T& m_data, int cf_flags = 0, hfpx_cf_info* info = nullptr);
 
 // src/IO: config (config_file_io.cpp:56-361), meshes and points
 // (mesh_file_io.cpp:28-605), csv output (data_file_io.h:131-168).

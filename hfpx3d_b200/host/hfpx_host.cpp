@@ -110,6 +110,86 @@ Array2D<double> make_3dbem_stress_f_s(double G, double nu, const DeviceMesh& m, 
   return out;
 }
 
+// ---- the volume-control iteration with cohesion and friction
+static std::vector<hfpx_cf_material> cf_materials(const Properties_T& prop) {
+  if (prop.f_c_param.empty()) throw Error(HFPX_ERR_ARG, "Properties_T has no contact parameters");
+  std::vector<hfpx_cf_material> m(prop.f_c_param.size());
+  for (size_t i = 0; i < m.size(); ++i) {
+    const F_C_Param_T& p = prop.f_c_param[i];
+    m[i] = {p.cr_open, p.peak_ts, p.cr_slip, p.peak_sc, p.peak_sf, p.res_sf, 0, 0};
+    if ((int64_t)i < prop.c_model_id.size(0)) {
+      m[i].cohesion_model = prop.c_model_id((int64_t)i, 0);
+      m[i].friction_model = prop.c_model_id((int64_t)i, 1);
+    }
+  }
+  return m;
+}
+
+// Frac_State_T sized for n_cp points (new entries 0)
+static void size_state(Frac_State_T& f, size_t n_cp) {
+  for (std::vector<double>* v : {&f.mr_open, &f.mr_slip, &f.friction_coef, &f.slip_cohesion, &f.open_cohesion})
+    if (v->size() != n_cp) v->resize(n_cp, 0.0);
+}
+
+static hfpx_cf_state cf_view(const Array2D<double>& dd, std::vector<double>& pp, Frac_State_T& f,
+                             const std::vector<int32_t>& mat_id, int64_t* dof_h) {
+  return hfpx_cf_state{const_cast<double*>(dd.data()), pp.data(), f.mr_open.data(), f.mr_slip.data(),
+                       f.friction_coef.data(), f.slip_cohesion.data(), f.open_cohesion.data(), mat_id.data(), dof_h};
+}
+
+static std::vector<int32_t> mat_ids(const std::vector<int>& mat_id, int64_t n_cp) {
+  if ((int64_t)mat_id.size() != n_cp) throw Error(HFPX_ERR_ARG, "mat_id needs one entry per collocation point");
+  return std::vector<int32_t>(mat_id.begin(), mat_id.end());
+}
+
+void match_f_c(const Properties_T& prop, const std::vector<int>& mat_id, const Array2D<double>& dd, bool,
+               Frac_State_T& f_state) {
+  const int64_t n_cp = dd.size(0);
+  if (dd.size(1) != 3) throw Error(HFPX_ERR_ARG, "dd must be n x 3");
+  const std::vector<hfpx_cf_material> m = cf_materials(prop);
+  const std::vector<int32_t> id = mat_ids(mat_id, n_cp);
+  size_state(f_state, (size_t)n_cp);
+  std::vector<double> pp((size_t)n_cp, 0.0);
+  hfpx_cf_state st = cf_view(dd, pp, f_state, id, nullptr);
+  check(hfpx_cf_match(context(), n_cp, m.data(), (int)m.size(), &st));
+}
+
+void update_mrd(const Properties_T& prop, const std::vector<int>& mat_id, const Array2D<double>& dd, bool,
+                Frac_State_T& f_state) {
+  const int64_t n_cp = dd.size(0);
+  if (dd.size(1) != 3) throw Error(HFPX_ERR_ARG, "dd must be n x 3");
+  const std::vector<hfpx_cf_material> m = cf_materials(prop);
+  const std::vector<int32_t> id = mat_ids(mat_id, n_cp);
+  size_state(f_state, (size_t)n_cp);
+  std::vector<double> pp((size_t)n_cp, 0.0);
+  hfpx_cf_state st = cf_view(dd, pp, f_state, id, nullptr);
+  check(hfpx_cf_update_mrd(context(), n_cp, m.data(), (int)m.size(), &st));
+}
+
+double vc_cf_iteration(const Mesh_Data_T&, const DeviceMatrix& orig_vc_sys, const DoF_Handle_T& orig_dof_h,
+                       const DeviceMesh& mesh, const Properties_T& prop, const Num_Param_T& n_par, const Load_T& load,
+                       double new_vol, Mesh_Data_T& m_data, int cf_flags, hfpx_cf_info* info_out) {
+  const int64_t n_el = orig_dof_h.dof_h.size(0), n_cp = 6 * n_el;
+  if (m_data.dd.size(0) != n_cp || m_data.dd.size(1) != 3) throw Error(HFPX_ERR_ARG, "m_data.dd must be (6 Ne) x 3");
+  if ((int64_t)m_data.pp.size() != n_cp) throw Error(HFPX_ERR_ARG, "m_data.pp needs one entry per collocation point");
+  if (load.inj_loc.size(0) < 1 || load.inj_loc.size(1) < 2) throw Error(HFPX_ERR_ARG, "load.inj_loc is empty");
+  const std::vector<hfpx_cf_material> m = cf_materials(prop);
+  const std::vector<int32_t> id = mat_ids(m_data.mat_id, n_cp);
+  size_state(m_data.frac_state, (size_t)n_cp);
+  Array2D<int64_t> dof_new(n_el, 18, -1);
+  hfpx_cf_state st = cf_view(m_data.dd, m_data.pp, m_data.frac_state, id, dof_new.data());
+  hfpx_cf_info info{};
+  // the injection point inj_loc(0, 0) * 6 + inj_loc(0, 1) (c_f_iteration.cpp:80)
+  const int64_t inj = load.inj_loc(0, 0) * 6 + load.inj_loc(0, 1);
+  check(hfpx_vc_cf_iteration(context(), mesh.get(), orig_vc_sys.get(), orig_dof_h.dof_h.data(), orig_dof_h.n_dof,
+                             m.data(), (int)m.size(), load.s_inf, inj, new_vol, n_par.is_dd_local ? 1 : 0, cf_flags,
+                             1e-12, &st, &info));
+  m_data.dof_h_dd.dof_h = dof_new;
+  m_data.dof_h_dd.n_dof = info.n_dof;
+  if (info_out) *info_out = info;
+  return info.residual;
+}
+
 LU::LU(DeviceMatrix& a, int mode) : a_(a) {
   int64_t info = 0;
   check(hfpx_lu_factor(context(), a.get(), mode, &info));

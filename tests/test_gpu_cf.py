@@ -282,3 +282,52 @@ def test_iteration_errors(ctx, cf_case):
     assert np.array_equal(gs.dd, st0.dd)
     del lu
     A.close()
+
+
+@pytest.mark.gpu
+def test_cpp_host_layer_matches_python(ctx, cf_case, tmp_path):
+    """hfpx::vc_cf_iteration / hfpx::update_mrd (the C++ host layer,
+    hfpx3d_b200/host) against the Python mirror on the same case, two steps
+    with all components and the releasing sign: both call the same C-ABI
+    (each its own mixed factorisation, refined to 1e-12)."""
+    import subprocess
+    from hfpx3d_b200 import build, engine
+    c = cf_case
+    nods, conn, st0, inj = c['nods'], c['conn'], c['st'], c['inj']
+    dof, n, dm = c['dof'], c['n'], c['dm']
+    ne = conn.shape[1]
+    exe = str(tmp_path / 'host_cf_main')
+    subprocess.run(['g++', '-O2', '-std=c++17', '-I' + os.path.join(ROOT, 'include'), '-I' + build.HOST,
+                    os.path.join(ROOT, 'tests', 'host_cf_main.cpp'), '-o', exe, '-L' + build.HERE, '-lhfpx_host',
+                    '-lhfpx_engine', '-Wl,-rpath,' + build.HERE], check=True, timeout=300)
+    A = engine.assemble(ctx, dm, dof, n, G, NU, is_dd_local=True, vc=True)
+    vol = 1.1 * float(A.block(n, 0, 1, n + 1)[0] @ dd_vector(st0.dd, dof, n))
+    keys = ['cr_open', 'peak_ts', 'cr_slip', 'peak_sc', 'peak_sf', 'res_sf', 'cohesion_model', 'friction_model']
+    np.save(tmp_path / 'mats.npy', np.array([[float(m[k]) for k in keys] for m in MATS]))
+    np.save(tmp_path / 'params.npy', np.concatenate([S_INF, [inj // 6, inj % 6, vol]])[:, None])
+    np.save(tmp_path / 'nods.npy', np.asfortranarray(nods, dtype=np.float64))
+    np.save(tmp_path / 'conn.npy', np.asfortranarray(conn, dtype=np.int64))
+    np.save(tmp_path / 'dd.npy', np.asfortranarray(st0.dd))
+    for k in ('pp', 'mr_open', 'mr_slip'):
+        np.save(tmp_path / f'{k}.npy', np.asarray(getattr(st0, k), dtype=np.float64)[:, None])
+    np.save(tmp_path / 'mat_id.npy', np.asarray(st0.mat_id, dtype=np.int64)[:, None])
+    flags = 3
+    r = subprocess.run([exe, str(tmp_path), '2', str(flags)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lu = engine.LU(ctx, A, engine.HFPX_LU_MIXED)
+    gs = engine.CfState(ne, dd=st0.dd, pp=st0.pp, mr_open=st0.mr_open, mr_slip=st0.mr_slip, mat_id=st0.mat_id)
+    for _ in range(2):
+        info = engine.vc_cf_iteration(ctx, dm, A, dof, n, MATS, gs, S_INF, inj, vol, is_dd_local=True,
+                                      all_components=True, release_sign=True)
+    engine.update_mrd(ctx, MATS, gs)
+    out_pp = np.load(tmp_path / 'out_pp.npy')
+    res = np.load(tmp_path / 'out_res.npy')
+    out_dd = np.load(tmp_path / 'out_dd.npy')
+    assert np.abs(out_dd - gs.dd).max() <= 1e-12 * np.abs(gs.dd).max()
+    assert np.abs(out_pp[:, 0] - gs.pp).max() <= 1e-12 * np.abs(gs.pp).max()
+    np.testing.assert_allclose(out_pp[:, 1], gs.mr_open, rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(out_pp[:, 2], gs.mr_slip, rtol=1e-10, atol=1e-14)
+    assert np.array_equal(np.load(tmp_path / 'out_dof.npy').astype(np.int64), gs.dof_h)
+    assert abs(res[0, 0] - info.residual) <= 1e-10 * info.residual and int(res[0, 1]) == info.n_dof
+    del lu
+    A.close()
