@@ -419,8 +419,14 @@ int hfpx_vc_cf_iteration(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* 
   if (n_keep == 0) return set_error(c, HFPX_ERR_SINGULAR, "every DoF is fixed: the truncated system is singular");
   // 5. the truncated system (mod_3dbem_system_vc, system_assembly.cpp:560-629)
   hfpx_solve_info si{};
-  constexpr int64_t kCapacitanceMax = 1024;
-  if (m->factored == 2 && k <= kCapacitanceMax) {
+  // The full system's factors with the capacitance correction cost k + 1
+  // refined solves, about 1.4e-12 s n^2 (k + 1) on a B200 (80 ms for
+  // n = 17770, k = 183); factoring the truncated system about 2.7e-14 s
+  // n_keep^3 (60 ms for n_keep = 13000).  Take the cheaper one.
+  const double nd = (double)n, nk = (double)n_keep;
+  const bool capacitance = m->factored == 2 && k <= 4096 &&
+                           ((flags & 4) || (double)(k + 1) * nd * nd < 0.02 * nk * nk * nk);
+  if (capacitance) {
     std::vector<int64_t> fx(fixed);
     rc = hfpx_lu_solve_fixed(c, m, fx.data(), k, b.data(), tol, &si);
     info->solver = 0;

@@ -210,7 +210,8 @@ enum : int {
   kScrRefR, kScrRefRf, kScrDof, kScrXtmp, kScrResidPart, kScrResidMax, kScrTrsvFlags, kScrTrsvTicket,
   kScrTrsvErr, kScrTslu, kScrGmresV, kScrGmresZ, kScrGmresH, kScrGmresZero, kScrHostNods, kScrHostConn,
   kScrHostSinf, kScrHostRhs, kScrPanelInv, kScrTcErr, kScrRowScale, kScrStressDd, kScrStressPts, kScrStressSinf,
-  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrGmresEst, kScrMixedY, kScrMixedBlk, kScrGrowList, kScrCount
+  kScrStressOut, kScrStressInfl, kScrStressVec, kScrStressSum, kScrGmresEst, kScrMixedY, kScrMixedBlk, kScrGrowList,
+  kScrRefColMax, kScrCount
 };
 
 // assembly.cu

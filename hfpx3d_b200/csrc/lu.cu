@@ -2084,6 +2084,23 @@ __global__ void permute_rows_kernel(const T* __restrict__ src, T* __restrict__ d
   dst[r + ld * c] = src[perm[r] + ld * c];
 }
 
+// out[j] = max_i |a[i + lda j]|, one CTA per column (the refinement's
+// per-column infinity norms in one launch and one copy to the host)
+__global__ void __launch_bounds__(256) colmax_kernel(const double* __restrict__ a, int64_t n, int64_t lda,
+                                                     double* __restrict__ out) {
+  __shared__ double red[256];
+  const double* col = a + lda * (int64_t)blockIdx.x;
+  double m = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += 256) m = fmax(m, fabs(col[i]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
 __global__ void d2f_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n, int64_t nrhs, int64_t lda,
                            int64_t ldb) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -2512,9 +2529,10 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
   double* x = (double*)ctx_scratch(c, kScrRefX, sizeof(double) * ldb * nrhs);
   double* r = (double*)ctx_scratch(c, kScrRefR, sizeof(double) * ldb * nrhs);
   float* rf = (float*)ctx_scratch(c, kScrRefRf, sizeof(float) * ldb * nrhs);
+  double* cmax = (double*)ctx_scratch(c, kScrRefColMax, sizeof(double) * nrhs);
   int32_t* d_perm = nullptr;
   int rc = 0;
-  if (!x || !r || !rf) rc = set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
+  if (!x || !r || !rf || !cmax) rc = set_error(c, HFPX_ERR_NOMEM, "refinement buffers");
   if (!rc) rc = build_perm(c, m, &d_perm);
   std::vector<double> bnorm(nrhs, 0.0), rnorm(nrhs, 0.0);
   const int64_t tot = n * nrhs;
@@ -2524,16 +2542,18 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
   if (!rc) {
     cudaMemsetAsync(x, 0, sizeof(double) * ldb * nrhs, c->stream);
     cudaMemcpyAsync(r, d_b, sizeof(double) * ldb * nrhs, cudaMemcpyDeviceToDevice, c->stream);
-    for (int64_t j = 0; j < nrhs; ++j) {
-      int idx = 0;
-      cublasSetPointerMode(H(c), CUBLAS_POINTER_MODE_HOST);
-      cublasIdamax(H(c), (int)n, d_b + ldb * j, 1, &idx);
-      double v = 0.0;
-      cudaMemcpyAsync(&v, d_b + ldb * j + (idx - 1), sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-      cudaStreamSynchronize(c->stream);
-      bnorm[j] = std::fabs(v) > 0 ? std::fabs(v) : 1.0;
-    }
-    for (it = 1; it <= max_iter; ++it) {
+    // per-column infinity norms: one launch, one copy
+    auto colmax = [&](const double* a, std::vector<double>& out) -> int {
+      ++g_launches;
+      colmax_kernel<<<(unsigned)nrhs, 256, 0, c->stream>>>(a, n, ldb, cmax);
+      int e = check_cuda(c, cudaMemcpyAsync(out.data(), cmax, sizeof(double) * nrhs, cudaMemcpyDeviceToHost,
+                                            c->stream), "column norms");
+      if (!e) e = check_cuda(c, cudaStreamSynchronize(c->stream), "column norms");
+      return e;
+    };
+    rc = colmax(d_b, bnorm);
+    for (double& v : bnorm) v = v > 0 ? v : 1.0;
+    for (it = 1; !rc && it <= max_iter; ++it) {
       ++g_launches;
       d2f_kernel<<<nb, 256, 0, c->stream>>>(r, rf, n, nrhs, ldb, ldb);
       rc = solve_factored<float>(c, m, m->d_f, rf, nrhs, ldb, d_perm);
@@ -2545,15 +2565,8 @@ int refine_solve(hfpx_ctx* c, const hfpx_matrix* m, double* d_b, int64_t nrhs, i
       cublasDgemm(H(c), CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)nrhs, (int)n, &mone, m->d_a, (int)m->ld, x, (int)ldb,
                   &one, r, (int)ldb);
       worst = 0.0;
-      for (int64_t j = 0; j < nrhs; ++j) {
-        int idx = 0;
-        cublasIdamax(H(c), (int)n, r + ldb * j, 1, &idx);
-        double v = 0.0;
-        cudaMemcpyAsync(&v, r + ldb * j + (idx - 1), sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-        cudaStreamSynchronize(c->stream);
-        rnorm[j] = std::fabs(v) / bnorm[j];
-        worst = std::max(worst, rnorm[j]);
-      }
+      if ((rc = colmax(r, rnorm))) break;
+      for (int64_t j = 0; j < nrhs; ++j) worst = std::max(worst, rnorm[j] / bnorm[j]);
       if (worst <= tol) break;
     }
     if (!rc) cudaMemcpyAsync(d_b, x, sizeof(double) * ldb * nrhs, cudaMemcpyDeviceToDevice, c->stream);

@@ -880,7 +880,7 @@ def update_mrd(ctx, materials, state: CfState):
 
 def vc_cf_iteration(ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, orig_dof_h, n_dof, materials, state: CfState,
                     s_inf, inj_cp, new_vol, is_dd_local=False, all_components=False, release_sign=False,
-                    tol=1e-12) -> CfInfo:
+                    reuse_factors=False, tol=1e-12) -> CfInfo:
     """One volume-control iteration with cohesion and friction
     (c_f_iteration.cpp:27-436) on the bordered matrix of orig_dof_h
     (unfactored, or factored with HFPX_LU_MIXED); updates `state` in place
@@ -888,7 +888,10 @@ def vc_cf_iteration(ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, orig_dof_h, n_
     all_components adds the normal traction adjustment to the right-hand side
     too (the reference adds the first two components); release_sign adds the
     adjustments with the sign that removes the excess traction (the
-    reference's sign doubles it)."""
+    reference's sign doubles it).  The truncated system is solved with the
+    full system's mixed factors (capacitance correction) when that is the
+    cheaper way, or always when reuse_factors is set and there are factors;
+    otherwise the truncated system is factored."""
     mats = _materials(materials)
     dof = _f(orig_dof_h, np.int64)
     si = np.ascontiguousarray(s_inf, dtype=np.float64)
@@ -898,7 +901,8 @@ def vc_cf_iteration(ctx, dmesh: DeviceMesh, matrix: DeviceMatrix, orig_dof_h, n_
     info = CfInfo()
     ctx.check(lib().hfpx_vc_cf_iteration(ctx.h, dmesh.h, matrix.h, _lp(dof), int(n_dof), mats, len(mats), _dp(si),
                                          int(inj_cp), float(new_vol), int(is_dd_local),
-                                         (1 if all_components else 0) | (2 if release_sign else 0),
+                                         (1 if all_components else 0) | (2 if release_sign else 0)
+                                         | (4 if reuse_factors else 0),
                                          float(tol), ctypes.byref(st), ctypes.byref(info)))
     state.n_dof = int(info.n_dof)
     return info

@@ -466,9 +466,11 @@ int hfpx_cf_update_mrd(hfpx_ctx *ctx, int64_t n_cp, const hfpx_cf_material *mats
  * DD (negative openings clamped) and the pressures of opened points.
  * `matrix` is the bordered matrix of orig_dof_h (make_3dbem_matrix_vc,
  * n_dof + 1 unknowns): unfactored, or factored with HFPX_LU_MIXED, which
- * keeps the operator.  With mixed factors and at most 1024 fixed DoF the
- * step reuses them (hfpx_lu_solve_fixed); otherwise it factors the
- * truncated system (hfpx_matrix_truncate, HFPX_LU_MIXED).  inj_cp is the
+ * keeps the operator.  With mixed factors and few fixed DoF (k + 1 <
+ * 0.02 n_keep^3 / n^2, where the k + 1 refined solves cost less than a new
+ * factorisation) the step reuses them (hfpx_lu_solve_fixed); otherwise it
+ * factors the truncated system (hfpx_matrix_truncate, HFPX_LU_MIXED);
+ * flags bit 2 reuses the mixed factors whenever there are any (k <= 4096).  inj_cp is the
  * injection point (6 el + node, load.inj_loc(0, 0..1)).  flags bit 0: add
  * all three components of the traction adjustments to the right-hand side
  * (the reference adds the first two, :262-268); bit 1: add them with the

@@ -222,7 +222,7 @@ def test_iteration_vs_oracle(ctx, cf_case, all_components, release, factored):
         pre = SimpleNamespace(dd=gs.dd.copy(), pp=gs.pp.copy(), mr_open=gs.mr_open, mr_slip=gs.mr_slip,
                               mat_id=gs.mat_id)
         info = engine.vc_cf_iteration(ctx, dm, A, dof, n, MATS, gs, S_INF, inj, 1.1 * vol, is_dd_local=True,
-                                      all_components=all_components, release_sign=release)
+                                      all_components=all_components, release_sign=release, reuse_factors=factored)
         new, oi = cf_ref.vc_cf_iteration(c['elems'], Ah, dof, MATS, pre, S_INF, inj, 1.1 * vol, is_dd_local=True,
                                          all_components=all_components, release_sign=release)
         if step == 0:
