@@ -189,6 +189,8 @@ __global__ void identity_kernel(double* X, int64_t nc) {
   if (i < nc) X[i + nc * i] = 1.0;
 }
 
+}  // namespace
+
 int env_agg_size() {
   if (const char* e = std::getenv("HFPX_PC_AGG")) {
     const int v = std::atoi(e);
@@ -240,17 +242,42 @@ bool build_coarse(const hfpx_mesh* m, int agg_size, CoarseSpace* cs) {
   std::vector<int32_t> lab(ne, 0);
   std::vector<double> sum(3 * na);
   std::vector<int64_t> cnt(na);
+  std::vector<int32_t> order(na);
+  std::vector<double> ox(na);
   for (int it = 0; it < 6; ++it) {  // a few Lloyd steps: the aggregates need to be compact, not optimal
     bool moved = false;
+    // The nearest centre of each centroid (the lowest index among equal
+    // distances): centres sorted by x and searched outward from the
+    // centroid's x, each direction ending where dx^2 alone exceeds the best
+    // distance (d2 >= dx^2 in floating point too, so the pruned centres are
+    // strictly farther and the choice is the full scan's).
+    for (int64_t a = 0; a < na; ++a) order[a] = (int32_t)a;
+    std::sort(order.begin(), order.end(), [&](int32_t u, int32_t v) {
+      return C[3 * u] < C[3 * v] || (C[3 * u] == C[3 * v] && u < v);
+    });
+    for (int64_t a = 0; a < na; ++a) ox[a] = C[3 * order[a]];
     for (int64_t e = 0; e < ne; ++e) {
-      int32_t best = 0;
+      int32_t best = -1;
       double bd = 1e300;
-      for (int64_t a = 0; a < na; ++a) {
+      auto visit = [&](int64_t q) {
+        const int32_t a = order[q];
         const double d = d2(e, &C[3 * a]);
-        if (d < bd) {
+        if (d < bd || (d == bd && a < best)) {
           bd = d;
-          best = (int32_t)a;
+          best = a;
         }
+      };
+      const double x = cen[3 * e];
+      const int64_t p = std::lower_bound(ox.begin(), ox.end(), x) - ox.begin();
+      for (int64_t q = p; q < na; ++q) {
+        const double dx = cen[3 * e] - ox[q];
+        if (dx * dx > bd) break;
+        visit(q);
+      }
+      for (int64_t q = p - 1; q >= 0; --q) {
+        const double dx = cen[3 * e] - ox[q];
+        if (dx * dx > bd) break;
+        visit(q);
       }
       moved = moved || best != lab[e];
       lab[e] = best;
@@ -344,6 +371,8 @@ bool build_coarse(const hfpx_mesh* m, int agg_size, CoarseSpace* cs) {
   return true;
 }
 
+namespace {
+
 void free_coarse(CoarseSpace* cs) {
   void* ps[] = {(void*)cs->d_ptr, (void*)cs->d_el, (void*)cs->d_agg_of, (void*)cs->d_w};
   pool_free_many(ps, 4);
@@ -367,7 +396,32 @@ std::shared_ptr<CoarseSpace> mesh_coarse(hfpx_ctx* c, const hfpx_mesh* mesh, int
       free_coarse(q);
       delete q;
     });
-    if (!p || !build_coarse(mesh, agg_size, p.get())) return nullptr;
+    if (!p) return nullptr;
+    MeshHostSetup* hs = mm->host_setup.get();
+    bool ready = false;
+    if (hs && agg_size == env_agg_size()) {  // made on the mesh's set-up thread
+      const SetupClock::time_point t0 = SetupClock::now();
+      hs->wait(2);
+      setup_note("coarse aggregates and basis (wait for the set-up thread)", ms_since(t0));
+      if (hs->coarse_ok && hs->coarse.agg_size == agg_size) {
+        const CoarseSpace& h = hs->coarse;
+        p->n_el = h.n_el;
+        p->n_agg = h.n_agg;
+        p->nc = h.nc;
+        p->agg_size = h.agg_size;
+        p->max_agg = h.max_agg;
+        p->agg_of = h.agg_of;
+        p->ptr = h.ptr;
+        p->el = h.el;
+        p->w = h.w;
+        ready = true;
+      }
+    }
+    if (!ready) {
+      const SetupClock::time_point t0 = SetupClock::now();
+      if (!build_coarse(mesh, agg_size, p.get())) return nullptr;
+      setup_note("coarse aggregates and basis", ms_since(t0));
+    }
     int rc = upload(c, &p->d_ptr, p->ptr, "coarse space");
     if (!rc) rc = upload(c, &p->d_el, p->el, "coarse space");
     if (!rc) rc = upload(c, &p->d_agg_of, p->agg_of, "coarse space");

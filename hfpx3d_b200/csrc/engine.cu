@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -16,6 +17,29 @@
 namespace hfpx {
 
 std::atomic<long long> g_launches{0};
+
+int wait_sleeping(hfpx_ctx* c, const char* what) {
+  if (!c->ev_sleep) {
+    if (int rc = check_cuda(c, cudaEventCreateWithFlags(&c->ev_sleep, cudaEventBlockingSync | cudaEventDisableTiming),
+                            what))
+      return rc;
+  }
+  int rc = check_cuda(c, cudaEventRecord(c->ev_sleep, c->stream), what);
+  if (!rc) rc = check_cuda(c, cudaEventSynchronize(c->ev_sleep), what);
+  return rc;
+}
+
+bool setup_profile() {
+  static const bool on = [] {
+    const char* e = std::getenv("HFPX_PROFILE");
+    return e && *e == '1';
+  }();
+  return on;
+}
+
+void setup_note(const char* what, double ms) {
+  if (setup_profile()) std::fprintf(stderr, "[hfpx profile] %s: %.3f ms (host)\n", what, ms);
+}
 
 void* ctx_scratch(hfpx_ctx* c, int slot, size_t bytes) {
   static_assert(kScrCount <= hfpx_ctx::kScratchSlots, "scratch slots");
@@ -95,6 +119,63 @@ static int64_t round_ld(int64_t n) { return ((n + 31) / 32) * 32; }
 
 using namespace hfpx;
 
+namespace hfpx {
+// The set-up thread of a mesh: pattern, coarse space, network inputs (host),
+// each part published as it finishes.  Failures (allocation) leave the part
+// to be made where it is needed.
+void start_mesh_setup(hfpx_mesh* m) {
+  if (m->n_el < kMeshSetupMinElems) return;
+  std::unique_ptr<MeshHostSetup> hs(new (std::nothrow) MeshHostSetup);
+  if (!hs) return;
+  MeshHostSetup* s = hs.get();
+  auto publish = [s](int part, bool ok) {
+    {
+      std::lock_guard<std::mutex> l(s->mu);
+      if (part == 1) s->pattern_ok = ok;
+      if (part == 2) s->coarse_ok = ok;
+      if (part == 3) s->graph_ok = ok;
+      s->done = part;
+    }
+    s->cv.notify_all();
+  };
+  try {
+    s->worker = std::thread([m, s, publish] {
+      SetupClock::time_point t0 = SetupClock::now();
+      bool ok = false;
+      try {
+        ok = pattern_host(m, &s->pattern);
+      } catch (...) {
+        ok = false;
+      }
+      publish(1, ok);
+      setup_note("set-up thread: pattern", ms_since(t0));
+      t0 = SetupClock::now();
+      const bool pat_ok = ok;
+      ok = false;
+      try {
+        ok = build_coarse(m, env_agg_size(), &s->coarse);
+      } catch (...) {
+        ok = false;
+      }
+      publish(2, ok);
+      setup_note("set-up thread: coarse space", ms_since(t0));
+      t0 = SetupClock::now();
+      ok = false;
+      try {
+        ok = pat_ok && graph_host_inputs(m, s->pattern, &s->graph);
+      } catch (...) {
+        ok = false;
+      }
+      publish(3, ok);
+      setup_note("set-up thread: network inputs", ms_since(t0));
+    });
+  } catch (...) {
+    return;  // no thread: every part is made where it is needed
+  }
+  m->host_setup = std::move(hs);
+}
+}  // namespace hfpx
+
 extern "C" {
 
 int hfpx_ctx_create(int device, hfpx_ctx** out) {
@@ -149,6 +230,7 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   if (c->d_flags) cudaFree(c->d_flags);
   for (void* p : c->scratch)
     if (p) cudaFree(p);
+  if (c->ev_sleep) cudaEventDestroy(c->ev_sleep);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->stream_panel) cudaStreamDestroy(c->stream_panel);
   if (c->stream_left) cudaStreamDestroy(c->stream_left);
@@ -235,10 +317,12 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
       m->h_vid[3 * e + j] = v;
       for (int k = 0; k < 3; ++k) m->h_vert[9 * e + 3 * j + k] = nods[k + ld_nods * v];
     }
+  // the preconditioners' mesh-only set-up runs on a host thread from here on
+  if (!rc) start_mesh_setup(m);
   if (!rc) rc = pool_alloc(c, &m->d_elem, elem_record_bytes() * n_el, "element records");
   if (!rc) launch_element_precompute(dn.as<double>(), ld_nods, dc.as<int64_t>(), ld_conn, n_el, beta, m->d_elem, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "element precompute");
-  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "element precompute");
+  if (!rc) rc = wait_sleeping(c, "element precompute");
   if (rc) {
     hfpx_mesh_destroy(m);
     return rc;
@@ -249,6 +333,7 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
 
 int hfpx_mesh_destroy(hfpx_mesh* m) {
   if (!m) return HFPX_OK;
+  if (m->host_setup && m->host_setup->worker.joinable()) m->host_setup->worker.join();
   if (m->gnn_graph) gnn_graph_release(m->gnn_graph);
   m->pattern.reset();
   pool_free(m->d_elem);
@@ -627,7 +712,7 @@ int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   if (!rc) launch_rhs(mesh->d_elem, mesh->n_el, dd, ds.as<double>(), n_rhs, dr.as<double>(), ld_rhs, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "rhs launch");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(rhs, dr.p, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyDeviceToHost, c->stream), "rhs back");
-  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "rhs");
+  if (!rc) rc = wait_sleeping(c, "rhs");
   return rc;
 }
 

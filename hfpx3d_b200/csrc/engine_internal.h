@@ -1,10 +1,14 @@
 // Internal declarations shared by the engine's translation units.
 #pragma once
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cstdint>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 #include <cuda_runtime.h>
 #include "../../include/hfpx_engine.h"
@@ -31,6 +35,9 @@ struct hfpx_ctx {
   int64_t trsv_cap = 0;
   int trsv_epoch = 0;
   unsigned long long trsv_base = 0;
+  // blocking-sync event: host waits that sleep instead of spinning, so the
+  // mesh set-up thread gets the core while the device works
+  cudaEvent_t ev_sleep = nullptr;
 };
 
 // Near-field pattern of a mesh: the elements sharing a vertex with element j
@@ -107,6 +114,37 @@ struct CoarseSpace {
   double* d_w = nullptr;
 };
 
+// The network's geometry inputs of a mesh (host arrays, the bf16 values as
+// their bit patterns): node rows n x kFN, edge rows E x kFE (the operator
+// columns zero), frames (9 per element) and sizes.
+struct GraphHostInputs {
+  std::vector<uint16_t> xn, xe;
+  std::vector<float> rot, size;
+};
+
+// Mesh-only set-up of the near-field preconditioners, made on a host thread
+// started by hfpx_mesh_create (meshes of kMeshSetupMinElems elements or
+// more) while the device assembles: the near-field pattern's host arrays,
+// the coarse aggregates and basis (default aggregate size) and the
+// network's geometry inputs, in that order.  Consumers wait for the part
+// they need and copy it; a part that failed is rebuilt where it is needed.
+struct MeshHostSetup {
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv;
+  int done = 0;                 // parts finished: 1 pattern, 2 + coarse, 3 + graph inputs
+  bool pattern_ok = false, coarse_ok = false, graph_ok = false;
+  NearPattern pattern;          // host arrays only
+  CoarseSpace coarse;           // host arrays only
+  GraphHostInputs graph;
+  // wait until `part` (1, 2, 3) is finished
+  void wait(int part) {
+    std::unique_lock<std::mutex> l(mu);
+    cv.wait(l, [&] { return done >= part; });
+  }
+};
+constexpr int64_t kMeshSetupMinElems = 1000;
+
 struct hfpx_mesh {
   int64_t n_el = 0;
   void* d_elem = nullptr;          // ElemRec[n_el]
@@ -120,6 +158,7 @@ struct hfpx_mesh {
   std::shared_ptr<NearPattern> pattern;
   std::shared_ptr<CoarseSpace> coarse;
   hfpx_gnn_graph* gnn_graph = nullptr;
+  std::unique_ptr<MeshHostSetup> host_setup;   // null for small meshes
 };
 
 struct hfpx_gnn;
@@ -169,6 +208,15 @@ struct hfpx_matrix {
 };
 
 namespace hfpx {
+// HFPX_PROFILE=1: host times of the set-up phases (pattern, coarse space,
+// network graph) to stderr
+using SetupClock = std::chrono::steady_clock;
+inline double ms_since(SetupClock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(SetupClock::now() - t0).count();
+}
+bool setup_profile();
+void setup_note(const char* what, double ms);
+
 // launches of this engine's own kernels in this process (library kernels excluded)
 extern std::atomic<long long> g_launches;
 
@@ -199,6 +247,8 @@ inline cudaError_t smem_attr_once(PerDeviceOnce& once, F* func, int bytes) {
 }
 int set_error(hfpx_ctx* c, int code, const std::string& msg);
 int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what);
+// wait for the context's stream with the calling thread asleep
+int wait_sleeping(hfpx_ctx* c, const char* what);
 // Work buffer `slot` of the context with at least `bytes` bytes (null when
 // the device is out of memory; the CUDA error state is cleared).  A slot
 // that grows is reallocated after the context's streams finish with it.
@@ -323,6 +373,16 @@ void tc_update_grouped(cudaStream_t st, int grid, const void* d_maps, const TcPr
 // precond.cu: near-field preconditioners on the FP64 matrix (block-Jacobi,
 // first-order Neumann, exact local inverse, learned) and their product
 int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p);
+// the host arrays of a mesh's pattern (false: no connectivity, or not symmetric)
+bool pattern_host(const hfpx_mesh* mesh, NearPattern* p);
+int upload_pattern(hfpx_ctx* c, NearPattern* p);
+// coarse.cu: aggregates and basis of a mesh (host), the default aggregate size
+bool build_coarse(const hfpx_mesh* m, int agg_size, CoarseSpace* cs);
+int env_agg_size();
+// gnn.cu: the network's geometry inputs of a mesh (host)
+bool graph_host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs* out);
+// engine.cu: start the mesh's set-up thread (meshes of kMeshSetupMinElems or more)
+void start_mesh_setup(hfpx_mesh* m);
 void free_pattern(NearPattern* p);
 // the mesh's coarse space with about agg_size elements per aggregate (built
 // on first use and kept with the mesh; rebuilt for another size)

@@ -35,7 +35,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
-#include <map>
+#include <utility>
 #include <random>
 #include <string>
 #include <vector>
@@ -727,46 +727,46 @@ void graph_destroy(hfpx_gnn_graph* g);
 // The mesh-only part of a graph: the pattern, the frames and sizes, the
 // geometry columns of the inputs (the operator columns are filled per
 // matrix by graph_fill).
-int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
-  *out = nullptr;
-  hfpx_gnn_graph* g = new (std::nothrow) hfpx_gnn_graph;
-  if (!g) return set_error(c, HFPX_ERR_NOMEM, "graph");
-  g->pat = mesh_pattern(c, mesh);
-  if (!g->pat) {
-    delete g;
-    return set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
-  }
-  int rc = 0;
-  const int64_t n = mesh->n_el, E = g->pat->n_edges;
-  g->n_nodes = n;
-  g->n_edges = E;
+// The mesh-only inputs of the network (host): per element its geometry row
+// and per pattern edge its geometry row (the operator columns stay zero),
+// its frame and size.
+bool host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs* out) {
+  const int64_t n = mesh->n_el, E = pat.n_edges;
+  if ((int64_t)mesh->h_vert.size() < 9 * n || (int64_t)mesh->h_vid.size() < 3 * n) return false;
   // host geometry: frames, sizes, features
   std::vector<Geo> geo(n);
   for (int64_t e = 0; e < n; ++e) geo[e] = element_geo(&mesh->h_vert[9 * e]);
   double smean = 0.0;
   for (const Geo& q : geo) smean += q.s;
   smean /= (double)n;
-  std::map<std::pair<int64_t, int64_t>, int> edge_count;
+  // how many elements share each element edge (1: a boundary edge): the
+  // (vertex pair, 3 e + k) keys sorted, counted by runs
+  std::vector<std::pair<std::pair<int64_t, int64_t>, int32_t>> ek((size_t)(3 * n));
   for (int64_t e = 0; e < n; ++e)
     for (int k = 0; k < 3; ++k) {
       int64_t a = mesh->h_vid[3 * e + k], b = mesh->h_vid[3 * e + (k + 1) % 3];
       if (a > b) std::swap(a, b);
-      ++edge_count[{a, b}];
+      ek[(size_t)(3 * e + k)] = {{a, b}, (int32_t)(3 * e + k)};
     }
+  std::sort(ek.begin(), ek.end());
+  std::vector<int32_t> edge_count((size_t)(3 * n));
+  for (size_t i = 0; i < ek.size();) {
+    size_t j = i;
+    while (j < ek.size() && ek[j].first == ek[i].first) ++j;
+    for (size_t q = i; q < j; ++q) edge_count[(size_t)ek[q].second] = (int32_t)(j - i);
+    i = j;
+  }
   std::vector<__nv_bfloat16> xn((size_t)n * kFN, __float2bfloat16_rn(0.f)), xe((size_t)E * kFE, __float2bfloat16_rn(0.f));
   std::vector<float> rot((size_t)9 * n), size(n);
   for (int64_t j = 0; j < n; ++j) {
     const Geo& q = geo[j];
     int boundary = 0;
-    for (int k = 0; k < 3; ++k) {
-      int64_t a = mesh->h_vid[3 * j + k], b = mesh->h_vid[3 * j + (k + 1) % 3];
-      if (a > b) std::swap(a, b);
-      if (edge_count[{a, b}] == 1) ++boundary;
-    }
-    const int deg = g->pat->ptr[j + 1] - g->pat->ptr[j];
+    for (int k = 0; k < 3; ++k)
+      if (edge_count[(size_t)(3 * j + k)] == 1) ++boundary;
+    const int deg = pat.ptr[j + 1] - pat.ptr[j];
     double curv = 0.0;
-    for (int32_t e = g->pat->ptr[j]; e < g->pat->ptr[j + 1]; ++e) {
-      const Geo& p = geo[g->pat->idx[e]];
+    for (int32_t e = pat.ptr[j]; e < pat.ptr[j + 1]; ++e) {
+      const Geo& p = geo[pat.idx[e]];
       curv += 1.0 - (p.r[6] * q.r[6] + p.r[7] * q.r[7] + p.r[8] * q.r[8]);
     }
     curv = deg ? curv / deg : 0.0;
@@ -775,8 +775,8 @@ int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
     for (int k = 0; k < kGeoN; ++k) xn[(size_t)j * kFN + k] = __float2bfloat16_rn(f[k]);
     for (int k = 0; k < 9; ++k) rot[9 * j + k] = (float)q.r[k];
     size[j] = (float)q.s;
-    for (int32_t e = g->pat->ptr[j]; e < g->pat->ptr[j + 1]; ++e) {
-      const int64_t i = g->pat->idx[e];
+    for (int32_t e = pat.ptr[j]; e < pat.ptr[j + 1]; ++e) {
+      const int64_t i = pat.idx[e];
       const Geo& p = geo[i];
       double d[3] = {(p.c[0] - q.c[0]) / q.s, (p.c[1] - q.c[1]) / q.s, (p.c[2] - q.c[2]) / q.s}, dl[3], nl[3], el[3];
       rot_apply(q.r, d, dl);
@@ -791,16 +791,56 @@ int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
       for (int k = 0; k < kGeoE; ++k) xe[(size_t)e * kFE + k] = __float2bfloat16_rn(fe[k]);
     }
   }
+  out->xn.resize(xn.size());
+  out->xe.resize(xe.size());
+  static_assert(sizeof(__nv_bfloat16) == sizeof(uint16_t), "bf16 bits");
+  std::memcpy(out->xn.data(), xn.data(), sizeof(uint16_t) * xn.size());
+  std::memcpy(out->xe.data(), xe.data(), sizeof(uint16_t) * xe.size());
+  out->rot = std::move(rot);
+  out->size = std::move(size);
+  return true;
+}
+
+int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
+  *out = nullptr;
+  hfpx_gnn_graph* g = new (std::nothrow) hfpx_gnn_graph;
+  if (!g) return set_error(c, HFPX_ERR_NOMEM, "graph");
+  g->pat = mesh_pattern(c, mesh);
+  if (!g->pat) {
+    delete g;
+    return set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
+  }
+  int rc = 0;
+  const int64_t n = mesh->n_el, E = g->pat->n_edges;
+  g->n_nodes = n;
+  g->n_edges = E;
+  // the geometry inputs: from the mesh's set-up thread, or made here
+  SetupClock::time_point t0 = SetupClock::now();
+  GraphHostInputs local;
+  const GraphHostInputs* in = nullptr;
+  MeshHostSetup* hs = const_cast<hfpx_mesh*>(mesh)->host_setup.get();
+  if (hs) {
+    hs->wait(3);
+    if (hs->graph_ok) in = &hs->graph;
+  }
+  if (!in) {
+    if (!host_inputs(mesh, *g->pat, &local)) rc = set_error(c, HFPX_ERR_STATE, "mesh has no host geometry");
+    in = &local;
+  }
+  setup_note(hs && hs->graph_ok ? "network graph inputs (wait for the set-up thread)" : "network graph inputs",
+             ms_since(t0));
+  t0 = SetupClock::now();
   g->d_size = galloc<float>(g, n, &rc, c);
   g->d_rot = galloc<float>(g, 9 * n, &rc, c);
   g->xn = galloc<__nv_bfloat16>(g, (size_t)n * kFN, &rc, c);
   g->xe = galloc<__nv_bfloat16>(g, (size_t)E * kFE, &rc, c);
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_size, size.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "sizes");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_rot, rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, c->stream), "frames");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xn, xn.data(), sizeof(__nv_bfloat16) * xn.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xe, xe.data(), sizeof(__nv_bfloat16) * xe.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_size, in->size.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "sizes");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_rot, in->rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, c->stream), "frames");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xn, in->xn.data(), sizeof(uint16_t) * in->xn.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
+  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xe, in->xe.data(), sizeof(uint16_t) * in->xe.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
   // the host vectors are pageable: finish the copies before they go
-  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "graph inputs");
+  if (!rc) rc = wait_sleeping(c, "graph inputs");
+  setup_note("network graph: uploads (with the queued work)", ms_since(t0));
   if (rc) {
     graph_destroy(g);
     return rc;
@@ -892,6 +932,10 @@ int gnn_correct_blocks(hfpx_ctx* c, const hfpx_gnn* net, const hfpx_mesh* mesh, 
 }
 
 void gnn_graph_release(hfpx_gnn_graph* g) { gnn::graph_destroy(g); }
+
+bool graph_host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs* out) {
+  return gnn::host_inputs(mesh, pat, out);
+}
 
 }  // namespace hfpx
 

@@ -22,10 +22,9 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
-#include <map>
+#include <utility>
 #include <mutex>
 #include <string>
-#include <set>
 #include <vector>
 #include "engine_internal.h"
 
@@ -222,22 +221,38 @@ T* dev_copy(hfpx_ctx* c, const std::vector<T>& h, int* rc) {
 
 }  // namespace
 
-int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
+bool pattern_host(const hfpx_mesh* mesh, NearPattern* p) {
   const int64_t ne = mesh->n_el;
-  if ((int64_t)mesh->h_vid.size() != 3 * ne) return set_error(c, HFPX_ERR_STATE, "mesh has no host connectivity");
-  std::map<int64_t, std::vector<int32_t>> v2e;
-  for (int64_t e = 0; e < ne; ++e)
-    for (int k = 0; k < 3; ++k) v2e[mesh->h_vid[3 * e + k]].push_back((int32_t)e);
+  if ((int64_t)mesh->h_vid.size() != 3 * ne) return false;
+  // vertex -> elements: the (vertex id, 3 e + k) pairs sorted, one run per
+  // vertex (elements ascending within a run); vslot[3 e + k] = the run of
+  // element e's vertex k
+  std::vector<std::pair<int64_t, int32_t>> ve((size_t)(3 * ne));
+  for (int64_t i = 0; i < 3 * ne; ++i) ve[(size_t)i] = {mesh->h_vid[i], (int32_t)i};
+  std::sort(ve.begin(), ve.end());
+  std::vector<int32_t> vstart, vel((size_t)(3 * ne)), vslot((size_t)(3 * ne));
+  for (size_t i = 0; i < ve.size(); ++i) {
+    if (i == 0 || ve[i].first != ve[i - 1].first) vstart.push_back((int32_t)i);
+    vel[i] = ve[i].second / 3;
+    vslot[(size_t)ve[i].second] = (int32_t)vstart.size() - 1;
+  }
+  vstart.push_back((int32_t)ve.size());
   p->n_el = ne;
   p->ptr.assign(ne + 1, 0);
   p->idx.clear();
   p->dst.clear();
   p->maxdeg = 0;
+  std::vector<int32_t> nb;
   for (int64_t j = 0; j < ne; ++j) {
-    std::set<int32_t> nb;
-    for (int k = 0; k < 3; ++k)
-      for (int32_t i : v2e[mesh->h_vid[3 * j + k]])
-        if (i != j) nb.insert(i);
+    // the elements sharing a vertex with j, ascending, without j
+    nb.clear();
+    for (int k = 0; k < 3; ++k) {
+      const int32_t v = vslot[(size_t)(3 * j + k)];
+      for (int32_t q = vstart[v]; q < vstart[v + 1]; ++q)
+        if (vel[q] != j) nb.push_back(vel[q]);
+    }
+    std::sort(nb.begin(), nb.end());
+    nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
     for (int32_t i : nb) {
       p->idx.push_back(i);
       p->dst.push_back((int32_t)j);
@@ -253,7 +268,7 @@ int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
       const int32_t i = p->idx[e];
       const auto b = p->idx.begin() + p->ptr[i], en = p->idx.begin() + p->ptr[i + 1];
       const auto it = std::lower_bound(b, en, (int32_t)j);
-      if (it == en || *it != (int32_t)j) return set_error(c, HFPX_ERR_STATE, "near-field pattern is not symmetric");
+      if (it == en || *it != (int32_t)j) return false;  // not symmetric
       p->rev[e] = (int32_t)(it - p->idx.begin());
     }
   p->rptr.assign(ne + 1, 0);
@@ -269,6 +284,17 @@ int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
     }
     p->rptr[i + 1] = (int32_t)p->rblk.size();
   }
+  return true;
+}
+
+int build_pattern(hfpx_ctx* c, const hfpx_mesh* mesh, NearPattern* p) {
+  if ((int64_t)mesh->h_vid.size() != 3 * mesh->n_el)
+    return set_error(c, HFPX_ERR_STATE, "mesh has no host connectivity");
+  if (!pattern_host(mesh, p)) return set_error(c, HFPX_ERR_STATE, "near-field pattern is not symmetric");
+  return upload_pattern(c, p);
+}
+
+int upload_pattern(hfpx_ctx* c, NearPattern* p) {
   int rc = 0;
   p->d_ptr = dev_copy(c, p->ptr, &rc);
   p->d_idx = dev_copy(c, p->idx, &rc);
@@ -287,7 +313,31 @@ std::shared_ptr<NearPattern> mesh_pattern(hfpx_ctx* c, const hfpx_mesh* mesh) {
       free_pattern(q);
       delete q;
     });
-    if (!p || build_pattern(c, mesh, p.get())) return nullptr;
+    if (!p) return nullptr;
+    const SetupClock::time_point t0 = SetupClock::now();
+    MeshHostSetup* hs = mm->host_setup.get();
+    if (hs) {  // made on the mesh's set-up thread
+      hs->wait(1);
+      if (hs->pattern_ok) {
+        const NearPattern& h = hs->pattern;
+        p->n_el = h.n_el;
+        p->n_edges = h.n_edges;
+        p->maxdeg = h.maxdeg;
+        p->ptr = h.ptr;
+        p->idx = h.idx;
+        p->dst = h.dst;
+        p->rev = h.rev;
+        p->rptr = h.rptr;
+        p->rblk = h.rblk;
+        p->rcol = h.rcol;
+      }
+    }
+    if (hs && hs->pattern_ok) {
+      if (upload_pattern(c, p.get())) return nullptr;
+    } else if (build_pattern(c, mesh, p.get())) {
+      return nullptr;
+    }
+    setup_note("near-field pattern", ms_since(t0));
     mm->pattern = p;
   }
   return mm->pattern;
@@ -512,10 +562,14 @@ int hfpx_precond_create(hfpx_ctx* c, const hfpx_mesh* mesh, const hfpx_matrix* m
   pc->pat = mesh_pattern(c, mesh);
   int rc = pc->pat ? 0 : set_error(c, HFPX_ERR_NOMEM, "near-field pattern");
   const int64_t nb = rc ? 0 : pc->pat->blocks();
+  SetupClock::time_point t0 = SetupClock::now();
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_blocks, sizeof(double) * 324 * nb, "blocks");
   if (!rc) rc = pool_alloc(c, (void**)&pc->d_dinv, sizeof(double) * 324 * pc->n_el, "block inverses");
   if (!rc && (kind & HFPX_PC_COARSE)) rc = coarse_alloc(c, pc);
+  setup_note("preconditioner buffers and coarse space", ms_since(t0));
+  t0 = SetupClock::now();
   if (!rc) rc = precond_fill(c, pc, mesh, m, net, shear_m);
+  setup_note("preconditioner fill (enqueue; network graph on first use)", ms_since(t0));
   if (rc) {
     hfpx_precond_destroy(pc);
     return rc;
