@@ -2650,6 +2650,14 @@ int lu_panel_factor_noalloc(hfpx_ctx* c, double* d_a, int64_t lda, int64_t m, in
                                                    smem, c->stream),
                     "panel launch");
   }
+  // Inside a stream capture the call records the clear and the kernel only:
+  // a host read (or a synchronisation) would end the capture with an error.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (!rc) rc = check_cuda(c, cudaStreamIsCapturing(c->stream, &cap), "capture status");
+  if (!rc && cap != cudaStreamCaptureStatusNone) {
+    *info = 0;
+    return HFPX_OK;
+  }
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(info, d_info, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream), "info");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "panel factorisation");
   if (!rc && *info != 0) rc = set_error(c, HFPX_ERR_SINGULAR, "zero pivot at column " + std::to_string(*info));

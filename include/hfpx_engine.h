@@ -219,7 +219,10 @@ int hfpx_gmres_device(hfpx_ctx *ctx, const hfpx_matrix *matrix, double *d_b, dou
  * HFPX_ERR_ARG.  Its pivot-search scratch is one static device array of
  * about 138 KB shared by every call: the first call on a device looks up its
  * address (make that first call before any stream capture), and calls that
- * overlap on the GPU race. */
+ * overlap on the GPU race.  Called while the context's stream is being
+ * captured (hfpx_ctx_stream), it records its work only: info is set to 0
+ * and a zero pivot is not reported (each replay of the graph factors the
+ * panel in place). */
 int hfpx_lu_panel_factor_noalloc(hfpx_ctx *ctx, double *d_a, int64_t lda, int64_t m, int w,
                                  int32_t *d_piv, int64_t *info);
 

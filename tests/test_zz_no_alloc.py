@@ -128,3 +128,43 @@ def test_allocates_nothing(ctx):
         call()
     # any cudaMalloc inside the call would take at least one 2 MiB page
     assert torch.cuda.mem_get_info(0)[0] == free0
+
+
+def test_captured_into_a_graph(ctx):
+    """The call inside a stream capture of the context's stream: the capture
+    ends cleanly (no host read, no synchronisation inside it), and each
+    replay of the graph factors the panel as a direct call does."""
+    import torch
+    from cuda.bindings import driver as cu
+    from hfpx3d_b200 import engine
+    rng = np.random.default_rng(6)
+    A = rng.standard_normal((3000, 24))
+    rc, F_ref, piv_ref, info_ref = factor_noalloc(ctx, A)   # also the first call on the device
+    assert rc == engine.HFPX_OK and info_ref == 0
+    d = torch.from_numpy(np.ascontiguousarray(A.T)).to('cuda:0')
+    piv = torch.full((24,), -7, dtype=torch.int32, device='cuda:0')
+    stream = ctypes.c_void_p()
+    ctx.check(engine.lib().hfpx_ctx_stream(ctx.h, ctypes.byref(stream)))
+    hs = cu.CUstream(stream.value)
+    torch.cuda.synchronize()
+
+    def ok(res):
+        err = res[0] if isinstance(res, tuple) else res
+        assert err == cu.CUresult.CUDA_SUCCESS, err
+        return res[1] if isinstance(res, tuple) and len(res) > 1 else None
+    ok(cu.cuStreamBeginCapture(hs, cu.CUstreamCaptureMode.CU_STREAM_CAPTURE_MODE_THREAD_LOCAL))
+    info = ctypes.c_int64(-1)
+    rc = engine.lib().hfpx_lu_panel_factor_noalloc(ctx.h, ctypes.c_void_p(d.data_ptr()), 3000, 3000, 24,
+                                                   ctypes.c_void_p(piv.data_ptr()), ctypes.byref(info))
+    graph = ok(cu.cuStreamEndCapture(hs))
+    assert rc == engine.HFPX_OK and info.value == 0
+    gexec = ok(cu.cuGraphInstantiate(graph, 0))
+    for _ in range(2):
+        d.copy_(torch.from_numpy(np.ascontiguousarray(A.T)))
+        piv.fill_(-7)
+        torch.cuda.synchronize()
+        ok(cu.cuGraphLaunch(gexec, hs))
+        ok(cu.cuStreamSynchronize(hs))
+        assert np.array_equal(d.cpu().numpy().T, F_ref) and np.array_equal(piv.cpu().numpy(), piv_ref)
+    ok(cu.cuGraphExecDestroy(gexec))
+    ok(cu.cuGraphDestroy(graph))
