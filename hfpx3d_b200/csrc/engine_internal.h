@@ -115,8 +115,8 @@ struct CoarseSpace {
 };
 
 // The network's geometry inputs of a mesh (host arrays, the bf16 values as
-// their bit patterns): node rows n x kFN, edge rows E x kFE (the operator
-// columns zero), frames (9 per element) and sizes.
+// their bit patterns): the geometry columns of the node rows (n x 8) and of
+// the edge rows (E x 12), frames (9 per element) and sizes.
 struct GraphHostInputs {
   std::vector<uint16_t> xn, xe;
   std::vector<float> rot, size;

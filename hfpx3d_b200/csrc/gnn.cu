@@ -756,7 +756,8 @@ bool host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs*
     for (size_t q = i; q < j; ++q) edge_count[(size_t)ek[q].second] = (int32_t)(j - i);
     i = j;
   }
-  std::vector<__nv_bfloat16> xn((size_t)n * kFN, __float2bfloat16_rn(0.f)), xe((size_t)E * kFE, __float2bfloat16_rn(0.f));
+  // the geometry columns only (the first kGeoN / kGeoE of each row)
+  std::vector<__nv_bfloat16> xn((size_t)n * kGeoN), xe((size_t)E * kGeoE);
   std::vector<float> rot((size_t)9 * n), size(n);
   for (int64_t j = 0; j < n; ++j) {
     const Geo& q = geo[j];
@@ -772,7 +773,7 @@ bool host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs*
     curv = deg ? curv / deg : 0.0;
     const float f[kGeoN] = {(float)std::log(q.s / smean), (float)q.l1, (float)q.x2, (float)q.y2, boundary / 3.f,
                             deg / 12.f, (float)(10.0 * curv), 1.f};
-    for (int k = 0; k < kGeoN; ++k) xn[(size_t)j * kFN + k] = __float2bfloat16_rn(f[k]);
+    for (int k = 0; k < kGeoN; ++k) xn[(size_t)j * kGeoN + k] = __float2bfloat16_rn(f[k]);
     for (int k = 0; k < 9; ++k) rot[9 * j + k] = (float)q.r[k];
     size[j] = (float)q.s;
     for (int32_t e = pat.ptr[j]; e < pat.ptr[j + 1]; ++e) {
@@ -788,7 +789,7 @@ bool host_inputs(const hfpx_mesh* mesh, const NearPattern& pat, GraphHostInputs*
       const float fe[kGeoE] = {(float)dl[0], (float)dl[1], (float)dl[2], (float)nl[0], (float)nl[1], (float)nl[2],
                                (float)el[0], (float)el[1], (float)el[2], (float)std::log(p.s / q.s),
                                (float)(shared - 1), 1.f};
-      for (int k = 0; k < kGeoE; ++k) xe[(size_t)e * kFE + k] = __float2bfloat16_rn(fe[k]);
+      for (int k = 0; k < kGeoE; ++k) xe[(size_t)e * kGeoE + k] = __float2bfloat16_rn(fe[k]);
     }
   }
   out->xn.resize(xn.size());
@@ -836,8 +837,28 @@ int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
   g->xe = galloc<__nv_bfloat16>(g, (size_t)E * kFE, &rc, c);
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_size, in->size.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream), "sizes");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->d_rot, in->rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, c->stream), "frames");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xn, in->xn.data(), sizeof(uint16_t) * in->xn.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
-  if (!rc) rc = check_cuda(c, cudaMemcpyAsync(g->xe, in->xe.data(), sizeof(uint16_t) * in->xe.size(), cudaMemcpyHostToDevice, c->stream), "inputs");
+  // the input rows: zero, then the geometry columns from the host (the
+  // operator columns are written per matrix by graph_fill)
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(g->xn, 0, sizeof(__nv_bfloat16) * (size_t)n * kFN, c->stream), "inputs");
+  if (!rc) rc = check_cuda(c, cudaMemsetAsync(g->xe, 0, sizeof(__nv_bfloat16) * (size_t)E * kFE, c->stream), "inputs");
+  // (one contiguous upload each, then a strided copy on the device: a
+  // strided copy from pageable host memory goes row by row)
+  uint16_t* sxn = galloc<uint16_t>(g, (size_t)n * kGeoN, &rc, c);
+  uint16_t* sxe = galloc<uint16_t>(g, (size_t)E * kGeoE, &rc, c);
+  if (!rc && n > 0)
+    rc = check_cuda(c, cudaMemcpyAsync(sxn, in->xn.data(), sizeof(uint16_t) * in->xn.size(), cudaMemcpyHostToDevice,
+                                       c->stream), "inputs");
+  if (!rc && E > 0)
+    rc = check_cuda(c, cudaMemcpyAsync(sxe, in->xe.data(), sizeof(uint16_t) * in->xe.size(), cudaMemcpyHostToDevice,
+                                       c->stream), "inputs");
+  if (!rc && n > 0)
+    rc = check_cuda(c, cudaMemcpy2DAsync(g->xn, sizeof(uint16_t) * kFN, sxn, sizeof(uint16_t) * kGeoN,
+                                         sizeof(uint16_t) * kGeoN, (size_t)n, cudaMemcpyDeviceToDevice, c->stream),
+                    "inputs");
+  if (!rc && E > 0)
+    rc = check_cuda(c, cudaMemcpy2DAsync(g->xe, sizeof(uint16_t) * kFE, sxe, sizeof(uint16_t) * kGeoE,
+                                         sizeof(uint16_t) * kGeoE, (size_t)E, cudaMemcpyDeviceToDevice, c->stream),
+                    "inputs");
   // the host vectors are pageable: finish the copies before they go
   if (!rc) rc = wait_sleeping(c, "graph inputs");
   setup_note("network graph: uploads (with the queued work)", ms_since(t0));
