@@ -231,6 +231,10 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   for (void* p : c->scratch)
     if (p) cudaFree(p);
   if (c->ev_sleep) cudaEventDestroy(c->ev_sleep);
+  if (c->stream_coarse) cudaStreamSynchronize(c->stream_coarse);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->stream_coarse) cudaStreamDestroy(c->stream_coarse);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->stream_panel) cudaStreamDestroy(c->stream_panel);
   if (c->stream_left) cudaStreamDestroy(c->stream_left);

@@ -38,6 +38,10 @@ struct hfpx_ctx {
   // blocking-sync event: host waits that sleep instead of spinning, so the
   // mesh set-up thread gets the core while the device works
   cudaEvent_t ev_sleep = nullptr;
+  // the coarse level's set-up runs on its own stream beside the near-field
+  // blocks (made on first use)
+  cudaStream_t stream_coarse = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // Near-field pattern of a mesh: the elements sharing a vertex with element j

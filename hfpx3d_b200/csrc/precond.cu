@@ -18,6 +18,7 @@
 //   learned:         the Neumann blocks plus corrections predicted by a graph
 //                    network (gnn.cu).
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdlib>
@@ -527,6 +528,20 @@ int precond_fill(hfpx_ctx* c, hfpx_precond* pc, const hfpx_mesh* mesh, const hfp
   int rc = check_cuda(c, cudaMemsetAsync(pc->d_blocks, 0, sizeof(double) * 324 * nb, c->stream), "blocks");
   if (!rc) rc = check_cuda(c, cudaMemsetAsync(err, 0, sizeof(int), c->stream), "status");
   const OpView A = op_view(m);
+  // The coarse level (A P, P^T A P, its LU and inverse) reads only the
+  // operator: it runs on a second stream beside the near-field blocks, which
+  // are enqueued first (the coarse set-up waits on the host for its LU).
+  const bool side = pc->cs != nullptr;
+  if (!rc && side) {
+    if (!c->stream_coarse)
+      rc = check_cuda(c, cudaStreamCreateWithFlags(&c->stream_coarse, cudaStreamNonBlocking), "coarse stream");
+    if (!rc && !c->ev_fork)
+      rc = check_cuda(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming), "coarse stream");
+    if (!rc && !c->ev_join)
+      rc = check_cuda(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "coarse stream");
+    if (!rc) rc = check_cuda(c, cudaEventRecord(c->ev_fork, c->stream), "coarse fork");
+    if (!rc) rc = check_cuda(c, cudaStreamWaitEvent(c->stream_coarse, c->ev_fork, 0), "coarse fork");
+  }
   if (!rc) rc = gather_diag_inverse(c, A, *pc->pat, pc->d_dinv, err);
   if (!rc) {
     if (pc->kind == HFPX_PC_LOCAL_INVERSE)
@@ -535,7 +550,15 @@ int precond_fill(hfpx_ctx* c, hfpx_precond* pc, const hfpx_mesh* mesh, const hfp
       rc = neumann_blocks(c, A, *pc->pat, pc->d_dinv, pc->d_blocks, pc->kind != HFPX_PC_BLOCK_JACOBI);
   }
   if (!rc && pc->kind == HFPX_PC_LEARNED) rc = gnn_correct_blocks(c, net, mesh, m, pc, shear_m);
-  if (!rc && pc->cs) rc = coarse_setup(c, pc, m);
+  if (!rc && side) {
+    cudaStream_t main = c->stream;
+    c->stream = c->stream_coarse;   // coarse_setup's kernels and cuSOLVER calls go to the side stream
+    rc = coarse_setup(c, pc, m);
+    c->stream = main;
+    cusolverDnSetStream(static_cast<cusolverDnHandle_t>(c->cusolver), main);
+    if (!rc) rc = check_cuda(c, cudaEventRecord(c->ev_join, c->stream_coarse), "coarse join");
+    if (!rc) rc = check_cuda(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0), "coarse join");
+  }
   int herr = 0;
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
   if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "preconditioner");
