@@ -18,17 +18,6 @@ namespace hfpx {
 
 std::atomic<long long> g_launches{0};
 
-int wait_sleeping(hfpx_ctx* c, const char* what) {
-  if (!c->ev_sleep) {
-    if (int rc = check_cuda(c, cudaEventCreateWithFlags(&c->ev_sleep, cudaEventBlockingSync | cudaEventDisableTiming),
-                            what))
-      return rc;
-  }
-  int rc = check_cuda(c, cudaEventRecord(c->ev_sleep, c->stream), what);
-  if (!rc) rc = check_cuda(c, cudaEventSynchronize(c->ev_sleep), what);
-  return rc;
-}
-
 bool setup_profile() {
   static const bool on = [] {
     const char* e = std::getenv("HFPX_PROFILE");
@@ -230,7 +219,6 @@ int hfpx_ctx_destroy(hfpx_ctx* c) {
   if (c->d_flags) cudaFree(c->d_flags);
   for (void* p : c->scratch)
     if (p) cudaFree(p);
-  if (c->ev_sleep) cudaEventDestroy(c->ev_sleep);
   if (c->stream_coarse) cudaStreamSynchronize(c->stream_coarse);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -326,7 +314,7 @@ int hfpx_mesh_create(hfpx_ctx* c, const double* nods, int64_t ld_nods, int64_t n
   if (!rc) rc = pool_alloc(c, &m->d_elem, elem_record_bytes() * n_el, "element records");
   if (!rc) launch_element_precompute(dn.as<double>(), ld_nods, dc.as<int64_t>(), ld_conn, n_el, beta, m->d_elem, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "element precompute");
-  if (!rc) rc = wait_sleeping(c, "element precompute");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "element precompute");
   if (rc) {
     hfpx_mesh_destroy(m);
     return rc;
@@ -716,7 +704,7 @@ int hfpx_rhs_sinf(hfpx_ctx* c, const hfpx_mesh* mesh, const int64_t* dof_h, int6
   if (!rc) launch_rhs(mesh->d_elem, mesh->n_el, dd, ds.as<double>(), n_rhs, dr.as<double>(), ld_rhs, c->stream);
   if (!rc) rc = check_cuda(c, cudaGetLastError(), "rhs launch");
   if (!rc) rc = check_cuda(c, cudaMemcpyAsync(rhs, dr.p, sizeof(double) * ld_rhs * n_rhs, cudaMemcpyDeviceToHost, c->stream), "rhs back");
-  if (!rc) rc = wait_sleeping(c, "rhs");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "rhs");
   return rc;
 }
 

@@ -35,9 +35,6 @@ struct hfpx_ctx {
   int64_t trsv_cap = 0;
   int trsv_epoch = 0;
   unsigned long long trsv_base = 0;
-  // blocking-sync event: host waits that sleep instead of spinning, so the
-  // mesh set-up thread gets the core while the device works
-  cudaEvent_t ev_sleep = nullptr;
   // the coarse level's set-up runs on its own stream beside the near-field
   // blocks (made on first use)
   cudaStream_t stream_coarse = nullptr;
@@ -251,8 +248,6 @@ inline cudaError_t smem_attr_once(PerDeviceOnce& once, F* func, int bytes) {
 }
 int set_error(hfpx_ctx* c, int code, const std::string& msg);
 int check_cuda(hfpx_ctx* c, cudaError_t e, const char* what);
-// wait for the context's stream with the calling thread asleep
-int wait_sleeping(hfpx_ctx* c, const char* what);
 // Work buffer `slot` of the context with at least `bytes` bytes (null when
 // the device is out of memory; the CUDA error state is cleared).  A slot
 // that grows is reallocated after the context's streams finish with it.

@@ -860,7 +860,7 @@ int graph_prepare(hfpx_ctx* c, const hfpx_mesh* mesh, hfpx_gnn_graph** out) {
                                          sizeof(uint16_t) * kGeoE, (size_t)E, cudaMemcpyDeviceToDevice, c->stream),
                     "inputs");
   // the host vectors are pageable: finish the copies before they go
-  if (!rc) rc = wait_sleeping(c, "graph inputs");
+  if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->stream), "graph inputs");
   setup_note("network graph: uploads (with the queued work)", ms_since(t0));
   if (rc) {
     graph_destroy(g);

@@ -21,6 +21,7 @@
 #include <cusolverDn.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <utility>
@@ -243,23 +244,34 @@ bool pattern_host(const hfpx_mesh* mesh, NearPattern* p) {
   p->idx.clear();
   p->dst.clear();
   p->maxdeg = 0;
-  std::vector<int32_t> nb;
+  p->idx.reserve((size_t)(24 * ne));
+  p->dst.reserve((size_t)(24 * ne));
   for (int64_t j = 0; j < ne; ++j) {
-    // the elements sharing a vertex with j, ascending, without j
-    nb.clear();
+    // the elements sharing a vertex with j, ascending, without j: a merge of
+    // the three vertices' element lists (each ascending), duplicates dropped
+    int32_t q[3], qe[3];
     for (int k = 0; k < 3; ++k) {
       const int32_t v = vslot[(size_t)(3 * j + k)];
-      for (int32_t q = vstart[v]; q < vstart[v + 1]; ++q)
-        if (vel[q] != j) nb.push_back(vel[q]);
+      q[k] = vstart[v];
+      qe[k] = vstart[v + 1];
     }
-    std::sort(nb.begin(), nb.end());
-    nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
-    for (int32_t i : nb) {
-      p->idx.push_back(i);
-      p->dst.push_back((int32_t)j);
+    const size_t before = p->idx.size();
+    int32_t last = -1;
+    for (;;) {
+      int32_t best = INT32_MAX;
+      for (int k = 0; k < 3; ++k)
+        if (q[k] < qe[k] && vel[q[k]] < best) best = vel[q[k]];
+      if (best == INT32_MAX) break;
+      for (int k = 0; k < 3; ++k)
+        while (q[k] < qe[k] && vel[q[k]] == best) ++q[k];
+      if (best != (int32_t)j && best != last) {
+        p->idx.push_back(best);
+        p->dst.push_back((int32_t)j);
+      }
+      last = best;
     }
     p->ptr[j + 1] = (int32_t)p->idx.size();
-    p->maxdeg = std::max(p->maxdeg, (int)nb.size());
+    p->maxdeg = std::max(p->maxdeg, (int)(p->idx.size() - before));
   }
   p->n_edges = (int64_t)p->idx.size();
   // reverse edges and the row view (the pattern is symmetric)
