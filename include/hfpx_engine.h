@@ -69,7 +69,11 @@ int64_t hfpx_dof_handle(const double *nods, int64_t ld_nods, int64_t n_nodes,
 /* ---- mesh: uploads the mesh and computes, once per element, what
  * make_el_r_tensor / make_el_tau_crd / make_el_sfm_uniform / el_cp_uniform
  * (src/Core/element_utilities.cpp:62-238, 364-395) give; the reference
- * recomputes these inside its pair loops (system_assembly.cpp:64-113). */
+ * recomputes these inside its pair loops (system_assembly.cpp:64-113).
+ * For meshes of 1000 elements or more it also starts one host thread that
+ * makes the near-field preconditioners' mesh-only set-up (pattern, coarse
+ * aggregates, network inputs) while the caller goes on (assembly);
+ * hfpx_mesh_destroy joins it. */
 int hfpx_mesh_create(hfpx_ctx *ctx, const double *nods, int64_t ld_nods, int64_t n_nodes,
                      const int64_t *conn, int64_t ld_conn, int64_t n_el, double beta,
                      hfpx_mesh **mesh);
