@@ -489,7 +489,9 @@ int hfpx_cf_update_mrd(hfpx_ctx *ctx, int64_t n_cp, const hfpx_cf_material *mats
  * DoF renumbering in element order (the reference's shared counter races
  * under OpenMP), DoF untouched by the checks stay active, tractions and the
  * volume from the original numbering, the clamped DD left in local
- * coordinates.  HFPX_ERR_SINGULAR when every DoF is fixed. */
+ * coordinates.  HFPX_ERR_SINGULAR when every DoF is fixed.  The call
+ * allocates its O(n) device buffers (and, on the truncated path, the
+ * truncated matrix) per step and returns with the stream synchronised. */
 int hfpx_vc_cf_iteration(hfpx_ctx *ctx, const hfpx_mesh *mesh, const hfpx_matrix *matrix,
                          const int64_t *orig_dof_h, int64_t n_dof, const hfpx_cf_material *mats, int n_mat,
                          const double *s_inf, int64_t inj_cp, double new_vol, int is_dd_local, int flags,
